@@ -1,0 +1,372 @@
+"""ctypes binding of the chainamps_b200 C ABI (include/chainamps_b200.h).
+
+The host-side mirror of the reference's call surface for the DMRG hot path:
+
+* ``TwoVertexComponents`` -- the reference class of the same name
+  (DMRG_routines.hpp:189-214): built from the left block, the MPO and the
+  right block; ``multiply`` is ``TwoVertexMPOMPSMultiply``
+  (DMRG_routines.hpp:248), ``HED`` the lowest eigenpair
+  (DMRG_routines.cpp:835-896);
+* ``TwoVertexComponents.SVD`` -- ``TwoVertexSVD`` / ``MPX_matrix::SVD``
+  (DMRG_routines.hpp:225, MPX_matrix.cpp:157-192);
+* ``make_left_block`` / ``make_right_block`` -- ``MakeLeftBlock`` /
+  ``MakeRightBlock`` (DMRG_routines.hpp:238-239).
+
+Tensors cross the boundary as ``MPXTensor``: the reference's MPX_matrix
+storage (directed charge-labelled indices plus one CSC matrix, first index
+fastest).  Errors raise ``CmpsError`` with the library's message, the
+counterpart of the reference printing and exiting.  There is no CPU
+fallback: if the CUDA library is missing, importing this module fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libchainamps_b200.so")
+
+CMPS_FP64 = 0
+CMPS_SPLIT_TF32 = 1
+
+
+class CmpsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"chainamps_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIBPATH):
+        raise ImportError(f"{LIBPATH} is not built: run `python -m chainamps_b200.build` "
+                          "(the CUDA library is required; there is no CPU fallback)")
+    return C.CDLL(LIBPATH)
+
+
+lib = _load()
+
+c_i64p = C.POINTER(C.c_int64)
+c_dblp = C.POINTER(C.c_double)
+
+
+class ChargeRules(C.Structure):
+    _fields_ = [("nq", C.c_int32), ("rules", C.POINTER(C.c_int16))]
+
+
+class MpxDesc(C.Structure):
+    _fields_ = [("num_indices", C.c_int32), ("num_row_indices", C.c_int32),
+                ("inward", C.POINTER(C.c_uint8)), ("physical", C.POINTER(C.c_uint8)),
+                ("sizes", c_i64p), ("charges", C.POINTER(C.c_int16)),
+                ("rows", C.c_int64), ("cols", C.c_int64),
+                ("colptr", c_i64p), ("rowind", c_i64p), ("values", c_dblp)]
+
+
+_SIGS = {
+    "cmps_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "cmps_context_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_last_error": (C.c_char_p, []),
+    "cmps_version": (C.c_char_p, []),
+    "cmps_heff_create": (C.c_int, [C.c_void_p, C.POINTER(ChargeRules), C.POINTER(MpxDesc), C.POINTER(MpxDesc),
+                                   C.POINTER(MpxDesc), C.c_int, C.POINTER(C.c_void_p)]),
+    "cmps_heff_create_from_blocks": (C.c_int, [C.c_void_p, C.POINTER(ChargeRules), C.c_void_p, C.POINTER(MpxDesc),
+                                               C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cmps_block_create": (C.c_int, [C.c_void_p, C.POINTER(ChargeRules), C.POINTER(MpxDesc), C.POINTER(MpxDesc),
+                                    C.c_int, C.POINTER(C.c_void_p)]),
+    "cmps_heff_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_heff_length": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),
+    "cmps_heff_allowed_indices": (C.c_int, [C.c_void_p, c_i64p]),
+    "cmps_heff_apply": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
+    "cmps_heff_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cmps_heff_flops": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
+    "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
+                                 C.POINTER(C.c_int)]),
+    "cmps_heff_set_theta": (C.c_int, [C.c_void_p, c_dblp]),
+    "cmps_heff_theta_svd": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]),
+    "cmps_svd_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_svd_info": (C.c_int, [C.c_void_p, c_i64p, c_dblp, c_i64p, c_i64p]),
+    "cmps_svd_copy": (C.c_int, [C.c_void_p, c_dblp, C.POINTER(C.c_int16), c_i64p, c_i64p, c_dblp, c_i64p, c_i64p,
+                                c_dblp]),
+    "cmps_heff_left_block": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cmps_heff_right_block": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cmps_block_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_block_info": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_i64p]),
+    "cmps_block_copy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int16), c_i64p, c_i64p, c_dblp]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def _check(code):
+    if code != 0:
+        raise CmpsError(code, lib.cmps_last_error().decode())
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+# ---------------------------------------------------------------------------
+@dataclass
+class MPXIndexSpec:
+    inward: bool
+    physical: bool
+    charges: np.ndarray  # (size, nq) int
+
+
+@dataclass
+class MPXTensor:
+    """MPX_matrix storage (MPX_matrix.hpp:61-66): indices, number of row
+    indices, CSC matrix (rows, cols, colptr, rowind, complex values)."""
+    indices: list
+    nrow: int
+    rows: int
+    cols: int
+    colptr: np.ndarray
+    rowind: np.ndarray
+    values: np.ndarray
+
+    def _desc(self):
+        keep = []
+        inward = np.array([1 if i.inward else 0 for i in self.indices], np.uint8)
+        phys = np.array([1 if i.physical else 0 for i in self.indices], np.uint8)
+        sizes = np.array([i.charges.shape[0] for i in self.indices], np.int64)
+        charges = np.ascontiguousarray(np.concatenate([np.asarray(i.charges, np.int16).reshape(i.charges.shape[0], -1)
+                                                       for i in self.indices], axis=0))
+        colptr = np.ascontiguousarray(self.colptr, np.int64)
+        rowind = np.ascontiguousarray(self.rowind, np.int64)
+        vals = np.ascontiguousarray(np.asarray(self.values, np.complex128)).view(np.float64)
+        if rowind.size == 0:
+            rowind = np.zeros(1, np.int64)
+            vals = np.zeros(2, np.float64)
+        keep += [inward, phys, sizes, charges, colptr, rowind, vals]
+        d = MpxDesc(len(self.indices), self.nrow, _p(inward, C.c_uint8), _p(phys, C.c_uint8), _p(sizes, C.c_int64),
+                    _p(charges, C.c_int16), self.rows, self.cols, _p(colptr, C.c_int64), _p(rowind, C.c_int64),
+                    _p(vals, C.c_double))
+        return d, keep
+
+
+def _rules(rules):
+    r = np.ascontiguousarray(np.asarray(rules, np.int16))
+    return ChargeRules(len(r), _p(r, C.c_int16)), r
+
+
+class Context:
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        _check(lib.cmps_context_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cmps_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TwoVertexComponents:
+    """TwoVertexComponents (DMRG_routines.hpp:189-214) on the GPU."""
+
+    def __init__(self, ctx: Context, rules, L, W: MPXTensor, R, precision=CMPS_FP64):
+        """L and R: MPXTensor (host, reference layout) or Block (device)."""
+        self.ctx = ctx
+        cr, self._r = _rules(rules)
+        dw, kw = W._desc()
+        h = C.c_void_p()
+        if isinstance(L, Block) and isinstance(R, Block):
+            _check(lib.cmps_heff_create_from_blocks(ctx.h, C.byref(cr), L.h, C.byref(dw), R.h, precision,
+                                                    C.byref(h)))
+        else:
+            dl, kl = L._desc()
+            dr, kr = R._desc()
+            _check(lib.cmps_heff_create(ctx.h, C.byref(cr), C.byref(dl), C.byref(dw), C.byref(dr), precision,
+                                        C.byref(h)))
+        self.h = h
+        self.nq = len(self._r)
+        n = C.c_int64()
+        full = C.c_int64()
+        _check(lib.cmps_heff_length(h, C.byref(n), C.byref(full)))
+        self.n = n.value
+        self.full_length = full.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.cmps_heff_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def length(self):
+        return self.full_length
+
+    @property
+    def allowed_indices(self):
+        out = np.zeros(self.n, np.int64)
+        _check(lib.cmps_heff_allowed_indices(self.h, _p(out, C.c_int64)))
+        return out
+
+    def multiply(self, x):
+        """TwoVertexMPOMPSMultiply: host vector in ARPACK order -> host vector."""
+        x = np.ascontiguousarray(np.asarray(x, np.complex128))
+        if x.shape != (self.n,):
+            raise ValueError("vector length differs from allowed_indices.size()")
+        out = np.empty_like(x)
+        _check(lib.cmps_heff_apply(self.h, _p(x.view(np.float64), C.c_double), _p(out.view(np.float64), C.c_double)))
+        return out
+
+    def multiply_device(self, d_in, d_out, stream=None):
+        """Device pointers (ints) to n complex doubles each."""
+        _check(lib.cmps_heff_apply_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
+                                          C.c_void_p(stream) if stream else None))
+
+    def flops(self):
+        a = C.c_double()
+        b = C.c_double()
+        _check(lib.cmps_heff_flops(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_precision(self, p):
+        _check(lib.cmps_heff_set_precision(self.h, p))
+
+    def HED(self, guess=None, tol=1e-10, max_restarts=50, krylov_dim=24, want_vector=True):
+        """Lowest eigenpair; returns (energy, eigenvector in ARPACK order or
+        None, matvec count)."""
+        g = None
+        if guess is not None:
+            g = np.ascontiguousarray(np.asarray(guess, np.complex128))
+        ev = C.c_double()
+        mv = C.c_int()
+        vec = np.empty(self.n, np.complex128) if want_vector else None
+        _check(lib.cmps_heff_eigs(self.h, None if g is None else _p(g.view(np.float64), C.c_double), tol,
+                                  max_restarts, krylov_dim, C.byref(ev),
+                                  None if vec is None else _p(vec.view(np.float64), C.c_double), C.byref(mv)))
+        return ev.value, vec, mv.value
+
+    def set_theta(self, theta):
+        t = np.ascontiguousarray(np.asarray(theta, np.complex128))
+        _check(lib.cmps_heff_set_theta(self.h, _p(t.view(np.float64), C.c_double)))
+
+    def SVD(self, chi=0, max_trunc=0.0):
+        s = C.c_void_p()
+        _check(lib.cmps_heff_theta_svd(self.h, chi, max_trunc, C.byref(s)))
+        return SVDResult(s, self.nq)
+
+    def make_left_block(self, svd: "SVDResult"):
+        b = C.c_void_p()
+        _check(lib.cmps_heff_left_block(self.h, svd.h, C.byref(b)))
+        return Block(b, self.nq)
+
+    def make_right_block(self, svd: "SVDResult"):
+        b = C.c_void_p()
+        _check(lib.cmps_heff_right_block(self.h, svd.h, C.byref(b)))
+        return Block(b, self.nq)
+
+
+class SVDResult:
+    def __init__(self, h, nq):
+        self.h = h
+        self.nq = nq
+        kept = C.c_int64()
+        disc = C.c_double()
+        nu = C.c_int64()
+        nv = C.c_int64()
+        _check(lib.cmps_svd_info(h, C.byref(kept), C.byref(disc), C.byref(nu), C.byref(nv)))
+        self.kept = kept.value
+        self.discarded = disc.value
+        self._nu, self._nv = nu.value, nv.value
+
+    def copy(self, u_rows, vd_cols):
+        k = self.kept
+        vals = np.zeros(k, np.float64)
+        ch = np.zeros((k, self.nq), np.int16)
+        ucp = np.zeros(k + 1, np.int64)
+        uri = np.zeros(max(1, self._nu), np.int64)
+        uv = np.zeros(max(1, self._nu), np.complex128)
+        vcp = np.zeros(vd_cols + 1, np.int64)
+        vri = np.zeros(max(1, self._nv), np.int64)
+        vv = np.zeros(max(1, self._nv), np.complex128)
+        _check(lib.cmps_svd_copy(self.h, _p(vals, C.c_double), _p(ch, C.c_int16), _p(ucp, C.c_int64),
+                                 _p(uri, C.c_int64), _p(uv.view(np.float64), C.c_double), _p(vcp, C.c_int64),
+                                 _p(vri, C.c_int64), _p(vv.view(np.float64), C.c_double)))
+        nu, nv = ucp[-1], vcp[-1]
+        return dict(values=vals, charges=ch.astype(np.int64), u=(ucp, uri[:nu], uv[:nu]),
+                    vd=(vcp, vri[:nv], vv[:nv]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.cmps_svd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Block:
+    """A new environment block kept on the device."""
+
+    def __init__(self, h, nq):
+        self.h = h
+        self.nq = nq
+        chi = C.c_int64()
+        D = C.c_int64()
+        nnz = C.c_int64()
+        _check(lib.cmps_block_info(h, C.byref(chi), C.byref(D), C.byref(nnz)))
+        self.chi, self.D, self._nnz = chi.value, D.value, nnz.value
+
+    def to_csc(self):
+        ch = np.zeros((self.chi, self.nq), np.int16)
+        cp = np.zeros(self.D * self.chi + 1, np.int64)
+        ri = np.zeros(max(1, self._nnz), np.int64)
+        v = np.zeros(max(1, self._nnz), np.complex128)
+        _check(lib.cmps_block_copy(self.h, _p(ch, C.c_int16), _p(cp, C.c_int64), _p(ri, C.c_int64),
+                                   _p(v.view(np.float64), C.c_double)))
+        n = cp[-1]
+        return ch.astype(np.int64), (cp, ri[:n], v[:n])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.cmps_block_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: bool):
+    """A reference-layout environment block (e.g. MakeDummyLeftBlock) as a
+    device Block."""
+    cr, r = _rules(rules)
+    db, kb = block._desc()
+    dw, kw = W._desc()
+    h = C.c_void_p()
+    _check(lib.cmps_block_create(ctx.h, C.byref(cr), C.byref(db), C.byref(dw), 1 if right else 0, C.byref(h)))
+    return Block(h, len(r))
+
+
+def version():
+    return lib.cmps_version().decode()

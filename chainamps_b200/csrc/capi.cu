@@ -1,0 +1,200 @@
+// C ABI entry points (include/chainamps_b200.h): argument checking, error
+// strings, context and handle lifetime.  No entry point aborts; every
+// failure is an int status plus cmps_last_error().
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "heff.h"
+
+namespace cmps {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+static int rules_from(const cmps_charge_rules* cr, Rules& r) {
+  if (!cr || cr->nq < 1 || cr->nq > kMaxQ || !cr->rules)
+    return fail(CMPS_ERR_ARG, "charge rules: need 1.." + std::to_string(kMaxQ) + " charges");
+  r.nq = cr->nq;
+  for (int i = 0; i < kMaxQ; ++i) r.n[i] = i < cr->nq ? cr->rules[i] : 0;
+  return CMPS_OK;
+}
+
+static int use_device(cmps_context* ctx) {
+  if (!ctx) return fail(CMPS_ERR_ARG, "null context");
+  CMPS_CUDA(cudaSetDevice(ctx->device));
+  return CMPS_OK;
+}
+
+}  // namespace cmps
+
+using namespace cmps;
+
+extern "C" {
+
+const char* cmps_last_error(void) { return g_last_error.c_str(); }
+
+const char* cmps_version(void) {
+  return "chainamps_b200 1.0 sm_100a: fp64 DMMA grouped zgemm, device Lanczos, cusolver block SVD";
+}
+
+int cmps_context_create(int device, cmps_context** out) {
+  if (!out) return fail(CMPS_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int n = 0;
+  CMPS_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(CMPS_ERR_ARG, "no such CUDA device");
+  CMPS_CUDA(cudaSetDevice(device));
+  auto* c = new (std::nothrow) cmps_context();
+  if (!c) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(CMPS_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  *out = c;
+  return CMPS_OK;
+}
+
+int cmps_context_destroy(cmps_context* ctx) {
+  if (!ctx) return CMPS_OK;
+  cudaSetDevice(ctx->device);
+  release_solver(ctx);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return CMPS_OK;
+}
+
+int cmps_heff_create(cmps_context* ctx, const cmps_charge_rules* rules, const cmps_mpx_desc* L,
+                     const cmps_mpx_desc* W, const cmps_mpx_desc* R, int precision, cmps_heff** out) {
+  if (!out) return fail(CMPS_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  CMPS_TRY(use_device(ctx));
+  Rules r;
+  CMPS_TRY(rules_from(rules, r));
+  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  auto h = std::unique_ptr<cmps_heff>(new (std::nothrow) cmps_heff());
+  if (!h) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  h->impl.reset(new (std::nothrow) Heff());
+  if (!h->impl) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  CMPS_TRY(h->impl->build(ctx, r, L, W, R));
+  CMPS_TRY(cmps_heff_set_precision(h.get(), precision));
+  *out = h.release();
+  return CMPS_OK;
+}
+
+int cmps_heff_create_from_blocks(cmps_context* ctx, const cmps_charge_rules* rules, const cmps_block* L,
+                                 const cmps_mpx_desc* W, const cmps_block* R, int precision, cmps_heff** out) {
+  if (!out || !L || !R) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  CMPS_TRY(use_device(ctx));
+  Rules r;
+  CMPS_TRY(rules_from(rules, r));
+  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  auto h = std::unique_ptr<cmps_heff>(new (std::nothrow) cmps_heff());
+  if (!h) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  h->impl.reset(new (std::nothrow) Heff());
+  if (!h->impl) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  CMPS_TRY(h->impl->build_from_envs(ctx, r, L->env, W, R->env));
+  CMPS_TRY(cmps_heff_set_precision(h.get(), precision));
+  *out = h.release();
+  return CMPS_OK;
+}
+
+int cmps_block_create(cmps_context* ctx, const cmps_charge_rules* rules, const cmps_mpx_desc* block,
+                      const cmps_mpx_desc* W, int right, cmps_block** out) {
+  if (!out || !block || !W) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  CMPS_TRY(use_device(ctx));
+  Rules r;
+  CMPS_TRY(rules_from(rules, r));
+  Heff tmp;
+  tmp.rules = r;
+  CMPS_TRY(tmp.parse_mpo(W));
+  auto b = std::unique_ptr<cmps_block>(new (std::nothrow) cmps_block());
+  if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  b->rules = r;
+  CMPS_TRY(build_env_from_desc(r, block, right != 0, b->env, tmp.D, tmp.bq));
+  *out = b.release();
+  return CMPS_OK;
+}
+
+int cmps_heff_destroy(cmps_heff* h) {
+  if (!h) return CMPS_OK;
+  if (h->impl && h->impl->ctx) cudaSetDevice(h->impl->ctx->device);
+  delete h;
+  return CMPS_OK;
+}
+
+int cmps_heff_length(const cmps_heff* h, int64_t* n_allowed, int64_t* full_length) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (n_allowed) *n_allowed = h->impl->n_allowed;
+  if (full_length) *full_length = h->impl->full_length;
+  return CMPS_OK;
+}
+
+int cmps_heff_allowed_indices(const cmps_heff* h, int64_t* out) {
+  if (!h || !h->impl || !out) return fail(CMPS_ERR_ARG, "null argument");
+  std::memcpy(out, h->impl->allowed.data(), sizeof(int64_t) * h->impl->allowed.size());
+  return CMPS_OK;
+}
+
+int cmps_heff_apply(cmps_heff* h, const double* in, double* out) {
+  if (!h || !h->impl || !in || !out) return fail(CMPS_ERR_ARG, "null argument");
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->apply_host(in, out);
+}
+
+int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void* stream) {
+  if (!h || !h->impl || !d_in || !d_out) return fail(CMPS_ERR_ARG, "null argument");
+  CMPS_TRY(use_device(h->impl->ctx));
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->impl->ctx->stream;
+  return h->impl->apply_device(d_in, d_out, st);
+}
+
+int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (canonical) *canonical = h->impl->flops_canonical;
+  if (executed) *executed = h->impl->flops_executed;
+  return CMPS_OK;
+}
+
+int cmps_heff_set_precision(cmps_heff* h, int precision) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  CMPS_TRY(prepare_precision(h->impl.get(), precision));
+  h->impl->precision = precision;
+  return CMPS_OK;
+}
+
+int cmps_heff_eigs(cmps_heff* h, const double* guess, double tol, int max_restarts, int krylov_dim,
+                   double* eval, double* evec, int* matvecs) {
+  if (!h || !h->impl || !eval) return fail(CMPS_ERR_ARG, "null argument");
+  if (!(tol > 0.0)) return fail(CMPS_ERR_ARG, "tolerance must be positive");
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->eigs(guess, tol, max_restarts, krylov_dim, eval, evec, matvecs);
+}
+
+int cmps_heff_set_theta(cmps_heff* h, const double* theta) {
+  if (!h || !h->impl || !theta) return fail(CMPS_ERR_ARG, "null argument");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  cudaStream_t st = H.ctx->stream;
+  CMPS_CUDA(cudaMemcpyAsync(H.d_io, theta, sizeof(double) * 2 * H.n_allowed, cudaMemcpyHostToDevice, st));
+  if (H.theta.len != H.th.total) CMPS_TRY(H.theta.alloc(H.th.total));
+  CMPS_TRY(launch_pack(H.d_io, H.d_pos, H.n_allowed, H.theta, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  H.have_theta = true;
+  return CMPS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,786 @@
+// Host side of the device-resident effective Hamiltonian: parsing of the
+// reference's MPX tensors, charge-sector structure, LeftPart / RightPart
+// formation, the two grouped-GEMM stages of the matvec and the Krylov
+// ground-state solver.
+//
+// Matvec (TwoVertexMPOMPSMultiply, DMRG_routines.cpp:898-945):
+//   LeftPart^{b1}[(s1', a0'), (s1, a0)]  = sum_b0 W[s1', b0, s1, b1] L^{b0}[a0', a0]
+//   RightPart^{b1}[(s2, a2), (s2', a2')] = sum_b2 W[s2', b1, s2, b2] R^{b2}[a2', a2]
+//   T^{b1}  = LeftPart^{b1} . Theta                       (stage 1)
+//   Theta'  = sum_b1 T^{b1} . RightPart^{b1}               (stage 2)
+// exactly the reference's (LeftPart . V) . RightPart order
+// (DMRG_routines.cpp:779, :943), with every operand held as dense
+// charge-sector blocks instead of CSC.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <set>
+
+#include "heff.h"
+
+namespace cmps {
+
+int gemm_tile_m();
+int gemm_tile_n();
+
+// ---------------------------------------------------------------------------
+QKey Rules::add(const QKey& a, const QKey& b) const {
+  QKey o = zero();
+  for (int i = 0; i < nq; ++i) {
+    int v = (int)a[i] + (int)b[i];
+    if (n[i] > 0) v = ((v % n[i]) + n[i]) % n[i];
+    o[i] = (int16_t)v;
+  }
+  return o;
+}
+QKey Rules::sub(const QKey& a, const QKey& b) const {
+  QKey o = zero();
+  for (int i = 0; i < nq; ++i) {
+    int v = (int)a[i] - (int)b[i];
+    if (n[i] > 0) v = ((v % n[i]) + n[i]) % n[i];
+    o[i] = (int16_t)v;
+  }
+  return o;
+}
+
+void Bond::build(const std::vector<QKey>& charges) {
+  sq.clear(); sdim.clear(); esec.assign(charges.size(), 0); epos.assign(charges.size(), 0);
+  selem.clear(); lookup.clear();
+  for (size_t e = 0; e < charges.size(); ++e) {
+    auto it = lookup.find(charges[e]);
+    int s;
+    if (it == lookup.end()) {
+      s = (int)sq.size();
+      lookup[charges[e]] = s;
+      sq.push_back(charges[e]);
+      sdim.push_back(0);
+      selem.emplace_back();
+    } else {
+      s = it->second;
+    }
+    esec[e] = s;
+    epos[e] = sdim[s]++;
+    selem[s].push_back((int64_t)e);
+  }
+}
+
+std::vector<QKey> Bond::element_charges() const {
+  std::vector<QKey> out(esec.size());
+  for (size_t e = 0; e < esec.size(); ++e) out[e] = sq[esec[e]];
+  return out;
+}
+
+int Planar::alloc(int64_t n) {
+  release();
+  len = n;
+  if (n == 0) return CMPS_OK;
+  cudaError_t e = cudaMalloc(&d, sizeof(double) * 2 * (size_t)n);
+  if (e != cudaSuccess) {
+    d = nullptr;
+    len = 0;
+    return fail(CMPS_ERR_NOMEM, std::string("device allocation of ") + std::to_string(16.0 * n / 1e9) +
+                                    " GB failed: " + cudaGetErrorString(e));
+  }
+  return CMPS_OK;
+}
+
+void Planar::release() {
+  if (d) cudaFree(d);
+  d = nullptr;
+  len = 0;
+}
+
+int64_t Env::block_rows(int b, int s) const {
+  int sp = partner[(size_t)b * a.nsec() + s];
+  return right ? a.sdim[s] : a.sdim[sp];
+}
+int64_t Env::block_cols(int b, int s) const {
+  int sp = partner[(size_t)b * a.nsec() + s];
+  return right ? a.sdim[sp] : a.sdim[s];
+}
+
+// ---------------------------------------------------------------------------
+// desc helpers
+static int check_desc(const cmps_mpx_desc* d, int nidx, const char* what) {
+  if (!d) return fail(CMPS_ERR_ARG, std::string(what) + ": null descriptor");
+  if (d->num_indices != nidx)
+    return fail(CMPS_ERR_ARG, std::string(what) + ": expected " + std::to_string(nidx) + " indices, got " +
+                                  std::to_string(d->num_indices));
+  if (d->num_row_indices < 0 || d->num_row_indices > d->num_indices)
+    return fail(CMPS_ERR_ARG, std::string(what) + ": bad num_row_indices");
+  int64_t r = 1, c = 1;
+  for (int i = 0; i < d->num_indices; ++i) {
+    if (d->sizes[i] < 1) return fail(CMPS_ERR_ARG, std::string(what) + ": empty index");
+    (i < d->num_row_indices ? r : c) *= d->sizes[i];
+  }
+  if (r != d->rows || c != d->cols)
+    return fail(CMPS_ERR_ARG, std::string(what) + ": matrix shape does not match index sizes");
+  if (d->colptr[0] != 0) return fail(CMPS_ERR_ARG, std::string(what) + ": colptr[0] != 0");
+  for (int64_t j = 0; j < d->cols; ++j)
+    if (d->colptr[j + 1] < d->colptr[j]) return fail(CMPS_ERR_ARG, std::string(what) + ": colptr not monotone");
+  int64_t nnz = d->colptr[d->cols];
+  for (int64_t p = 0; p < nnz; ++p)
+    if (d->rowind[p] < 0 || d->rowind[p] >= d->rows)
+      return fail(CMPS_ERR_ARG, std::string(what) + ": row index out of range");
+  return CMPS_OK;
+}
+
+int parse_index_charges(const Rules& r, const cmps_mpx_desc* d, int idx, std::vector<QKey>& out) {
+  int64_t off = 0;
+  for (int i = 0; i < idx; ++i) off += d->sizes[i];
+  out.assign(d->sizes[idx], r.zero());
+  for (int64_t e = 0; e < d->sizes[idx]; ++e) {
+    QKey q = r.zero();
+    for (int c = 0; c < r.nq; ++c) {
+      int v = d->charges[(off + e) * r.nq + c];
+      if (r.n[c] > 0) v = ((v % r.n[c]) + r.n[c]) % r.n[c];
+      q[c] = (int16_t)v;
+    }
+    out[e] = q;
+  }
+  return CMPS_OK;
+}
+
+// Visit every stored entry with its multi-index (first index fastest).
+template <typename F>
+static void for_each_entry(const cmps_mpx_desc* d, F&& f) {
+  int k = d->num_indices, nr = d->num_row_indices;
+  std::vector<int64_t> mi(k, 0);
+  for (int64_t c = 0; c < d->cols; ++c) {
+    int64_t cc = c;
+    for (int i = nr; i < k; ++i) {
+      mi[i] = cc % d->sizes[i];
+      cc /= d->sizes[i];
+    }
+    for (int64_t p = d->colptr[c]; p < d->colptr[c + 1]; ++p) {
+      int64_t rr = d->rowind[p];
+      for (int i = 0; i < nr; ++i) {
+        mi[i] = rr % d->sizes[i];
+        rr /= d->sizes[i];
+      }
+      f(mi.data(), d->values[2 * p], d->values[2 * p + 1]);
+    }
+  }
+}
+
+// L: a' = 1, b = 3, a = 5.  R: a' = 0, b = 2, a = 4.  Blocks are allocated
+// for every (b, sector) with a charge-consistent partner sector.
+int build_env_from_desc(const Rules& r, const cmps_mpx_desc* d, bool right, Env& env, int D,
+                        const std::vector<QKey>& bq) {
+  const char* what = right ? "right block" : "left block";
+  CMPS_TRY(check_desc(d, 6, what));
+  const int ia = right ? 4 : 5, iap = right ? 0 : 1, ib = right ? 2 : 3;
+  for (int i = 0; i < 6; ++i)
+    if (i != ia && i != iap && i != ib && d->sizes[i] != 1)
+      return fail(CMPS_ERR_ARG, std::string(what) + ": index " + std::to_string(i) + " must be a size-1 dummy");
+  if (d->sizes[ib] != D) return fail(CMPS_ERR_ARG, std::string(what) + ": MPO index size differs from W");
+  std::vector<QKey> qa, qap, qb;
+  parse_index_charges(r, d, ia, qa);
+  parse_index_charges(r, d, iap, qap);
+  parse_index_charges(r, d, ib, qb);
+  if (qa.size() != qap.size() || qa != qap)
+    return fail(CMPS_ERR_ARG, std::string(what) + ": bra and ket bond indices differ");
+  if (qb != bq) return fail(CMPS_ERR_ARG, std::string(what) + ": MPO index charges differ from W");
+  env.right = right;
+  env.a.build(qa);
+  env.D = D;
+  env.bq = bq;
+  const int ns = env.a.nsec();
+  env.off.assign((size_t)D * ns, -1);
+  env.partner.assign((size_t)D * ns, -1);
+  int64_t total = 0;
+  for (int b = 0; b < D; ++b)
+    for (int s = 0; s < ns; ++s) {
+      int sp = env.a.find(r.add(env.a.sq[s], bq[b]));
+      if (sp < 0) continue;
+      env.partner[(size_t)b * ns + s] = sp;
+      env.off[(size_t)b * ns + s] = total;
+      total += env.a.sdim[s] * env.a.sdim[sp];
+    }
+  std::vector<double> h(2 * (size_t)total, 0.0);
+  int status = CMPS_OK;
+  for_each_entry(d, [&](const int64_t* mi, double re, double im) {
+    if (status != CMPS_OK) return;
+    int64_t a = mi[ia], ap = mi[iap], b = mi[ib];
+    int s = env.a.esec[a], sp = env.a.esec[ap];
+    if (env.partner[(size_t)b * ns + s] != sp) {
+      if (re != 0.0 || im != 0.0) status = fail(CMPS_ERR_CHARGE, std::string(what) + ": entry violates charge conservation");
+      return;
+    }
+    int64_t o = env.off[(size_t)b * ns + s];
+    int64_t p = env.a.epos[a], pp = env.a.epos[ap];
+    int64_t e = right ? o + p * env.a.sdim[sp] + pp : o + pp * env.a.sdim[s] + p;
+    h[e] += re;
+    h[total + e] += im;
+  });
+  if (status != CMPS_OK) return status;
+  CMPS_TRY(env.data.alloc(total));
+  if (total) CMPS_CUDA(cudaMemcpy(env.data.d, h.data(), sizeof(double) * 2 * total, cudaMemcpyHostToDevice));
+  return CMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+Heff::~Heff() {
+  L.data.release();
+  R.data.release();
+  LP.release();
+  RP.release();
+  T.release();
+  x.release();
+  y.release();
+  theta.release();
+  kv.release();
+  stage1.release();
+  stage2.release();
+  ops.release();
+  if (d_pos) cudaFree(d_pos);
+  if (d_io) cudaFree(d_io);
+  if (d_lp_blocks) cudaFree(d_lp_blocks);
+  if (d_lp_terms) cudaFree(d_lp_terms);
+  if (d_rp_blocks) cudaFree(d_rp_blocks);
+  if (d_rp_terms) cudaFree(d_rp_terms);
+}
+
+template <typename T>
+static int upload_vec(const std::vector<T>& v, T** d) {
+  if (*d) cudaFree(*d);
+  *d = nullptr;
+  if (v.empty()) return CMPS_OK;
+  CMPS_CUDA(cudaMalloc((void**)d, sizeof(T) * v.size()));
+  CMPS_CUDA(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return CMPS_OK;
+}
+
+int Heff::build(cmps_context* c, const Rules& r, const cmps_mpx_desc* Ld, const cmps_mpx_desc* Wd,
+                const cmps_mpx_desc* Rd) {
+  ctx = c;
+  rules = r;
+  CMPS_TRY(parse_mpo(Wd));
+  CMPS_TRY(build_env_from_desc(r, Ld, false, L, D, bq));
+  CMPS_TRY(build_env_from_desc(r, Rd, true, R, D, bq));
+  return finish();
+}
+
+int copy_env(const Env& src, Env& dst) {
+  dst.a = src.a;
+  dst.D = src.D;
+  dst.bq = src.bq;
+  dst.off = src.off;
+  dst.partner = src.partner;
+  dst.right = src.right;
+  CMPS_TRY(dst.data.alloc(src.data.len));
+  if (src.data.len)
+    CMPS_CUDA(cudaMemcpy(dst.data.d, src.data.d, sizeof(double) * 2 * src.data.len, cudaMemcpyDeviceToDevice));
+  return CMPS_OK;
+}
+
+int Heff::build_from_envs(cmps_context* c, const Rules& r, const Env& Lsrc, const cmps_mpx_desc* Wd,
+                          const Env& Rsrc) {
+  ctx = c;
+  rules = r;
+  CMPS_TRY(parse_mpo(Wd));
+  if (Lsrc.right || !Rsrc.right) return fail(CMPS_ERR_ARG, "block handedness: need a left and a right block");
+  if (Lsrc.D != D || Rsrc.D != D || Lsrc.bq != bq || Rsrc.bq != bq)
+    return fail(CMPS_ERR_ARG, "block MPO index differs from W");
+  CMPS_TRY(copy_env(Lsrc, L));
+  CMPS_TRY(copy_env(Rsrc, R));
+  return finish();
+}
+
+int Heff::parse_mpo(const cmps_mpx_desc* Wd) {
+  const Rules& r = rules;
+  CMPS_TRY(check_desc(Wd, 4, "MPO"));
+  d = (int)Wd->sizes[0];
+  D = (int)Wd->sizes[1];
+  if (Wd->sizes[2] != d || Wd->sizes[3] != D) return fail(CMPS_ERR_ARG, "MPO: index sizes inconsistent");
+  std::vector<QKey> sig2, bq3;
+  parse_index_charges(r, Wd, 0, sigq);
+  parse_index_charges(r, Wd, 2, sig2);
+  parse_index_charges(r, Wd, 1, bq);
+  parse_index_charges(r, Wd, 3, bq3);
+  if (sigq != sig2 || bq != bq3) return fail(CMPS_ERR_ARG, "MPO: row and column index charges differ");
+  W.clear();
+  int status = CMPS_OK;
+  for_each_entry(Wd, [&](const int64_t* mi, double re, double im) {
+    if (re == 0.0 && im == 0.0) return;
+    int sp = (int)mi[0], bl = (int)mi[1], s = (int)mi[2], br = (int)mi[3];
+    if (r.add(sigq[sp], bq[bl]) != r.add(sigq[s], bq[br])) {
+      status = fail(CMPS_ERR_CHARGE, "MPO: entry violates charge conservation");
+      return;
+    }
+    W.push_back(WEntry{sp, bl, s, br, re, im});
+  });
+  if (status != CMPS_OK) return status;
+  return CMPS_OK;
+}
+
+int Heff::finish() {
+  const Rules& r = rules;
+  const Bond& A0 = L.a;
+  const Bond& A2 = R.a;
+  // ---- theta space ----
+  // middle charges ordered by first appearance over columns c = s2 + d*a2
+  // ascending (the block order of GetAllBlockColumns, MPX_matrix.cpp:365-385)
+  std::set<QKey> rowm;
+  for (int s1 = 0; s1 < d; ++s1)
+    for (int s = 0; s < A0.nsec(); ++s) rowm.insert(r.add(sigq[s1], A0.sq[s]));
+  th = ThetaSpace();
+  for (int64_t a2 = 0; a2 < A2.size(); ++a2)
+    for (int s2 = 0; s2 < d; ++s2) {
+      QKey m = r.sub(A2.sq[A2.esec[a2]], sigq[s2]);
+      if (!rowm.count(m) || th.mfind.count(m)) continue;
+      th.mfind[m] = (int)th.mq.size();
+      th.mq.push_back(m);
+    }
+  const int nm = (int)th.mq.size();
+  th.nrows.assign(nm, 0);
+  th.ncols.assign(nm, 0);
+  th.base.assign(nm, 0);
+  th.rowoff.assign(nm, std::vector<int64_t>(d, -1));
+  th.coloff.assign(nm, std::vector<int64_t>(d, -1));
+  for (int m = 0; m < nm; ++m) {
+    for (int s1 = 0; s1 < d; ++s1) {
+      int s = A0.find(r.sub(th.mq[m], sigq[s1]));
+      if (s < 0) continue;
+      th.rowoff[m][s1] = th.nrows[m];
+      th.nrows[m] += A0.sdim[s];
+    }
+    for (int s2 = 0; s2 < d; ++s2) {
+      int t = A2.find(r.add(th.mq[m], sigq[s2]));
+      if (t < 0) continue;
+      th.coloff[m][s2] = th.ncols[m];
+      th.ncols[m] += A2.sdim[t];
+    }
+    th.base[m] = th.total;
+    th.total += th.nrows[m] * th.ncols[m];
+  }
+  // ---- allowed indices, ARPACK order (DMRG_routines.cpp:808-824) ----
+  full_length = (int64_t)d * A0.size() * d * A2.size();
+  std::map<QKey, std::vector<int>> sig_by_q;
+  for (int s1 = 0; s1 < d; ++s1) sig_by_q[sigq[s1]].push_back(s1);
+  allowed.clear();
+  allowed.reserve(th.total);
+  std::vector<int64_t> pos;
+  pos.reserve(th.total);
+  const int64_t chiL = A0.size();
+  for (int64_t a2 = 0; a2 < A2.size(); ++a2) {
+    const QKey qa2 = A2.sq[A2.esec[a2]];
+    for (int s2 = 0; s2 < d; ++s2) {
+      QKey m = r.sub(qa2, sigq[s2]);
+      int im = th.find(m);
+      if (im < 0) continue;
+      const int64_t colpart = s2 + (int64_t)d * a2;
+      const int64_t col = th.coloff[im][s2] + A2.epos[a2];
+      for (int64_t a0 = 0; a0 < chiL; ++a0) {
+        QKey need = r.sub(m, A0.sq[A0.esec[a0]]);
+        auto it = sig_by_q.find(need);
+        if (it == sig_by_q.end()) continue;
+        for (int s1 : it->second) {
+          allowed.push_back(s1 + (int64_t)d * a0 + (int64_t)d * chiL * colpart);
+          int64_t row = th.rowoff[im][s1] + A0.epos[a0];
+          pos.push_back(th.base[im] + row * th.ncols[im] + col);
+        }
+      }
+    }
+  }
+  n_allowed = (int64_t)allowed.size();
+  if (n_allowed != th.total) return fail(CMPS_ERR_STATE, "internal: allowed count differs from sector total");
+  CMPS_TRY(upload_vec(pos, &d_pos));
+
+  // ---- LeftPart blocks: key (b1, s1', s1, a0-sector s) ----
+  lp_off.clear();
+  lp_blocks.clear();
+  lp_terms.clear();
+  std::map<std::array<int, 4>, std::vector<AxpyTerm>> lpt;
+  for (const WEntry& w : W) {
+    for (int s = 0; s < A0.nsec(); ++s) {
+      int64_t lo = L.off[(size_t)w.bl * A0.nsec() + s];
+      if (lo < 0) continue;
+      QKey m = r.add(sigq[w.s], A0.sq[s]);
+      if (th.find(m) < 0 || th.find(r.add(m, bq[w.br])) < 0) continue;
+      lpt[{w.br, w.sp, w.s, s}].push_back(AxpyTerm{lo, w.wr, w.wi});
+    }
+  }
+  int64_t lp_total = 0;
+  for (auto& kv2 : lpt) {
+    const auto& key = kv2.first;
+    int s = key[3];
+    // partner sector: q(s') = q(s) + q(b0) = q(s) + q(s1) + q(b1) - q(s1')
+    QKey qsp = r.sub(r.add(r.add(A0.sq[s], sigq[key[2]]), bq[key[0]]), sigq[key[1]]);
+    int sp = A0.find(qsp);
+    if (sp < 0) continue;
+    int64_t len = A0.sdim[sp] * A0.sdim[s];
+    lp_off[key] = lp_total;
+    lp_blocks.push_back(AxpyBlock{lp_total, len, (int32_t)lp_terms.size(), (int32_t)(lp_terms.size() + kv2.second.size())});
+    for (auto& t : kv2.second) lp_terms.push_back(t);
+    lp_total += len;
+  }
+  // ---- RightPart blocks: key (b1, s2, s2', a2-sector t) ----
+  rp_off.clear();
+  rp_blocks.clear();
+  rp_terms.clear();
+  std::map<std::array<int, 4>, std::vector<AxpyTerm>> rpt;
+  for (const WEntry& w : W) {
+    for (int t = 0; t < A2.nsec(); ++t) {
+      int64_t ro = R.off[(size_t)w.br * A2.nsec() + t];
+      if (ro < 0) continue;
+      QKey m = r.sub(A2.sq[t], sigq[w.s]);
+      if (th.find(m) < 0 || th.find(r.add(m, bq[w.bl])) < 0) continue;
+      rpt[{w.bl, w.s, w.sp, t}].push_back(AxpyTerm{ro, w.wr, w.wi});
+    }
+  }
+  int64_t rp_total = 0;
+  for (auto& kv2 : rpt) {
+    const auto& key = kv2.first;
+    int t = key[3];
+    // q(t') = q(t) + q(b2) = q(t) + q(s2') + q(b1) - q(s2)
+    QKey qtp = r.sub(r.add(r.add(A2.sq[t], sigq[key[2]]), bq[key[0]]), sigq[key[1]]);
+    int tp = A2.find(qtp);
+    if (tp < 0) continue;
+    int64_t len = A2.sdim[t] * A2.sdim[tp];
+    rp_off[key] = rp_total;
+    rp_blocks.push_back(AxpyBlock{rp_total, len, (int32_t)rp_terms.size(), (int32_t)(rp_terms.size() + kv2.second.size())});
+    for (auto& tt : kv2.second) rp_terms.push_back(tt);
+    rp_total += len;
+  }
+  CMPS_TRY(LP.alloc(lp_total));
+  CMPS_TRY(RP.alloc(rp_total));
+  CMPS_TRY(upload_vec(lp_blocks, &d_lp_blocks));
+  CMPS_TRY(upload_vec(lp_terms, &d_lp_terms));
+  CMPS_TRY(upload_vec(rp_blocks, &d_rp_blocks));
+  CMPS_TRY(upload_vec(rp_terms, &d_rp_terms));
+
+  // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
+  std::set<int> b1s;
+  for (auto& kv2 : lp_off) b1s.insert(kv2.first[0]);
+  std::set<int> b1r;
+  for (auto& kv2 : rp_off) b1r.insert(kv2.first[0]);
+  t_base.assign((size_t)D * nm, -1);
+  stage1 = GemmPlan();
+  int64_t t_total = 0;
+  flops_executed = 0.0;
+  for (int b1 : b1s) {
+    if (!b1r.count(b1)) continue;
+    for (int m = 0; m < nm; ++m) {
+      int mp = th.find(r.add(th.mq[m], bq[b1]));
+      if (mp < 0) continue;
+      std::vector<GemmTask> tasks;
+      std::vector<GemmTerm> terms;
+      int64_t ldc = th.ncols[m];
+      for (int s1p = 0; s1p < d; ++s1p) {
+        if (th.rowoff[mp][s1p] < 0) continue;
+        int sp = A0.find(r.sub(th.mq[mp], sigq[s1p]));
+        GemmTask task{};
+        task.c_off = th.rowoff[mp][s1p] * ldc;  // relative to T block base, fixed below
+        task.m = (int32_t)A0.sdim[sp];
+        task.n = (int32_t)th.ncols[m];
+        task.ldc = (int32_t)ldc;
+        task.t0 = (int32_t)terms.size();
+        for (int s1 = 0; s1 < d; ++s1) {
+          if (th.rowoff[m][s1] < 0) continue;
+          int s = A0.find(r.sub(th.mq[m], sigq[s1]));
+          auto it = lp_off.find({b1, s1p, s1, s});
+          if (it == lp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = it->second;
+          tm.lda = (int32_t)A0.sdim[s];
+          tm.k = (int32_t)A0.sdim[s];
+          tm.b_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m];
+          tm.ldb = (int32_t)th.ncols[m];
+          terms.push_back(tm);
+        }
+        task.t1 = (int32_t)terms.size();
+        tasks.push_back(task);
+      }
+      if (terms.empty()) continue;
+      int64_t tb = t_total;
+      t_base[(size_t)b1 * nm + m] = tb;
+      t_total += th.nrows[mp] * th.ncols[m];
+      int32_t term_base = (int32_t)stage1.terms.size();
+      for (auto& tm : terms) {
+        stage1.terms.push_back(tm);
+      }
+      for (auto& task : tasks) {
+        task.c_off += tb;
+        task.t0 += term_base;
+        task.t1 += term_base;
+        for (int q = task.t0; q < task.t1; ++q)
+          flops_executed += 8.0 * task.m * (double)task.n * stage1.terms[q].k;
+        stage1.tasks.push_back(task);
+      }
+    }
+  }
+  CMPS_TRY(T.alloc(t_total));
+  // ---- stage 2: Theta'_m' = sum_b1 T^{b1}_{m'-q(b1)} . RightPart^{b1} ----
+  stage2 = GemmPlan();
+  for (int mp = 0; mp < nm; ++mp) {
+    for (int s2p = 0; s2p < d; ++s2p) {
+      if (th.coloff[mp][s2p] < 0) continue;
+      int tp = A2.find(r.add(th.mq[mp], sigq[s2p]));
+      GemmTask task{};
+      task.c_off = th.base[mp] + th.coloff[mp][s2p];
+      task.m = (int32_t)th.nrows[mp];
+      task.n = (int32_t)A2.sdim[tp];
+      task.ldc = (int32_t)th.ncols[mp];
+      task.t0 = (int32_t)stage2.terms.size();
+      for (int b1 = 0; b1 < D; ++b1) {
+        int m = th.find(r.sub(th.mq[mp], bq[b1]));
+        if (m < 0) continue;
+        int64_t tb = t_base[(size_t)b1 * nm + m];
+        if (tb < 0) continue;
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int t = A2.find(r.add(th.mq[m], sigq[s2]));
+          auto it = rp_off.find({b1, s2, s2p, t});
+          if (it == rp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = tb + th.coloff[m][s2];
+          tm.lda = (int32_t)th.ncols[m];
+          tm.k = (int32_t)A2.sdim[t];
+          tm.b_off = it->second;
+          tm.ldb = (int32_t)A2.sdim[tp];
+          stage2.terms.push_back(tm);
+          flops_executed += 8.0 * task.m * (double)task.n * tm.k;
+        }
+      }
+      task.t1 = (int32_t)stage2.terms.size();
+      stage2.tasks.push_back(task);
+    }
+  }
+  CMPS_TRY(stage1.validate(false, false, lp_total, th.total, t_total, "stage 1"));
+  CMPS_TRY(stage2.validate(false, false, t_total, rp_total, th.total, "stage 2"));
+  for (const AxpyBlock& b : lp_blocks)
+    for (int q = b.t0; q < b.t1; ++q)
+      if (b.dst_off + b.len > lp_total || lp_terms[q].src_off + b.len > L.data.len)
+        return fail(CMPS_ERR_STATE, "LeftPart block range outside its buffer");
+  for (const AxpyBlock& b : rp_blocks)
+    for (int q = b.t0; q < b.t1; ++q)
+      if (b.dst_off + b.len > rp_total || rp_terms[q].src_off + b.len > R.data.len)
+        return fail(CMPS_ERR_STATE, "RightPart block range outside its buffer");
+  for (int64_t p : pos)
+    if (p < 0 || p >= th.total) return fail(CMPS_ERR_STATE, "pack map entry outside the sector blocks");
+  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n()));
+  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n()));
+  cudaStream_t st = ctx->stream;
+  CMPS_TRY(launch_block_axpy(d_lp_blocks, (int)lp_blocks.size(), d_lp_terms, L.data, LP, st));
+  CMPS_TRY(launch_block_axpy(d_rp_blocks, (int)rp_blocks.size(), d_rp_terms, R.data, RP, st));
+
+  // ---- canonical four-stage flop count ----
+  {
+    double f = 0.0;
+    std::set<int> usedbl, usedbr;
+    for (const WEntry& w : W) { usedbl.insert(w.bl); usedbr.insert(w.br); }
+    for (int m = 0; m < nm; ++m)
+      for (int s1 = 0; s1 < d; ++s1) {
+        if (th.rowoff[m][s1] < 0) continue;
+        int s = A0.find(r.sub(th.mq[m], sigq[s1]));
+        for (int b0 : usedbl) {
+          int64_t lo = L.off[(size_t)b0 * A0.nsec() + s];
+          if (lo < 0) continue;
+          int sp = L.partner[(size_t)b0 * A0.nsec() + s];
+          f += 8.0 * A0.sdim[sp] * (double)A0.sdim[s] * th.ncols[m];            // L . theta
+        }
+        for (const WEntry& w : W) {
+          if (w.s != s1) continue;
+          int64_t lo = L.off[(size_t)w.bl * A0.nsec() + s];
+          if (lo < 0) continue;
+          int sp = L.partner[(size_t)w.bl * A0.nsec() + s];
+          f += 8.0 * A0.sdim[sp] * (double)th.ncols[m];                          // W1
+        }
+      }
+    for (int m = 0; m < nm; ++m)
+      for (int s2 = 0; s2 < d; ++s2) {
+        if (th.coloff[m][s2] < 0) continue;
+        int t = A2.find(r.add(th.mq[m], sigq[s2]));
+        for (const WEntry& w : W) {
+          if (w.s != s2) continue;
+          int mp = th.find(r.add(th.mq[m], bq[w.bl]));
+          if (mp < 0) continue;
+          f += 8.0 * th.nrows[mp] * (double)A2.sdim[t];                         // W2
+        }
+        for (int b2 : usedbr) {
+          int64_t ro = R.off[(size_t)b2 * A2.nsec() + t];
+          if (ro < 0) continue;
+          int tp = R.partner[(size_t)b2 * A2.nsec() + t];
+          f += 8.0 * th.nrows[m] * (double)A2.sdim[t] * A2.sdim[tp];             // . R
+        }
+      }
+    flops_canonical = f;
+  }
+  CMPS_TRY(x.alloc(th.total));
+  CMPS_TRY(y.alloc(th.total));
+  CMPS_CUDA(cudaMalloc(&d_io, sizeof(double) * 2 * std::max<int64_t>(1, n_allowed)));
+  CMPS_TRY(ops.init(th.total));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  return CMPS_OK;
+}
+
+int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
+  if (precision != CMPS_FP64) return fail(CMPS_ERR_ARG, "requested precision is not built into this library");
+  CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
+  CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
+  return CMPS_OK;
+}
+
+int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
+  CMPS_TRY(launch_pack(din, d_pos, n_allowed, x, st));
+  CMPS_TRY(apply_theta(x, y, st));
+  CMPS_TRY(launch_unpack(y, d_pos, n_allowed, dout, st));
+  return CMPS_OK;
+}
+
+int Heff::apply_host(const double* in, double* out) {
+  cudaStream_t st = ctx->stream;
+  size_t bytes = sizeof(double) * 2 * n_allowed;
+  CMPS_CUDA(cudaMemcpyAsync(d_io, in, bytes, cudaMemcpyHostToDevice, st));
+  CMPS_TRY(apply_device(d_io, d_io, st));
+  CMPS_CUDA(cudaMemcpyAsync(out, d_io, bytes, cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  return CMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Small dense symmetric eigenproblem (cyclic Jacobi): lowest eigenpair.
+static void jacobi_lowest(int n, const std::vector<double>& Ain, double* lam, std::vector<double>& vec) {
+  std::vector<double> A(Ain), V((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) off += A[(size_t)p * n + q] * A[(size_t)p * n + q];
+    if (off < 1e-300) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = A[(size_t)p * n + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+        double tau = (aqq - app) / (2.0 * apq);
+        double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+        double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * akp - s * akq;
+          A[(size_t)k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * apk - s * aqk;
+          A[(size_t)q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = c * vkp - s * vkq;
+          V[(size_t)k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  int best = 0;
+  for (int i = 1; i < n; ++i)
+    if (A[(size_t)i * n + i] < A[(size_t)best * n + best]) best = i;
+  *lam = A[(size_t)best * n + best];
+  vec.assign(n, 0.0);
+  for (int k = 0; k < n; ++k) vec[k] = V[(size_t)k * n + best];
+}
+
+// Lanczos with full re-orthogonalisation (classical Gram-Schmidt, twice)
+// and explicit restarts from the Ritz vector.
+int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, double* eval, double* evec,
+               int* matvecs) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = th.total;
+  if (n == 0) return fail(CMPS_ERR_STATE, "empty effective Hamiltonian");
+  if (kdim < 2) kdim = 2;
+  if (kdim > 96) kdim = 96;
+  if ((int64_t)kdim > n) kdim = (int)n;
+  if (kv_dim != kdim || kv.len != (int64_t)kdim * n) {
+    CMPS_TRY(kv.alloc((int64_t)kdim * n));
+    kv_dim = kdim;
+  }
+  auto vr = [&](int j) { return kv.re() + (int64_t)j * n; };
+  auto vi = [&](int j) { return kv.im() + (int64_t)j * n; };
+  // start vector into x
+  if (guess) {
+    CMPS_CUDA(cudaMemcpyAsync(d_io, guess, sizeof(double) * 2 * n_allowed, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(launch_pack(d_io, d_pos, n_allowed, x, st));
+  }
+  double nrm = 0.0;
+  if (guess) CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
+  if (!guess || !(nrm > 1e-300)) {
+    CMPS_TRY(ops.random(x.re(), x.im(), 0x5eed1234ULL, st));
+    CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
+  }
+  int nmv = 0;
+  double lam = 0.0;
+  bool converged = false;
+  std::vector<double> h(2 * 128), h2(2 * 128), alpha, beta, ycoef;
+  for (int restart = 0; restart < std::max(1, max_restarts) && !converged; ++restart) {
+    CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), vr(0), vi(0), st));
+    alpha.clear();
+    beta.clear();
+    int k = 0;
+    double last_beta = 0.0;
+    for (int j = 0; j < kdim; ++j) {
+      // y = H v_j; the basis vector is copied into the planar work vector x
+      CMPS_CUDA(cudaMemcpyAsync(x.re(), vr(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      CMPS_CUDA(cudaMemcpyAsync(x.im(), vi(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      CMPS_TRY(apply_theta(x, y, st));
+      ++nmv;
+      // Gram-Schmidt against v_0..v_j, twice
+      CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h.data(), st));
+      CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h.data(), y.re(), y.im(), -1.0, st));
+      CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h2.data(), st));
+      CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h2.data(), y.re(), y.im(), -1.0, st));
+      alpha.push_back(h[2 * j] + h2[2 * j]);
+      double b2 = 0.0;
+      CMPS_TRY(ops.norm2(y.re(), y.im(), &b2, st));
+      double b = std::sqrt(std::max(0.0, b2));
+      k = j + 1;
+      last_beta = b;
+      if (j + 1 < kdim) {
+        if (b < 1e-14 * std::max(1.0, std::fabs(alpha.back()))) break;  // invariant subspace
+        beta.push_back(b);
+        CMPS_TRY(ops.scale_copy(y.re(), y.im(), 1.0 / b, vr(j + 1), vi(j + 1), st));
+      }
+    }
+    // tridiagonal T (k x k)
+    std::vector<double> Tm((size_t)k * k, 0.0);
+    for (int i = 0; i < k; ++i) Tm[(size_t)i * k + i] = alpha[i];
+    for (int i = 0; i + 1 < k; ++i) Tm[(size_t)i * k + i + 1] = Tm[(size_t)(i + 1) * k + i] = beta[i];
+    jacobi_lowest(k, Tm, &lam, ycoef);
+    double resid = std::fabs(last_beta * ycoef[k - 1]);
+    CMPS_TRY(ops.combine(kv.re(), kv.im(), n, k, ycoef.data(), x.re(), x.im(), st));
+    CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
+    if (resid <= tol * std::max(1.0, std::fabs(lam)) || k < kdim) converged = true;
+  }
+  // normalise the Ritz vector
+  CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), x.re(), x.im(), st));
+  // HED post-processing (DMRG_routines.cpp:870-889)
+  double mx2 = 0.0;
+  int64_t imx = 0;
+  CMPS_TRY(ops.absmax(x.re(), x.im(), &mx2, &imx, st));
+  double mr = 0.0, mi = 0.0;
+  CMPS_CUDA(cudaMemcpyAsync(&mr, x.re() + imx, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaMemcpyAsync(&mi, x.im() + imx, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  double mabs = std::sqrt(mx2);
+  // phase = |max| / max = conj(max) / |max|
+  double pr = mr / mabs, pi = -mi / mabs;
+  CMPS_TRY(ops.phase_drop(x.re(), x.im(), pr, pi, 2.220446049250313e-16 * mabs, st));
+  if (theta.len != n) CMPS_TRY(theta.alloc(n));
+  CMPS_CUDA(cudaMemcpyAsync(theta.d, x.d, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
+  have_theta = true;
+  if (evec) {
+    CMPS_TRY(launch_unpack(theta, d_pos, n_allowed, d_io, st));
+    CMPS_CUDA(cudaMemcpyAsync(evec, d_io, sizeof(double) * 2 * n_allowed, cudaMemcpyDeviceToHost, st));
+  }
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  *eval = lam;
+  if (matvecs) *matvecs = nmv;
+  if (!converged) return fail(CMPS_ERR_SOLVER, "Lanczos did not reach the requested residual");
+  return CMPS_OK;
+}
+
+}  // namespace cmps

@@ -1,0 +1,111 @@
+// Device-resident two-vertex effective Hamiltonian (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+#include "kernels.h"
+
+struct cmps_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* solver = nullptr;  // cusolverDnHandle_t, created on first SVD
+};
+
+namespace cmps {
+
+// Two-vertex wavefunction space: Theta = sum over middle charges m of dense
+// blocks Theta_m[(sigma1, a0), (sigma2, a2)], q(sigma1)+q(a0) = m =
+// q(a2)-q(sigma2).  Rows are grouped by sigma1 (each sigma1 contributes the
+// whole a0-sector of charge m - q(sigma1)), columns by sigma2 (a2-sector of
+// charge m + q(sigma2)); blocks are row-major.
+struct ThetaSpace {
+  std::vector<QKey> mq;                     // middle charges
+  std::map<QKey, int> mfind;
+  std::vector<int64_t> nrows, ncols, base;  // per m
+  std::vector<std::vector<int64_t>> rowoff, coloff;  // [m][sigma] -> offset or -1
+  int64_t total = 0;
+  int find(const QKey& q) const {
+    auto it = mfind.find(q);
+    return it == mfind.end() ? -1 : it->second;
+  }
+};
+
+struct SvdResult;
+
+struct Heff {
+  cmps_context* ctx = nullptr;
+  Rules rules;
+  int d = 0;
+  std::vector<QKey> sigq;       // basis charges
+  Env L, R;                     // environments (device)
+  std::vector<WEntry> W;        // non-zero MPO entries
+  int D = 0;
+  std::vector<QKey> bq;         // MPO bond charges
+  std::vector<int16_t> bq_raw;  // as given (for export)
+  ThetaSpace th;
+  int64_t n_allowed = 0, full_length = 0;
+  std::vector<int64_t> allowed;  // ARPACK order -> full linear index
+  int64_t* d_pos = nullptr;      // ARPACK order -> theta block offset
+  // LeftPart / RightPart sector blocks
+  Planar LP, RP;
+  std::vector<AxpyBlock> lp_blocks, rp_blocks;
+  std::vector<AxpyTerm> lp_terms, rp_terms;
+  AxpyBlock* d_lp_blocks = nullptr;
+  AxpyTerm* d_lp_terms = nullptr;
+  AxpyBlock* d_rp_blocks = nullptr;
+  AxpyTerm* d_rp_terms = nullptr;
+  std::map<std::array<int, 4>, int64_t> lp_off, rp_off;  // (b1, sigma', sigma, sector) -> offset
+  std::vector<int64_t> t_base;   // [b1 * nm + m] -> offset into T, -1 if absent
+  Planar T;                      // stage-1 intermediate
+  GemmPlan stage1, stage2;
+  double flops_canonical = 0.0, flops_executed = 0.0;
+  int precision = CMPS_FP64;
+  // work vectors
+  Planar x, y;                   // theta-space vectors
+  double* d_io = nullptr;        // interleaved staging (2 * n_allowed doubles)
+  bool have_theta = false;
+  Planar theta;                  // last eigenvector (theta space)
+  // Krylov basis
+  Planar kv;                     // kdim vectors of length th.total (planar, stride th.total)
+  int kv_dim = 0;
+  VecOps ops;
+
+  ~Heff();
+  int build(cmps_context* c, const Rules& r, const cmps_mpx_desc* Ld, const cmps_mpx_desc* Wd,
+            const cmps_mpx_desc* Rd);
+  int build_from_envs(cmps_context* c, const Rules& r, const Env& Lsrc, const cmps_mpx_desc* Wd, const Env& Rsrc);
+  int parse_mpo(const cmps_mpx_desc* Wd);
+  int finish();  // sector structure, LeftPart/RightPart, GEMM plans (L, R, W set)
+  int apply_theta(const Planar& in, Planar& out, cudaStream_t st);  // theta-space matvec
+  int apply_host(const double* in, double* out);
+  int apply_device(const double* din, double* dout, cudaStream_t st);
+  int eigs(const double* guess, double tol, int max_restarts, int kdim, double* eval, double* evec,
+           int* matvecs);
+};
+
+// Split-precision operands for the tcgen05 path (split_tf32.cu).
+int prepare_precision(Heff* h, int precision);
+// cuSOLVER handle owned by the context (svd.cu).
+void release_solver(cmps_context* ctx);
+
+int copy_env(const Env& src, Env& dst);
+
+int build_env_from_desc(const Rules& r, const cmps_mpx_desc* desc, bool right, Env& env, int D,
+                        const std::vector<QKey>& bq);
+int parse_index_charges(const Rules& r, const cmps_mpx_desc* desc, int idx, std::vector<QKey>& out);
+
+}  // namespace cmps
+
+struct cmps_heff {
+  std::unique_ptr<cmps::Heff> impl;
+};
+
+struct cmps_block {
+  cmps::Rules rules;
+  cmps::Env env;
+  ~cmps_block() { env.data.release(); }
+};

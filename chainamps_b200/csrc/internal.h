@@ -1,0 +1,145 @@
+// Internal declarations of the chainamps_b200 library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <array>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "chainamps_b200.h"
+
+namespace cmps {
+
+constexpr int kMaxQ = 4;  // charges per state (QuantumNumberInt each)
+using QKey = std::array<int16_t, kMaxQ>;
+
+// Error reporting: thread-local last-error string, returned codes.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define CMPS_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t _e = (call);                                                         \
+    if (_e != cudaSuccess)                                                           \
+      return ::cmps::fail(CMPS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+#define CMPS_TRY(call)            \
+  do {                            \
+    int _s = (call);              \
+    if (_s != CMPS_OK) return _s; \
+  } while (0)
+
+// Charge arithmetic of State (states.hpp:176-206).
+struct Rules {
+  int nq = 0;
+  int16_t n[kMaxQ] = {0, 0, 0, 0};
+  QKey add(const QKey& a, const QKey& b) const;
+  QKey sub(const QKey& a, const QKey& b) const;
+  QKey zero() const { return QKey{0, 0, 0, 0}; }
+};
+
+// Elements of one bond index grouped by charge.  Element order is the
+// reference's element order; sectors are numbered by first appearance.
+struct Bond {
+  std::vector<QKey> sq;                     // charge of each sector
+  std::vector<int64_t> sdim;                // elements per sector
+  std::vector<int32_t> esec;                // element -> sector
+  std::vector<int64_t> epos;                // element -> position inside its sector
+  std::vector<std::vector<int64_t>> selem;  // sector -> elements in order
+  std::map<QKey, int> lookup;
+  int64_t size() const { return (int64_t)esec.size(); }
+  int nsec() const { return (int)sq.size(); }
+  int find(const QKey& q) const {
+    auto it = lookup.find(q);
+    return it == lookup.end() ? -1 : it->second;
+  }
+  void build(const std::vector<QKey>& charges);
+  std::vector<QKey> element_charges() const;
+};
+
+// Device buffer of complex values stored as two planes (re then im).
+struct Planar {
+  double* d = nullptr;
+  int64_t len = 0;  // complex elements
+  double* re() const { return d; }
+  double* im() const { return d + len; }
+  int alloc(int64_t n);
+  void release();
+};
+
+// An environment (left or right block) on the device.  Block (b, s) of a
+// left block is the dense [a', a] matrix L^b restricted to a-sector s and
+// a'-sector s' = sector(q_s + q_b), row-major (dim s') x (dim s).  A right
+// block stores R^b transposed: [a, a'], (dim t) x (dim t').
+struct Env {
+  Bond a;
+  int D = 0;
+  std::vector<QKey> bq;         // MPO bond charges
+  std::vector<int64_t> off;     // D * nsec, -1 if the block is absent
+  std::vector<int32_t> partner; // D * nsec: s' (the a' sector) or -1
+  Planar data;
+  bool right = false;
+  int64_t block_rows(int b, int s) const;
+  int64_t block_cols(int b, int s) const;
+};
+
+struct WEntry {
+  int sp, bl, s, br;
+  double wr, wi;
+};
+
+// Grouped complex GEMM work description (device arrays).
+struct GemmTask {
+  int64_t c_off;
+  int32_t m, n, ldc;
+  int32_t t0, t1;  // term range
+  int32_t pad;
+};
+struct GemmTerm {
+  int64_t a_off, b_off;
+  int32_t k, lda, ldb, pad;
+};
+struct GemmTile {
+  int32_t task, m0, n0, pad;
+};
+
+struct GemmPlan {
+  std::vector<GemmTask> tasks;
+  std::vector<GemmTerm> terms;
+  std::vector<GemmTile> tiles;
+  GemmTask* d_tasks = nullptr;
+  GemmTerm* d_terms = nullptr;
+  GemmTile* d_tiles = nullptr;
+  double flops = 0.0;
+  int upload(int bm, int bn);
+  // Host check, before any launch, that every operand and output range lies
+  // inside its buffer (lengths in complex elements).
+  int validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t c_len, const char* what) const;
+  void release();
+};
+
+// Block AXPY lists: dst block = sum_t w_t * src_t (same shapes).
+struct AxpyBlock {
+  int64_t dst_off, len;
+  int32_t t0, t1;
+};
+struct AxpyTerm {
+  int64_t src_off;
+  double wr, wi;
+};
+
+// ---- kernels (launchers) ---------------------------------------------------
+int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
+                      Planar& C, cudaStream_t st);
+int launch_pack(const double* in_interleaved, const int64_t* pos, int64_t n, Planar& dst,
+                cudaStream_t st);
+int launch_unpack(const Planar& src, const int64_t* pos, int64_t n, double* out_interleaved,
+                  cudaStream_t st);
+int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,
+                      const Planar& src, Planar& dst, cudaStream_t st);
+
+}  // namespace cmps

@@ -1,0 +1,345 @@
+// Memory-bound kernels of the hot path: ARPACK-order <-> sector-block
+// gathers/scatters, block AXPY lists (LeftPart / RightPart formation), and
+// the FP64 vector kernels of the device Krylov solver.  All are
+// grid-stride loops sized to a multiple of the SM count.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+#include "kernels.h"
+
+namespace cmps {
+
+namespace {
+
+int grid_for(int64_t n, int threads) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t want = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)sms * 8;
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+__global__ void k_pack(const double2* __restrict__ in, const int64_t* __restrict__ pos, int64_t n,
+                       double* __restrict__ re, double* __restrict__ im) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 v = in[i];
+    int64_t p = pos[i];
+    re[p] = v.x;
+    im[p] = v.y;
+  }
+}
+
+__global__ void k_unpack(const double* __restrict__ re, const double* __restrict__ im,
+                         const int64_t* __restrict__ pos, int64_t n, double2* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t p = pos[i];
+    out[i] = make_double2(re[p], im[p]);
+  }
+}
+
+// One CTA per destination block; dst = sum_t w_t src_t.
+__global__ void k_block_axpy(const AxpyBlock* __restrict__ blocks, const AxpyTerm* __restrict__ terms,
+                             const double* __restrict__ sr, const double* __restrict__ si,
+                             double* __restrict__ dr, double* __restrict__ di) {
+  const AxpyBlock b = blocks[blockIdx.x];
+  for (int64_t e = threadIdx.x; e < b.len; e += blockDim.x) {
+    double xr = 0.0, xi = 0.0;
+    for (int t = b.t0; t < b.t1; ++t) {
+      const AxpyTerm tm = terms[t];
+      double vr = sr[tm.src_off + e], vi = si[tm.src_off + e];
+      xr += tm.wr * vr - tm.wi * vi;
+      xi += tm.wr * vi + tm.wi * vr;
+    }
+    dr[b.dst_off + e] = xr;
+    di[b.dst_off + e] = xi;
+  }
+}
+
+// ---- Krylov vector kernels (planar FP64 vectors of length n) ----------------
+constexpr int RED_THREADS = 256;
+
+// partial[j][blk] = sum_i conj(V_j[i]) * w[i] over this CTA's slice, j < k.
+__global__ void k_multidot(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv,
+                           int k, const double* __restrict__ wr, const double* __restrict__ wi, int64_t n,
+                           double* __restrict__ partial) {
+  extern __shared__ double red[];
+  for (int j = 0; j < k; ++j) {
+    double sr = 0.0, si = 0.0;
+    const double* vr = Vr + (int64_t)j * ldv;
+    const double* vi = Vi + (int64_t)j * ldv;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      double ar = vr[i], ai = vi[i], br = wr[i], bi = wi[i];
+      sr += ar * br + ai * bi;
+      si += ar * bi - ai * br;
+    }
+    red[threadIdx.x] = sr;
+    red[threadIdx.x + blockDim.x] = si;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        red[threadIdx.x] += red[threadIdx.x + s];
+        red[threadIdx.x + blockDim.x] += red[threadIdx.x + s + blockDim.x];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      partial[(2 * j) * gridDim.x + blockIdx.x] = red[0];
+      partial[(2 * j + 1) * gridDim.x + blockIdx.x] = red[blockDim.x];
+    }
+    __syncthreads();
+  }
+}
+
+// out[r] = sum_b partial[r][b], r < rows (one warp-per-row, deterministic order).
+__global__ void k_reduce_rows(const double* __restrict__ partial, int nb, int rows, double* __restrict__ out) {
+  int r = blockIdx.x;
+  if (r >= rows) return;
+  __shared__ double red[RED_THREADS];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(int64_t)r * nb + b];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[r] = red[0];
+}
+
+// w -= sum_j h_j V_j  (h complex, k <= 64 in constant-like global memory)
+__global__ void k_multiaxpy(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k,
+                            const double* __restrict__ h, double* __restrict__ wr, double* __restrict__ wi,
+                            int64_t n, double sign) {
+  __shared__ double hs[2 * 128];
+  for (int j = threadIdx.x; j < 2 * k; j += blockDim.x) hs[j] = h[j];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double xr = 0.0, xi = 0.0;
+    for (int j = 0; j < k; ++j) {
+      double hr = hs[2 * j], hi = hs[2 * j + 1];
+      double vr = Vr[(int64_t)j * ldv + i], vi = Vi[(int64_t)j * ldv + i];
+      xr += hr * vr - hi * vi;
+      xi += hr * vi + hi * vr;
+    }
+    wr[i] += sign * xr;
+    wi[i] += sign * xi;
+  }
+}
+
+__global__ void k_scale_copy(const double* __restrict__ xr, const double* __restrict__ xi, double s,
+                             double* __restrict__ yr, double* __restrict__ yi, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    yr[i] = s * xr[i];
+    yi[i] = s * xi[i];
+  }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdULL;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ULL;
+  x ^= x >> 33;
+  return x;
+}
+
+__global__ void k_random(double* __restrict__ re, double* __restrict__ im, int64_t n, uint64_t seed) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t a = mix64(seed ^ (2 * (uint64_t)i + 1));
+    uint64_t b = mix64(a + 0x9e3779b97f4a7c15ULL);
+    re[i] = ((double)(a >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+    im[i] = ((double)(b >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+  }
+}
+
+// per-CTA max |x| and its index
+__global__ void k_absmax(const double* __restrict__ re, const double* __restrict__ im, int64_t n,
+                         double* __restrict__ pval, int64_t* __restrict__ pidx) {
+  __shared__ double sv[RED_THREADS];
+  __shared__ int64_t si[RED_THREADS];
+  double best = -1.0;
+  int64_t bi = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double a = re[i] * re[i] + im[i] * im[i];
+    if (a > best) { best = a; bi = i; }
+  }
+  sv[threadIdx.x] = best;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      double o = sv[threadIdx.x + s];
+      int64_t oi = si[threadIdx.x + s];
+      if (o > sv[threadIdx.x] || (o == sv[threadIdx.x] && oi < si[threadIdx.x])) {
+        sv[threadIdx.x] = o;
+        si[threadIdx.x] = oi;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pval[blockIdx.x] = sv[0];
+    pidx[blockIdx.x] = si[0];
+  }
+}
+
+// x *= phase; drop |x| <= thr; FixComplexPrecision (sparse_interface.cpp:28-32)
+__global__ void k_phase_drop(double* __restrict__ re, double* __restrict__ im, int64_t n, double pr, double pi,
+                             double thr) {
+  const double eps = 2.220446049250313e-16;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double a = re[i], b = im[i];
+    double xr = a * pr - b * pi, xi = a * pi + b * pr;
+    if (sqrt(xr * xr + xi * xi) > thr) {
+      if (fabs(xi / xr) < eps) xi = 0.0;
+      else if (fabs(xr / xi) < eps) xr = 0.0;
+    } else {
+      xr = 0.0;
+      xi = 0.0;
+    }
+    re[i] = xr;
+    im[i] = xi;
+  }
+}
+
+// y = sum_j c_j V_j (c real)
+__global__ void k_combine(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k,
+                          const double* __restrict__ c, double* __restrict__ yr, double* __restrict__ yi, int64_t n) {
+  __shared__ double cs[128];
+  for (int j = threadIdx.x; j < k; j += blockDim.x) cs[j] = c[j];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double xr = 0.0, xi = 0.0;
+    for (int j = 0; j < k; ++j) {
+      xr += cs[j] * Vr[(int64_t)j * ldv + i];
+      xi += cs[j] * Vi[(int64_t)j * ldv + i];
+    }
+    yr[i] = xr;
+    yi[i] = xi;
+  }
+}
+
+}  // namespace
+
+int launch_pack(const double* in, const int64_t* pos, int64_t n, Planar& dst, cudaStream_t st) {
+  if (n == 0) return CMPS_OK;
+  k_pack<<<grid_for(n, 256), 256, 0, st>>>((const double2*)in, pos, n, dst.re(), dst.im());
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int launch_unpack(const Planar& src, const int64_t* pos, int64_t n, double* out, cudaStream_t st) {
+  if (n == 0) return CMPS_OK;
+  k_unpack<<<grid_for(n, 256), 256, 0, st>>>(src.re(), src.im(), pos, n, (double2*)out);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms, const Planar& src,
+                      Planar& dst, cudaStream_t st) {
+  if (nblocks == 0) return CMPS_OK;
+  k_block_axpy<<<nblocks, 256, 0, st>>>(d_blocks, d_terms, src.re(), src.im(), dst.re(), dst.im());
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+// ---- Krylov helpers ---------------------------------------------------------
+int VecOps::init(int64_t n_) {
+  n = n_;
+  nb = grid_for(n, RED_THREADS);
+  if (nb > 1024) nb = 1024;
+  CMPS_CUDA(cudaMalloc(&d_partial, sizeof(double) * 2 * 128 * nb));
+  CMPS_CUDA(cudaMalloc(&d_small, sizeof(double) * 2 * 128 * 2));
+  CMPS_CUDA(cudaMalloc(&d_pidx, sizeof(int64_t) * nb));
+  return CMPS_OK;
+}
+
+void VecOps::release() {
+  if (d_partial) cudaFree(d_partial);
+  if (d_small) cudaFree(d_small);
+  if (d_pidx) cudaFree(d_pidx);
+  d_partial = d_small = nullptr;
+  d_pidx = nullptr;
+}
+
+int VecOps::multidot(const double* Vr, const double* Vi, int64_t ldv, int k, const double* wr, const double* wi,
+                     double* h_host, cudaStream_t st) {
+  if (k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  k_multidot<<<nb, RED_THREADS, 2 * RED_THREADS * sizeof(double), st>>>(Vr, Vi, ldv, k, wr, wi, n, d_partial);
+  CMPS_CUDA(cudaGetLastError());
+  k_reduce_rows<<<2 * k, RED_THREADS, 0, st>>>(d_partial, nb, 2 * k, d_small);
+  CMPS_CUDA(cudaGetLastError());
+  if (h_host) {
+    CMPS_CUDA(cudaMemcpyAsync(h_host, d_small, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, st));
+    CMPS_CUDA(cudaStreamSynchronize(st));
+  }
+  return CMPS_OK;
+}
+
+int VecOps::multiaxpy(const double* Vr, const double* Vi, int64_t ldv, int k, const double* h_host, double* wr,
+                      double* wi, double sign, cudaStream_t st) {
+  if (k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  CMPS_CUDA(cudaMemcpyAsync(d_small + 256, h_host, sizeof(double) * 2 * k, cudaMemcpyHostToDevice, st));
+  k_multiaxpy<<<grid_for(n, 256), 256, 0, st>>>(Vr, Vi, ldv, k, d_small + 256, wr, wi, n, sign);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::norm2(const double* xr, const double* xi, double* out, cudaStream_t st) {
+  double h[2];
+  CMPS_TRY(multidot(xr, xi, 0, 1, xr, xi, h, st));
+  *out = h[0];
+  return CMPS_OK;
+}
+
+int VecOps::scale_copy(const double* xr, const double* xi, double s, double* yr, double* yi, cudaStream_t st) {
+  k_scale_copy<<<grid_for(n, 256), 256, 0, st>>>(xr, xi, s, yr, yi, n);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::random(double* re, double* im, uint64_t seed, cudaStream_t st) {
+  k_random<<<grid_for(n, 256), 256, 0, st>>>(re, im, n, seed);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::combine(const double* Vr, const double* Vi, int64_t ldv, int k, const double* c_host, double* yr,
+                    double* yi, cudaStream_t st) {
+  if (k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  CMPS_CUDA(cudaMemcpyAsync(d_small + 256, c_host, sizeof(double) * k, cudaMemcpyHostToDevice, st));
+  k_combine<<<grid_for(n, 256), 256, 0, st>>>(Vr, Vi, ldv, k, d_small + 256, yr, yi, n);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::absmax(const double* re, const double* im, double* val, int64_t* idx, cudaStream_t st) {
+  k_absmax<<<nb, RED_THREADS, 0, st>>>(re, im, n, d_partial, d_pidx);
+  CMPS_CUDA(cudaGetLastError());
+  std::vector<double> pv(nb);
+  std::vector<int64_t> pi(nb);
+  CMPS_CUDA(cudaMemcpyAsync(pv.data(), d_partial, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaMemcpyAsync(pi.data(), d_pidx, sizeof(int64_t) * nb, cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  double best = -1.0;
+  int64_t bi = 0;
+  for (int b = 0; b < nb; ++b)
+    if (pv[b] > best || (pv[b] == best && pi[b] < bi)) {
+      best = pv[b];
+      bi = pi[b];
+    }
+  *val = best;
+  *idx = bi;
+  return CMPS_OK;
+}
+
+int VecOps::phase_drop(double* re, double* im, double pr, double pi, double thr, cudaStream_t st) {
+  k_phase_drop<<<grid_for(n, 256), 256, 0, st>>>(re, im, n, pr, pi, thr);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+}  // namespace cmps

@@ -1,0 +1,36 @@
+// FP64 vector kernels of the device Krylov solver (see kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cmps {
+
+// Planar FP64 complex vectors of a fixed length n; reductions are two-pass
+// (per-CTA partials, then a fixed-order reduction) so results are
+// deterministic run to run.
+struct VecOps {
+  int64_t n = 0;
+  int nb = 0;
+  double* d_partial = nullptr;
+  double* d_small = nullptr;
+  int64_t* d_pidx = nullptr;
+  int init(int64_t n);
+  void release();
+  // h[j] = <V_j, w> (conjugate-linear in V), k vectors with stride ldv; h_host gets 2k doubles.
+  int multidot(const double* Vr, const double* Vi, int64_t ldv, int k, const double* wr, const double* wi,
+               double* h_host, cudaStream_t st);
+  // w += sign * sum_j h_j V_j
+  int multiaxpy(const double* Vr, const double* Vi, int64_t ldv, int k, const double* h_host, double* wr,
+                double* wi, double sign, cudaStream_t st);
+  int norm2(const double* xr, const double* xi, double* out, cudaStream_t st);
+  int scale_copy(const double* xr, const double* xi, double s, double* yr, double* yi, cudaStream_t st);
+  int random(double* re, double* im, uint64_t seed, cudaStream_t st);
+  // y = sum_j c_j V_j, c real
+  int combine(const double* Vr, const double* Vi, int64_t ldv, int k, const double* c_host, double* yr,
+              double* yi, cudaStream_t st);
+  int absmax(const double* re, const double* im, double* val_sq, int64_t* idx, cudaStream_t st);
+  int phase_drop(double* re, double* im, double pr, double pi, double thr, cudaStream_t st);
+};
+
+}  // namespace cmps

@@ -1,0 +1,759 @@
+// Charge-block SVD truncation of the two-vertex wavefunction and the
+// environment updates that consume its factors.
+//
+// SVD (SparseMatrix::SVD, sparse_interface.cpp:1248-1406): for every
+// middle-charge block Theta_m (the column-charge blocks of
+// GetAllBlockColumns, MPX_matrix.cpp:365-385): skip it if its weight is
+// <= eps^2; restrict to its non-empty rows and columns (TranslationBlock,
+// sparse_interface.hpp:367-376); FP64 SVD on the device (cuSOLVER gesvdj);
+// drop |u| <= eps/rows and |v| <= eps/cols.  Then the global descending
+// sort (ties: first seen), chi cap, truncation-weight cut and 1e-3
+// degeneracy extension decide the kept count of every block.
+//
+// Environment updates (MakeLeftBlock / MakeRightBlock,
+// DMRG_routines.cpp:594-611) reuse the handle's LeftPart / RightPart:
+//   L'^{b1} = U^H (LeftPart^{b1} U),   R'^{b1} = (V^dag RightPart^{b1}) V^dag^H
+// as grouped GEMMs; the blocks stay on the device.
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <set>
+
+#include "heff.h"
+
+namespace cmps {
+
+struct SvdResult {
+  Rules rules;
+  int d = 0;
+  std::vector<QKey> sigq;
+  Bond a0, a2;
+  ThetaSpace th;
+  std::vector<int64_t> kept;            // per m
+  std::vector<int64_t> uoff, voff;      // per m, offsets into U / Vd
+  Planar U, Vd;                         // U_m: nrows[m] x kept[m]; Vd_m: kept[m] x ncols[m] (row-major)
+  std::vector<double> values;           // kept, global descending order
+  std::vector<std::pair<int, int64_t>> order;  // global index -> (m, j)
+  std::vector<std::vector<int64_t>> gidx;      // [m][j] -> global index
+  double discarded = 0.0;
+};
+
+static const double kEps = 2.220446049250313e-16;
+
+void release_solver(cmps_context* ctx) {
+  if (ctx && ctx->solver) {
+    cusolverDnDestroy((cusolverDnHandle_t)ctx->solver);
+    ctx->solver = nullptr;
+  }
+}
+
+static int get_solver(cmps_context* ctx, cusolverDnHandle_t* out) {
+  if (!ctx->solver) {
+    cusolverDnHandle_t h;
+    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return fail(CMPS_ERR_CUDA, "cusolverDnCreate failed");
+    ctx->solver = h;
+  }
+  cusolverDnSetStream((cusolverDnHandle_t)ctx->solver, ctx->stream);
+  *out = (cusolverDnHandle_t)ctx->solver;
+  return CMPS_OK;
+}
+
+namespace {
+
+__global__ void k_nzflags(const double* __restrict__ re, const double* __restrict__ im, int64_t rows,
+                          int64_t cols, int* __restrict__ rflag, int* __restrict__ cflag,
+                          double* __restrict__ weight) {
+  double w = 0.0;
+  int64_t n = rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    double a = re[e], b = im[e];
+    if (a != 0.0 || b != 0.0) {
+      rflag[e / cols] = 1;
+      cflag[e % cols] = 1;
+      w += a * a + b * b;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+  if ((threadIdx.x & 31) == 0 && w != 0.0) atomicAdd(weight, w);
+}
+
+// compacted block, column-major interleaved: A[i + nr*j] = Theta[rows[i], cols[j]]
+__global__ void k_gather_cm(const double* __restrict__ re, const double* __restrict__ im, int64_t ld,
+                            const int64_t* __restrict__ rows, int64_t nr, const int64_t* __restrict__ cols,
+                            int64_t nc, double2* __restrict__ A) {
+  int64_t n = nr * nc;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = e % nr, j = e / nr;
+    int64_t o = rows[i] * ld + cols[j];
+    A[e] = make_double2(re[o], im[o]);
+  }
+}
+
+// U_m[rows[i], j] = Ucm[i + nr*j] (j < k), |u| <= thr dropped; U_m row-major ld = k.
+__global__ void k_scatter_u(const double2* __restrict__ Ucm, int64_t nr, int64_t k, const int64_t* __restrict__ rows,
+                            double thr, double* __restrict__ ur, double* __restrict__ ui) {
+  int64_t n = nr * k;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = e % nr, j = e / nr;
+    double2 v = Ucm[e];
+    bool keep = sqrt(v.x * v.x + v.y * v.y) > thr;
+    int64_t o = rows[i] * k + j;
+    ur[o] = keep ? v.x : 0.0;
+    ui[o] = keep ? v.y : 0.0;
+  }
+}
+
+// Vd_m[j, cols[c]] = conj(Vcm[c + nc*j]); Vd_m row-major ld = ncols.
+__global__ void k_scatter_vd(const double2* __restrict__ Vcm, int64_t nc, int64_t k, const int64_t* __restrict__ cols,
+                             int64_t ld, double thr, double* __restrict__ vr, double* __restrict__ vi) {
+  int64_t n = nc * k;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c = e % nc, j = e / nc;
+    double2 v = Vcm[e];
+    bool keep = sqrt(v.x * v.x + v.y * v.y) > thr;
+    int64_t o = j * ld + cols[c];
+    vr[o] = keep ? v.x : 0.0;
+    vi[o] = keep ? -v.y : 0.0;
+  }
+}
+
+int grid_of(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)g;
+}
+
+}  // namespace
+
+// Kept count of SparseMatrix::SVD (sparse_interface.cpp:1346-1376).
+static int64_t truncation_length(const std::vector<double>& sv, int64_t D, double max_trunc) {
+  const int64_t N = (int64_t)sv.size();
+  int64_t length = (D > 0 && D < N) ? D : N;
+  double trunc_error = 0.0;
+  int64_t tl = N;
+  while (trunc_error < max_trunc && tl > 0) {
+    trunc_error += sv[tl - 1] * sv[tl - 1];
+    --tl;
+  }
+  ++tl;
+  if (tl < length) length = tl;
+  while (length < N && (sv[length - 1] - sv[length]) / sv[length - 1] < 1.0e-3) ++length;
+  return length;
+}
+
+static int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
+  if (!H.have_theta) return fail(CMPS_ERR_STATE, "no wavefunction: call cmps_heff_eigs or cmps_heff_set_theta first");
+  cudaStream_t st = H.ctx->stream;
+  cusolverDnHandle_t sol;
+  CMPS_TRY(get_solver(H.ctx, &sol));
+  const ThetaSpace& th = H.th;
+  const int nm = (int)th.mq.size();
+  out.rules = H.rules;
+  out.d = H.d;
+  out.sigq = H.sigq;
+  out.a0 = H.L.a;
+  out.a2 = H.R.a;
+  out.th = th;
+  struct Blk {
+    std::vector<int64_t> rows, cols;
+    std::vector<double> s;
+    double2* dU = nullptr;
+    double2* dV = nullptr;
+    int64_t* drows = nullptr;
+    int64_t* dcols = nullptr;
+  };
+  std::vector<Blk> blk(nm);
+  int64_t maxr = 1, maxc = 1;
+  for (int m = 0; m < nm; ++m) {
+    maxr = std::max(maxr, th.nrows[m]);
+    maxc = std::max(maxc, th.ncols[m]);
+  }
+  int* dflags = nullptr;
+  double* dweight = nullptr;
+  double2* dA = nullptr;
+  double* dS = nullptr;
+  int* dinfo = nullptr;
+  auto cleanup = [&]() {
+    if (dflags) cudaFree(dflags);
+    if (dweight) cudaFree(dweight);
+    if (dA) cudaFree(dA);
+    if (dS) cudaFree(dS);
+    if (dinfo) cudaFree(dinfo);
+    for (auto& b : blk) {
+      if (b.dU) cudaFree(b.dU);
+      if (b.dV) cudaFree(b.dV);
+      if (b.drows) cudaFree(b.drows);
+      if (b.dcols) cudaFree(b.dcols);
+    }
+  };
+  int status = CMPS_OK;
+  do {
+    if (cudaMalloc(&dflags, sizeof(int) * (maxr + maxc)) != cudaSuccess ||
+        cudaMalloc(&dweight, sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dA, sizeof(double2) * maxr * maxc) != cudaSuccess ||
+        cudaMalloc(&dS, sizeof(double) * std::min(maxr, maxc)) != cudaSuccess ||
+        cudaMalloc(&dinfo, sizeof(int)) != cudaSuccess) {
+      status = fail(CMPS_ERR_NOMEM, "SVD workspace allocation failed");
+      break;
+    }
+    gesvdjInfo_t params;
+    cusolverDnCreateGesvdjInfo(&params);
+    cusolverDnXgesvdjSetTolerance(params, 0.0);   // 0: machine precision
+    cusolverDnXgesvdjSetMaxSweeps(params, 100);
+    cusolverDnXgesvdjSetSortEig(params, 1);
+    for (int m = 0; m < nm && status == CMPS_OK; ++m) {
+      const int64_t R = th.nrows[m], C = th.ncols[m];
+      if (R == 0 || C == 0) continue;
+      const double* bre = H.theta.re() + th.base[m];
+      const double* bim = H.theta.im() + th.base[m];
+      cudaMemsetAsync(dflags, 0, sizeof(int) * (R + C), st);
+      cudaMemsetAsync(dweight, 0, sizeof(double), st);
+      k_nzflags<<<grid_of(R * C), 256, 0, st>>>(bre, bim, R, C, dflags, dflags + R, dweight);
+      std::vector<int> fl(R + C);
+      double w = 0.0;
+      cudaMemcpyAsync(fl.data(), dflags, sizeof(int) * (R + C), cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(&w, dweight, sizeof(double), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) { status = fail(CMPS_ERR_CUDA, "SVD flag pass failed"); break; }
+      if (w <= kEps * kEps) continue;  // empty block (sparse_interface.cpp:1279)
+      Blk& b = blk[m];
+      for (int64_t i = 0; i < R; ++i) if (fl[i]) b.rows.push_back(i);
+      for (int64_t j = 0; j < C; ++j) if (fl[R + j]) b.cols.push_back(j);
+      const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
+      const int64_t mn = std::min(nr, nc);
+      if (cudaMalloc(&b.drows, sizeof(int64_t) * nr) != cudaSuccess ||
+          cudaMalloc(&b.dcols, sizeof(int64_t) * nc) != cudaSuccess ||
+          cudaMalloc(&b.dU, sizeof(double2) * nr * mn) != cudaSuccess ||
+          cudaMalloc(&b.dV, sizeof(double2) * nc * mn) != cudaSuccess) {
+        status = fail(CMPS_ERR_NOMEM, "SVD block allocation failed");
+        break;
+      }
+      cudaMemcpyAsync(b.drows, b.rows.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(b.dcols, b.cols.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, st);
+      k_gather_cm<<<grid_of(nr * nc), 256, 0, st>>>(bre, bim, C, b.drows, nr, b.dcols, nc, dA);
+      int lwork = 0;
+      if (cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc, (cuDoubleComplex*)dA,
+                                       (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr, (cuDoubleComplex*)b.dV,
+                                       (int)nc, &lwork, params) != CUSOLVER_STATUS_SUCCESS) {
+        status = fail(CMPS_ERR_SOLVER, "gesvdj buffer query failed");
+        break;
+      }
+      cuDoubleComplex* work = nullptr;
+      if (cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess) {
+        status = fail(CMPS_ERR_NOMEM, "SVD work allocation failed");
+        break;
+      }
+      cusolverStatus_t cs = cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
+                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr,
+                                              (cuDoubleComplex*)b.dV, (int)nc, work, lwork, dinfo, params);
+      int info = 0;
+      b.s.resize(mn);
+      cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+      cudaError_t ce = cudaStreamSynchronize(st);
+      cudaFree(work);
+      if (cs != CUSOLVER_STATUS_SUCCESS || ce != cudaSuccess) { status = fail(CMPS_ERR_SOLVER, "gesvdj failed"); break; }
+      if (info < 0) { status = fail(CMPS_ERR_SOLVER, "gesvdj: invalid argument"); break; }
+      // info > 0: not converged to tolerance within max sweeps; values still usable
+    }
+    cusolverDnDestroyGesvdjInfo(params);
+    if (status != CMPS_OK) break;
+    // ---- global selection ----
+    struct SV { double v; int m; int64_t j; };
+    std::vector<SV> all;
+    for (int m = 0; m < nm; ++m)
+      for (int64_t j = 0; j < (int64_t)blk[m].s.size(); ++j) all.push_back(SV{blk[m].s[j], m, j});
+    if (all.empty()) { status = fail(CMPS_ERR_SOLVER, "no singular values (empty wavefunction)"); break; }
+    std::stable_sort(all.begin(), all.end(), [](const SV& a, const SV& b) { return a.v > b.v; });
+    std::vector<double> sv(all.size());
+    for (size_t i = 0; i < all.size(); ++i) sv[i] = all[i].v;
+    const int64_t length = truncation_length(sv, chi, max_trunc);
+    out.values.assign(sv.begin(), sv.begin() + length);
+    out.discarded = 0.0;
+    for (size_t i = length; i < sv.size(); ++i) out.discarded += sv[i] * sv[i];
+    out.kept.assign(nm, 0);
+    out.order.clear();
+    for (int64_t g = 0; g < length; ++g) {
+      out.order.push_back({all[g].m, all[g].j});
+      out.kept[all[g].m] = std::max(out.kept[all[g].m], all[g].j + 1);
+    }
+    out.gidx.assign(nm, {});
+    for (int m = 0; m < nm; ++m) out.gidx[m].assign(out.kept[m], -1);
+    for (int64_t g = 0; g < length; ++g) out.gidx[all[g].m][all[g].j] = g;
+    // ---- factors ----
+    out.uoff.assign(nm, 0);
+    out.voff.assign(nm, 0);
+    int64_t ut = 0, vt = 0;
+    for (int m = 0; m < nm; ++m) {
+      out.uoff[m] = ut;
+      out.voff[m] = vt;
+      ut += th.nrows[m] * out.kept[m];
+      vt += out.kept[m] * th.ncols[m];
+    }
+    if ((status = out.U.alloc(ut)) != CMPS_OK) break;
+    if ((status = out.Vd.alloc(vt)) != CMPS_OK) break;
+    if (ut) cudaMemsetAsync(out.U.d, 0, sizeof(double) * 2 * ut, st);
+    if (vt) cudaMemsetAsync(out.Vd.d, 0, sizeof(double) * 2 * vt, st);
+    for (int m = 0; m < nm; ++m) {
+      const int64_t k = out.kept[m];
+      if (k == 0) continue;
+      Blk& b = blk[m];
+      const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
+      const int64_t mn = std::min(nr, nc);
+      (void)mn;
+      k_scatter_u<<<grid_of(nr * k), 256, 0, st>>>(b.dU, nr, k, b.drows, kEps / (double)nr, out.U.re() + out.uoff[m],
+                                                   out.U.im() + out.uoff[m]);
+      k_scatter_vd<<<grid_of(nc * k), 256, 0, st>>>(b.dV, nc, k, b.dcols, th.ncols[m], kEps / (double)nc,
+                                                    out.Vd.re() + out.voff[m], out.Vd.im() + out.voff[m]);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) { status = fail(CMPS_ERR_CUDA, "SVD scatter failed"); break; }
+  } while (false);
+  cleanup();
+  return status;
+}
+
+// New bond built from the kept singular vectors, in the reference's element
+// order (descending singular value).
+static void new_bond(const SvdResult& s, Bond& b, std::vector<int>& sec_of_m) {
+  std::vector<QKey> q(s.order.size());
+  for (size_t g = 0; g < s.order.size(); ++g) q[g] = s.th.mq[s.order[g].first];
+  b.build(q);
+  sec_of_m.assign(s.th.mq.size(), -1);
+  for (size_t m = 0; m < s.th.mq.size(); ++m) sec_of_m[m] = s.kept[m] ? b.find(s.th.mq[m]) : -1;
+}
+
+static int alloc_env(const Rules& r, const Bond& a, int D, const std::vector<QKey>& bq, bool right, Env& env) {
+  env.right = right;
+  env.a = a;
+  env.D = D;
+  env.bq = bq;
+  const int ns = a.nsec();
+  env.off.assign((size_t)D * ns, -1);
+  env.partner.assign((size_t)D * ns, -1);
+  int64_t total = 0;
+  for (int b = 0; b < D; ++b)
+    for (int s = 0; s < ns; ++s) {
+      int sp = a.find(r.add(a.sq[s], bq[b]));
+      if (sp < 0) continue;
+      env.partner[(size_t)b * ns + s] = sp;
+      env.off[(size_t)b * ns + s] = total;
+      total += a.sdim[s] * a.sdim[sp];
+    }
+  CMPS_TRY(env.data.alloc(total));
+  if (total) CMPS_CUDA(cudaMemset(env.data.d, 0, sizeof(double) * 2 * total));
+  return CMPS_OK;
+}
+
+static int left_update(Heff& H, const SvdResult& s, Env& out) {
+  const Rules& r = H.rules;
+  const ThetaSpace& th = s.th;
+  const int nm = (int)th.mq.size();
+  const int d = H.d;
+  const Bond& A0 = H.L.a;
+  Bond nb;
+  std::vector<int> sec;
+  new_bond(s, nb, sec);
+  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, false, out));
+  // X^{b1}_m = LeftPart^{b1} U_m  (rows L(m'), cols kept[m])
+  std::set<int> b1s;
+  for (auto& kv : H.lp_off) b1s.insert(kv.first[0]);
+  GemmPlan px, pl;
+  std::vector<int64_t> xbase((size_t)H.D * nm, -1);
+  int64_t xt = 0;
+  for (int b1 : b1s)
+    for (int m = 0; m < nm; ++m) {
+      const int64_t k = s.kept[m];
+      if (!k) continue;
+      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      if (mp < 0 || !s.kept[mp]) continue;
+      std::vector<GemmTask> tasks;
+      std::vector<GemmTerm> terms;
+      for (int s1p = 0; s1p < d; ++s1p) {
+        if (th.rowoff[mp][s1p] < 0) continue;
+        int sp = A0.find(r.sub(th.mq[mp], H.sigq[s1p]));
+        GemmTask t{};
+        t.c_off = th.rowoff[mp][s1p] * k;
+        t.m = (int32_t)A0.sdim[sp];
+        t.n = (int32_t)k;
+        t.ldc = (int32_t)k;
+        t.t0 = (int32_t)terms.size();
+        for (int s1 = 0; s1 < d; ++s1) {
+          if (th.rowoff[m][s1] < 0) continue;
+          int sa = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+          auto it = H.lp_off.find({b1, s1p, s1, sa});
+          if (it == H.lp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = it->second;
+          tm.lda = (int32_t)A0.sdim[sa];
+          tm.k = (int32_t)A0.sdim[sa];
+          tm.b_off = s.uoff[m] + th.rowoff[m][s1] * k;
+          tm.ldb = (int32_t)k;
+          terms.push_back(tm);
+        }
+        t.t1 = (int32_t)terms.size();
+        tasks.push_back(t);
+      }
+      if (terms.empty()) continue;
+      int64_t xb = xt;
+      xbase[(size_t)b1 * nm + m] = xb;
+      xt += th.nrows[mp] * k;
+      int32_t tb = (int32_t)px.terms.size();
+      for (auto& tm : terms) px.terms.push_back(tm);
+      for (auto& t : tasks) {
+        t.c_off += xb;
+        t.t0 += tb;
+        t.t1 += tb;
+        px.tasks.push_back(t);
+      }
+      // L'^{b1}: (kept[m'] x kept[m]) = U_{m'}^H X
+      GemmTask lt{};
+      const int ns = nb.nsec();
+      lt.c_off = out.off[(size_t)b1 * ns + sec[m]];
+      lt.m = (int32_t)s.kept[mp];
+      lt.n = (int32_t)k;
+      lt.ldc = (int32_t)k;
+      lt.t0 = (int32_t)pl.terms.size();
+      GemmTerm tm{};
+      tm.a_off = s.uoff[mp];
+      tm.lda = (int32_t)s.kept[mp];
+      tm.k = (int32_t)th.nrows[mp];
+      tm.b_off = xb;
+      tm.ldb = (int32_t)k;
+      pl.terms.push_back(tm);
+      lt.t1 = (int32_t)pl.terms.size();
+      pl.tasks.push_back(lt);
+    }
+  Planar X;
+  CMPS_TRY(X.alloc(xt));
+  int status = CMPS_OK;
+  do {
+    if ((status = px.validate(false, false, H.LP.len, s.U.len, xt, "left update X")) != CMPS_OK) break;
+    if ((status = pl.validate(true, false, s.U.len, xt, out.data.len, "left update")) != CMPS_OK) break;
+    if ((status = px.upload(64, 64)) != CMPS_OK) break;
+    if ((status = pl.upload(64, 64)) != CMPS_OK) break;
+    Planar Ucopy = s.U;  // non-owning view
+    if ((status = launch_zgemm_fp64(px, false, false, H.LP, Ucopy, X, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = launch_zgemm_fp64(pl, true, false, Ucopy, X, out.data, H.ctx->stream)) != CMPS_OK) break;
+    if (cudaStreamSynchronize(H.ctx->stream) != cudaSuccess) status = fail(CMPS_ERR_CUDA, "left block update failed");
+  } while (false);
+  px.release();
+  pl.release();
+  X.release();
+  return status;
+}
+
+static int right_update(Heff& H, const SvdResult& s, Env& out) {
+  const Rules& r = H.rules;
+  const ThetaSpace& th = s.th;
+  const int nm = (int)th.mq.size();
+  const int d = H.d;
+  const Bond& A2 = H.R.a;
+  Bond nb;
+  std::vector<int> sec;
+  new_bond(s, nb, sec);
+  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, true, out));
+  std::set<int> b1s;
+  for (auto& kv : H.rp_off) b1s.insert(kv.first[0]);
+  GemmPlan py, pr;
+  int64_t yt = 0;
+  for (int b1 : b1s)
+    for (int m = 0; m < nm; ++m) {
+      const int64_t k = s.kept[m];
+      if (!k) continue;
+      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      if (mp < 0 || !s.kept[mp]) continue;
+      // Y^{b1}_m = Vd_m RightPart^{b1}: (k x ncols[m'])
+      std::vector<GemmTask> tasks;
+      std::vector<GemmTerm> terms;
+      for (int s2p = 0; s2p < d; ++s2p) {
+        if (th.coloff[mp][s2p] < 0) continue;
+        int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
+        GemmTask t{};
+        t.c_off = th.coloff[mp][s2p];
+        t.m = (int32_t)k;
+        t.n = (int32_t)A2.sdim[tp];
+        t.ldc = (int32_t)th.ncols[mp];
+        t.t0 = (int32_t)terms.size();
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int ta = A2.find(r.add(th.mq[m], H.sigq[s2]));
+          auto it = H.rp_off.find({b1, s2, s2p, ta});
+          if (it == H.rp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = s.voff[m] + th.coloff[m][s2];
+          tm.lda = (int32_t)th.ncols[m];
+          tm.k = (int32_t)A2.sdim[ta];
+          tm.b_off = it->second;
+          tm.ldb = (int32_t)A2.sdim[tp];
+          terms.push_back(tm);
+        }
+        t.t1 = (int32_t)terms.size();
+        tasks.push_back(t);
+      }
+      if (terms.empty()) continue;
+      int64_t yb = yt;
+      yt += k * th.ncols[mp];
+      int32_t tb = (int32_t)py.terms.size();
+      for (auto& tm : terms) py.terms.push_back(tm);
+      for (auto& t : tasks) {
+        t.c_off += yb;
+        t.t0 += tb;
+        t.t1 += tb;
+        py.tasks.push_back(t);
+      }
+      // R'^{b1} stored [a, a']: (kept[m] x kept[m']) = Y Vd_{m'}^H
+      GemmTask rt{};
+      const int ns = nb.nsec();
+      rt.c_off = out.off[(size_t)b1 * ns + sec[m]];
+      rt.m = (int32_t)k;
+      rt.n = (int32_t)s.kept[mp];
+      rt.ldc = (int32_t)s.kept[mp];
+      rt.t0 = (int32_t)pr.terms.size();
+      GemmTerm tm{};
+      tm.a_off = yb;
+      tm.lda = (int32_t)th.ncols[mp];
+      tm.k = (int32_t)th.ncols[mp];
+      tm.b_off = s.voff[mp];
+      tm.ldb = (int32_t)th.ncols[mp];
+      pr.terms.push_back(tm);
+      rt.t1 = (int32_t)pr.terms.size();
+      pr.tasks.push_back(rt);
+    }
+  Planar Y;
+  CMPS_TRY(Y.alloc(yt));
+  int status = CMPS_OK;
+  do {
+    if ((status = py.validate(false, false, s.Vd.len, H.RP.len, yt, "right update Y")) != CMPS_OK) break;
+    if ((status = pr.validate(false, true, yt, s.Vd.len, out.data.len, "right update")) != CMPS_OK) break;
+    if ((status = py.upload(64, 64)) != CMPS_OK) break;
+    if ((status = pr.upload(64, 64)) != CMPS_OK) break;
+    Planar Vview = s.Vd;
+    if ((status = launch_zgemm_fp64(py, false, false, Vview, H.RP, Y, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = launch_zgemm_fp64(pr, false, true, Y, Vview, out.data, H.ctx->stream)) != CMPS_OK) break;
+    if (cudaStreamSynchronize(H.ctx->stream) != cudaSuccess) status = fail(CMPS_ERR_CUDA, "right block update failed");
+  } while (false);
+  py.release();
+  pr.release();
+  Y.release();
+  return status;
+}
+
+}  // namespace cmps
+
+struct cmps_svd {
+  cmps::SvdResult r;
+  ~cmps_svd() {
+    r.U.release();
+    r.Vd.release();
+  }
+};
+
+
+using namespace cmps;
+
+extern "C" {
+
+int cmps_heff_theta_svd(cmps_heff* h, int64_t chi, double max_trunc, cmps_svd** out) {
+  if (!h || !h->impl || !out) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (chi < 0) return fail(CMPS_ERR_ARG, "negative bond dimension");
+  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  auto* s = new (std::nothrow) cmps_svd();
+  if (!s) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  int st = theta_svd(*h->impl, chi, max_trunc, s->r);
+  if (st != CMPS_OK) {
+    delete s;
+    return st;
+  }
+  *out = s;
+  return CMPS_OK;
+}
+
+int cmps_svd_destroy(cmps_svd* s) {
+  delete s;
+  return CMPS_OK;
+}
+
+int cmps_svd_info(const cmps_svd* s, int64_t* kept, double* discarded, int64_t* nnz_u, int64_t* nnz_vd) {
+  if (!s) return fail(CMPS_ERR_ARG, "null handle");
+  const SvdResult& r = s->r;
+  if (kept) *kept = (int64_t)r.values.size();
+  if (discarded) *discarded = r.discarded;
+  // upper bounds: every stored element of the kept factor columns / rows
+  int64_t nu = 0, nv = 0;
+  for (size_t m = 0; m < r.kept.size(); ++m) {
+    nu += r.th.nrows[m] * r.kept[m];
+    nv += r.kept[m] * r.th.ncols[m];
+  }
+  if (nnz_u) *nnz_u = nu;
+  if (nnz_vd) *nnz_vd = nv;
+  return CMPS_OK;
+}
+
+int cmps_svd_copy(const cmps_svd* s, double* values, int16_t* new_charges, int64_t* u_colptr, int64_t* u_rowind,
+                  double* u_values, int64_t* vd_colptr, int64_t* vd_rowind, double* vd_values) {
+  if (!s) return fail(CMPS_ERR_ARG, "null handle");
+  const SvdResult& r = s->r;
+  const int64_t kept = (int64_t)r.values.size();
+  const int nq = r.rules.nq;
+  const ThetaSpace& th = r.th;
+  const int d = r.d;
+  if (values) std::memcpy(values, r.values.data(), sizeof(double) * kept);
+  if (new_charges)
+    for (int64_t g = 0; g < kept; ++g)
+      for (int c = 0; c < nq; ++c) new_charges[g * nq + c] = th.mq[r.order[g].first][c];
+  std::vector<double> U(2 * r.U.len), V(2 * r.Vd.len);
+  if (r.U.len) CMPS_CUDA(cudaMemcpy(U.data(), r.U.d, sizeof(double) * 2 * r.U.len, cudaMemcpyDeviceToHost));
+  if (r.Vd.len) CMPS_CUDA(cudaMemcpy(V.data(), r.Vd.d, sizeof(double) * 2 * r.Vd.len, cudaMemcpyDeviceToHost));
+  // U: (d * chiL) x kept, row = s1 + d * a0, column g
+  if (u_colptr) {
+    int64_t p = 0;
+    u_colptr[0] = 0;
+    std::vector<std::pair<int64_t, std::pair<double, double>>> col;
+    for (int64_t g = 0; g < kept; ++g) {
+      const int m = r.order[g].first;
+      const int64_t j = r.order[g].second, k = r.kept[m];
+      col.clear();
+      for (int s1 = 0; s1 < d; ++s1) {
+        if (th.rowoff[m][s1] < 0) continue;
+        int sa = r.a0.find(r.rules.sub(th.mq[m], r.sigq[s1]));
+        for (int64_t q = 0; q < r.a0.sdim[sa]; ++q) {
+          int64_t o = r.uoff[m] + (th.rowoff[m][s1] + q) * k + j;
+          double re = U[o], im = U[r.U.len + o];
+          if (re == 0.0 && im == 0.0) continue;
+          col.push_back({s1 + (int64_t)d * r.a0.selem[sa][q], {re, im}});
+        }
+      }
+      std::sort(col.begin(), col.end(), [](auto& a, auto& b) { return a.first < b.first; });
+      for (auto& e : col) {
+        if (u_rowind) u_rowind[p] = e.first;
+        if (u_values) { u_values[2 * p] = e.second.first; u_values[2 * p + 1] = e.second.second; }
+        ++p;
+      }
+      u_colptr[g + 1] = p;
+    }
+  }
+  // V^dagger: kept x (d * chiR), column c = s2 + d * a2
+  if (vd_colptr) {
+    const int64_t chiR = r.a2.size();
+    std::vector<std::vector<std::pair<int64_t, std::pair<double, double>>>> cols(d * chiR);
+    for (int m = 0; m < (int)th.mq.size(); ++m) {
+      const int64_t k = r.kept[m];
+      for (int64_t j = 0; j < k; ++j) {
+        const int64_t g = r.gidx[m][j];
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int t = r.a2.find(r.rules.add(th.mq[m], r.sigq[s2]));
+          for (int64_t q = 0; q < r.a2.sdim[t]; ++q) {
+            int64_t o = r.voff[m] + j * th.ncols[m] + th.coloff[m][s2] + q;
+            double re = V[o], im = V[r.Vd.len + o];
+            if (re == 0.0 && im == 0.0) continue;
+            cols[s2 + (int64_t)d * r.a2.selem[t][q]].push_back({g, {re, im}});
+          }
+        }
+      }
+    }
+    int64_t p = 0;
+    vd_colptr[0] = 0;
+    for (int64_t c = 0; c < d * chiR; ++c) {
+      auto& cl = cols[c];
+      std::sort(cl.begin(), cl.end(), [](auto& a, auto& b) { return a.first < b.first; });
+      for (auto& e : cl) {
+        if (vd_rowind) vd_rowind[p] = e.first;
+        if (vd_values) { vd_values[2 * p] = e.second.first; vd_values[2 * p + 1] = e.second.second; }
+        ++p;
+      }
+      vd_colptr[c + 1] = p;
+    }
+  }
+  return CMPS_OK;
+}
+
+int cmps_heff_left_block(cmps_heff* h, const cmps_svd* s, cmps_block** out) {
+  if (!h || !h->impl || !s || !out) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  auto* b = new (std::nothrow) cmps_block();
+  if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  b->rules = h->impl->rules;
+  int st = left_update(*h->impl, s->r, b->env);
+  if (st != CMPS_OK) { delete b; return st; }
+  *out = b;
+  return CMPS_OK;
+}
+
+int cmps_heff_right_block(cmps_heff* h, const cmps_svd* s, cmps_block** out) {
+  if (!h || !h->impl || !s || !out) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  auto* b = new (std::nothrow) cmps_block();
+  if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
+  b->rules = h->impl->rules;
+  int st = right_update(*h->impl, s->r, b->env);
+  if (st != CMPS_OK) { delete b; return st; }
+  *out = b;
+  return CMPS_OK;
+}
+
+int cmps_block_destroy(cmps_block* b) {
+  delete b;
+  return CMPS_OK;
+}
+
+int cmps_block_info(const cmps_block* b, int64_t* chi, int64_t* mpo_dim, int64_t* nnz) {
+  if (!b) return fail(CMPS_ERR_ARG, "null handle");
+  if (chi) *chi = b->env.a.size();
+  if (mpo_dim) *mpo_dim = b->env.D;
+  if (nnz) *nnz = b->env.data.len;  // upper bound
+  return CMPS_OK;
+}
+
+int cmps_block_copy(const cmps_block* b, int16_t* a_charges, int64_t* colptr, int64_t* rowind, double* values) {
+  if (!b) return fail(CMPS_ERR_ARG, "null handle");
+  const Env& e = b->env;
+  const int nq = b->rules.nq;
+  const int64_t chi = e.a.size();
+  if (a_charges)
+    for (int64_t i = 0; i < chi; ++i)
+      for (int c = 0; c < nq; ++c) a_charges[i * nq + c] = e.a.sq[e.a.esec[i]][c];
+  if (!colptr) return CMPS_OK;
+  std::vector<double> h(2 * e.data.len);
+  if (e.data.len) CMPS_CUDA(cudaMemcpy(h.data(), e.data.d, sizeof(double) * 2 * e.data.len, cudaMemcpyDeviceToHost));
+  // matrix rows a', cols b + D * a
+  const int ns = e.a.nsec();
+  int64_t p = 0;
+  colptr[0] = 0;
+  std::vector<std::pair<int64_t, std::pair<double, double>>> col;
+  for (int64_t a = 0; a < chi; ++a) {
+    const int s = e.a.esec[a];
+    const int64_t pa = e.a.epos[a];
+    for (int bb = 0; bb < e.D; ++bb) {
+      col.clear();
+      int64_t o = e.off[(size_t)bb * ns + s];
+      if (o >= 0) {
+        int sp = e.partner[(size_t)bb * ns + s];
+        for (int64_t q = 0; q < e.a.sdim[sp]; ++q) {
+          int64_t ap = e.a.selem[sp][q];
+          int64_t idx = e.right ? o + pa * e.a.sdim[sp] + q : o + q * e.a.sdim[s] + pa;
+          double re = h[idx], im = h[e.data.len + idx];
+          if (re == 0.0 && im == 0.0) continue;
+          col.push_back({ap, {re, im}});
+        }
+        std::sort(col.begin(), col.end(), [](auto& x, auto& y) { return x.first < y.first; });
+      }
+      for (auto& v : col) {
+        if (rowind) rowind[p] = v.first;
+        if (values) { values[2 * p] = v.second.first; values[2 * p + 1] = v.second.second; }
+        ++p;
+      }
+      colptr[bb + (int64_t)e.D * a + 1] = p;
+    }
+  }
+  return CMPS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,274 @@
+// Grouped complex-double GEMM on the FP64 tensor path (DMMA, mma.sync
+// m8n8k4 f64) for sm_100a.
+//
+// One launch runs a whole list of independent output tiles.  Each output
+// region ("task") is C = sum over its terms of op(A_t) op(B_t), where every
+// term has its own A block, B block and K -- the K-concatenation that turns
+// the charge-sector structure of H_eff (sum over MPO indices and physical
+// states) into a single accumulation.  Complex operands are stored as two
+// planes (re, im) of one allocation; a complex MAC is four real DMMAs.
+// Operands are staged global -> shared with 8-byte cp.async (zero-filled
+// outside the block), double buffered.  op(A) is A or A^H (A stored K x M),
+// op(B) is B or B^H (B stored N x K), all row-major with leading dimensions.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "internal.h"
+
+namespace cmps {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, LDS = 68;  // LDS = BM + 4: conflict-free 8-byte fragment reads
+constexpr int NTHREADS = 128;
+constexpr int STAGES = 2;
+constexpr int PLANE = BK * LDS;                      // doubles per plane per operand per stage
+constexpr int STAGE_DOUBLES = 4 * PLANE;             // A re, A im, B re, B im
+constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DOUBLES * sizeof(double);
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Issue the cp.async copies of one (term, k-tile) into stage buffer `buf`.
+template <bool AH, bool BH>
+__device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k0, int m0, int n0, int M,
+                                           int N, const double* __restrict__ Ar,
+                                           const double* __restrict__ Ai, const double* __restrict__ Br,
+                                           const double* __restrict__ Bi) {
+  double* sAr = buf;
+  double* sAi = buf + PLANE;
+  double* sBr = buf + 2 * PLANE;
+  double* sBi = buf + 3 * PLANE;
+  const int tid = threadIdx.x;
+  const int K = t.k;
+#pragma unroll
+  for (int j = 0; j < (BM * BK) / NTHREADS; ++j) {
+    int idx = tid + j * NTHREADS;
+    int kk, mm;
+    if (!AH) { kk = idx % BK; mm = idx / BK; }   // A[m][k]: consecutive threads along k
+    else     { kk = idx / BM; mm = idx % BM; }   // A stored [k][m]: along m
+    int gm = m0 + mm, gk = k0 + kk;
+    bool ok = (gm < M) && (gk < K);
+    int64_t o = ok ? (AH ? t.a_off + (int64_t)gk * t.lda + gm : t.a_off + (int64_t)gm * t.lda + gk) : 0;
+    cp_async8(sAr + kk * LDS + mm, Ar + o, ok);
+    cp_async8(sAi + kk * LDS + mm, Ai + o, ok);
+  }
+#pragma unroll
+  for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
+    int idx = tid + j * NTHREADS;
+    int kk, nn;
+    if (!BH) { kk = idx / BN; nn = idx % BN; }   // B[k][n]: along n
+    else     { kk = idx % BK; nn = idx / BK; }   // B stored [n][k]: along k
+    int gn = n0 + nn, gk = k0 + kk;
+    bool ok = (gn < N) && (gk < K);
+    int64_t o = ok ? (BH ? t.b_off + (int64_t)gn * t.ldb + gk : t.b_off + (int64_t)gk * t.ldb + gn) : 0;
+    cp_async8(sBr + kk * LDS + nn, Br + o, ok);
+    cp_async8(sBi + kk * LDS + nn, Bi + o, ok);
+  }
+}
+
+template <bool AH, bool BH>
+__global__ void __launch_bounds__(NTHREADS, 2)
+zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restrict__ tasks,
+                   const GemmTerm* __restrict__ terms, const double* __restrict__ Ar,
+                   const double* __restrict__ Ai, const double* __restrict__ Br,
+                   const double* __restrict__ Bi, double* __restrict__ Cr, double* __restrict__ Ci) {
+  extern __shared__ double smem[];
+  const GemmTile tile = tiles[blockIdx.x];
+  const GemmTask task = tasks[tile.task];
+  const int m0 = tile.m0, n0 = tile.n0, M = task.m, N = task.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int gid = lane >> 2, tig = lane & 3;
+
+  double accr[4][4][2], acci[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      accr[i][j][0] = accr[i][j][1] = 0.0;
+      acci[i][j][0] = acci[i][j][1] = 0.0;
+    }
+
+  // iteration cursor over (term, k-tile)
+  int cur_t = task.t0, cur_k = 0;
+  int nxt_t = cur_t, nxt_k = 0;
+  bool have = cur_t < task.t1;
+  if (have) {
+    GemmTerm t = terms[cur_t];
+    load_stage<AH, BH>(smem, t, 0, m0, n0, M, N, Ar, Ai, Br, Bi);
+    cp_commit();
+    nxt_k = BK;
+    if (nxt_k >= t.k) { nxt_t = cur_t + 1; nxt_k = 0; }
+  }
+  int stage = 0;
+  while (have) {
+    bool more = nxt_t < task.t1;
+    if (more) {
+      GemmTerm t = terms[nxt_t];
+      load_stage<AH, BH>(smem + (stage ^ 1) * STAGE_DOUBLES, t, nxt_k, m0, n0, M, N, Ar, Ai, Br, Bi);
+      cp_commit();
+      cp_wait1();
+    } else {
+      cp_wait0();
+    }
+    __syncthreads();
+    const double* sAr = smem + stage * STAGE_DOUBLES;
+    const double* sAi = sAr + PLANE;
+    const double* sBr = sAr + 2 * PLANE;
+    const double* sBi = sAr + 3 * PLANE;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        int mm = wm * 32 + i * 8 + gid;
+        ar[i] = sAr[(kk + tig) * LDS + mm];
+        ai[i] = sAi[(kk + tig) * LDS + mm];
+        if (AH) ai[i] = -ai[i];
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int nn = wn * 32 + j * 8 + gid;
+        br[j] = sBr[(kk + tig) * LDS + nn];
+        bi[j] = sBi[(kk + tig) * LDS + nn];
+        if (BH) bi[j] = -bi[j];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(accr[i][j][0], accr[i][j][1], ar[i], br[j]);
+          dmma(accr[i][j][0], accr[i][j][1], nai[i], bi[j]);
+          dmma(acci[i][j][0], acci[i][j][1], ar[i], bi[j]);
+          dmma(acci[i][j][0], acci[i][j][1], ai[i], br[j]);
+        }
+    }
+    __syncthreads();
+    // advance
+    have = more;
+    if (more) {
+      cur_t = nxt_t;
+      cur_k = nxt_k;
+      GemmTerm t = terms[cur_t];
+      nxt_k = cur_k + BK;
+      nxt_t = cur_t;
+      if (nxt_k >= t.k) { nxt_t = cur_t + 1; nxt_k = 0; }
+      stage ^= 1;
+    }
+  }
+  // epilogue
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int gm = m0 + wm * 32 + i * 8 + gid;
+        int gn = n0 + wn * 32 + j * 8 + 2 * tig + e;
+        if (gm < M && gn < N) {
+          int64_t o = task.c_off + (int64_t)gm * task.ldc + gn;
+          Cr[o] = accr[i][j][e];
+          Ci[o] = acci[i][j][e];
+        }
+      }
+}
+
+template <bool AH, bool BH>
+int launch_variant(const GemmPlan& p, const Planar& A, const Planar& B, Planar& C, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    CMPS_CUDA(cudaFuncSetAttribute(zgemm_grouped_fp64<AH, BH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)SMEM_BYTES));
+    configured = true;
+  }
+  if (p.tiles.empty()) return CMPS_OK;
+  const int64_t ntiles = (int64_t)p.tiles.size();
+  if (ntiles > 0x7fffffff) return fail(CMPS_ERR_ARG, "too many GEMM tiles");
+  zgemm_grouped_fp64<AH, BH><<<(unsigned)ntiles, NTHREADS, SMEM_BYTES, st>>>(
+      p.d_tiles, p.d_tasks, p.d_terms, A.re(), A.im(), B.re(), B.im(), C.re(), C.im());
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+}  // namespace
+
+int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B, Planar& C,
+                      cudaStream_t st) {
+  if (!a_h && !b_h) return launch_variant<false, false>(p, A, B, C, st);
+  if (a_h && !b_h) return launch_variant<true, false>(p, A, B, C, st);
+  if (!a_h && b_h) return launch_variant<false, true>(p, A, B, C, st);
+  return launch_variant<true, true>(p, A, B, C, st);
+}
+
+int GemmPlan::upload(int bm, int bn) {
+  tiles.clear();
+  for (size_t i = 0; i < tasks.size(); ++i) {
+    const GemmTask& t = tasks[i];
+    for (int m0 = 0; m0 < t.m; m0 += bm)
+      for (int n0 = 0; n0 < t.n; n0 += bn) tiles.push_back(GemmTile{(int32_t)i, m0, n0, 0});
+  }
+  release();
+  auto up = [](auto& v, auto** d) -> int {
+    if (v.empty()) return CMPS_OK;
+    size_t bytes = v.size() * sizeof(v[0]);
+    CMPS_CUDA(cudaMalloc((void**)d, bytes));
+    CMPS_CUDA(cudaMemcpy(*d, v.data(), bytes, cudaMemcpyHostToDevice));
+    return CMPS_OK;
+  };
+  CMPS_TRY(up(tasks, &d_tasks));
+  CMPS_TRY(up(terms, &d_terms));
+  CMPS_TRY(up(tiles, &d_tiles));
+  return CMPS_OK;
+}
+
+int GemmPlan::validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t c_len, const char* what) const {
+  for (const GemmTask& t : tasks) {
+    if (t.m < 0 || t.n < 0 || t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)terms.size())
+      return fail(CMPS_ERR_STATE, std::string(what) + ": malformed task");
+    if (t.m == 0 || t.n == 0) continue;
+    if (t.ldc < t.n || t.c_off < 0 || t.c_off + (int64_t)(t.m - 1) * t.ldc + t.n > c_len)
+      return fail(CMPS_ERR_STATE, std::string(what) + ": output range outside its buffer");
+    for (int q = t.t0; q < t.t1; ++q) {
+      const GemmTerm& tm = terms[q];
+      if (tm.k <= 0) return fail(CMPS_ERR_STATE, std::string(what) + ": empty term");
+      // A is M x K (row-major, lda >= K) or stored K x M (lda >= M)
+      int64_t arows = a_h ? tm.k : t.m, acols = a_h ? t.m : tm.k;
+      int64_t brows = b_h ? t.n : tm.k, bcols = b_h ? tm.k : t.n;
+      if (tm.lda < acols || tm.a_off < 0 || tm.a_off + (arows - 1) * tm.lda + acols > a_len)
+        return fail(CMPS_ERR_STATE, std::string(what) + ": A operand range outside its buffer");
+      if (tm.ldb < bcols || tm.b_off < 0 || tm.b_off + (brows - 1) * tm.ldb + bcols > b_len)
+        return fail(CMPS_ERR_STATE, std::string(what) + ": B operand range outside its buffer");
+    }
+  }
+  return CMPS_OK;
+}
+
+void GemmPlan::release() {
+  if (d_tasks) cudaFree(d_tasks);
+  if (d_terms) cudaFree(d_terms);
+  if (d_tiles) cudaFree(d_tiles);
+  d_tasks = nullptr;
+  d_terms = nullptr;
+  d_tiles = nullptr;
+}
+
+int gemm_tile_m() { return BM; }
+int gemm_tile_n() { return BN; }
+
+}  // namespace cmps

@@ -1,0 +1,170 @@
+/*
+ * chainamps_b200 -- C ABI of the B200 implementation of the ChainAMPS
+ * two-site DMRG hot path (effective-Hamiltonian matvec, Krylov ground state,
+ * charge-block SVD truncation, environment updates).
+ *
+ * Every entry point returns an int status (CMPS_OK == 0) and never aborts;
+ * cmps_last_error() gives a one-line description of the last failure on the
+ * calling thread.  Complex numbers are interleaved (re, im) doubles, exactly
+ * std::complex<double> as the reference stores them.  Tensors cross the
+ * boundary in the reference's own storage: an MPX_matrix is a list of
+ * directed, charge-labelled indices plus one CSC matrix whose rows combine the
+ * first num_row_indices indices and whose columns combine the rest, first
+ * index fastest (MPX_matrix.cpp:219-236, MPXIndex.cpp:8-24,
+ * sparse_interface.cpp:85-91).  Charges are QuantumNumberInt (short)
+ * (common_defs.hpp:20); Z_N charges add modulo N, N <= 0 means Z
+ * (states.hpp:176-206).
+ */
+#ifndef CHAINAMPS_B200_H
+#define CHAINAMPS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CMPS_OK = 0,
+  CMPS_ERR_ARG = 1,        /* bad argument / inconsistent shapes */
+  CMPS_ERR_CHARGE = 2,     /* a stored entry violates charge conservation */
+  CMPS_ERR_CUDA = 3,       /* CUDA runtime / driver failure */
+  CMPS_ERR_NOMEM = 4,      /* device allocation failed */
+  CMPS_ERR_SOLVER = 5,     /* eigensolver / SVD did not converge */
+  CMPS_ERR_STATE = 6       /* call out of order (e.g. no eigenvector yet) */
+};
+
+enum {
+  CMPS_FP64 = 0,           /* all contraction arithmetic in complex double */
+  CMPS_SPLIT_TF32 = 1      /* contractions as 3-term split TF32 on tcgen05, FP32 accumulate */
+};
+
+typedef struct cmps_context cmps_context;
+typedef struct cmps_heff cmps_heff;
+typedef struct cmps_svd cmps_svd;
+typedef struct cmps_block cmps_block;
+
+/* Charge rules of the model: nq entries, the N of each Z_N charge (<=0: Z). */
+typedef struct {
+  int32_t nq;
+  const int16_t* rules;
+} cmps_charge_rules;
+
+/* One MPX_matrix as the reference stores it (MPX_matrix.hpp:61-66).
+ * charges: for index i, element e, component c:
+ *   charges[(offset_i + e) * nq + c], offset_i = sum_{j<i} sizes[j].
+ * Physical indices carry the basis charges like any other index. */
+typedef struct {
+  int32_t num_indices;
+  int32_t num_row_indices;
+  const uint8_t* inward;      /* [num_indices] 1 = ingoing */
+  const uint8_t* physical;    /* [num_indices] */
+  const int64_t* sizes;       /* [num_indices] */
+  const int16_t* charges;     /* [sum(sizes) * nq] */
+  int64_t rows, cols;         /* CSC matrix shape */
+  const int64_t* colptr;      /* [cols + 1] */
+  const int64_t* rowind;      /* [nnz] */
+  const double* values;       /* [2 * nnz] interleaved complex */
+} cmps_mpx_desc;
+
+/* ---- context ---------------------------------------------------------- */
+int cmps_context_create(int device, cmps_context** out);
+int cmps_context_destroy(cmps_context* ctx);
+const char* cmps_last_error(void);
+/* Library build string (architecture, kernels compiled in). */
+const char* cmps_version(void);
+
+/* ---- effective Hamiltonian (TwoVertexComponents) ----------------------
+ * Replaces the TwoVertexComponents constructor (DMRG_routines.cpp:779-833):
+ * L is the 6-index left block (a' = index 1, b = index 3, a = index 5; the
+ * rest size-1 dummies: MakeLeftBlock / MakeInitialLeftBlock /
+ * MakeDummyLeftBlock, DMRG_routines.cpp:583-632), W the 4-index MPO
+ * (sigma', b_left, sigma, b_right: make_model.hpp:613-618), R the 6-index
+ * right block (a' = 0, b = 2, a = 4).  Everything is uploaded once and kept
+ * on the device as charge-sector block lists; LeftPart and RightPart are
+ * formed on the device. */
+int cmps_heff_create(cmps_context* ctx, const cmps_charge_rules* rules,
+                     const cmps_mpx_desc* L, const cmps_mpx_desc* W,
+                     const cmps_mpx_desc* R, int precision, cmps_heff** out);
+/* Same, with the environments taken from device-resident blocks produced by
+ * cmps_heff_left_block / cmps_heff_right_block (no host round trip); the
+ * blocks are copied, the caller keeps ownership. */
+int cmps_heff_create_from_blocks(cmps_context* ctx, const cmps_charge_rules* rules,
+                                 const cmps_block* L, const cmps_mpx_desc* W,
+                                 const cmps_block* R, int precision, cmps_heff** out);
+/* Upload a reference-layout block (6-index MPX_matrix, left or right) as a
+ * device block, e.g. the dummy end blocks (MakeDummyLeftBlock /
+ * MakeDummyRightBlock, DMRG_routines.cpp:613-653).  W gives the MPO index. */
+int cmps_block_create(cmps_context* ctx, const cmps_charge_rules* rules,
+                      const cmps_mpx_desc* block, const cmps_mpx_desc* W, int right,
+                      cmps_block** out);
+int cmps_heff_destroy(cmps_heff* h);
+/* n_allowed = allowed_indices.size() (the ARPACK vector length);
+ * full_length = TwoVertexComponents::length() (DMRG_routines.hpp:211). */
+int cmps_heff_length(const cmps_heff* h, int64_t* n_allowed, int64_t* full_length);
+/* allowed_indices in ARPACK order (DMRG_routines.cpp:808-824). */
+int cmps_heff_allowed_indices(const cmps_heff* h, int64_t* out);
+/* Replaces TwoVertexMPOMPSMultiply (DMRG_routines.cpp:898-974): in and out
+ * are HOST arrays of n_allowed complex doubles (ARPACK's workd slices). */
+int cmps_heff_apply(cmps_heff* h, const double* in, double* out);
+/* Same on DEVICE arrays, stream-ordered on `stream` (cudaStream_t or NULL). */
+int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void* stream);
+/* Algorithmic flops of one apply: canonical = L.theta, W1, W2, .R stages
+ * over non-zero MPO entries (8 per complex MAC); executed = what the two
+ * grouped GEMM launches actually issue. */
+int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
+/* Switch the contraction arithmetic of an existing handle (CMPS_FP64 or
+ * CMPS_SPLIT_TF32). */
+int cmps_heff_set_precision(cmps_heff* h, int precision);
+
+/* Lowest eigenpair (smallest real part) of H_eff, device Lanczos in FP64
+ * with full re-orthogonalisation and explicit restarts.  Replaces
+ * TwoVertexComponents::HED -> arpack::arpack_eigs (DMRG_routines.cpp:835-896,
+ * arpack_interface.hpp:174-237); the eigenvector is post-processed as HED
+ * does: phase of the largest entry removed, entries <= eps*max dropped,
+ * FixComplexPrecision.  guess: host, n_allowed complex, or NULL.  evec:
+ * host, n_allowed complex, or NULL (the vector stays on the device for
+ * cmps_heff_theta_svd either way).  tol: residual norm / |eigenvalue|. */
+int cmps_heff_eigs(cmps_heff* h, const double* guess, double tol, int max_restarts,
+                   int krylov_dim, double* eval, double* evec, int* matvecs);
+
+/* ---- charge-block SVD of the two-vertex wavefunction ------------------
+ * Replaces TwoVertexSVD -> MPX_matrix::SVD -> SparseMatrix::SVD
+ * (DMRG_routines.hpp:225, MPX_matrix.cpp:157-192,
+ * sparse_interface.cpp:1248-1406) for the eigenvector last produced by
+ * cmps_heff_eigs (or loaded with cmps_heff_set_theta).  Truncation rule of
+ * the reference: keep min(chi, total); drop the smallest values while their
+ * squared sum stays below max_trunc; extend over values within 1e-3 relative
+ * of the last kept one. */
+int cmps_heff_set_theta(cmps_heff* h, const double* theta);
+int cmps_heff_theta_svd(cmps_heff* h, int64_t chi, double max_trunc, cmps_svd** out);
+int cmps_svd_destroy(cmps_svd* s);
+/* kept values (descending), discarded weight, sizes of the U and V^dagger
+ * CSC matrices in the reference layout (U: rows = (sigma1, a0), V^dagger:
+ * cols = (sigma2, a2)). */
+int cmps_svd_info(const cmps_svd* s, int64_t* kept, double* discarded_weight,
+                  int64_t* nnz_u, int64_t* nnz_vd);
+/* values[kept]; new bond charges[kept * nq]; U and V^dagger in CSC. */
+int cmps_svd_copy(const cmps_svd* s, double* values, int16_t* new_charges,
+                  int64_t* u_colptr, int64_t* u_rowind, double* u_values,
+                  int64_t* vd_colptr, int64_t* vd_rowind, double* vd_values);
+
+/* ---- environment updates ---------------------------------------------
+ * New left block L' = A^dagger (W (L A)) from the handle's L and W and the
+ * U of `s` (MakeLeftBlock, DMRG_routines.cpp:594-602); new right block
+ * R' = B^dagger (W (R B)) from V^dagger of `s` (MakeRightBlock, :603-611).
+ * The result stays on the device; cmps_block_info / cmps_block_copy export
+ * it as the reference's 6-index MPX_matrix (rows = a', cols = (b, a)). */
+int cmps_heff_left_block(cmps_heff* h, const cmps_svd* s, cmps_block** out);
+int cmps_heff_right_block(cmps_heff* h, const cmps_svd* s, cmps_block** out);
+int cmps_block_destroy(cmps_block* b);
+int cmps_block_info(const cmps_block* b, int64_t* chi, int64_t* mpo_dim, int64_t* nnz);
+/* a_charges[chi * nq] (the new bond), CSC of the (chi) x (mpo_dim * chi)
+ * matrix: row = a', col = b + mpo_dim * a. */
+int cmps_block_copy(const cmps_block* b, int16_t* a_charges, int64_t* colptr,
+                    int64_t* rowind, double* values);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAINAMPS_B200_H */
