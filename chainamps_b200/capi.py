@@ -81,6 +81,7 @@ _SIGS = {
     "cmps_heff_apply": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
     "cmps_heff_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_flops": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
+    "cmps_heff_time_stages": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, c_dblp]),
     "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
                                  C.POINTER(C.c_int)]),
@@ -237,6 +238,13 @@ class TwoVertexComponents:
         """Device pointers (ints) to n complex doubles each."""
         _check(lib.cmps_heff_apply_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
                                           C.c_void_p(stream) if stream else None))
+
+    def time_stages(self, d_in, d_out, stream=None, reps=3):
+        """Average ms of [gather, stage 1, stage 2, scatter] (CUDA events)."""
+        ms = np.zeros(4, np.float64)
+        _check(lib.cmps_heff_time_stages(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
+                                         C.c_void_p(stream) if stream else None, reps, _p(ms, C.c_double)))
+        return ms
 
     def flops(self):
         a = C.c_double()

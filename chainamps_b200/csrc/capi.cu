@@ -161,6 +161,37 @@ int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void
   return h->impl->apply_device(d_in, d_out, st);
 }
 
+int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void* stream, int reps, double* ms) {
+  if (!h || !h->impl || !d_in || !d_out || !ms || reps < 1) return fail(CMPS_ERR_ARG, "bad argument");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));
+  double acc[4] = {0, 0, 0, 0};
+  int status = CMPS_OK;
+  for (int r = 0; r < reps && status == CMPS_OK; ++r) {
+    cudaEventRecord(ev[0], st);
+    status = launch_pack(d_in, H.d_pos, H.n_allowed, H.x, st);
+    cudaEventRecord(ev[1], st);
+    if (status == CMPS_OK) status = H.apply_stage(1, H.x, H.y, st);
+    cudaEventRecord(ev[2], st);
+    if (status == CMPS_OK) status = H.apply_stage(2, H.x, H.y, st);
+    cudaEventRecord(ev[3], st);
+    if (status == CMPS_OK) status = launch_unpack(H.y, H.d_pos, H.n_allowed, d_out, st);
+    cudaEventRecord(ev[4], st);
+    if (cudaEventSynchronize(ev[4]) != cudaSuccess) status = fail(CMPS_ERR_CUDA, "stage timing failed");
+    for (int k = 0; k < 4 && status == CMPS_OK; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  return status;
+}
+
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {
   if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
   if (canonical) *canonical = h->impl->flops_canonical;

@@ -618,10 +618,15 @@ int Heff::finish() {
   return CMPS_OK;
 }
 
-int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
+int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
   if (precision != CMPS_FP64) return fail(CMPS_ERR_ARG, "requested precision is not built into this library");
-  CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
-  CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
+  if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
+  return launch_zgemm_fp64(stage2, false, false, T, RP, out, st);
+}
+
+int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
+  CMPS_TRY(apply_stage(1, in, out, st));
+  CMPS_TRY(apply_stage(2, in, out, st));
   return CMPS_OK;
 }
 

@@ -81,6 +81,7 @@ struct Heff {
   int parse_mpo(const cmps_mpx_desc* Wd);
   int finish();  // sector structure, LeftPart/RightPart, GEMM plans (L, R, W set)
   int apply_theta(const Planar& in, Planar& out, cudaStream_t st);  // theta-space matvec
+  int apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st);  // 1: T = LP in, 2: out = T RP
   int apply_host(const double* in, double* out);
   int apply_device(const double* din, double* dout, cudaStream_t st);
   int eigs(const double* guess, double tol, int max_restarts, int kdim, double* eval, double* evec,

@@ -1,0 +1,221 @@
+"""Reference-layout inputs for the hot path: the Hamiltonian MPO of a vertex
+model and seeded synthetic environment blocks, as ``MPXTensor`` objects
+ready for the C ABI.
+
+The MPO follows the reference's ``MakeGeneralHMPO`` (make_model.hpp:471-621):
+bond index = [identity, one slot per (coupling, charge difference), local
+terms row], bond dimension 2 + n_couplings * n_charge_differences, the
+vertex Hamiltonian and single-vertex terms at (last, first), the first
+operator of each coupling in column 0 and coupling * second operator in the
+last row, split by the charge difference of each matrix element
+(``QNCombinations``, states.cpp:191-252).  The padded zero slots are kept,
+exactly as the reference builds them; the device structure skips them.
+
+Vertex models used by the workloads:
+* spin-1/2 XXZ chain (one site per vertex, total-Sz charge);
+* ``legs`` coupled spin-1/2 Heisenberg chains with one rung per vertex
+  (local dimension 2**legs, total-Sz charge, rung coupling inside the
+  vertex Hamiltonian, intra-chain couplings between vertices).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .capi import MPXTensor, MPXIndexSpec
+
+
+def _charge_add(a, b, rules):
+    out = np.asarray(a, np.int64) + np.asarray(b, np.int64)
+    for i, n in enumerate(rules):
+        if n > 0:
+            out[..., i] %= n
+    return out
+
+
+def _charge_neg(a, rules):
+    out = -np.asarray(a, np.int64)
+    for i, n in enumerate(rules):
+        if n > 0:
+            out[..., i] %= n
+    return out
+
+
+def charge_difference_slots(charges, rules):
+    """QNCombinations(basis, minus): (involution states, ordered states)."""
+    seen = []
+    for a in charges:
+        for b in charges:
+            t = tuple(int(x) for x in _charge_add(a, _charge_neg(b, rules), rules))
+            if t not in seen:
+                seen.append(t)
+    invol = [t for t in seen if tuple(int(x) for x in _charge_neg(np.array(t), rules)) == t]
+    rest = [t for t in seen if t not in invol]
+    front, back = [], []
+    if rest:
+        front.insert(0, rest.pop(0))
+        i = 0
+        while i < len(rest):
+            if tuple(int(x) for x in _charge_neg(np.array(rest[i]), rules)) == front[0]:
+                back.append(rest.pop(i))
+                if not rest:
+                    break
+                front.insert(0, rest.pop(0))
+                i = 0
+            else:
+                i += 1
+    return invol, front + back
+
+
+def general_hmpo(charges, rules, hamiltonian, operators, couplings):
+    """MakeGeneralHMPO.  couplings: list of (op1, op2 or None, value)."""
+    charges = np.asarray(charges, np.int64)
+    d = charges.shape[0]
+    nq = len(rules)
+    inter = [c for c in couplings if c[1]]
+    local = [c for c in couplings if not c[1]]
+    invol, ordered = charge_difference_slots(charges, rules)
+    ndiff = len(invol) + len(ordered)
+    D = 2 + len(inter) * ndiff
+    W = np.zeros((d, D, d, D), np.complex128)
+    for i in range(d):
+        W[i, 0, i, 0] = 1.0
+        W[i, D - 1, i, D - 1] = 1.0
+    W[:, D - 1, :, 0] += hamiltonian
+    for op, _, val in local:
+        W[:, D - 1, :, 0] += val * operators[op]
+
+    def slot(diff, same):
+        t = tuple(int(x) for x in diff)
+        tn = tuple(int(x) for x in _charge_neg(diff, rules))
+        if t == tn:
+            li = invol.index(t) if t in invol else 0
+            return li, li
+        if tn in ordered:
+            li = ordered.index(tn)
+            return len(invol) + li, ndiff - li - 1
+        return 0, 0
+
+    for b, (o1, o2, val) in enumerate(inter):
+        base = 1 + b * ndiff
+        A, B = operators[o1], operators[o2]
+        same = o1 == o2
+        for col in range(d):
+            for i in range(d):
+                if A[i, col] != 0:
+                    ro, co = slot(_charge_add(charges[i], _charge_neg(charges[col], rules), rules), same)
+                    W[i, base + ro, col, 0] += A[i, col]
+                    if same:
+                        W[i, D - 1, col, base + co] += val * A[i, col]
+        if not same:
+            for col in range(d):
+                for i in range(d):
+                    if B[i, col] != 0:
+                        _, co = slot(_charge_add(charges[i], _charge_neg(charges[col], rules), rules), True)
+                        W[i, D - 1, col, base + co] += val * B[i, col]
+    bq = [np.zeros(nq, np.int64)]
+    for _ in inter:
+        bq += [np.array(t, np.int64) for t in invol] + [np.array(t, np.int64) for t in ordered]
+    bq.append(np.zeros(nq, np.int64))
+    bq = np.stack(bq).reshape(D, nq)
+    return W, bq
+
+
+def dense_to_tensor(indices, nrow, data):
+    """Dense tensor (one axis per index, index order) -> MPXTensor (CSC of
+    the matrix form, first index fastest)."""
+    shp = data.shape
+    rows = int(np.prod(shp[:nrow]))
+    cols = int(np.prod(shp[nrow:]))
+    M = data.reshape((rows, cols), order="F")
+    nzr, nzc = np.nonzero(M.T)  # column-major order of non-zeros
+    colptr = np.zeros(cols + 1, np.int64)
+    np.add.at(colptr, nzr + 1, 1)
+    colptr = np.cumsum(colptr)
+    return MPXTensor(indices, nrow, rows, cols, colptr, nzc.astype(np.int64), M[nzc, nzr])
+
+
+def mpo_tensor(charges, W, bq):
+    charges = np.asarray(charges, np.int64)
+    idx = [MPXIndexSpec(True, True, charges), MPXIndexSpec(True, False, bq),
+           MPXIndexSpec(False, True, charges), MPXIndexSpec(False, False, bq)]
+    return dense_to_tensor(idx, 2, W)
+
+
+def pauli():
+    return (np.array([[0, 1], [1, 0]], np.complex128), np.array([[0, -1j], [1j, 0]], np.complex128),
+            np.array([[1, 0], [0, -1]], np.complex128))
+
+
+def xxz_model(jxy=1.0, jz=1.0, h=0.0):
+    """Spin-1/2 XXZ chain, Pauli operators, basis {+1, -1} with a Z charge."""
+    sx, sy, sz = pauli()
+    ops = {"Sx": sx, "Sy": sy, "Sz": sz}
+    ch = np.array([[1], [-1]], np.int64)
+    cps = [("Sx", "Sx", jxy), ("Sy", "Sy", jxy), ("Sz", "Sz", jz)]
+    if h:
+        cps.append(("Sz", None, h))
+    W, bq = general_hmpo(ch, (0,), np.zeros((2, 2), np.complex128), ops, cps)
+    return (0,), ch, W, bq
+
+
+def ladder_model(legs=4, j=1.0, j_perp=0.5):
+    """``legs`` spin-1/2 chains, one rung per vertex (S = sigma/2)."""
+    sx, sy, sz = [p / 2 for p in pauli()]
+    eye = np.eye(2, dtype=np.complex128)
+    d = 2 ** legs
+
+    def site(op, k):
+        m = np.array([[1.0]], np.complex128)
+        for q in range(legs):
+            m = np.kron(m, op if q == k else eye)
+        return m
+    ops = {}
+    for k in range(legs):
+        ops[f"Sx{k}"], ops[f"Sy{k}"], ops[f"Sz{k}"] = site(sx, k), site(sy, k), site(sz, k)
+    H = np.zeros((d, d), np.complex128)
+    for k in range(legs - 1):
+        for a in "xyz":
+            H += j_perp * ops[f"S{a}{k}"] @ ops[f"S{a}{k + 1}"]
+    ch = np.zeros((d, 1), np.int64)
+    for s in range(d):
+        ch[s, 0] = sum(1 if ((s >> (legs - 1 - q)) & 1) == 0 else -1 for q in range(legs))
+    cps = [(f"S{a}{k}", f"S{a}{k}", j) for k in range(legs) for a in "xyz"]
+    W, bq = general_hmpo(ch, (0,), H, ops, cps)
+    return (0,), ch, W, bq
+
+
+def gaussian_bond(chi, step=2, width=3.5, offset=0):
+    """Bond charges with a discretised Gaussian sector-size profile (the
+    shape of a converged total-Sz distribution), ``chi`` elements, charges
+    offset + step * k."""
+    ks = np.arange(-40, 41)
+    p = np.exp(-0.5 * (ks * step / width) ** 2)
+    p /= p.sum()
+    n = np.floor(p * chi).astype(int)
+    rem = chi - n.sum()
+    order = np.argsort(-(p * chi - n))
+    n[order[:rem]] += 1
+    q = np.concatenate([np.full(c, offset + step * k) for k, c in zip(ks, n) if c > 0])
+    return q.reshape(-1, 1).astype(np.int64)
+
+
+def random_environment(rng, rules, bond, bq, used_b, right):
+    """Seeded random environment block obeying q(a') = q(b) + q(a), only on
+    the MPO slots in ``used_b``; complex Gaussian entries, Hermitian in (a', a)
+    for each b paired with its conjugate slot is not imposed."""
+    chi = bond.shape[0]
+    D = bq.shape[0]
+    nq = len(rules)
+    vals = np.zeros((chi, D, chi), np.complex128)
+    for b in used_b:
+        ok = np.all(bond[:, None, :] == _charge_add(bq[b][None, None, :], bond[None, :, :], rules), axis=-1)
+        nzr, nzc = np.nonzero(ok)
+        vals[nzr, b, nzc] = (rng.standard_normal(nzr.size) + 1j * rng.standard_normal(nzr.size)) / np.sqrt(2)
+    z = np.zeros((1, nq), np.int64)
+    if not right:
+        idx = [MPXIndexSpec(False, False, z), MPXIndexSpec(True, False, bond), MPXIndexSpec(True, False, z),
+               MPXIndexSpec(False, False, bq), MPXIndexSpec(True, False, z), MPXIndexSpec(False, False, bond)]
+        return dense_to_tensor(idx, 3, vals.reshape(1, chi, 1, D, 1, chi))
+    idx = [MPXIndexSpec(False, False, bond), MPXIndexSpec(True, False, z), MPXIndexSpec(True, False, bq),
+           MPXIndexSpec(False, False, z), MPXIndexSpec(True, False, bond), MPXIndexSpec(False, False, z)]
+    return dense_to_tensor(idx, 2, vals.reshape(chi, 1, D, 1, chi, 1))

@@ -113,6 +113,13 @@ int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void
  * over non-zero MPO entries (8 per complex MAC); executed = what the two
  * grouped GEMM launches actually issue. */
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
+/* Stage timing for roofline accounting: runs `reps` device applies on
+ * `stream` (cudaStream_t or NULL) and returns the average duration in ms of
+ * each launch, measured with CUDA events on that stream:
+ * ms[0] gather (ARPACK order -> sector blocks), ms[1] stage-1 grouped GEMM,
+ * ms[2] stage-2 grouped GEMM, ms[3] scatter. */
+int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void* stream,
+                          int reps, double* ms);
 /* Switch the contraction arithmetic of an existing handle (CMPS_FP64 or
  * CMPS_SPLIT_TF32). */
 int cmps_heff_set_precision(cmps_heff* h, int precision);
