@@ -225,12 +225,16 @@ class TwoVertexComponents:
         _check(lib.cmps_heff_allowed_indices(self.h, _p(out, C.c_int64)))
         return out
 
-    def multiply(self, x):
-        """TwoVertexMPOMPSMultiply: host vector in ARPACK order -> host vector."""
+    def multiply(self, x, out=None):
+        """TwoVertexMPOMPSMultiply: host vector in ARPACK order -> host vector
+        (written into ``out`` when given, e.g. a pinned buffer)."""
         x = np.ascontiguousarray(np.asarray(x, np.complex128))
         if x.shape != (self.n,):
             raise ValueError("vector length differs from allowed_indices.size()")
-        out = np.empty_like(x)
+        if out is None:
+            out = np.empty_like(x)
+        elif out.shape != x.shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous complex128 vector of the same length")
         _check(lib.cmps_heff_apply(self.h, _p(x.view(np.float64), C.c_double), _p(out.view(np.float64), C.c_double)))
         return out
 
