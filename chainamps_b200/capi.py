@@ -81,6 +81,7 @@ _SIGS = {
     "cmps_heff_apply": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
     "cmps_heff_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_flops": (C.c_int, [C.c_void_p, c_dblp, c_dblp]),
+    "cmps_heff_apply_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_time_stages": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, c_dblp]),
     "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,

@@ -113,6 +113,21 @@ int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void
  * over non-zero MPO entries (8 per complex MAC); executed = what the two
  * grouped GEMM launches actually issue. */
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
+/* H_eff matvec that allocates nothing (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc when they apply H_eff: an
+ * eigensolver callback (ARPACK's MV, called hundreds of times per step)
+ * inside a host application whose device memory belongs to its own pool or
+ * caching allocator, where an allocation from the callback would fail or
+ * would add an allocation and a device-wide synchronisation per iteration.
+ * Same inputs and result as cmps_heff_apply_device (FP64 handles only), but
+ * its scratch -- the gathered vector, the stage-1 intermediate and the
+ * stage-2 output, 4 * n_allowed + 2 * |T| doubles -- lives in one static
+ * device array of at most 32 MiB held by every GPU that loads the library;
+ * larger problems are rejected with CMPS_ERR_ARG.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress), so make the
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race.  Nothing in it needs to start at zero. */
+int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, double* d_out, void* stream);
 /* Stage timing for roofline accounting: runs `reps` device applies on
  * `stream` (cudaStream_t or NULL) and returns the average duration in ms of
  * each launch, measured with CUDA events on that stream:
