@@ -224,6 +224,7 @@ int build_env_from_desc(const Rules& r, const cmps_mpx_desc* d, bool right, Env&
 
 // ---------------------------------------------------------------------------
 Heff::~Heff() {
+  release_split(this);
   L.data.release();
   R.data.release();
   LP.release();
@@ -619,20 +620,32 @@ int Heff::finish() {
 }
 
 int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
-  if (precision != CMPS_FP64) return fail(CMPS_ERR_ARG, "requested precision is not built into this library");
+  if (precision == CMPS_SPLIT_TF32) return apply_split_stage(*this, which, in, out, st);
   if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
   return launch_zgemm_fp64(stage2, false, false, T, RP, out, st);
 }
 
 int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
+  if (precision == CMPS_SPLIT_TF32) return apply_split(*this, in, out, st);
   CMPS_TRY(apply_stage(1, in, out, st));
   CMPS_TRY(apply_stage(2, in, out, st));
   return CMPS_OK;
 }
 
+int Heff::apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st) {
+  CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
+  CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
+  return CMPS_OK;
+}
+
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
   CMPS_TRY(launch_pack(din, d_pos, n_allowed, x, st));
-  CMPS_TRY(apply_theta(x, y, st));
+  if (precision == CMPS_SPLIT_TF32) {
+    CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
+    CMPS_TRY(apply_split_stage(*this, 2, x, y, st));
+  } else {
+    CMPS_TRY(apply_theta(x, y, st));
+  }
   CMPS_TRY(launch_unpack(y, d_pos, n_allowed, dout, st));
   return CMPS_OK;
 }
@@ -720,6 +733,9 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   int nmv = 0;
   double lam = 0.0;
   bool converged = false;
+  // the split-TF32 operator is accurate to ~1e-6 relative: converge the Ritz
+  // vector to that floor, the energy comes from an FP64 Rayleigh quotient
+  if (precision == CMPS_SPLIT_TF32) tol = std::max(tol, 3e-6);
   std::vector<double> h(2 * 128), h2(2 * 128), alpha, beta, ycoef;
   for (int restart = 0; restart < std::max(1, max_restarts) && !converged; ++restart) {
     CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), vr(0), vi(0), st));
@@ -762,6 +778,14 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   }
   // normalise the Ritz vector
   CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), x.re(), x.im(), st));
+  if (precision == CMPS_SPLIT_TF32) {
+    // FP64 Rayleigh quotient <x|H|x> (x normalised): energy error ~ |dx|^2
+    CMPS_TRY(apply_theta_fp64(x, y, st));
+    ++nmv;
+    std::vector<double> rq(2);
+    CMPS_TRY(ops.multidot(x.re(), x.im(), 0, 1, y.re(), y.im(), rq.data(), st));
+    lam = rq[0];
+  }
   // HED post-processing (DMRG_routines.cpp:870-889)
   double mx2 = 0.0;
   int64_t imx = 0;

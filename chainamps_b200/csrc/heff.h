@@ -35,6 +35,7 @@ struct ThetaSpace {
 };
 
 struct SvdResult;
+struct SplitState;
 
 struct Heff {
   cmps_context* ctx = nullptr;
@@ -64,6 +65,7 @@ struct Heff {
   GemmPlan stage1, stage2;
   double flops_canonical = 0.0, flops_executed = 0.0;
   int precision = CMPS_FP64;
+  SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)
   // work vectors
   Planar x, y;                   // theta-space vectors
   double* d_io = nullptr;        // interleaved staging (2 * n_allowed doubles)
@@ -81,6 +83,7 @@ struct Heff {
   int parse_mpo(const cmps_mpx_desc* Wd);
   int finish();  // sector structure, LeftPart/RightPart, GEMM plans (L, R, W set)
   int apply_theta(const Planar& in, Planar& out, cudaStream_t st);  // theta-space matvec
+  int apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st);
   int apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st);  // 1: T = LP in, 2: out = T RP
   int apply_host(const double* in, double* out);
   int apply_device(const double* din, double* dout, cudaStream_t st);
@@ -90,6 +93,10 @@ struct Heff {
 
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);
+void release_split(Heff* h);
+int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st);
+int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
+int split_error(Heff& H);
 // cuSOLVER handle owned by the context (svd.cu).
 void release_solver(cmps_context* ctx);
 

@@ -1,13 +1,475 @@
-// Split-precision (3-term TF32 on tcgen05, FP32 accumulate) operand
-// preparation.  The FP64 path needs nothing extra.
+// Split-precision (3-term TF32 on tcgen05, FP32 accumulate) form of the
+// H_eff matvec: operand preparation, tensor maps and the two stage plans.
+//
+// Layouts (FP32, four planes re_hi, re_lo, im_hi, im_lo per buffer):
+//  * S1A  -- stage-1 A operand: theta transposed per (m, sigma1) chunk,
+//            [r][a0] with r running over the padded right index of m (each
+//            sigma2 chunk starts on a 4-element boundary) and ld = pad4(dim a0);
+//  * LPS  -- stage-1 B operand: LeftPart blocks [a0'][a0], ld = pad4(dim a0);
+//  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad];
+//  * RPTS -- stage-2 B operand: RightPart blocks transposed, [a2'][a2].
+// Every block base is 128-byte aligned and every leading dimension a multiple
+// of 4 floats, as the TMA requires; the K tail of every operand is zero-filled
+// by the TMA (out-of-bounds fill), padding rows of S1A are zero.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+#include <set>
+
 #include "heff.h"
+#include "tc_gemm.h"
 
 namespace cmps {
 
+struct SplitState {
+  std::vector<int64_t> ldS;                     // per a0 sector
+  std::vector<int64_t> ldR;                     // per a2 sector
+  std::vector<std::vector<int64_t>> coloff_pad;  // [m][sigma2]
+  std::vector<int64_t> ncols_pad;               // per m
+  float* buf = nullptr;                         // one allocation for S1A, LPS, TS, RPTS
+  int64_t s1a_off = 0, s1a_len = 0, lps_off = 0, lps_len = 0, ts_off = 0, ts_len = 0, rpt_off = 0, rpt_len = 0;
+  int64_t* d_theta_map = nullptr;
+  int* d_err = nullptr;
+  int* h_err = nullptr;  // pinned
+  tc::TcPlan p1, p2;
+  float* plane_base(int64_t off) const { return buf + off; }
+};
+
+namespace {
+
+inline int64_t pad4(int64_t x) { return (x + 3) & ~int64_t(3); }
+inline int64_t align32(int64_t x) { return (x + 31) & ~int64_t(31); }
+
+__device__ __forceinline__ float rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+__device__ __forceinline__ void split4(double re, double im, float* p0, float* p1, float* p2, float* p3) {
+  const float hr = rna((float)re), hi = rna((float)im);
+  *p0 = hr;
+  *p1 = rna((float)(re - (double)hr));
+  *p2 = hi;
+  *p3 = rna((float)(im - (double)hi));
+}
+
+struct SplitBlock {
+  int64_t src_off, dst_off;
+  int32_t rows, cols, ld_dst, transpose;
+};
+
+// dst (4 planes) <- split(src block), optionally transposed.
+__global__ void k_split_blocks(const SplitBlock* __restrict__ blocks, const double* __restrict__ sr,
+                               const double* __restrict__ si, float* __restrict__ dst, int64_t plane) {
+  const SplitBlock b = blocks[blockIdx.x];
+  const int64_t n = (int64_t)b.rows * b.cols;
+  for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
+    const int64_t r = e / b.cols, c = e % b.cols;
+    const int64_t o = b.transpose ? b.dst_off + c * b.ld_dst + r : b.dst_off + r * b.ld_dst + c;
+    split4(sr[b.src_off + e], si[b.src_off + e], dst + o, dst + o + plane, dst + o + 2 * plane, dst + o + 3 * plane);
+  }
+}
+
+__global__ void k_split_theta(const double* __restrict__ re, const double* __restrict__ im,
+                              const int64_t* __restrict__ map, int64_t n, float* __restrict__ dst, int64_t plane) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = map[e];
+    split4(re[e], im[e], dst + o, dst + o + plane, dst + o + 2 * plane, dst + o + 3 * plane);
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int encoder() {
+  if (g_encode) return CMPS_OK;
+  cudaDriverEntryPointQueryResult q;
+  void* fn = nullptr;
+  CMPS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || !fn) return fail(CMPS_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  return CMPS_OK;
+}
+
+// 3-D map over one operand block: (K, rows, 4 planes); box (16, 128, 4).
+// `base_off` is the block's element offset inside its plane of `plane`
+// elements; the block must lie inside the plane.
+int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t ld, int64_t plane, CUtensorMap* out) {
+  float* base = plane0 + base_off;
+  if (((uintptr_t)base & 15) || (ld * 4) % 16 || (plane * 4) % 16 || K < 1 || rows < 1 || K > ld)
+    return fail(CMPS_ERR_STATE, "tensor map: misaligned operand block");
+  if (base_off < 0 || base_off + (rows - 1) * ld + K > plane)
+    return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
+  cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, 4};
+  cuuint64_t strides[2] = {(cuuint64_t)(ld * 4), (cuuint64_t)(plane * 4)};
+  cuuint32_t box[3] = {16, 128, 4};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(CMPS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return CMPS_OK;
+}
+
+void add_tiles(tc::TcPlan& p, int32_t task, int32_t m, int32_t n) {
+  for (int32_t m0 = 0; m0 < m; m0 += 128)
+    for (int32_t n0 = 0; n0 < n; n0 += 128) p.tiles.push_back(tc::TcTile{task, m0, n0, 0});
+}
+
+}  // namespace
+
+namespace tc {
+int TcPlan::upload() {
+  release();
+  auto up = [](auto& v, auto** d) -> int {
+    if (v.empty()) return CMPS_OK;
+    size_t bytes = v.size() * sizeof(v[0]);
+    CMPS_CUDA(cudaMalloc((void**)d, bytes));
+    CMPS_CUDA(cudaMemcpy(*d, v.data(), bytes, cudaMemcpyHostToDevice));
+    return CMPS_OK;
+  };
+  CMPS_TRY(up(tasks, &d_tasks));
+  CMPS_TRY(up(terms, &d_terms));
+  CMPS_TRY(up(tiles, &d_tiles));
+  CMPS_TRY(up(amaps, &d_amaps));
+  CMPS_TRY(up(bmaps, &d_bmaps));
+  return CMPS_OK;
+}
+void TcPlan::release() {
+  if (d_tasks) cudaFree(d_tasks);
+  if (d_terms) cudaFree(d_terms);
+  if (d_tiles) cudaFree(d_tiles);
+  if (d_amaps) cudaFree(d_amaps);
+  if (d_bmaps) cudaFree(d_bmaps);
+  d_tasks = nullptr;
+  d_terms = nullptr;
+  d_tiles = nullptr;
+  d_amaps = nullptr;
+  d_bmaps = nullptr;
+}
+}  // namespace tc
+
+void release_split(Heff* h) {
+  if (!h || !h->split) return;
+  SplitState* s = h->split;
+  s->p1.release();
+  s->p2.release();
+  if (s->buf) cudaFree(s->buf);
+  if (s->d_theta_map) cudaFree(s->d_theta_map);
+  if (s->d_err) cudaFree(s->d_err);
+  if (s->h_err) cudaFreeHost(s->h_err);
+  delete s;
+  h->split = nullptr;
+}
+
+static int build_split(Heff& H) {
+  CMPS_TRY(encoder());
+  const Rules& r = H.rules;
+  const ThetaSpace& th = H.th;
+  const Bond& A0 = H.L.a;
+  const Bond& A2 = H.R.a;
+  const int d = H.d, nm = (int)th.mq.size();
+  auto* S = new SplitState();
+  H.split = S;
+  S->ldS.resize(A0.nsec());
+  for (int s = 0; s < A0.nsec(); ++s) S->ldS[s] = pad4(A0.sdim[s]);
+  S->ldR.resize(A2.nsec());
+  for (int t = 0; t < A2.nsec(); ++t) S->ldR[t] = pad4(A2.sdim[t]);
+  S->coloff_pad.assign(nm, std::vector<int64_t>(d, -1));
+  S->ncols_pad.assign(nm, 0);
+  for (int m = 0; m < nm; ++m) {
+    int64_t o = 0;
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
+      S->coloff_pad[m][s2] = o;
+      o += pad4(A2.sdim[t]);
+    }
+    S->ncols_pad[m] = o;
+  }
+  // ---- sizes and offsets (elements per plane) ----
+  std::map<std::pair<int, int>, int64_t> s1a_chunk;  // (m, sigma1) -> offset
+  int64_t s1a = 0;
+  for (int m = 0; m < nm; ++m)
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (th.rowoff[m][s1] < 0) continue;
+      int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+      s1a_chunk[{m, s1}] = s1a;
+      s1a += align32(S->ncols_pad[m] * S->ldS[s]);
+    }
+  std::map<std::array<int, 4>, int64_t> lps_blk;
+  std::vector<SplitBlock> lpsb;
+  int64_t lps = 0;
+  for (auto& kv : H.lp_off) {
+    const auto& key = kv.first;  // (b1, s1', s1, s)
+    int s = key[3];
+    int sp = A0.find(r.sub(r.add(r.add(A0.sq[s], H.sigq[key[2]]), H.bq[key[0]]), H.sigq[key[1]]));
+    lps_blk[key] = lps;
+    lpsb.push_back(SplitBlock{kv.second, lps, (int32_t)A0.sdim[sp], (int32_t)A0.sdim[s], (int32_t)S->ldS[s], 0});
+    lps += align32(A0.sdim[sp] * S->ldS[s]);
+  }
+  std::vector<int64_t> ts_base((size_t)H.D * nm, -1);
+  int64_t ts = 0;
+  for (int b1 = 0; b1 < H.D; ++b1)
+    for (int m = 0; m < nm; ++m) {
+      if (H.t_base[(size_t)b1 * nm + m] < 0) continue;
+      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      ts_base[(size_t)b1 * nm + m] = ts;
+      ts += align32(th.nrows[mp] * S->ncols_pad[m]);
+    }
+  std::map<std::array<int, 4>, int64_t> rpt_blk;
+  std::vector<SplitBlock> rptb;
+  int64_t rpt = 0;
+  for (auto& kv : H.rp_off) {
+    const auto& key = kv.first;  // (b1, s2, s2', t)
+    int t = key[3];
+    int tp = A2.find(r.sub(r.add(r.add(A2.sq[t], H.sigq[key[2]]), H.bq[key[0]]), H.sigq[key[1]]));
+    rpt_blk[key] = rpt;
+    // RP block is [a2][a2'] (dim t x dim t'); stored transposed [a2'][a2], ld = pad4(dim t)
+    rptb.push_back(SplitBlock{kv.second, rpt, (int32_t)A2.sdim[t], (int32_t)A2.sdim[tp], (int32_t)S->ldR[t], 1});
+    rpt += align32(A2.sdim[tp] * S->ldR[t]);
+  }
+  S->s1a_off = 0;
+  S->s1a_len = align32(std::max<int64_t>(s1a, 32));
+  S->lps_off = 4 * S->s1a_len;
+  S->lps_len = align32(std::max<int64_t>(lps, 32));
+  S->ts_off = S->lps_off + 4 * S->lps_len;
+  S->ts_len = align32(std::max<int64_t>(ts, 32));
+  S->rpt_off = S->ts_off + 4 * S->ts_len;
+  S->rpt_len = align32(std::max<int64_t>(rpt, 32));
+  const int64_t total = S->rpt_off + 4 * S->rpt_len;
+  if (cudaMalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
+    return fail(CMPS_ERR_NOMEM, "split-TF32 operand allocation failed");
+  CMPS_CUDA(cudaMemset(S->buf, 0, sizeof(float) * total));
+  CMPS_CUDA(cudaMalloc(&S->d_err, sizeof(int)));
+  CMPS_CUDA(cudaMemset(S->d_err, 0, sizeof(int)));
+  CMPS_CUDA(cudaMallocHost(&S->h_err, sizeof(int)));
+  // ---- split LeftPart / RightPart ----
+  {
+    SplitBlock* d = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<SplitBlock>& v = pass == 0 ? lpsb : rptb;
+      if (v.empty()) continue;
+      for (auto& b : v) {
+        const int64_t rows = b.transpose ? b.cols : b.rows;  // rows of the destination layout
+        const int64_t cols = b.transpose ? b.rows : b.cols;
+        const int64_t len = pass == 0 ? S->lps_len : S->rpt_len;
+        if (b.dst_off + (rows - 1) * b.ld_dst + cols > len || b.ld_dst < cols)
+          return fail(CMPS_ERR_STATE, "split block outside its buffer");
+      }
+      CMPS_CUDA(cudaMalloc(&d, sizeof(SplitBlock) * v.size()));
+      CMPS_CUDA(cudaMemcpy(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice));
+      const Planar& src = pass == 0 ? H.LP : H.RP;
+      float* dst = S->buf + (pass == 0 ? S->lps_off : S->rpt_off);
+      const int64_t plane = pass == 0 ? S->lps_len : S->rpt_len;
+      k_split_blocks<<<(unsigned)v.size(), 256, 0, H.ctx->stream>>>(d, src.re(), src.im(), dst, plane);
+      CMPS_CUDA(cudaGetLastError());
+      CMPS_CUDA(cudaStreamSynchronize(H.ctx->stream));
+      cudaFree(d);
+    }
+  }
+  // ---- theta -> S1A map ----
+  {
+    std::vector<int64_t> map(th.total, -1);
+    for (int m = 0; m < nm; ++m)
+      for (int s1 = 0; s1 < d; ++s1) {
+        if (th.rowoff[m][s1] < 0) continue;
+        int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+        const int64_t ch = s1a_chunk[{m, s1}];
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
+          for (int64_t p = 0; p < A0.sdim[s]; ++p)
+            for (int64_t c = 0; c < A2.sdim[t]; ++c) {
+              const int64_t src = th.base[m] + (th.rowoff[m][s1] + p) * th.ncols[m] + th.coloff[m][s2] + c;
+              map[src] = ch + (S->coloff_pad[m][s2] + c) * S->ldS[s] + p;
+            }
+        }
+      }
+    for (int64_t v : map)
+      if (v < 0 || v >= S->s1a_len) return fail(CMPS_ERR_STATE, "theta split map incomplete");
+    CMPS_CUDA(cudaMalloc(&S->d_theta_map, sizeof(int64_t) * std::max<int64_t>(1, th.total)));
+    CMPS_CUDA(cudaMemcpy(S->d_theta_map, map.data(), sizeof(int64_t) * th.total, cudaMemcpyHostToDevice));
+  }
+  // ---- stage 1 plan: C1[r_pad, a0'] = sum S1A[r_pad, a0] LPS[a0', a0] ----
+  tc::TcPlan& p1 = S->p1;
+  std::map<std::pair<int, int>, int32_t> amap1;
+  for (auto& kv : s1a_chunk) {
+    int m = kv.first.first, s1 = kv.first.second;
+    int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+    CUtensorMap cm;
+    CMPS_TRY(make_map(S->buf + S->s1a_off, kv.second, A0.sdim[s], S->ncols_pad[m], S->ldS[s], S->s1a_len, &cm));
+    amap1[kv.first] = (int32_t)p1.amaps.size();
+    p1.amaps.push_back(cm);
+  }
+  std::map<std::array<int, 4>, int32_t> bmap1;
+  for (size_t i = 0; i < lpsb.size(); ++i) {
+    const SplitBlock& b = lpsb[i];
+    CUtensorMap cm;
+    CMPS_TRY(make_map(S->buf + S->lps_off, b.dst_off, b.cols, b.rows, b.ld_dst, S->lps_len, &cm));
+    p1.bmaps.push_back(cm);
+  }
+  {
+    int32_t i = 0;
+    for (auto& kv : lps_blk) bmap1[kv.first] = i++;  // same order as lpsb (both follow lp_off order)
+  }
+  for (int b1 = 0; b1 < H.D; ++b1)
+    for (int m = 0; m < nm; ++m) {
+      const int64_t tb = ts_base[(size_t)b1 * nm + m];
+      if (tb < 0) continue;
+      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      for (int s1p = 0; s1p < d; ++s1p) {
+        if (th.rowoff[mp][s1p] < 0) continue;
+        int sp = A0.find(r.sub(th.mq[mp], H.sigq[s1p]));
+        tc::TcTask task{};
+        task.out_off = tb + th.rowoff[mp][s1p] * S->ncols_pad[m];
+        task.row_stride = 1;
+        task.col_stride = S->ncols_pad[m];
+        task.m = (int32_t)S->ncols_pad[m];
+        task.n = (int32_t)A0.sdim[sp];
+        task.t0 = (int32_t)p1.terms.size();
+        for (int s1 = 0; s1 < d; ++s1) {
+          if (th.rowoff[m][s1] < 0) continue;
+          int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+          auto it = bmap1.find({b1, s1p, s1, s});
+          if (it == bmap1.end()) continue;
+          p1.terms.push_back(tc::TcTerm{amap1[{m, s1}], it->second, 0, (int32_t)A0.sdim[s]});
+        }
+        task.t1 = (int32_t)p1.terms.size();
+        // output range check (four planes of TS)
+        if (task.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(task.n - 1) * task.col_stride >=
+            S->ts_len)
+          return fail(CMPS_ERR_STATE, "stage-1 output outside TS");
+        add_tiles(p1, (int32_t)p1.tasks.size(), task.m, task.n);
+        p1.tasks.push_back(task);
+      }
+    }
+  // ---- stage 2 plan: C2[l', a2'] = sum TS[l', r_pad] RPTS[a2', a2] ----
+  tc::TcPlan& p2 = S->p2;
+  std::vector<int32_t> amap2((size_t)H.D * nm, -1);
+  for (int b1 = 0; b1 < H.D; ++b1)
+    for (int m = 0; m < nm; ++m) {
+      const int64_t tb = ts_base[(size_t)b1 * nm + m];
+      if (tb < 0) continue;
+      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      CUtensorMap cm;
+      CMPS_TRY(make_map(S->buf + S->ts_off, tb, S->ncols_pad[m], th.nrows[mp], S->ncols_pad[m], S->ts_len, &cm));
+      amap2[(size_t)b1 * nm + m] = (int32_t)p2.amaps.size();
+      p2.amaps.push_back(cm);
+    }
+  std::map<std::array<int, 4>, int32_t> bmap2;
+  {
+    int32_t i = 0;
+    for (auto& kv : rpt_blk) {
+      const SplitBlock& b = rptb[i];
+      CUtensorMap cm;
+      // destination layout [a2'][a2]: rows = dim t', K = dim t
+      CMPS_TRY(make_map(S->buf + S->rpt_off, b.dst_off, b.rows, b.cols, b.ld_dst, S->rpt_len, &cm));
+      p2.bmaps.push_back(cm);
+      bmap2[kv.first] = i++;
+    }
+  }
+  for (int mp = 0; mp < nm; ++mp)
+    for (int s2p = 0; s2p < d; ++s2p) {
+      if (th.coloff[mp][s2p] < 0) continue;
+      int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
+      tc::TcTask task{};
+      task.out_off = th.base[mp] + th.coloff[mp][s2p];
+      task.row_stride = th.ncols[mp];
+      task.col_stride = 1;
+      task.m = (int32_t)th.nrows[mp];
+      task.n = (int32_t)A2.sdim[tp];
+      task.t0 = (int32_t)p2.terms.size();
+      for (int b1 = 0; b1 < H.D; ++b1) {
+        int m = th.find(r.sub(th.mq[mp], H.bq[b1]));
+        if (m < 0) continue;
+        const int32_t am = amap2[(size_t)b1 * nm + m];
+        if (am < 0) continue;
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
+          auto it = bmap2.find({b1, s2, s2p, t});
+          if (it == bmap2.end()) continue;
+          p2.terms.push_back(tc::TcTerm{am, it->second, (int32_t)S->coloff_pad[m][s2], (int32_t)A2.sdim[t]});
+        }
+      }
+      task.t1 = (int32_t)p2.terms.size();
+      if (task.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(task.n - 1) * task.col_stride >=
+          th.total)
+        return fail(CMPS_ERR_STATE, "stage-2 output outside theta");
+      add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
+      p2.tasks.push_back(task);
+    }
+  // plan integrity: every term names an existing map, every tile an existing task
+  for (const tc::TcPlan* p : {&p1, &p2}) {
+    for (const tc::TcTerm& tm : p->terms)
+      if (tm.a_map < 0 || tm.a_map >= (int32_t)p->amaps.size() || tm.b_map < 0 ||
+          tm.b_map >= (int32_t)p->bmaps.size() || tm.k < 1 || (tm.a_x0 & 3))
+        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad term");
+    for (const tc::TcTask& t : p->tasks)
+      if (t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)p->terms.size() || t.m < 1 || t.n < 1 || t.out_off < 0)
+        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
+    for (const tc::TcTile& tl : p->tiles)
+      if (tl.task < 0 || tl.task >= (int32_t)p->tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
+  }
+  CMPS_TRY(p1.upload());
+  CMPS_TRY(p2.upload());
+  return CMPS_OK;
+}
+
 int prepare_precision(Heff* h, int precision) {
   if (precision == CMPS_FP64) return CMPS_OK;
-  (void)h;
-  return fail(CMPS_ERR_ARG, "split-TF32 contraction path is not available in this build");
+  if (precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (h->split) return CMPS_OK;
+  int st = build_split(*h);
+  if (st != CMPS_OK) release_split(h);
+  return st;
+}
+
+// theta-space matvec in split precision: FP64 planar in -> FP64 planar out.
+int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
+  SplitState* S = H.split;
+  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
+  const int64_t n = H.th.total;
+  CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
+  int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  if (n > 0) {
+    k_split_theta<<<std::max(grid, 1), 256, 0, st>>>(in.re(), in.im(), S->d_theta_map, n, S->buf + S->s1a_off,
+                                                     S->s1a_len);
+    CMPS_CUDA(cudaGetLastError());
+  }
+  CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st));
+  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st));
+  CMPS_CUDA(cudaMemcpyAsync(S->h_err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  if (*S->h_err) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(*S->h_err) + ")");
+  return CMPS_OK;
+}
+
+int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st) {
+  SplitState* S = H.split;
+  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
+  const int64_t n = H.th.total;
+  if (which == 1) {
+    CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    k_split_theta<<<std::max(grid, 1), 256, 0, st>>>(in.re(), in.im(), S->d_theta_map, n, S->buf + S->s1a_off,
+                                                     S->s1a_len);
+    CMPS_CUDA(cudaGetLastError());
+    return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st);
+  }
+  return tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st);
+}
+
+int split_error(Heff& H) {
+  SplitState* S = H.split;
+  if (!S) return CMPS_OK;
+  int e = 0;
+  CMPS_CUDA(cudaMemcpy(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(e) + ")");
+  return CMPS_OK;
 }
 
 }  // namespace cmps

@@ -1,0 +1,323 @@
+// Split-precision grouped complex GEMM on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, accumulators in TMEM, operands staged by TMA).
+//
+// Every complex operand X is held as four FP32 planes
+//   re_hi, re_lo, im_hi, im_lo   (hi = x rounded to TF32, lo = x - hi rounded to TF32)
+// in one allocation (plane stride P).  A complex product is accumulated as
+//   Re += Ah_r Bh_r + Ah_r Bl_r + Al_r Bh_r - (Ah_i Bh_i + Ah_i Bl_i + Al_i Bh_i)
+//   Im += Ah_r Bh_i + Ah_r Bl_i + Al_r Bh_i +  Ah_i Bh_r + Ah_i Bl_r + Al_i Bh_r
+// i.e. 12 MMAs of 128 x N x 8 per k-step, FP32 accumulation, the minus sign
+// carried by the instruction descriptor's negate-A bit.  Both operands are
+// K-major (C[m,n] = sum_k A[m,k] B[n,k]); each operand block has its own 3-D
+// tensor map (K, rows, 4 planes) and one TMA load brings all four planes of a
+// 128-row x 16-column tile (SWIZZLE_64B).
+//
+// One CTA computes one 128 x N (N <= 128) output tile of one task, whose
+// terms are K-concatenated: warp 0 issues TMA loads into a 3-stage ring,
+// warp 1 issues the MMAs, warps 2-5 drain TMEM and write the output.  Every
+// mbarrier wait is bounded: on time-out the kernel raises an error word,
+// skips the remaining work, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tc_gemm.h"
+
+namespace cmps {
+namespace tc {
+
+constexpr int kThreads = 192;
+constexpr int kStages = 3;
+constexpr int kBN = 128, kBK = 16;
+constexpr int kPlaneTileBytes = 128 * kBK * 4;          // 8 KB: 128 rows x 64 B
+constexpr int kOperandBytes = 4 * kPlaneTileBytes;      // 32 KB: four planes
+constexpr int kStageBytes = 2 * kOperandBytes;          // A + B
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint32_t kTmemCols = 256;                      // Re at col 0, Im at col 128
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait (wall-clock limit): returns false, and raises *err, when the
+// limit is reached or another CTA already raised it.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  const unsigned long long t0 = now_ns();
+  while (!mbar_try(bar, parity)) {
+    if (now_ns() - t0 > kWaitLimitNs) {
+      atomicExch(err, code);
+      return false;
+    }
+    if (*(volatile int*)err) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, SWIZZLE_64B: 64-byte rows, 8-row
+// groups 512 B apart (SBO), version 1.
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;             // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;    // SBO
+  d |= (uint64_t)1 << 46;             // version
+  d |= (uint64_t)4 << 61;             // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: kind::tf32, D f32, A/B tf32, K-major, M = 128.
+__device__ __forceinline__ uint32_t idesc_tf32(int n, bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+tc_split_gemm(const TcTile* __restrict__ tiles, const TcTask* __restrict__ tasks, const TcTerm* __restrict__ terms,
+              const CUtensorMap* __restrict__ amaps, const CUtensorMap* __restrict__ bmaps, float* __restrict__ out32,
+              int64_t out32_plane, double* __restrict__ out64, int64_t out64_plane, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* accum = empty + kStages;
+  uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const TcTile tile = tiles[blockIdx.x];
+  const TcTask task = tasks[tile.task];
+  const int m0 = tile.m0, n0 = tile.n0;
+  const int ntile = min(kBN, task.n - n0);
+  const int nmma = (ntile + 15) & ~15;  // MMA N: multiple of 16 for M = 128
+  // iterations: sum over terms of ceil(k / 16)
+  int iters = 0;
+  for (int t = task.t0; t < task.t1; ++t) iters += (terms[t].k + kBK - 1) / kBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0 && iters > 0) {
+      int t = task.t0, k0 = 0;
+      int issued = 0;
+      for (int it = 0; it < iters; ++it) {
+        const int s = it % kStages;
+        const uint32_t ph = (uint32_t)((it / kStages) & 1);
+        if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) break;
+        const TcTerm tm = terms[t];
+        uint8_t* sa = smem + s * kStageBytes;
+        uint8_t* sb = sa + kOperandBytes;
+        mbar_expect_tx(&full[s], kStageBytes);
+        tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, m0, 0, &full[s]);
+        tma_load_3d(sb, bmaps + tm.b_map, k0, n0, 0, &full[s]);
+        ++issued;
+        k0 += kBK;
+        if (k0 >= tm.k) {
+          k0 = 0;
+          ++t;
+        }
+      }
+      if (issued < iters) {
+        // error path: let the copies already in flight land before exiting
+        for (int it = max(0, issued - kStages); it < issued; ++it) {
+          const unsigned long long t0 = now_ns();
+          while (!mbar_try(&full[it % kStages], (uint32_t)((it / kStages) & 1)) && now_ns() - t0 < kWaitLimitNs) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0 && iters > 0) {
+      const uint32_t id_pos = idesc_tf32(nmma, false), id_neg = idesc_tf32(nmma, true);
+      const uint32_t d_re = tmem, d_im = tmem + 128;
+      bool ok = true;
+      for (int it = 0; it < iters; ++it) {
+        const int s = it % kStages;
+        const uint32_t ph = (uint32_t)((it / kStages) & 1);
+        if (!mbar_wait(&full[s], ph, err, 2)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_u32(smem + s * kStageBytes);
+        const uint32_t b0 = a0 + kOperandBytes;
+#pragma unroll
+        for (int kk = 0; kk < kBK / 8; ++kk) {
+          // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
+          uint64_t A[4], B[4];
+#pragma unroll
+          for (int p = 0; p < 4; ++p) {
+            A[p] = smem_desc_sw64(a0 + p * kPlaneTileBytes + kk * 32);
+            B[p] = smem_desc_sw64(b0 + p * kPlaneTileBytes + kk * 32);
+          }
+          const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+          umma_tf32(d_re, A[0], B[0], id_pos, acc);
+          umma_tf32(d_re, A[0], B[1], id_pos, 1u);
+          umma_tf32(d_re, A[1], B[0], id_pos, 1u);
+          umma_tf32(d_re, A[2], B[2], id_neg, 1u);
+          umma_tf32(d_re, A[2], B[3], id_neg, 1u);
+          umma_tf32(d_re, A[3], B[2], id_neg, 1u);
+          umma_tf32(d_im, A[0], B[2], id_pos, acc);
+          umma_tf32(d_im, A[0], B[3], id_pos, 1u);
+          umma_tf32(d_im, A[1], B[2], id_pos, 1u);
+          umma_tf32(d_im, A[2], B[0], id_pos, 1u);
+          umma_tf32(d_im, A[2], B[1], id_pos, 1u);
+          umma_tf32(d_im, A[3], B[0], id_pos, 1u);
+        }
+        umma_commit(&empty[s]);
+      }
+      (void)ok;
+      umma_commit(accum);
+    }
+  } else {
+    // ---------------- epilogue: warps 2..5 ----------------
+    const int quad = warp & 3;            // TMEM lane quadrant this warp may access
+    const int row = quad * 32 + lane;     // accumulator row within the tile
+    const int gm = m0 + row;
+    int have = iters > 0 ? 1 : 0;
+    if (have) {
+      if (lane == 0) {
+        mbar_wait(accum, 0, err, 3);
+        if (*(volatile int*)err) have = 0;
+      }
+      have = __shfl_sync(0xffffffffu, have, 0);  // warp-uniform: tcgen05.ld is warp-collective
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool row_ok = gm < task.m;
+    for (int c = 0; c < nmma; c += 16) {
+      float vr[16], vi[16];
+      if (have) {
+        const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
+        tmem_ld16(tmem + lane_base + c, vr);
+        tmem_ld16(tmem + lane_base + 128 + c, vi);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
+      }
+      if (!row_ok) continue;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int j = c + i;
+        if (j >= ntile) break;
+        const int64_t o = task.out_off + (int64_t)gm * task.row_stride + (int64_t)(n0 + j) * task.col_stride;
+        if (MODE == 1) {
+          // stage-1 output: split into the four planes stage 2 reads
+          const float hr = tf32_rna(vr[i]), hi = tf32_rna(vi[i]);
+          out32[o] = hr;
+          out32[o + out32_plane] = tf32_rna(vr[i] - hr);
+          out32[o + 2 * out32_plane] = hi;
+          out32[o + 3 * out32_plane] = tf32_rna(vi[i] - hi);
+        } else {
+          out64[o] = (double)vr[i];
+          out64[o + out64_plane] = (double)vi[i];
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+int smem_bytes() { return kSmemBytes; }
+
+int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double* out64, int64_t out64_plane,
+           int* d_err, cudaStream_t st) {
+  if (p.tiles.empty()) return CMPS_OK;
+  if (p.tiles.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many tcgen05 tiles");
+  if (mode == 1) {
+    static bool cfg1 = false;
+    if (!cfg1) {
+      CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+      cfg1 = true;
+    }
+    tc_split_gemm<1><<<(unsigned)p.tiles.size(), kThreads, kSmemBytes, st>>>(
+        p.d_tiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+  } else {
+    static bool cfg2 = false;
+    if (!cfg2) {
+      CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+      cfg2 = true;
+    }
+    tc_split_gemm<2><<<(unsigned)p.tiles.size(), kThreads, kSmemBytes, st>>>(
+        p.d_tiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+  }
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+}  // namespace tc
+}  // namespace cmps

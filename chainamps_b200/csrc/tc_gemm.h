@@ -1,0 +1,51 @@
+// Split-TF32 tcgen05 grouped GEMM (internal).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "internal.h"
+
+namespace cmps {
+namespace tc {
+
+// One output region: element (i, j) of C lands at out_off + i*row_stride + j*col_stride.
+struct TcTask {
+  int64_t out_off;
+  int64_t row_stride, col_stride;
+  int32_t m, n;
+  int32_t t0, t1;
+};
+// One K-concatenated term: A tile at (a_x0 + k, row) of map a_map, B tile at (k, row) of b_map.
+struct TcTerm {
+  int32_t a_map, b_map, a_x0, k;
+};
+struct TcTile {
+  int32_t task, m0, n0, pad;
+};
+
+struct TcPlan {
+  std::vector<TcTask> tasks;
+  std::vector<TcTerm> terms;
+  std::vector<TcTile> tiles;
+  std::vector<CUtensorMap> amaps, bmaps;
+  TcTask* d_tasks = nullptr;
+  TcTerm* d_terms = nullptr;
+  TcTile* d_tiles = nullptr;
+  CUtensorMap* d_amaps = nullptr;
+  CUtensorMap* d_bmaps = nullptr;
+  int upload();
+  void release();
+};
+
+int smem_bytes();
+// mode 1: FP32 split output (four planes, plane stride out32_plane);
+// mode 2: FP64 planar output (re, im; plane stride out64_plane).
+int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double* out64, int64_t out64_plane,
+           int* d_err, cudaStream_t st);
+
+}  // namespace tc
+}  // namespace cmps
