@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--chi", type=int, default=512)
-    p.add_argument("--precision", default="fp64", choices=["fp64", "split_tf32"])
+    p.add_argument("--precision", default="both", choices=["both", "fp64", "split_tf32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -169,89 +169,127 @@ def main():
     from chainamps_b200 import Context, TwoVertexComponents, CMPS_FP64, CMPS_SPLIT_TF32
     wl = workload(a.chi)
     ctx = Context(local)
-    prec = CMPS_FP64 if a.precision == "fp64" else CMPS_SPLIT_TF32
-    h = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=prec)
-    canonical, executed = h.flops()
-    n = h.n
     # a dedicated (non-default) stream: the library launches on exactly this
     # stream, so the CUDA events below bracket the kernels themselves
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     assert stream.cuda_stream != 0
-    x = torch.randn(n, dtype=torch.complex128, device="cuda")
-    y = torch.empty_like(x)
-    for _ in range(max(3, a.warmup)):
-        h.multiply_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
-    torch.cuda.synchronize()
-    stop = threading.Event()
-    clk = []
-    th = threading.Thread(target=clocks_sampler, args=(stop, clk), daemon=True)
-    th.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(a.steps):
-        h.multiply_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.steps
-    if dist:
-        dist.barrier()
-    stop.set()
-    th.join(timeout=5)
-    # per-stage times (same stream, CUDA events)
-    st = h.time_stages(x.data_ptr(), y.data_ptr(), stream.cuda_stream, reps=3)
-    # end to end through the C ABI with host buffers
-    xh = torch.randn(n, dtype=torch.complex128).pin_memory().numpy()
-    yh = torch.empty(n, dtype=torch.complex128).pin_memory().numpy()
-    h.multiply(xh, out=yh)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_steps = max(3, a.steps // 2)
-    for _ in range(e2e_steps):
+
+    def measure(h, steps, warm):
+        n = h.n
+        x = torch.randn(n, dtype=torch.complex128, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(max(3, warm)):
+            h.multiply_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        h.status()
+        stop = threading.Event()
+        clk = []
+        th = threading.Thread(target=clocks_sampler, args=(stop, clk), daemon=True)
+        th.start()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            h.multiply_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            dist.barrier()
+        stop.set()
+        th.join(timeout=5)
+        h.status()
+        st = h.time_stages(x.data_ptr(), y.data_ptr(), stream.cuda_stream, reps=3)
+        ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist:
+            dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        return float(ms_t.item()), st, summarize_clocks(clk)
+
+    def e2e(h, steps):
+        n = h.n
+        xh = torch.randn(n, dtype=torch.complex128).pin_memory().numpy()
+        yh = torch.empty(n, dtype=torch.complex128).pin_memory().numpy()
         h.multiply(xh, out=yh)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    # FP64 library GEMM ceiling on this GPU (cuBLAS zgemm via torch)
-    A = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
-    B = torch.randn(4096, 4096, dtype=torch.complex128, device="cuda")
-    for _ in range(2):
-        A @ B
-    torch.cuda.synchronize()
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
-    g0.record()
-    for _ in range(5):
-        A @ B
-    g1.record()
-    torch.cuda.synchronize()
-    zgemm_tflops = 8 * 4096 ** 3 * 5 / (g0.elapsed_time(g1) * 1e-3) / 1e12
-    del A, B
-    ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = canonical * world / (ms_max * 1e-3) / 1e12
-    gemm_ms = st[1] + st[2]
-    achieved = canonical / (gemm_ms * 1e-3) / 1e12
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            h.multiply(xh, out=yh)
+        return (time.perf_counter() - t0) / steps
+
+    def gemm_peak(dtype, nn=8192, reps=5):
+        A = torch.randn(nn, nn, dtype=dtype, device="cuda")
+        B = torch.randn(nn, nn, dtype=dtype, device="cuda")
+        for _ in range(2):
+            A @ B
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(reps):
+            A @ B
+        g1.record()
+        torch.cuda.synchronize()
+        f = (8 if dtype.is_complex else 2) * nn ** 3 * reps
+        return f / (g0.elapsed_time(g1) * 1e-3) / 1e12
+
+    want = ["fp64", "split_tf32"] if a.precision == "both" else [a.precision]
+    res = {}
+    canonical = executed = n = None
+    for p in want:
+        prec = CMPS_FP64 if p == "fp64" else CMPS_SPLIT_TF32
+        h = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=prec)
+        canonical, executed = h.flops()
+        n = h.n
+        ms, st, clk = measure(h, a.steps, a.warmup)
+        e2e_s = e2e(h, max(3, a.steps // 2))
+        res[p] = dict(ms=ms, st=st, clk=clk, e2e_s=e2e_s)
+        del h
+        torch.cuda.empty_cache()
+    zgemm = gemm_peak(torch.complex128, 4096)
+    torch.backends.cuda.matmul.allow_tf32 = True
+    tf32 = gemm_peak(torch.float32, 8192)
+    head = "split_tf32" if "split_tf32" in res else "fp64"
+    r = res[head]
+    gemm_ms = r["st"][1] + r["st"][2]
+    if head == "fp64":
+        ach = canonical / (gemm_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": zgemm, "unit": "TFLOP/s", "frac": ach / zgemm,
+                "traffic": None, "kernel": "zgemm_grouped_fp64 (stage 1 + stage 2)",
+                "peak_source": "live cuBLAS complex128 GEMM 4096^3 on this GPU (FP64 DMMA); MEASURED_PEAKS.json "
+                               "holds only bf16/HBM",
+                "achieved_is": "canonical complex flops / stage time"}
+    else:
+        ach = 3.0 * executed / (gemm_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": tf32, "unit": "TFLOP/s", "frac": ach / tf32,
+                "traffic": None, "kernel": "tc_split_gemm<1> + tc_split_gemm<2> (tcgen05 kind::tf32)",
+                "peak_source": "live cuBLAS TF32 GEMM 8192^3 on this GPU; MEASURED_PEAKS.json holds only bf16/HBM",
+                "achieved_is": "TF32 tensor flops issued by the 3-term split (3 x 8 flops per complex MAC) / "
+                               "stage time; canonical complex rate in `value`"}
+    roof["stage_ms"] = {"gather": r["st"][0], "stage1": r["st"][1], "stage2": r["st"][2], "scatter": r["st"][3]}
+    roof["flops_canonical"] = canonical
+    roof["flops_executed_complex"] = executed
+    value = canonical * world / (r["ms"] * 1e-3) / 1e12
     line = {"metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": a.steps,
-            "warmup": max(3, a.warmup), "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "complex128" if prec == CMPS_FP64 else "split-tf32/fp32-acc",
+            "warmup": max(3, a.warmup), "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "complex128" if head == "fp64" else "split-tf32 x3, fp32 accumulate",
             "data": "synthetic", "config": cfg,
-            "e2e": {"value": canonical / e2e_s / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n,
-                    "d2h_bytes_per_step": 16 * n, "ms_per_step": e2e_s * 1e3},
-            "gpu_launches": 4 * a.steps,
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": zgemm_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / zgemm_tflops, "traffic": None,
-                         "peak_source": "live cuBLAS complex128 GEMM 4096^3 on this GPU (FP64 DMMA path); "
-                                        "MEASURED_PEAKS.json holds only bf16/HBM",
-                         "kernel": "zgemm_grouped_fp64 (stage 1 + stage 2)",
-                         "stage_ms": {"gather": st[0], "stage1": st[1], "stage2": st[2], "scatter": st[3]},
-                         "flops_canonical": canonical, "flops_executed": executed,
-                         "executed_tflops": executed / (gemm_ms * 1e-3) / 1e12},
-            "n_allowed": n, "clocks": summarize_clocks(clk)}
+            "e2e": {"value": canonical / r["e2e_s"] / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 16 * n, "ms_per_step": r["e2e_s"] * 1e3},
+            "gpu_launches": (5 if head == "split_tf32" else 4) * a.steps,
+            "roofline": roof, "n_allowed": n, "clocks": r["clk"],
+            "peaks_measured_live": {"cublas_zgemm_tflops": zgemm, "cublas_tf32_tflops": tf32}}
+    if "fp64" in res and head != "fp64":
+        f = res["fp64"]
+        line["fp64_form"] = {"value": canonical / (f["ms"] * 1e-3) / 1e12, "ms_per_step": f["ms"],
+                             "e2e_ms_per_step": f["e2e_s"] * 1e3,
+                             "stage_ms": {"gather": f["st"][0], "stage1": f["st"][1], "stage2": f["st"][2],
+                                          "scatter": f["st"][3]},
+                             "roofline_frac_vs_zgemm": canonical / ((f["st"][1] + f["st"][2]) * 1e-3) / 1e12 / zgemm}
+        line["speedup_mixed_vs_fp64"] = f["ms"] / r["ms"]
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t, setup, cores, _ = cpu_port(wl, 1)
         line["cpu_baseline"] = {"value": canonical / t / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
@@ -259,7 +297,6 @@ def main():
                                 "seconds": t}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del h
     ctx.close()
     if dist:
         dist.destroy_process_group()

@@ -84,6 +84,7 @@ _SIGS = {
     "cmps_heff_apply_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_time_stages": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, c_dblp]),
     "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_heff_status": (C.c_int, [C.c_void_p]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
                                  C.POINTER(C.c_int)]),
     "cmps_heff_set_theta": (C.c_int, [C.c_void_p, c_dblp]),
@@ -97,6 +98,12 @@ _SIGS = {
     "cmps_block_destroy": (C.c_int, [C.c_void_p]),
     "cmps_block_info": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_i64p]),
     "cmps_block_copy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int16), c_i64p, c_i64p, c_dblp]),
+    "cmps_dmrg_create": (C.c_int, [C.c_void_p, C.POINTER(ChargeRules), C.POINTER(MpxDesc), C.POINTER(C.c_int16),
+                                   C.c_int, C.POINTER(C.c_void_p)]),
+    "cmps_dmrg_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_dmrg_set_solver": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
+    "cmps_dmrg_grow": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
+    "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -257,6 +264,10 @@ class TwoVertexComponents:
         _check(lib.cmps_heff_flops(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def status(self):
+        """Raise if a device kernel recorded an asynchronous failure."""
+        _check(lib.cmps_heff_status(self.h))
+
     def set_precision(self, p):
         _check(lib.cmps_heff_set_precision(self.h, p))
 
@@ -361,6 +372,55 @@ class Block:
     def close(self):
         if getattr(self, "h", None):
             lib.cmps_block_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class iDMRG:
+    """Device-resident iDMRG growth (SuperBlock::grow_two_vertex,
+    DMRG_routines.cpp:346-374; iDMRG::run, iDMRG_routines.cpp:19-33)."""
+
+    def __init__(self, ctx: Context, rules, W: MPXTensor, target=None, precision=CMPS_FP64, tol=1e-10,
+                 max_restarts=50, krylov_dim=24):
+        self.ctx = ctx
+        cr, self._r = _rules(rules)
+        dw, kw = W._desc()
+        t = None
+        if target is not None:
+            self._t = np.ascontiguousarray(np.asarray(target, np.int16))
+            t = _p(self._t, C.c_int16)
+        h = C.c_void_p()
+        _check(lib.cmps_dmrg_create(ctx.h, C.byref(cr), C.byref(dw), t, precision, C.byref(h)))
+        self.h = h
+        _check(lib.cmps_dmrg_set_solver(h, tol, max_restarts, krylov_dim))
+        self.last = None
+
+    def grow(self, chi=0, max_trunc=0.0):
+        """One step; returns dict(energy, energy_per, entropy, truncation,
+        fidelity, chi, matvecs, ms=[env, eigensolve, svd, total])."""
+        row = np.zeros(5, np.float64)
+        bd = C.c_int64()
+        mv = C.c_int()
+        ms = np.zeros(4, np.float64)
+        _check(lib.cmps_dmrg_grow(self.h, chi, max_trunc, _p(row, C.c_double), C.byref(bd), C.byref(mv),
+                                  _p(ms, C.c_double)))
+        self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
+                         chi=bd.value, matvecs=mv.value, ms=ms)
+        return self.last
+
+    def values(self):
+        v = np.zeros(self.last["chi"], np.float64)
+        _check(lib.cmps_dmrg_values(self.h, _p(v, C.c_double)))
+        return v
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.cmps_dmrg_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -189,7 +189,16 @@ int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void*
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  if (status == CMPS_OK) status = split_error(H);
   return status;
+}
+
+int cmps_heff_status(cmps_heff* h) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  CMPS_TRY(use_device(h->impl->ctx));
+  CMPS_CUDA(cudaStreamSynchronize(h->impl->ctx->stream));
+  CMPS_CUDA(cudaDeviceSynchronize());
+  return split_error(*h->impl);
 }
 
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {

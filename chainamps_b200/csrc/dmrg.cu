@@ -1,0 +1,382 @@
+// Device-resident iDMRG growth (SuperBlock::grow_two_vertex,
+// DMRG_routines.cpp:346-374): every step builds the new environments from the
+// previous step's H_eff and SVD on the device (MakeLeftBlock / MakeRightBlock,
+// :594-611), forms the new H_eff, predicts its start vector on the device
+// (MakePrediction, :693-707), solves for the ground state and truncates.
+// Nothing but scalars and singular values crosses to the host.
+//
+// Prediction: with U, s, V^dagger of the last step and lambda_prev of the one
+// before, the guess for the next two-vertex wavefunction is
+//   G(s1''=s2, k, s2''=s1, new) = s_k s_new sum_j V^dagger[k,(s2,j)] U[(s1,j),new] / lambda_prev[j]
+// (the contraction of ALambdaR, the inverse previous lambda and LambdaLB in
+// MakePrediction), computed as one grouped FP64 GEMM into the new theta blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "heff.h"
+
+namespace cmps {
+
+namespace {
+
+// out[r, c] = in[r, c] * rs[r] * cs[c] over one row-major block
+__global__ void k_scale_block(const double* __restrict__ ir, const double* __restrict__ ii, int64_t rows, int64_t cols,
+                              const double* __restrict__ rs, const double* __restrict__ cs, double* __restrict__ orr,
+                              double* __restrict__ oi) {
+  const int64_t n = rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / cols, c = e % cols;
+    const double f = (rs ? rs[r] : 1.0) * (cs ? cs[c] : 1.0);
+    orr[e] = ir[e] * f;
+    oi[e] = ii[e] * f;
+  }
+}
+
+int grid_n(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+double entropy_of(const std::vector<double>& v) {
+  double s = 0.0;
+  for (double x : v)
+    if (x != 0.0) s -= x * x * std::log(x * x);
+  return s;
+}
+
+}  // namespace
+
+struct Dmrg {
+  cmps_context* ctx = nullptr;
+  Rules rules;
+  int precision = CMPS_FP64;
+  // deep copy of the MPO descriptor
+  std::vector<uint8_t> w_in, w_ph;
+  std::vector<int64_t> w_sz, w_cp, w_ri;
+  std::vector<int16_t> w_ch;
+  std::vector<double> w_val;
+  cmps_mpx_desc W{};
+  QKey target{};
+  int D = 0;
+  std::vector<QKey> bq;
+  int64_t size = 0;
+  std::unique_ptr<Heff> heff;
+  std::unique_ptr<SvdResult> svd;
+  std::vector<double> lambda, prev_lambda;
+  double tol = 1e-10;
+  int restarts = 50, kdim = 24;
+  int last_matvecs = 0;
+  double last_ms[4] = {0, 0, 0, 0};  // env update, eigensolve, svd, total
+
+  ~Dmrg() {
+    if (svd) {
+      svd->U.release();
+      svd->Vd.release();
+    }
+  }
+  int dummy_blocks(Env& L, Env& R);
+  int predict(Heff& next, bool* ok);
+  int grow(int64_t chi, double trunc, double* out);
+};
+
+int Dmrg::dummy_blocks(Env& L, Env& R) {
+  // MakeDummyLeftBlock / MakeDummyRightBlock (DMRG_routines.cpp:613-653)
+  const int nq = rules.nq;
+  auto build = [&](bool right, Env& e) -> int {
+    std::vector<uint8_t> in(6), ph(6, 0);
+    std::vector<int64_t> sz(6, 1);
+    std::vector<int16_t> ch;
+    int ib = right ? 2 : 3;
+    sz[ib] = D;
+    if (!right) in = {0, 1, 1, 0, 1, 0};
+    else in = {0, 1, 1, 0, 1, 0};
+    for (int i = 0; i < 6; ++i) {
+      for (int64_t k = 0; k < sz[i]; ++k)
+        for (int c = 0; c < nq; ++c) {
+          int16_t v = 0;
+          if (i == ib) v = bq[k][c];
+          else if (right && (i == 0 || i == 4)) v = target[c];
+          ch.push_back(v);
+        }
+    }
+    std::vector<int64_t> cp = {0, 1}, ri = {right ? 0 : (int64_t)(D - 1)};
+    std::vector<double> val = {1.0, 0.0};
+    cmps_mpx_desc d{6, right ? 3 : 4, in.data(), ph.data(), sz.data(), ch.data(), (int64_t)D, 1,
+                    cp.data(), ri.data(), val.data()};
+    return build_env_from_desc(rules, &d, right, e, D, bq);
+  };
+  CMPS_TRY(build(false, L));
+  CMPS_TRY(build(true, R));
+  return CMPS_OK;
+}
+
+// Fill next.x with the prediction; *ok = false when it does not apply.
+int Dmrg::predict(Heff& next, bool* ok) {
+  *ok = false;
+  if (!svd || prev_lambda.empty()) return CMPS_OK;
+  const SvdResult& S = *svd;
+  if (S.a0.element_charges() != S.a2.element_charges()) return CMPS_OK;  // pairing by position needs equal bonds
+  if ((int64_t)prev_lambda.size() != S.a0.size()) return CMPS_OK;
+  cudaStream_t st = ctx->stream;
+  const ThetaSpace& to = S.th;       // previous theta space
+  const ThetaSpace& tn = next.th;    // next theta space
+  const int nmo = (int)to.mq.size();
+  const int d = next.d;
+  // scaled factors: Vs = diag(s) Vd ; Us = diag(1/lambda_prev) U diag(s)
+  Planar Us, Vs;
+  CMPS_TRY(Us.alloc(std::max<int64_t>(1, S.U.len)));
+  CMPS_TRY(Vs.alloc(std::max<int64_t>(1, S.Vd.len)));
+  std::vector<double> rs, cs;
+  double* d_scale = nullptr;
+  int status = CMPS_OK;
+  for (int m = 0; m < nmo && status == CMPS_OK; ++m) {
+    const int64_t k = S.kept[m];
+    if (!k) continue;
+    std::vector<double> colsc(k), urow(to.nrows[m], 0.0);
+    for (int64_t j = 0; j < k; ++j) colsc[j] = lambda[S.gidx[m][j]];
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (to.rowoff[m][s1] < 0) continue;
+      int sa = S.a0.find(S.rules.sub(to.mq[m], S.sigq[s1]));
+      for (int64_t p = 0; p < S.a0.sdim[sa]; ++p) {
+        const double lp = prev_lambda[S.a0.selem[sa][p]];
+        urow[to.rowoff[m][s1] + p] = lp != 0.0 ? 1.0 / lp : 0.0;
+      }
+    }
+    const size_t nb = urow.size() + 2 * colsc.size();
+    std::vector<double> hostbuf;
+    hostbuf.insert(hostbuf.end(), urow.begin(), urow.end());
+    hostbuf.insert(hostbuf.end(), colsc.begin(), colsc.end());
+    hostbuf.insert(hostbuf.end(), colsc.begin(), colsc.end());
+    if (cudaMalloc(&d_scale, sizeof(double) * nb) != cudaSuccess) {
+      status = fail(CMPS_ERR_NOMEM, "prediction scale allocation failed");
+      break;
+    }
+    cudaMemcpy(d_scale, hostbuf.data(), sizeof(double) * nb, cudaMemcpyHostToDevice);
+    const double* d_urow = d_scale;
+    const double* d_ucol = d_scale + urow.size();
+    const double* d_vrow = d_ucol + k;
+    k_scale_block<<<grid_n(to.nrows[m] * k), 256, 0, st>>>(S.U.re() + S.uoff[m], S.U.im() + S.uoff[m], to.nrows[m],
+                                                          k, d_urow, d_ucol, Us.re() + S.uoff[m],
+                                                          Us.im() + S.uoff[m]);
+    k_scale_block<<<grid_n(k * to.ncols[m]), 256, 0, st>>>(S.Vd.re() + S.voff[m], S.Vd.im() + S.voff[m], k,
+                                                          to.ncols[m], d_vrow, nullptr, Vs.re() + S.voff[m],
+                                                          Vs.im() + S.voff[m]);
+    cudaStreamSynchronize(st);
+    cudaFree(d_scale);
+    d_scale = nullptr;
+  }
+  // grouped GEMM plan into the next theta blocks
+  GemmPlan p;
+  if (status == CMPS_OK) {
+    for (int mn = 0; mn < (int)tn.mq.size(); ++mn)
+      for (int a = 0; a < d; ++a) {            // sigma1'' = old sigma2
+        if (tn.rowoff[mn][a] < 0) continue;
+        const int mk = to.find(next.rules.sub(tn.mq[mn], next.sigq[a]));
+        if (mk < 0 || !S.kept[mk] || to.coloff[mk][a] < 0) continue;
+        for (int b = 0; b < d; ++b) {          // sigma2'' = old sigma1
+          if (tn.coloff[mn][b] < 0) continue;
+          const int mw = to.find(next.rules.add(tn.mq[mn], next.sigq[b]));
+          if (mw < 0 || !S.kept[mw] || to.rowoff[mw][b] < 0) continue;
+          const int t = S.a2.find(S.rules.add(to.mq[mk], S.sigq[a]));
+          const int s = S.a0.find(S.rules.sub(to.mq[mw], S.sigq[b]));
+          if (t < 0 || s < 0 || S.a2.sdim[t] != S.a0.sdim[s]) continue;
+          // the next theta's row chunk must be exactly the kept states of block mk (and columns of mw)
+          const int sr = next.L.a.find(to.mq[mk]);
+          const int sc = next.R.a.find(to.mq[mw]);
+          if (sr < 0 || sc < 0 || next.L.a.sdim[sr] != S.kept[mk] || next.R.a.sdim[sc] != S.kept[mw]) continue;
+          GemmTask task{};
+          task.c_off = tn.base[mn] + tn.rowoff[mn][a] * tn.ncols[mn] + tn.coloff[mn][b];
+          task.m = (int32_t)S.kept[mk];
+          task.n = (int32_t)S.kept[mw];
+          task.ldc = (int32_t)tn.ncols[mn];
+          task.t0 = (int32_t)p.terms.size();
+          GemmTerm tm{};
+          tm.a_off = S.voff[mk] + to.coloff[mk][a];
+          tm.lda = (int32_t)to.ncols[mk];
+          tm.k = (int32_t)S.a2.sdim[t];
+          tm.b_off = S.uoff[mw] + to.rowoff[mw][b] * S.kept[mw];
+          tm.ldb = (int32_t)S.kept[mw];
+          p.terms.push_back(tm);
+          task.t1 = (int32_t)p.terms.size();
+          p.tasks.push_back(task);
+        }
+      }
+    if (!p.tasks.empty()) {
+      status = p.validate(false, false, Vs.len, Us.len, tn.total, "prediction");
+      if (status == CMPS_OK) status = p.upload(64, 64);
+      if (status == CMPS_OK) {
+        cudaMemsetAsync(next.x.d, 0, sizeof(double) * 2 * tn.total, st);
+        status = launch_zgemm_fp64(p, false, false, Vs, Us, next.x, st);
+      }
+      if (status == CMPS_OK && cudaStreamSynchronize(st) != cudaSuccess)
+        status = fail(CMPS_ERR_CUDA, "prediction GEMM failed");
+      if (status == CMPS_OK) *ok = true;
+    }
+  }
+  p.release();
+  Us.release();
+  Vs.release();
+  return status;
+}
+
+int Dmrg::grow(int64_t chi, double trunc, double* out) {
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));
+  cudaEventRecord(ev[0], st);
+  Env L, R;
+  if (size == 0) {
+    CMPS_TRY(dummy_blocks(L, R));
+  } else {
+    CMPS_TRY(left_update(*heff, *svd, L));
+    CMPS_TRY(right_update(*heff, *svd, R));
+  }
+  auto next = std::unique_ptr<Heff>(new Heff());
+  next->ctx = ctx;
+  next->rules = rules;
+  CMPS_TRY(next->parse_mpo(&W));
+  next->L = L;   // ownership of the device blocks moves to `next`
+  next->R = R;
+  CMPS_TRY(next->finish());
+  CMPS_TRY(prepare_precision(next.get(), precision));
+  next->precision = precision;
+  bool have_guess = false;
+  CMPS_TRY(predict(*next, &have_guess));
+  // the previous step's factors and H_eff are no longer needed
+  if (svd) {
+    svd->U.release();
+    svd->Vd.release();
+    svd.reset();
+  }
+  heff = std::move(next);
+  cudaEventRecord(ev[1], st);
+  double e = 0.0;
+  int nmv = 0;
+  int rc = heff->eigs(nullptr, tol, restarts, kdim, &e, nullptr, &nmv, have_guess);
+  if (rc != CMPS_OK && rc != CMPS_ERR_SOLVER) return rc;
+  last_matvecs = nmv;
+  cudaEventRecord(ev[2], st);
+  svd.reset(new SvdResult());
+  CMPS_TRY(theta_svd(*heff, chi, trunc, *svd));
+  cudaEventRecord(ev[3], st);
+  cudaEventSynchronize(ev[3]);
+  float t01 = 0, t12 = 0, t23 = 0;
+  cudaEventElapsedTime(&t01, ev[0], ev[1]);
+  cudaEventElapsedTime(&t12, ev[1], ev[2]);
+  cudaEventElapsedTime(&t23, ev[2], ev[3]);
+  last_ms[0] = t01;
+  last_ms[1] = t12;
+  last_ms[2] = t23;
+  last_ms[3] = t01 + t12 + t23;
+  for (auto& ee : ev) cudaEventDestroy(ee);
+  // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
+  std::vector<double> v = svd->values;
+  double sq = 0.0;
+  for (double x : v) sq += x * x;
+  if (!(sq > 0.0)) return fail(CMPS_ERR_SOLVER, "square sum error: no weight kept");
+  const double f = std::sqrt(1.0 / sq);
+  for (double& x : v) x *= f;
+  prev_lambda = size == 0 ? std::vector<double>(1, 1.0) : lambda;
+  lambda = v;
+  size += 2;
+  out[0] = e;
+  out[1] = e / (double)size;
+  out[2] = entropy_of(lambda);
+  out[3] = svd->discarded;
+  out[4] = std::nan("");
+  return rc;
+}
+
+}  // namespace cmps
+
+struct cmps_dmrg {
+  std::unique_ptr<cmps::Dmrg> impl;
+};
+
+using namespace cmps;
+
+extern "C" {
+
+int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cmps_mpx_desc* W,
+                     const int16_t* target, int precision, cmps_dmrg** out) {
+  if (!ctx || !rules || !W || !out) return fail(CMPS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  CMPS_CUDA(cudaSetDevice(ctx->device));
+  auto d = std::unique_ptr<cmps_dmrg>(new cmps_dmrg());
+  d->impl.reset(new Dmrg());
+  Dmrg& D = *d->impl;
+  D.ctx = ctx;
+  if (rules->nq < 1 || rules->nq > kMaxQ) return fail(CMPS_ERR_ARG, "charge rules: bad count");
+  D.rules.nq = rules->nq;
+  for (int i = 0; i < rules->nq; ++i) D.rules.n[i] = rules->rules[i];
+  D.precision = precision;
+  // deep copy of W
+  const int k = W->num_indices;
+  if (k != 4) return fail(CMPS_ERR_ARG, "MPO: expected 4 indices");
+  D.w_in.assign(W->inward, W->inward + k);
+  D.w_ph.assign(W->physical, W->physical + k);
+  D.w_sz.assign(W->sizes, W->sizes + k);
+  int64_t nch = 0;
+  for (int i = 0; i < k; ++i) nch += W->sizes[i];
+  D.w_ch.assign(W->charges, W->charges + nch * rules->nq);
+  D.w_cp.assign(W->colptr, W->colptr + W->cols + 1);
+  const int64_t nnz = W->colptr[W->cols];
+  D.w_ri.assign(W->rowind, W->rowind + nnz);
+  D.w_val.assign(W->values, W->values + 2 * nnz);
+  if (D.w_ri.empty()) {
+    D.w_ri.push_back(0);
+    D.w_val.push_back(0.0);
+    D.w_val.push_back(0.0);
+  }
+  D.W = cmps_mpx_desc{4, W->num_row_indices, D.w_in.data(), D.w_ph.data(), D.w_sz.data(), D.w_ch.data(),
+                      W->rows, W->cols, D.w_cp.data(), D.w_ri.data(), D.w_val.data()};
+  Heff probe;
+  probe.rules = D.rules;
+  CMPS_TRY(probe.parse_mpo(&D.W));
+  D.D = probe.D;
+  D.bq = probe.bq;
+  for (int c = 0; c < rules->nq; ++c) {
+    int v = target ? target[c] : 0;
+    if (D.rules.n[c] > 0) v = ((v % D.rules.n[c]) + D.rules.n[c]) % D.rules.n[c];
+    D.target[c] = (int16_t)v;
+  }
+  *out = d.release();
+  return CMPS_OK;
+}
+
+int cmps_dmrg_destroy(cmps_dmrg* d) {
+  if (d && d->impl && d->impl->ctx) cudaSetDevice(d->impl->ctx->device);
+  delete d;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_set_solver(cmps_dmrg* d, double tol, int max_restarts, int krylov_dim) {
+  if (!d || !d->impl || !(tol > 0.0)) return fail(CMPS_ERR_ARG, "bad argument");
+  d->impl->tol = tol;
+  d->impl->restarts = max_restarts;
+  d->impl->kdim = krylov_dim;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
+                   double* ms4) {
+  if (!d || !d->impl || !row5) return fail(CMPS_ERR_ARG, "null argument");
+  Dmrg& D = *d->impl;
+  CMPS_CUDA(cudaSetDevice(D.ctx->device));
+  int rc = D.grow(chi, max_trunc, row5);
+  if (bond_dim) *bond_dim = (int64_t)D.lambda.size();
+  if (matvecs) *matvecs = D.last_matvecs;
+  if (ms4)
+    for (int i = 0; i < 4; ++i) ms4[i] = D.last_ms[i];
+  return rc;
+}
+
+int cmps_dmrg_values(const cmps_dmrg* d, double* values) {
+  if (!d || !d->impl || !values) return fail(CMPS_ERR_ARG, "null argument");
+  std::memcpy(values, d->impl->lambda.data(), sizeof(double) * d->impl->lambda.size());
+  return CMPS_OK;
+}
+
+}  // extern "C"

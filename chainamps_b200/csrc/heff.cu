@@ -706,7 +706,7 @@ static void jacobi_lowest(int n, const std::vector<double>& Ain, double* lam, st
 // Lanczos with full re-orthogonalisation (classical Gram-Schmidt, twice)
 // and explicit restarts from the Ritz vector.
 int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, double* eval, double* evec,
-               int* matvecs) {
+               int* matvecs, bool start_in_x) {
   cudaStream_t st = ctx->stream;
   const int64_t n = th.total;
   if (n == 0) return fail(CMPS_ERR_STATE, "empty effective Hamiltonian");
@@ -725,8 +725,9 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
     CMPS_TRY(launch_pack(d_io, d_pos, n_allowed, x, st));
   }
   double nrm = 0.0;
-  if (guess) CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
-  if (!guess || !(nrm > 1e-300)) {
+  const bool have_start = guess || start_in_x;
+  if (have_start) CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
+  if (!have_start || !(nrm > 1e-300)) {
     CMPS_TRY(ops.random(x.re(), x.im(), 0x5eed1234ULL, st));
     CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
   }

@@ -87,9 +87,30 @@ struct Heff {
   int apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st);  // 1: T = LP in, 2: out = T RP
   int apply_host(const double* in, double* out);
   int apply_device(const double* din, double* dout, cudaStream_t st);
+  // start_in_x: the start vector is already in x (theta layout, device)
   int eigs(const double* guess, double tol, int max_restarts, int kdim, double* eval, double* evec,
-           int* matvecs);
+           int* matvecs, bool start_in_x = false);
 };
+
+// Result of the charge-block SVD of theta (svd.cu).
+struct SvdResult {
+  Rules rules;
+  int d = 0;
+  std::vector<QKey> sigq;
+  Bond a0, a2;
+  ThetaSpace th;
+  std::vector<int64_t> kept;            // per m
+  std::vector<int64_t> uoff, voff;      // per m, offsets into U / Vd
+  Planar U, Vd;                         // U_m: nrows[m] x kept[m]; Vd_m: kept[m] x ncols[m] (row-major)
+  std::vector<double> values;           // kept, global descending order
+  std::vector<std::pair<int, int64_t>> order;  // global index -> (m, j)
+  std::vector<std::vector<int64_t>> gidx;      // [m][j] -> global index
+  double discarded = 0.0;
+};
+
+int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out);
+int left_update(Heff& H, const SvdResult& s, Env& out);
+int right_update(Heff& H, const SvdResult& s, Env& out);
 
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);

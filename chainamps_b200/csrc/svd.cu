@@ -27,21 +27,6 @@
 
 namespace cmps {
 
-struct SvdResult {
-  Rules rules;
-  int d = 0;
-  std::vector<QKey> sigq;
-  Bond a0, a2;
-  ThetaSpace th;
-  std::vector<int64_t> kept;            // per m
-  std::vector<int64_t> uoff, voff;      // per m, offsets into U / Vd
-  Planar U, Vd;                         // U_m: nrows[m] x kept[m]; Vd_m: kept[m] x ncols[m] (row-major)
-  std::vector<double> values;           // kept, global descending order
-  std::vector<std::pair<int, int64_t>> order;  // global index -> (m, j)
-  std::vector<std::vector<int64_t>> gidx;      // [m][j] -> global index
-  double discarded = 0.0;
-};
-
 static const double kEps = 2.220446049250313e-16;
 
 void release_solver(cmps_context* ctx) {
@@ -146,7 +131,7 @@ static int64_t truncation_length(const std::vector<double>& sv, int64_t D, doubl
   return length;
 }
 
-static int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
+int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
   if (!H.have_theta) return fail(CMPS_ERR_STATE, "no wavefunction: call cmps_heff_eigs or cmps_heff_set_theta first");
   cudaStream_t st = H.ctx->stream;
   cusolverDnHandle_t sol;
@@ -348,7 +333,7 @@ static int alloc_env(const Rules& r, const Bond& a, int D, const std::vector<QKe
   return CMPS_OK;
 }
 
-static int left_update(Heff& H, const SvdResult& s, Env& out) {
+int left_update(Heff& H, const SvdResult& s, Env& out) {
   const Rules& r = H.rules;
   const ThetaSpace& th = s.th;
   const int nm = (int)th.mq.size();
@@ -446,7 +431,7 @@ static int left_update(Heff& H, const SvdResult& s, Env& out) {
   return status;
 }
 
-static int right_update(Heff& H, const SvdResult& s, Env& out) {
+int right_update(Heff& H, const SvdResult& s, Env& out) {
   const Rules& r = H.rules;
   const ThetaSpace& th = s.th;
   const int nm = (int)th.mq.size();

@@ -135,6 +135,10 @@ int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, double* d_o
  * ms[2] stage-2 grouped GEMM, ms[3] scatter. */
 int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void* stream,
                           int reps, double* ms);
+/* Synchronises the handle's stream and reports any failure the device
+ * kernels recorded asynchronously (a bounded tcgen05 pipeline wait that
+ * timed out); CMPS_OK otherwise. */
+int cmps_heff_status(cmps_heff* h);
 /* Switch the contraction arithmetic of an existing handle (CMPS_FP64 or
  * CMPS_SPLIT_TF32). */
 int cmps_heff_set_precision(cmps_heff* h, int precision);
@@ -185,6 +189,30 @@ int cmps_block_info(const cmps_block* b, int64_t* chi, int64_t* mpo_dim, int64_t
  * matrix: row = a', col = b + mpo_dim * a. */
 int cmps_block_copy(const cmps_block* b, int16_t* a_charges, int64_t* colptr,
                     int64_t* rowind, double* values);
+
+/* ---- device-resident iDMRG growth (SuperBlock) -------------------------
+ * Replaces SuperBlock::grow_two_vertex (DMRG_routines.cpp:346-374) with
+ * everything on the device: the new environments come from the previous
+ * step's H_eff and SVD (MakeLeftBlock / MakeRightBlock), the start vector
+ * from the device form of MakePrediction (:693-707), then the ground state
+ * (cmps_heff_eigs) and the truncated SVD.  The first call solves the two
+ * vertex problem on the dummy end blocks (MakeDummyLeftBlock /
+ * MakeDummyRightBlock, :613-653), as SuperBlock::initialise does (:309-344).
+ * target: the target charges (nq values, NULL = all zero). */
+typedef struct cmps_dmrg cmps_dmrg;
+int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cmps_mpx_desc* W,
+                     const int16_t* target, int precision, cmps_dmrg** out);
+int cmps_dmrg_destroy(cmps_dmrg* d);
+int cmps_dmrg_set_solver(cmps_dmrg* d, double tol, int max_restarts, int krylov_dim);
+/* One growth step.  row5 = {energy, energy / vertices, entropy, truncation,
+ * fidelity (NaN: not computed)} -- the Data row of iDMRG_DRV's energies
+ * file; bond_dim = kept states; matvecs = H_eff applications; ms4 = device
+ * time of {environment update + H_eff build + prediction, eigensolve, SVD,
+ * total} in ms (CUDA events).  Any output pointer but row5 may be NULL. */
+int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim,
+                   int* matvecs, double* ms4);
+/* The current (rescaled) singular values, bond_dim of them, descending. */
+int cmps_dmrg_values(const cmps_dmrg* d, double* values);
 
 #ifdef __cplusplus
 }
