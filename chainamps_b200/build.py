@@ -21,7 +21,7 @@ def nvcc_cmd(out=LIB, extra=()):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     return [os.path.join(CUDA, "bin", "nvcc"), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo",
             "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-            *extra, *srcs, "-o", out, "-L", os.path.join(CUDA, "lib64"), "-lcusolver",
+            *extra, *srcs, "-o", out, "-L", os.path.join(CUDA, "lib64"), "-lcusolver", "-lcublas",
             "-Xlinker", "-rpath=" + os.path.join(CUDA, "lib64")]
 
 

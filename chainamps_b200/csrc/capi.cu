@@ -20,6 +20,20 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+int copy_wait(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  if (!bytes) return CMPS_OK;
+  CMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  return CMPS_OK;
+}
+
+int zero_wait(void* dst, size_t bytes, cudaStream_t st) {
+  if (!bytes) return CMPS_OK;
+  CMPS_CUDA(cudaMemsetAsync(dst, 0, bytes, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  return CMPS_OK;
+}
+
 static int rules_from(const cmps_charge_rules* cr, Rules& r) {
   if (!cr || cr->nq < 1 || cr->nq > kMaxQ || !cr->rules)
     return fail(CMPS_ERR_ARG, "charge rules: need 1.." + std::to_string(kMaxQ) + " charges");
@@ -31,6 +45,7 @@ static int rules_from(const cmps_charge_rules* cr, Rules& r) {
 static int use_device(cmps_context* ctx) {
   if (!ctx) return fail(CMPS_ERR_ARG, "null context");
   CMPS_CUDA(cudaSetDevice(ctx->device));
+  cudaGetLastError();  // drop a stale non-sticky error of an unrelated earlier call
   return CMPS_OK;
 }
 
@@ -123,15 +138,16 @@ int cmps_block_create(cmps_context* ctx, const cmps_charge_rules* rules, const c
   auto b = std::unique_ptr<cmps_block>(new (std::nothrow) cmps_block());
   if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   b->rules = r;
-  CMPS_TRY(build_env_from_desc(r, block, right != 0, b->env, tmp.D, tmp.bq));
+  CMPS_TRY(build_env_from_desc(r, block, right != 0, b->env, tmp.D, tmp.bq, ctx->stream));
   *out = b.release();
   return CMPS_OK;
 }
 
 int cmps_heff_destroy(cmps_heff* h) {
   if (!h) return CMPS_OK;
-  if (h->impl && h->impl->ctx) cudaSetDevice(h->impl->ctx->device);
+  if (h->impl) cudaSetDevice(h->impl->device);
   delete h;
+  cudaGetLastError();
   return CMPS_OK;
 }
 

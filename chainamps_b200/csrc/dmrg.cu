@@ -49,6 +49,7 @@ double entropy_of(const std::vector<double>& v) {
 
 struct Dmrg {
   cmps_context* ctx = nullptr;
+  int device = 0;
   Rules rules;
   int precision = CMPS_FP64;
   // deep copy of the MPO descriptor
@@ -104,7 +105,7 @@ int Dmrg::dummy_blocks(Env& L, Env& R) {
     std::vector<double> val = {1.0, 0.0};
     cmps_mpx_desc d{6, right ? 3 : 4, in.data(), ph.data(), sz.data(), ch.data(), (int64_t)D, 1,
                     cp.data(), ri.data(), val.data()};
-    return build_env_from_desc(rules, &d, right, e, D, bq);
+    return build_env_from_desc(rules, &d, right, e, D, bq, ctx->stream);
   };
   CMPS_TRY(build(false, L));
   CMPS_TRY(build(true, R));
@@ -152,7 +153,8 @@ int Dmrg::predict(Heff& next, bool* ok) {
       status = fail(CMPS_ERR_NOMEM, "prediction scale allocation failed");
       break;
     }
-    cudaMemcpy(d_scale, hostbuf.data(), sizeof(double) * nb, cudaMemcpyHostToDevice);
+    if ((status = copy_wait(d_scale, hostbuf.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, st)) != CMPS_OK)
+      break;
     const double* d_urow = d_scale;
     const double* d_ucol = d_scale + urow.size();
     const double* d_vrow = d_ucol + k;
@@ -204,7 +206,7 @@ int Dmrg::predict(Heff& next, bool* ok) {
       }
     if (!p.tasks.empty()) {
       status = p.validate(false, false, Vs.len, Us.len, tn.total, "prediction");
-      if (status == CMPS_OK) status = p.upload(64, 64);
+      if (status == CMPS_OK) status = p.upload(64, 64, st);
       if (status == CMPS_OK) {
         cudaMemsetAsync(next.x.d, 0, sizeof(double) * 2 * tn.total, st);
         status = launch_zgemm_fp64(p, false, false, Vs, Us, next.x, st);
@@ -234,6 +236,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   }
   auto next = std::unique_ptr<Heff>(new Heff());
   next->ctx = ctx;
+  next->device = ctx->device;
   next->rules = rules;
   CMPS_TRY(next->parse_mpo(&W));
   next->L = L;   // ownership of the device blocks moves to `next`
@@ -308,6 +311,7 @@ int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cm
   d->impl.reset(new Dmrg());
   Dmrg& D = *d->impl;
   D.ctx = ctx;
+  D.device = ctx->device;
   if (rules->nq < 1 || rules->nq > kMaxQ) return fail(CMPS_ERR_ARG, "charge rules: bad count");
   D.rules.nq = rules->nq;
   for (int i = 0; i < rules->nq; ++i) D.rules.n[i] = rules->rules[i];
@@ -347,8 +351,9 @@ int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cm
 }
 
 int cmps_dmrg_destroy(cmps_dmrg* d) {
-  if (d && d->impl && d->impl->ctx) cudaSetDevice(d->impl->ctx->device);
+  if (d && d->impl) cudaSetDevice(d->impl->device);
   delete d;
+  cudaGetLastError();
   return CMPS_OK;
 }
 
@@ -364,7 +369,7 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
                    double* ms4) {
   if (!d || !d->impl || !row5) return fail(CMPS_ERR_ARG, "null argument");
   Dmrg& D = *d->impl;
-  CMPS_CUDA(cudaSetDevice(D.ctx->device));
+  CMPS_CUDA(cudaSetDevice(D.device));
   int rc = D.grow(chi, max_trunc, row5);
   if (bond_dim) *bond_dim = (int64_t)D.lambda.size();
   if (matvecs) *matvecs = D.last_matvecs;

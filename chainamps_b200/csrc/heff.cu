@@ -169,7 +169,7 @@ static void for_each_entry(const cmps_mpx_desc* d, F&& f) {
 // L: a' = 1, b = 3, a = 5.  R: a' = 0, b = 2, a = 4.  Blocks are allocated
 // for every (b, sector) with a charge-consistent partner sector.
 int build_env_from_desc(const Rules& r, const cmps_mpx_desc* d, bool right, Env& env, int D,
-                        const std::vector<QKey>& bq) {
+                        const std::vector<QKey>& bq, cudaStream_t st) {
   const char* what = right ? "right block" : "left block";
   CMPS_TRY(check_desc(d, 6, what));
   const int ia = right ? 4 : 5, iap = right ? 0 : 1, ib = right ? 2 : 3;
@@ -218,7 +218,7 @@ int build_env_from_desc(const Rules& r, const cmps_mpx_desc* d, bool right, Env&
   });
   if (status != CMPS_OK) return status;
   CMPS_TRY(env.data.alloc(total));
-  if (total) CMPS_CUDA(cudaMemcpy(env.data.d, h.data(), sizeof(double) * 2 * total, cudaMemcpyHostToDevice));
+  CMPS_TRY(copy_wait(env.data.d, h.data(), sizeof(double) * 2 * total, cudaMemcpyHostToDevice, st));
   return CMPS_OK;
 }
 
@@ -246,26 +246,26 @@ Heff::~Heff() {
 }
 
 template <typename T>
-static int upload_vec(const std::vector<T>& v, T** d) {
+static int upload_vec(const std::vector<T>& v, T** d, cudaStream_t st) {
   if (*d) cudaFree(*d);
   *d = nullptr;
   if (v.empty()) return CMPS_OK;
   CMPS_CUDA(cudaMalloc((void**)d, sizeof(T) * v.size()));
-  CMPS_CUDA(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
-  return CMPS_OK;
+  return copy_wait(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
 }
 
 int Heff::build(cmps_context* c, const Rules& r, const cmps_mpx_desc* Ld, const cmps_mpx_desc* Wd,
                 const cmps_mpx_desc* Rd) {
   ctx = c;
+  device = c->device;
   rules = r;
   CMPS_TRY(parse_mpo(Wd));
-  CMPS_TRY(build_env_from_desc(r, Ld, false, L, D, bq));
-  CMPS_TRY(build_env_from_desc(r, Rd, true, R, D, bq));
+  CMPS_TRY(build_env_from_desc(r, Ld, false, L, D, bq, c->stream));
+  CMPS_TRY(build_env_from_desc(r, Rd, true, R, D, bq, c->stream));
   return finish();
 }
 
-int copy_env(const Env& src, Env& dst) {
+int copy_env(const Env& src, Env& dst, cudaStream_t st) {
   dst.a = src.a;
   dst.D = src.D;
   dst.bq = src.bq;
@@ -273,21 +273,21 @@ int copy_env(const Env& src, Env& dst) {
   dst.partner = src.partner;
   dst.right = src.right;
   CMPS_TRY(dst.data.alloc(src.data.len));
-  if (src.data.len)
-    CMPS_CUDA(cudaMemcpy(dst.data.d, src.data.d, sizeof(double) * 2 * src.data.len, cudaMemcpyDeviceToDevice));
+  CMPS_TRY(copy_wait(dst.data.d, src.data.d, sizeof(double) * 2 * src.data.len, cudaMemcpyDeviceToDevice, st));
   return CMPS_OK;
 }
 
 int Heff::build_from_envs(cmps_context* c, const Rules& r, const Env& Lsrc, const cmps_mpx_desc* Wd,
                           const Env& Rsrc) {
   ctx = c;
+  device = c->device;
   rules = r;
   CMPS_TRY(parse_mpo(Wd));
   if (Lsrc.right || !Rsrc.right) return fail(CMPS_ERR_ARG, "block handedness: need a left and a right block");
   if (Lsrc.D != D || Rsrc.D != D || Lsrc.bq != bq || Rsrc.bq != bq)
     return fail(CMPS_ERR_ARG, "block MPO index differs from W");
-  CMPS_TRY(copy_env(Lsrc, L));
-  CMPS_TRY(copy_env(Rsrc, R));
+  CMPS_TRY(copy_env(Lsrc, L, c->stream));
+  CMPS_TRY(copy_env(Rsrc, R, c->stream));
   return finish();
 }
 
@@ -389,7 +389,7 @@ int Heff::finish() {
   }
   n_allowed = (int64_t)allowed.size();
   if (n_allowed != th.total) return fail(CMPS_ERR_STATE, "internal: allowed count differs from sector total");
-  CMPS_TRY(upload_vec(pos, &d_pos));
+  CMPS_TRY(upload_vec(pos, &d_pos, ctx->stream));
 
   // ---- LeftPart blocks: key (b1, s1', s1, a0-sector s) ----
   lp_off.clear();
@@ -449,10 +449,10 @@ int Heff::finish() {
   }
   CMPS_TRY(LP.alloc(lp_total));
   CMPS_TRY(RP.alloc(rp_total));
-  CMPS_TRY(upload_vec(lp_blocks, &d_lp_blocks));
-  CMPS_TRY(upload_vec(lp_terms, &d_lp_terms));
-  CMPS_TRY(upload_vec(rp_blocks, &d_rp_blocks));
-  CMPS_TRY(upload_vec(rp_terms, &d_rp_terms));
+  CMPS_TRY(upload_vec(lp_blocks, &d_lp_blocks, ctx->stream));
+  CMPS_TRY(upload_vec(lp_terms, &d_lp_terms, ctx->stream));
+  CMPS_TRY(upload_vec(rp_blocks, &d_rp_blocks, ctx->stream));
+  CMPS_TRY(upload_vec(rp_terms, &d_rp_terms, ctx->stream));
 
   // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
   std::set<int> b1s;
@@ -563,8 +563,8 @@ int Heff::finish() {
         return fail(CMPS_ERR_STATE, "RightPart block range outside its buffer");
   for (int64_t p : pos)
     if (p < 0 || p >= th.total) return fail(CMPS_ERR_STATE, "pack map entry outside the sector blocks");
-  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n()));
-  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n()));
+  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
+  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   cudaStream_t st = ctx->stream;
   CMPS_TRY(launch_block_axpy(d_lp_blocks, (int)lp_blocks.size(), d_lp_terms, L.data, LP, st));
   CMPS_TRY(launch_block_axpy(d_rp_blocks, (int)rp_blocks.size(), d_rp_terms, R.data, RP, st));
@@ -657,6 +657,7 @@ int Heff::apply_host(const double* in, double* out) {
   CMPS_TRY(apply_device(d_io, d_io, st));
   CMPS_CUDA(cudaMemcpyAsync(out, d_io, bytes, cudaMemcpyDeviceToHost, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
+  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(split_error(*this));
   return CMPS_OK;
 }
 
@@ -733,59 +734,66 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   }
   int nmv = 0;
   double lam = 0.0;
-  bool converged = false;
-  // the split-TF32 operator is accurate to ~1e-6 relative: converge the Ritz
-  // vector to that floor, the energy comes from an FP64 Rayleigh quotient
-  if (precision == CMPS_SPLIT_TF32) tol = std::max(tol, 3e-6);
   std::vector<double> h(2 * 128), h2(2 * 128), alpha, beta, ycoef;
-  for (int restart = 0; restart < std::max(1, max_restarts) && !converged; ++restart) {
-    CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), vr(0), vi(0), st));
-    alpha.clear();
-    beta.clear();
-    int k = 0;
-    double last_beta = 0.0;
-    for (int j = 0; j < kdim; ++j) {
-      // y = H v_j; the basis vector is copied into the planar work vector x
-      CMPS_CUDA(cudaMemcpyAsync(x.re(), vr(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-      CMPS_CUDA(cudaMemcpyAsync(x.im(), vi(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-      CMPS_TRY(apply_theta(x, y, st));
-      ++nmv;
-      // Gram-Schmidt against v_0..v_j, twice
-      CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h.data(), st));
-      CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h.data(), y.re(), y.im(), -1.0, st));
-      CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h2.data(), st));
-      CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h2.data(), y.re(), y.im(), -1.0, st));
-      alpha.push_back(h[2 * j] + h2[2 * j]);
-      double b2 = 0.0;
-      CMPS_TRY(ops.norm2(y.re(), y.im(), &b2, st));
-      double b = std::sqrt(std::max(0.0, b2));
-      k = j + 1;
-      last_beta = b;
-      if (j + 1 < kdim) {
-        if (b < 1e-14 * std::max(1.0, std::fabs(alpha.back()))) break;  // invariant subspace
-        beta.push_back(b);
-        CMPS_TRY(ops.scale_copy(y.re(), y.im(), 1.0 / b, vr(j + 1), vi(j + 1), st));
+  // One restarted-Lanczos run from the vector in x (norm^2 in nrm), with the
+  // split-TF32 or the FP64 operator; leaves the normalised Ritz vector in x.
+  auto lanczos = [&](bool fp64, double tol_run, int restarts, int kd, bool* conv) -> int {
+    *conv = false;
+    for (int restart = 0; restart < std::max(1, restarts) && !*conv; ++restart) {
+      CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), vr(0), vi(0), st));
+      alpha.clear();
+      beta.clear();
+      int k = 0;
+      double last_beta = 0.0;
+      for (int j = 0; j < kd; ++j) {
+        // y = H v_j; the basis vector is copied into the planar work vector x
+        CMPS_CUDA(cudaMemcpyAsync(x.re(), vr(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        CMPS_CUDA(cudaMemcpyAsync(x.im(), vi(j), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        if (fp64) CMPS_TRY(apply_theta_fp64(x, y, st));
+        else CMPS_TRY(apply_theta(x, y, st));
+        ++nmv;
+        // Gram-Schmidt against v_0..v_j, twice
+        CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h.data(), st));
+        CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h.data(), y.re(), y.im(), -1.0, st));
+        CMPS_TRY(ops.multidot(kv.re(), kv.im(), n, j + 1, y.re(), y.im(), h2.data(), st));
+        CMPS_TRY(ops.multiaxpy(kv.re(), kv.im(), n, j + 1, h2.data(), y.re(), y.im(), -1.0, st));
+        alpha.push_back(h[2 * j] + h2[2 * j]);
+        double b2 = 0.0;
+        CMPS_TRY(ops.norm2(y.re(), y.im(), &b2, st));
+        double b = std::sqrt(std::max(0.0, b2));
+        k = j + 1;
+        last_beta = b;
+        if (j + 1 < kd) {
+          if (b < 1e-14 * std::max(1.0, std::fabs(alpha.back()))) break;  // invariant subspace
+          beta.push_back(b);
+          CMPS_TRY(ops.scale_copy(y.re(), y.im(), 1.0 / b, vr(j + 1), vi(j + 1), st));
+        }
       }
+      // tridiagonal T (k x k)
+      std::vector<double> Tm((size_t)k * k, 0.0);
+      for (int i = 0; i < k; ++i) Tm[(size_t)i * k + i] = alpha[i];
+      for (int i = 0; i + 1 < k; ++i) Tm[(size_t)i * k + i + 1] = Tm[(size_t)(i + 1) * k + i] = beta[i];
+      jacobi_lowest(k, Tm, &lam, ycoef);
+      double resid = std::fabs(last_beta * ycoef[k - 1]);
+      CMPS_TRY(ops.combine(kv.re(), kv.im(), n, k, ycoef.data(), x.re(), x.im(), st));
+      CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
+      if (resid <= tol_run * std::max(1.0, std::fabs(lam)) || k < kd) *conv = true;
     }
-    // tridiagonal T (k x k)
-    std::vector<double> Tm((size_t)k * k, 0.0);
-    for (int i = 0; i < k; ++i) Tm[(size_t)i * k + i] = alpha[i];
-    for (int i = 0; i + 1 < k; ++i) Tm[(size_t)i * k + i + 1] = Tm[(size_t)(i + 1) * k + i] = beta[i];
-    jacobi_lowest(k, Tm, &lam, ycoef);
-    double resid = std::fabs(last_beta * ycoef[k - 1]);
-    CMPS_TRY(ops.combine(kv.re(), kv.im(), n, k, ycoef.data(), x.re(), x.im(), st));
-    CMPS_TRY(ops.norm2(x.re(), x.im(), &nrm, st));
-    if (resid <= tol * std::max(1.0, std::fabs(lam)) || k < kdim) converged = true;
-  }
-  // normalise the Ritz vector
-  CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), x.re(), x.im(), st));
+    CMPS_TRY(ops.scale_copy(x.re(), x.im(), 1.0 / std::sqrt(nrm), x.re(), x.im(), st));
+    nrm = 1.0;
+    return CMPS_OK;
+  };
+  bool converged = false;
   if (precision == CMPS_SPLIT_TF32) {
-    // FP64 Rayleigh quotient <x|H|x> (x normalised): energy error ~ |dx|^2
-    CMPS_TRY(apply_theta_fp64(x, y, st));
-    ++nmv;
-    std::vector<double> rq(2);
-    CMPS_TRY(ops.multidot(x.re(), x.im(), 0, 1, y.re(), y.im(), rq.data(), st));
-    lam = rq[0];
+    // Split-TF32 products accumulate in FP32 over K up to ~1e4-1e5 terms, so
+    // the operator is accurate to ~1e-5 relative: the Krylov work runs on it
+    // down to that floor, then a short FP64 Lanczos refines the Ritz vector
+    // to the requested tolerance and gives the energy.
+    bool c1 = false;
+    CMPS_TRY(lanczos(false, std::max(tol, 2e-5), std::min(std::max(1, max_restarts), 4), kdim, &c1));
+    CMPS_TRY(lanczos(true, tol, max_restarts, std::min(kdim, 12), &converged));
+  } else {
+    CMPS_TRY(lanczos(true, tol, max_restarts, kdim, &converged));
   }
   // HED post-processing (DMRG_routines.cpp:870-889)
   double mx2 = 0.0;

@@ -13,6 +13,7 @@ struct cmps_context {
   int device = 0;
   cudaStream_t stream = nullptr;
   void* solver = nullptr;  // cusolverDnHandle_t, created on first SVD
+  void* blas = nullptr;    // cublasHandle_t, created on first SVD (Gram matrices of big sectors)
 };
 
 namespace cmps {
@@ -39,6 +40,7 @@ struct SplitState;
 
 struct Heff {
   cmps_context* ctx = nullptr;
+  int device = 0;                // copied from ctx at build: valid even if ctx is destroyed first
   Rules rules;
   int d = 0;
   std::vector<QKey> sigq;       // basis charges
@@ -121,10 +123,10 @@ int split_error(Heff& H);
 // cuSOLVER handle owned by the context (svd.cu).
 void release_solver(cmps_context* ctx);
 
-int copy_env(const Env& src, Env& dst);
+int copy_env(const Env& src, Env& dst, cudaStream_t st);
 
 int build_env_from_desc(const Rules& r, const cmps_mpx_desc* desc, bool right, Env& env, int D,
-                        const std::vector<QKey>& bq);
+                        const std::vector<QKey>& bq, cudaStream_t st);
 int parse_index_charges(const Rules& r, const cmps_mpx_desc* desc, int idx, std::vector<QKey>& out);
 
 }  // namespace cmps

@@ -33,6 +33,14 @@ int fail(int code, const std::string& msg);
     if (_s != CMPS_OK) return _s; \
   } while (0)
 
+// Copies and fills outside the matvec.  The library's streams are created
+// non-blocking, so the legacy default stream (plain cudaMemcpy / cudaMemset)
+// is not ordered with them: a fill could land after the kernels that write the
+// buffer, an upload after the kernels that read it.  These issue the copy on
+// the stream the neighbouring kernels use and wait for it before returning.
+int copy_wait(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st);
+int zero_wait(void* dst, size_t bytes, cudaStream_t st);
+
 // Charge arithmetic of State (states.hpp:176-206).
 struct Rules {
   int nq = 0;
@@ -115,7 +123,7 @@ struct GemmPlan {
   GemmTerm* d_terms = nullptr;
   GemmTile* d_tiles = nullptr;
   double flops = 0.0;
-  int upload(int bm, int bn);
+  int upload(int bm, int bn, cudaStream_t st);
   // Host check, before any launch, that every operand and output range lies
   // inside its buffer (lengths in complex elements).
   int validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t c_len, const char* what) const;

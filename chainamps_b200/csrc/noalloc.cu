@@ -65,9 +65,9 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
     return fail(CMPS_ERR_ARG, "no-allocation matvec: this H_eff needs " + std::to_string(need * 8) +
                                   " bytes of scratch, above the static maximum of " +
                                   std::to_string(kNoAllocScratchDoubles * 8) + " bytes");
-  CMPS_CUDA(cudaSetDevice(H.ctx->device));
+  CMPS_CUDA(cudaSetDevice(H.device));
   double* base = nullptr;
-  CMPS_TRY(scratch_address(H.ctx->device, &base));
+  CMPS_TRY(scratch_address(H.device, &base));
   cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
   // non-owning views into the static array
   Planar x, t, y;

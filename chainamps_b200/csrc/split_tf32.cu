@@ -121,14 +121,13 @@ void add_tiles(tc::TcPlan& p, int32_t task, int32_t m, int32_t n) {
 }  // namespace
 
 namespace tc {
-int TcPlan::upload() {
+int TcPlan::upload(cudaStream_t st) {
   release();
-  auto up = [](auto& v, auto** d) -> int {
+  auto up = [st](auto& v, auto** d) -> int {
     if (v.empty()) return CMPS_OK;
     size_t bytes = v.size() * sizeof(v[0]);
     CMPS_CUDA(cudaMalloc((void**)d, bytes));
-    CMPS_CUDA(cudaMemcpy(*d, v.data(), bytes, cudaMemcpyHostToDevice));
-    return CMPS_OK;
+    return copy_wait(*d, v.data(), bytes, cudaMemcpyHostToDevice, st);
   };
   CMPS_TRY(up(tasks, &d_tasks));
   CMPS_TRY(up(terms, &d_terms));
@@ -242,9 +241,10 @@ static int build_split(Heff& H) {
   const int64_t total = S->rpt_off + 4 * S->rpt_len;
   if (cudaMalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
     return fail(CMPS_ERR_NOMEM, "split-TF32 operand allocation failed");
-  CMPS_CUDA(cudaMemset(S->buf, 0, sizeof(float) * total));
+  // zero fill: padding rows and columns of every operand must read as zero
+  CMPS_TRY(zero_wait(S->buf, sizeof(float) * total, H.ctx->stream));
   CMPS_CUDA(cudaMalloc(&S->d_err, sizeof(int)));
-  CMPS_CUDA(cudaMemset(S->d_err, 0, sizeof(int)));
+  CMPS_TRY(zero_wait(S->d_err, sizeof(int), H.ctx->stream));
   CMPS_CUDA(cudaMallocHost(&S->h_err, sizeof(int)));
   // ---- split LeftPart / RightPart ----
   {
@@ -260,7 +260,7 @@ static int build_split(Heff& H) {
           return fail(CMPS_ERR_STATE, "split block outside its buffer");
       }
       CMPS_CUDA(cudaMalloc(&d, sizeof(SplitBlock) * v.size()));
-      CMPS_CUDA(cudaMemcpy(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice));
+      CMPS_TRY(copy_wait(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice, H.ctx->stream));
       const Planar& src = pass == 0 ? H.LP : H.RP;
       float* dst = S->buf + (pass == 0 ? S->lps_off : S->rpt_off);
       const int64_t plane = pass == 0 ? S->lps_len : S->rpt_len;
@@ -291,7 +291,8 @@ static int build_split(Heff& H) {
     for (int64_t v : map)
       if (v < 0 || v >= S->s1a_len) return fail(CMPS_ERR_STATE, "theta split map incomplete");
     CMPS_CUDA(cudaMalloc(&S->d_theta_map, sizeof(int64_t) * std::max<int64_t>(1, th.total)));
-    CMPS_CUDA(cudaMemcpy(S->d_theta_map, map.data(), sizeof(int64_t) * th.total, cudaMemcpyHostToDevice));
+    CMPS_TRY(copy_wait(S->d_theta_map, map.data(), sizeof(int64_t) * th.total, cudaMemcpyHostToDevice,
+                       H.ctx->stream));
   }
   // ---- stage 1 plan: C1[r_pad, a0'] = sum S1A[r_pad, a0] LPS[a0', a0] ----
   tc::TcPlan& p1 = S->p1;
@@ -402,6 +403,19 @@ static int build_split(Heff& H) {
       add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
       p2.tasks.push_back(task);
     }
+  // heaviest tiles first: the persistent kernel deals tiles round-robin to
+  // the SMs, so this ordering balances the per-SM work
+  for (tc::TcPlan* p : {&p1, &p2}) {
+    auto cost = [&](const tc::TcTile& t) {
+      const tc::TcTask& k = p->tasks[t.task];
+      int64_t it = 0;
+      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + 15) / 16;
+      const int64_t n = std::min<int64_t>(128, k.n - t.n0);
+      return (it + 2) * ((n + 15) / 16);  // +2: fixed per-tile cost (epilogue)
+    };
+    std::stable_sort(p->tiles.begin(), p->tiles.end(),
+                     [&](const tc::TcTile& a, const tc::TcTile& b) { return cost(a) > cost(b); });
+  }
   // plan integrity: every term names an existing map, every tile an existing task
   for (const tc::TcPlan* p : {&p1, &p2}) {
     for (const tc::TcTerm& tm : p->terms)
@@ -414,8 +428,8 @@ static int build_split(Heff& H) {
     for (const tc::TcTile& tl : p->tiles)
       if (tl.task < 0 || tl.task >= (int32_t)p->tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
   }
-  CMPS_TRY(p1.upload());
-  CMPS_TRY(p2.upload());
+  CMPS_TRY(p1.upload(H.ctx->stream));
+  CMPS_TRY(p2.upload(H.ctx->stream));
   return CMPS_OK;
 }
 
@@ -467,7 +481,7 @@ int split_error(Heff& H) {
   SplitState* S = H.split;
   if (!S) return CMPS_OK;
   int e = 0;
-  CMPS_CUDA(cudaMemcpy(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  CMPS_TRY(copy_wait(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, H.ctx->stream));
   if (e) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(e) + ")");
   return CMPS_OK;
 }

@@ -15,6 +15,7 @@
 //   L'^{b1} = U^H (LeftPart^{b1} U),   R'^{b1} = (V^dag RightPart^{b1}) V^dag^H
 // as grouped GEMMs; the blocks stay on the device.
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -34,6 +35,21 @@ void release_solver(cmps_context* ctx) {
     cusolverDnDestroy((cusolverDnHandle_t)ctx->solver);
     ctx->solver = nullptr;
   }
+  if (ctx && ctx->blas) {
+    cublasDestroy((cublasHandle_t)ctx->blas);
+    ctx->blas = nullptr;
+  }
+}
+
+static int get_blas(cmps_context* ctx, cublasHandle_t* out) {
+  if (!ctx->blas) {
+    cublasHandle_t h;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return fail(CMPS_ERR_CUDA, "cublasCreate failed");
+    ctx->blas = h;
+  }
+  cublasSetStream((cublasHandle_t)ctx->blas, ctx->stream);
+  *out = (cublasHandle_t)ctx->blas;
+  return CMPS_OK;
 }
 
 static int get_solver(cmps_context* ctx, cusolverDnHandle_t* out) {
@@ -106,6 +122,26 @@ __global__ void k_scatter_vd(const double2* __restrict__ Vcm, int64_t nc, int64_
   }
 }
 
+// F[:, j] = E[:, p-1-j] (eigenvectors in descending eigenvalue order)
+__global__ void k_reverse_cols(const double2* __restrict__ E, int64_t p, double2* __restrict__ F) {
+  const int64_t n = p * p;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % p, j = e / p;
+    F[e] = E[i + p * (p - 1 - j)];
+  }
+}
+
+// G[:, j] /= s[j]  (column-major, rows x cols); zero columns where s[j] == 0
+__global__ void k_scale_cols_inv(double2* __restrict__ G, int64_t rows, int64_t cols, const double* __restrict__ s) {
+  const int64_t n = rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / rows;
+    const double f = s[j] > 0.0 ? 1.0 / s[j] : 0.0;
+    G[e].x *= f;
+    G[e].y *= f;
+  }
+}
+
 int grid_of(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g < 1) g = 1;
@@ -116,9 +152,11 @@ int grid_of(int64_t n) {
 }  // namespace
 
 // Kept count of SparseMatrix::SVD (sparse_interface.cpp:1346-1376).
-static int64_t truncation_length(const std::vector<double>& sv, int64_t D, double max_trunc) {
+static int64_t truncation_length(const std::vector<double>& sv, int64_t D, double max_trunc,
+                                 bool* weight_decided = nullptr) {
   const int64_t N = (int64_t)sv.size();
   int64_t length = (D > 0 && D < N) ? D : N;
+  const int64_t cap = length;
   double trunc_error = 0.0;
   int64_t tl = N;
   while (trunc_error < max_trunc && tl > 0) {
@@ -127,6 +165,7 @@ static int64_t truncation_length(const std::vector<double>& sv, int64_t D, doubl
   }
   ++tl;
   if (tl < length) length = tl;
+  if (weight_decided) *weight_decided = tl < cap;
   while (length < N && (sv[length - 1] - sv[length]) / sv[length - 1] < 1.0e-3) ++length;
   return length;
 }
@@ -147,6 +186,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
   struct Blk {
     std::vector<int64_t> rows, cols;
     std::vector<double> s;
+    bool eig = false;
     double2* dU = nullptr;
     double2* dV = nullptr;
     int64_t* drows = nullptr;
@@ -191,6 +231,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     cusolverDnXgesvdjSetTolerance(params, 0.0);   // 0: machine precision
     cusolverDnXgesvdjSetMaxSweeps(params, 100);
     cusolverDnXgesvdjSetSortEig(params, 1);
+    cublasHandle_t blas;
+    if ((status = get_blas(H.ctx, &blas)) != CMPS_OK) break;
+    // ---- pass 1: empty-block skip and row/column pruning ----
     for (int m = 0; m < nm && status == CMPS_OK; ++m) {
       const int64_t R = th.nrows[m], C = th.ncols[m];
       if (R == 0 || C == 0) continue;
@@ -219,44 +262,138 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       }
       cudaMemcpyAsync(b.drows, b.rows.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(b.dcols, b.cols.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, st);
+    }
+    if (status != CMPS_OK) { cusolverDnDestroyGesvdjInfo(params); break; }
+    // ---- pass 2: factor every block ----
+    // exact: one-sided Jacobi SVD (gesvdj).  Otherwise, for sectors of at least
+    // kEigMin rows and columns, the Hermitian route: eigenpairs of the smaller
+    // Gram matrix (A A^H or A^H A, zheevd), the other factor by one GEMM.  Its
+    // singular values carry an absolute error ~eps * s_max, so it is only
+    // accepted below when the bond-dimension cap, not the weight cut, decides
+    // the kept count and every kept value is far above that floor.
+    const int64_t kEigMin = 192;
+    auto factor = [&](int m, bool exact) -> int {
+      Blk& b = blk[m];
+      const int64_t C = th.ncols[m];
+      const double* bre = H.theta.re() + th.base[m];
+      const double* bim = H.theta.im() + th.base[m];
+      const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
+      const int64_t mn = std::min(nr, nc);
       k_gather_cm<<<grid_of(nr * nc), 256, 0, st>>>(bre, bim, C, b.drows, nr, b.dcols, nc, dA);
-      int lwork = 0;
-      if (cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc, (cuDoubleComplex*)dA,
-                                       (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr, (cuDoubleComplex*)b.dV,
-                                       (int)nc, &lwork, params) != CUSOLVER_STATUS_SUCCESS) {
-        status = fail(CMPS_ERR_SOLVER, "gesvdj buffer query failed");
-        break;
-      }
-      cuDoubleComplex* work = nullptr;
-      if (cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess) {
-        status = fail(CMPS_ERR_NOMEM, "SVD work allocation failed");
-        break;
-      }
-      cusolverStatus_t cs = cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
-                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr,
-                                              (cuDoubleComplex*)b.dV, (int)nc, work, lwork, dinfo, params);
-      int info = 0;
       b.s.resize(mn);
-      cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
-      cudaError_t ce = cudaStreamSynchronize(st);
-      cudaFree(work);
-      if (cs != CUSOLVER_STATUS_SUCCESS || ce != cudaSuccess) { status = fail(CMPS_ERR_SOLVER, "gesvdj failed"); break; }
-      if (info < 0) { status = fail(CMPS_ERR_SOLVER, "gesvdj: invalid argument"); break; }
-      // info > 0: not converged to tolerance within max sweeps; values still usable
+      if (exact || mn < kEigMin) {
+        b.eig = false;
+        int lwork = 0;
+        if (cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc, (cuDoubleComplex*)dA,
+                                         (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr, (cuDoubleComplex*)b.dV,
+                                         (int)nc, &lwork, params) != CUSOLVER_STATUS_SUCCESS)
+          return fail(CMPS_ERR_SOLVER, "gesvdj buffer query failed");
+        cuDoubleComplex* work = nullptr;
+        if (cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+          return fail(CMPS_ERR_NOMEM, "SVD work allocation failed");
+        cusolverStatus_t cs = cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
+                                                (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr,
+                                                (cuDoubleComplex*)b.dV, (int)nc, work, lwork, dinfo, params);
+        int info = 0;
+        cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaError_t ce = cudaStreamSynchronize(st);
+        cudaFree(work);
+        if (cs != CUSOLVER_STATUS_SUCCESS || ce != cudaSuccess) return fail(CMPS_ERR_SOLVER, "gesvdj failed");
+        if (info < 0) return fail(CMPS_ERR_SOLVER, "gesvdj: invalid argument");
+        return CMPS_OK;  // info > 0: not converged to tolerance within max sweeps; values still usable
+      }
+      b.eig = true;
+      const bool left = nr <= nc;  // eigenvectors of A A^H give U; of A^H A give V
+      const int p = (int)(left ? nr : nc);
+      double2* G = nullptr;   // Gram matrix, then its eigenvectors
+      double* W = nullptr;
+      int lwork = 0;
+      if (cudaMalloc(&G, sizeof(double2) * (size_t)p * p) != cudaSuccess ||
+          cudaMalloc(&W, sizeof(double) * p) != cudaSuccess) {
+        if (G) cudaFree(G);
+        return fail(CMPS_ERR_NOMEM, "Gram matrix allocation failed");
+      }
+      const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+      cublasStatus_t bs;
+      if (left)
+        bs = cublasZgemm(blas, CUBLAS_OP_N, CUBLAS_OP_C, p, p, (int)nc, &one, (cuDoubleComplex*)dA, (int)nr,
+                         (cuDoubleComplex*)dA, (int)nr, &zero, (cuDoubleComplex*)G, p);
+      else
+        bs = cublasZgemm(blas, CUBLAS_OP_C, CUBLAS_OP_N, p, p, (int)nr, &one, (cuDoubleComplex*)dA, (int)nr,
+                         (cuDoubleComplex*)dA, (int)nr, &zero, (cuDoubleComplex*)G, p);
+      int rc = CMPS_OK;
+      cuDoubleComplex* work = nullptr;
+      if (bs != CUBLAS_STATUS_SUCCESS) rc = fail(CMPS_ERR_CUDA, "Gram matrix GEMM failed");
+      if (rc == CMPS_OK && cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
+                                                       (cuDoubleComplex*)G, p, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "zheevd buffer query failed");
+      if (rc == CMPS_OK && cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+        rc = fail(CMPS_ERR_NOMEM, "zheevd work allocation failed");
+      if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
+                                            (cuDoubleComplex*)G, p, W, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "zheevd failed");
+      std::vector<double> w(p);
+      int info = 0;
+      if (rc == CMPS_OK) {
+        cudaMemcpyAsync(w.data(), W, sizeof(double) * p, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess || info != 0) rc = fail(CMPS_ERR_SOLVER, "zheevd did not converge");
+      }
+      if (rc == CMPS_OK) {
+        for (int j = 0; j < p; ++j) b.s[j] = std::sqrt(std::max(0.0, w[p - 1 - j]));
+        cudaMemcpyAsync(dS, b.s.data(), sizeof(double) * p, cudaMemcpyHostToDevice, st);
+        double2* F = left ? b.dU : b.dV;   // the factor from the eigenvectors, descending order
+        double2* O = left ? b.dV : b.dU;   // the other factor
+        k_reverse_cols<<<grid_of((int64_t)p * p), 256, 0, st>>>(G, p, F);
+        if (left)  // V = A^H U S^-1
+          bs = cublasZgemm(blas, CUBLAS_OP_C, CUBLAS_OP_N, (int)nc, p, (int)nr, &one, (cuDoubleComplex*)dA, (int)nr,
+                           (cuDoubleComplex*)F, (int)nr, &zero, (cuDoubleComplex*)O, (int)nc);
+        else       // U = A V S^-1
+          bs = cublasZgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)nr, p, (int)nc, &one, (cuDoubleComplex*)dA, (int)nr,
+                           (cuDoubleComplex*)F, (int)nc, &zero, (cuDoubleComplex*)O, (int)nr);
+        if (bs != CUBLAS_STATUS_SUCCESS) rc = fail(CMPS_ERR_CUDA, "second factor GEMM failed");
+        k_scale_cols_inv<<<grid_of((left ? nc : nr) * (int64_t)p), 256, 0, st>>>(O, left ? nc : nr, p, dS);
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(CMPS_ERR_CUDA, "eigen-route SVD failed");
+      }
+      if (work) cudaFree(work);
+      cudaFree(G);
+      cudaFree(W);
+      return rc;
+    };
+    for (int m = 0; m < nm && status == CMPS_OK; ++m)
+      if (!blk[m].rows.empty()) status = factor(m, false);
+    // ---- global selection (redone with exact factors where the Gram route is not accurate enough) ----
+    struct SV { double v; int m; int64_t j; };
+    std::vector<SV> all;
+    std::vector<double> sv;
+    int64_t length = 0;
+    for (int pass = 0; pass < 2 && status == CMPS_OK; ++pass) {
+      all.clear();
+      for (int m = 0; m < nm; ++m)
+        for (int64_t j = 0; j < (int64_t)blk[m].s.size(); ++j) all.push_back(SV{blk[m].s[j], m, j});
+      if (all.empty()) { status = fail(CMPS_ERR_SOLVER, "no singular values (empty wavefunction)"); break; }
+      std::stable_sort(all.begin(), all.end(), [](const SV& a, const SV& b) { return a.v > b.v; });
+      sv.assign(all.size(), 0.0);
+      for (size_t i = 0; i < all.size(); ++i) sv[i] = all[i].v;
+      bool weight_decided = false;
+      length = truncation_length(sv, chi, max_trunc, &weight_decided);
+      const double floor2 = 1e-10 * sv[0] * sv[0];
+      bool redo = false;
+      for (int m = 0; m < nm; ++m) {
+        if (!blk[m].eig) continue;
+        bool low = false;
+        for (int64_t g = 0; g < length; ++g)
+          if (all[g].m == m && all[g].v * all[g].v < floor2) low = true;
+        if (weight_decided || low) {
+          redo = true;
+          if ((status = factor(m, true)) != CMPS_OK) break;
+        }
+      }
+      if (!redo) break;
     }
     cusolverDnDestroyGesvdjInfo(params);
     if (status != CMPS_OK) break;
-    // ---- global selection ----
-    struct SV { double v; int m; int64_t j; };
-    std::vector<SV> all;
-    for (int m = 0; m < nm; ++m)
-      for (int64_t j = 0; j < (int64_t)blk[m].s.size(); ++j) all.push_back(SV{blk[m].s[j], m, j});
-    if (all.empty()) { status = fail(CMPS_ERR_SOLVER, "no singular values (empty wavefunction)"); break; }
-    std::stable_sort(all.begin(), all.end(), [](const SV& a, const SV& b) { return a.v > b.v; });
-    std::vector<double> sv(all.size());
-    for (size_t i = 0; i < all.size(); ++i) sv[i] = all[i].v;
-    const int64_t length = truncation_length(sv, chi, max_trunc);
     out.values.assign(sv.begin(), sv.begin() + length);
     out.discarded = 0.0;
     for (size_t i = length; i < sv.size(); ++i) out.discarded += sv[i] * sv[i];
@@ -311,7 +448,8 @@ static void new_bond(const SvdResult& s, Bond& b, std::vector<int>& sec_of_m) {
   for (size_t m = 0; m < s.th.mq.size(); ++m) sec_of_m[m] = s.kept[m] ? b.find(s.th.mq[m]) : -1;
 }
 
-static int alloc_env(const Rules& r, const Bond& a, int D, const std::vector<QKey>& bq, bool right, Env& env) {
+static int alloc_env(const Rules& r, const Bond& a, int D, const std::vector<QKey>& bq, bool right, Env& env,
+                     cudaStream_t st) {
   env.right = right;
   env.a = a;
   env.D = D;
@@ -329,8 +467,7 @@ static int alloc_env(const Rules& r, const Bond& a, int D, const std::vector<QKe
       total += a.sdim[s] * a.sdim[sp];
     }
   CMPS_TRY(env.data.alloc(total));
-  if (total) CMPS_CUDA(cudaMemset(env.data.d, 0, sizeof(double) * 2 * total));
-  return CMPS_OK;
+  return zero_wait(env.data.d, sizeof(double) * 2 * total, st);
 }
 
 int left_update(Heff& H, const SvdResult& s, Env& out) {
@@ -342,7 +479,7 @@ int left_update(Heff& H, const SvdResult& s, Env& out) {
   Bond nb;
   std::vector<int> sec;
   new_bond(s, nb, sec);
-  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, false, out));
+  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, false, out, H.ctx->stream));
   // X^{b1}_m = LeftPart^{b1} U_m  (rows L(m'), cols kept[m])
   std::set<int> b1s;
   for (auto& kv : H.lp_off) b1s.insert(kv.first[0]);
@@ -418,8 +555,8 @@ int left_update(Heff& H, const SvdResult& s, Env& out) {
   do {
     if ((status = px.validate(false, false, H.LP.len, s.U.len, xt, "left update X")) != CMPS_OK) break;
     if ((status = pl.validate(true, false, s.U.len, xt, out.data.len, "left update")) != CMPS_OK) break;
-    if ((status = px.upload(64, 64)) != CMPS_OK) break;
-    if ((status = pl.upload(64, 64)) != CMPS_OK) break;
+    if ((status = px.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = pl.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
     Planar Ucopy = s.U;  // non-owning view
     if ((status = launch_zgemm_fp64(px, false, false, H.LP, Ucopy, X, H.ctx->stream)) != CMPS_OK) break;
     if ((status = launch_zgemm_fp64(pl, true, false, Ucopy, X, out.data, H.ctx->stream)) != CMPS_OK) break;
@@ -440,7 +577,7 @@ int right_update(Heff& H, const SvdResult& s, Env& out) {
   Bond nb;
   std::vector<int> sec;
   new_bond(s, nb, sec);
-  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, true, out));
+  CMPS_TRY(alloc_env(r, nb, H.D, H.bq, true, out, H.ctx->stream));
   std::set<int> b1s;
   for (auto& kv : H.rp_off) b1s.insert(kv.first[0]);
   GemmPlan py, pr;
@@ -514,8 +651,8 @@ int right_update(Heff& H, const SvdResult& s, Env& out) {
   do {
     if ((status = py.validate(false, false, s.Vd.len, H.RP.len, yt, "right update Y")) != CMPS_OK) break;
     if ((status = pr.validate(false, true, yt, s.Vd.len, out.data.len, "right update")) != CMPS_OK) break;
-    if ((status = py.upload(64, 64)) != CMPS_OK) break;
-    if ((status = pr.upload(64, 64)) != CMPS_OK) break;
+    if ((status = py.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = pr.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
     Planar Vview = s.Vd;
     if ((status = launch_zgemm_fp64(py, false, false, Vview, H.RP, Y, H.ctx->stream)) != CMPS_OK) break;
     if ((status = launch_zgemm_fp64(pr, false, true, Y, Vview, out.data, H.ctx->stream)) != CMPS_OK) break;
@@ -546,7 +683,7 @@ int cmps_heff_theta_svd(cmps_heff* h, int64_t chi, double max_trunc, cmps_svd** 
   if (!h || !h->impl || !out) return fail(CMPS_ERR_ARG, "null argument");
   *out = nullptr;
   if (chi < 0) return fail(CMPS_ERR_ARG, "negative bond dimension");
-  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  CMPS_CUDA(cudaSetDevice(h->impl->device));
   auto* s = new (std::nothrow) cmps_svd();
   if (!s) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   int st = theta_svd(*h->impl, chi, max_trunc, s->r);
@@ -661,7 +798,7 @@ int cmps_svd_copy(const cmps_svd* s, double* values, int16_t* new_charges, int64
 int cmps_heff_left_block(cmps_heff* h, const cmps_svd* s, cmps_block** out) {
   if (!h || !h->impl || !s || !out) return fail(CMPS_ERR_ARG, "null argument");
   *out = nullptr;
-  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  CMPS_CUDA(cudaSetDevice(h->impl->device));
   auto* b = new (std::nothrow) cmps_block();
   if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   b->rules = h->impl->rules;
@@ -674,7 +811,7 @@ int cmps_heff_left_block(cmps_heff* h, const cmps_svd* s, cmps_block** out) {
 int cmps_heff_right_block(cmps_heff* h, const cmps_svd* s, cmps_block** out) {
   if (!h || !h->impl || !s || !out) return fail(CMPS_ERR_ARG, "null argument");
   *out = nullptr;
-  CMPS_CUDA(cudaSetDevice(h->impl->ctx->device));
+  CMPS_CUDA(cudaSetDevice(h->impl->device));
   auto* b = new (std::nothrow) cmps_block();
   if (!b) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   b->rules = h->impl->rules;

@@ -12,14 +12,20 @@
 // tensor map (K, rows, 4 planes) and one TMA load brings all four planes of a
 // 128-row x 16-column tile (SWIZZLE_64B).
 //
-// One CTA computes one 128 x N (N <= 128) output tile of one task, whose
-// terms are K-concatenated: warp 0 issues TMA loads into a 3-stage ring,
-// warp 1 issues the MMAs, warps 2-5 drain TMEM and write the output.  Every
-// mbarrier wait is bounded: on time-out the kernel raises an error word,
-// skips the remaining work, frees its TMEM and returns.
+// Persistent: one CTA per SM walks a list of 128 x N (N <= 128) output tiles
+// (tile i of CTA b is tiles[b + i * gridDim]; the host orders tiles by
+// decreasing work), each the K-concatenation of its task's terms.  Warp 0
+// issues TMA loads into a 3-stage ring and runs ahead across tile boundaries,
+// warp 1 issues the MMAs into one of two TMEM accumulator buffers, warps 2-5
+// drain the other buffer and write the output, so the epilogue of a tile
+// overlaps the loads and MMAs of the next.  Every mbarrier wait is bounded:
+// on time-out the kernel raises an error word, skips the remaining work,
+// frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "tc_gemm.h"
 
@@ -33,7 +39,7 @@ constexpr int kPlaneTileBytes = 128 * kBK * 4;          // 8 KB: 128 rows x 64 B
 constexpr int kOperandBytes = 4 * kPlaneTileBytes;      // 32 KB: four planes
 constexpr int kStageBytes = 2 * kOperandBytes;          // A + B
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
-constexpr uint32_t kTmemCols = 256;                      // Re at col 0, Im at col 128
+constexpr uint32_t kTmemCols = 512;                      // two buffers of {Re at +0, Im at +128}
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -71,6 +77,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* e
     if (*(volatile int*)err) return false;
   }
   return true;
+}
+
+// The tensor maps live in global memory, written by a host copy before the
+// launch.  A freed plan's maps can leave descriptors cached for an address
+// that a later plan reuses, so the issuing thread orders its TMA reads of a
+// map after the generic-proxy write with an acquire fence on that map.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"((uint64_t)map) : "memory");
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
@@ -127,32 +141,29 @@ __device__ __forceinline__ float tf32_rna(float x) {
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_split_gemm(const TcTile* __restrict__ tiles, const TcTask* __restrict__ tasks, const TcTerm* __restrict__ terms,
-              const CUtensorMap* __restrict__ amaps, const CUtensorMap* __restrict__ bmaps, float* __restrict__ out32,
-              int64_t out32_plane, double* __restrict__ out64, int64_t out64_plane, int* __restrict__ err) {
+tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __restrict__ tasks,
+              const TcTerm* __restrict__ terms, const CUtensorMap* __restrict__ amaps,
+              const CUtensorMap* __restrict__ bmaps, float* __restrict__ out32, int64_t out32_plane,
+              double* __restrict__ out64, int64_t out64_plane, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accum = empty + kStages;
-  uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+  uint64_t* tfull = empty + kStages;   // [2]: accumulator buffer ready for the epilogue
+  uint64_t* tempty = tfull + 2;        // [2]: accumulator buffer drained by the epilogue
+  uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const TcTile tile = tiles[blockIdx.x];
-  const TcTask task = tasks[tile.task];
-  const int m0 = tile.m0, n0 = tile.n0;
-  const int ntile = min(kBN, task.n - n0);
-  const int nmma = (ntile + 15) & ~15;  // MMA N: multiple of 16 for M = 128
-  // iterations: sum over terms of ceil(k / 16)
-  int iters = 0;
-  for (int t = task.t0; t < task.t1; ++t) iters += (terms[t].k + kBK - 1) / kBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -166,123 +177,158 @@ tc_split_gemm(const TcTile* __restrict__ tiles, const TcTask* __restrict__ tasks
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
-    // ---------------- TMA producer ----------------
-    if (lane == 0 && iters > 0) {
-      int t = task.t0, k0 = 0;
-      int issued = 0;
-      for (int it = 0; it < iters; ++it) {
-        const int s = it % kStages;
-        const uint32_t ph = (uint32_t)((it / kStages) & 1);
-        if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) break;
-        const TcTerm tm = terms[t];
-        uint8_t* sa = smem + s * kStageBytes;
-        uint8_t* sb = sa + kOperandBytes;
-        mbar_expect_tx(&full[s], kStageBytes);
-        tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, m0, 0, &full[s]);
-        tma_load_3d(sb, bmaps + tm.b_map, k0, n0, 0, &full[s]);
-        ++issued;
-        k0 += kBK;
-        if (k0 >= tm.k) {
-          k0 = 0;
-          ++t;
+    // ---------------- TMA producer: runs ahead across tile boundaries ----------------
+    if (lane == 0) {
+      int it = 0;  // global iteration counter of this CTA
+      bool ok = true;
+      for (int ti = blockIdx.x; ti < ntiles && ok; ti += gridDim.x) {
+        const TcTile tile = tiles[ti];
+        const TcTask task = tasks[tile.task];
+        for (int t = task.t0; t < task.t1 && ok; ++t) {
+          const TcTerm tm = terms[t];
+          tensormap_acquire(amaps + tm.a_map);
+          tensormap_acquire(bmaps + tm.b_map);
+          for (int k0 = 0; k0 < tm.k; k0 += kBK, ++it) {
+            const int s = it % kStages;
+            const uint32_t ph = (uint32_t)((it / kStages) & 1);
+            if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
+              ok = false;
+              break;
+            }
+            uint8_t* sa = smem + s * kStageBytes;
+            uint8_t* sb = sa + kOperandBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
+            tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
+          }
         }
       }
-      if (issued < iters) {
-        // error path: let the copies already in flight land before exiting
-        for (int it = max(0, issued - kStages); it < issued; ++it) {
+      if (!ok) {
+        // let the copies already in flight land before the CTA exits
+        for (int j = max(0, it - kStages); j < it; ++j) {
           const unsigned long long t0 = now_ns();
-          while (!mbar_try(&full[it % kStages], (uint32_t)((it / kStages) & 1)) && now_ns() - t0 < kWaitLimitNs) {
+          while (!mbar_try(&full[j % kStages], (uint32_t)((j / kStages) & 1)) && now_ns() - t0 < kWaitLimitNs) {
           }
         }
       }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
-    if (lane == 0 && iters > 0) {
-      const uint32_t id_pos = idesc_tf32(nmma, false), id_neg = idesc_tf32(nmma, true);
-      const uint32_t d_re = tmem, d_im = tmem + 128;
+    if (lane == 0) {
+      int it = 0, tc = 0;
       bool ok = true;
-      for (int it = 0; it < iters; ++it) {
-        const int s = it % kStages;
-        const uint32_t ph = (uint32_t)((it / kStages) & 1);
-        if (!mbar_wait(&full[s], ph, err, 2)) {
+      for (int ti = blockIdx.x; ti < ntiles && ok; ti += gridDim.x, ++tc) {
+        const TcTile tile = tiles[ti];
+        const TcTask task = tasks[tile.task];
+        const int ntile = min(kBN, task.n - tile.n0);
+        const int nmma = (ntile + 15) & ~15;  // multiple of 16 for M = 128
+        const uint32_t id_pos = idesc_tf32(nmma, false), id_neg = idesc_tf32(nmma, true);
+        const int buf = tc & 1;
+        const uint32_t use = (uint32_t)(tc >> 1);
+        if (!mbar_wait(&tempty[buf], (use & 1u) ^ 1u, err, 4)) {
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a0 = smem_u32(smem + s * kStageBytes);
-        const uint32_t b0 = a0 + kOperandBytes;
+        const uint32_t d_re = tmem + (uint32_t)(buf * 256), d_im = d_re + 128;
+        bool first = true;
+        for (int t = task.t0; t < task.t1 && ok; ++t) {
+          const int kt = terms[t].k;
+          for (int k0 = 0; k0 < kt; k0 += kBK, ++it) {
+            const int s = it % kStages;
+            const uint32_t ph = (uint32_t)((it / kStages) & 1);
+            if (!mbar_wait(&full[s], ph, err, 2)) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(smem + s * kStageBytes);
+            const uint32_t b0 = a0 + kOperandBytes;
 #pragma unroll
-        for (int kk = 0; kk < kBK / 8; ++kk) {
-          // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
-          uint64_t A[4], B[4];
+            for (int kk = 0; kk < kBK / 8; ++kk) {
+              // planes: 0 re_hi, 1 re_lo, 2 im_hi, 3 im_lo
+              uint64_t A[4], B[4];
 #pragma unroll
-          for (int p = 0; p < 4; ++p) {
-            A[p] = smem_desc_sw64(a0 + p * kPlaneTileBytes + kk * 32);
-            B[p] = smem_desc_sw64(b0 + p * kPlaneTileBytes + kk * 32);
+              for (int p = 0; p < 4; ++p) {
+                A[p] = smem_desc_sw64(a0 + p * kPlaneTileBytes + kk * 32);
+                B[p] = smem_desc_sw64(b0 + p * kPlaneTileBytes + kk * 32);
+              }
+              const uint32_t acc = first ? 0u : 1u;
+              first = false;
+              umma_tf32(d_re, A[0], B[0], id_pos, acc);
+              umma_tf32(d_re, A[0], B[1], id_pos, 1u);
+              umma_tf32(d_re, A[1], B[0], id_pos, 1u);
+              umma_tf32(d_re, A[2], B[2], id_neg, 1u);
+              umma_tf32(d_re, A[2], B[3], id_neg, 1u);
+              umma_tf32(d_re, A[3], B[2], id_neg, 1u);
+              umma_tf32(d_im, A[0], B[2], id_pos, acc);
+              umma_tf32(d_im, A[0], B[3], id_pos, 1u);
+              umma_tf32(d_im, A[1], B[2], id_pos, 1u);
+              umma_tf32(d_im, A[2], B[0], id_pos, 1u);
+              umma_tf32(d_im, A[2], B[1], id_pos, 1u);
+              umma_tf32(d_im, A[3], B[0], id_pos, 1u);
+            }
+            umma_commit(&empty[s]);
           }
-          const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
-          umma_tf32(d_re, A[0], B[0], id_pos, acc);
-          umma_tf32(d_re, A[0], B[1], id_pos, 1u);
-          umma_tf32(d_re, A[1], B[0], id_pos, 1u);
-          umma_tf32(d_re, A[2], B[2], id_neg, 1u);
-          umma_tf32(d_re, A[2], B[3], id_neg, 1u);
-          umma_tf32(d_re, A[3], B[2], id_neg, 1u);
-          umma_tf32(d_im, A[0], B[2], id_pos, acc);
-          umma_tf32(d_im, A[0], B[3], id_pos, 1u);
-          umma_tf32(d_im, A[1], B[2], id_pos, 1u);
-          umma_tf32(d_im, A[2], B[0], id_pos, 1u);
-          umma_tf32(d_im, A[2], B[1], id_pos, 1u);
-          umma_tf32(d_im, A[3], B[0], id_pos, 1u);
         }
-        umma_commit(&empty[s]);
+        umma_commit(&tfull[buf]);  // arrives at once for a tile without terms
       }
-      (void)ok;
-      umma_commit(accum);
     }
   } else {
     // ---------------- epilogue: warps 2..5 ----------------
-    const int quad = warp & 3;            // TMEM lane quadrant this warp may access
-    const int row = quad * 32 + lane;     // accumulator row within the tile
-    const int gm = m0 + row;
-    int have = iters > 0 ? 1 : 0;
-    if (have) {
+    const int quad = warp & 3;  // TMEM lane quadrant this warp may access
+    const int row = quad * 32 + lane;
+    int tc = 0;
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x, ++tc) {
+      const TcTile tile = tiles[ti];
+      const TcTask task = tasks[tile.task];
+      const int ntile = min(kBN, task.n - tile.n0);
+      const int nmma = (ntile + 15) & ~15;
+      const int buf = tc & 1;
+      const uint32_t use = (uint32_t)(tc >> 1);
+      int have = task.t1 > task.t0 ? 1 : 0;
+      int alive = 1;
       if (lane == 0) {
-        mbar_wait(accum, 0, err, 3);
-        if (*(volatile int*)err) have = 0;
+        if (!mbar_wait(&tfull[buf], use & 1u, err, 3)) alive = 0;
+        if (*(volatile int*)err) alive = 0;
       }
-      have = __shfl_sync(0xffffffffu, have, 0);  // warp-uniform: tcgen05.ld is warp-collective
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool row_ok = gm < task.m;
-    for (int c = 0; c < nmma; c += 16) {
-      float vr[16], vi[16];
-      if (have) {
-        const uint32_t lane_base = (uint32_t)(quad * 32) << 16;
-        tmem_ld16(tmem + lane_base + c, vr);
-        tmem_ld16(tmem + lane_base + 128 + c, vi);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
-      }
-      if (!row_ok) continue;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int j = c + i;
-        if (j >= ntile) break;
-        const int64_t o = task.out_off + (int64_t)gm * task.row_stride + (int64_t)(n0 + j) * task.col_stride;
-        if (MODE == 1) {
-          // stage-1 output: split into the four planes stage 2 reads
-          const float hr = tf32_rna(vr[i]), hi = tf32_rna(vi[i]);
-          out32[o] = hr;
-          out32[o + out32_plane] = tf32_rna(vr[i] - hr);
-          out32[o + 2 * out32_plane] = hi;
-          out32[o + 3 * out32_plane] = tf32_rna(vi[i] - hi);
+      alive = __shfl_sync(0xffffffffu, alive, 0);  // warp-uniform: tcgen05.ld is warp-collective
+      if (!alive) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int gm = tile.m0 + row;
+      const bool row_ok = gm < task.m;
+      const uint32_t tbase = tmem + (uint32_t)(buf * 256) + ((uint32_t)(quad * 32) << 16);
+      for (int c = 0; c < nmma; c += 16) {
+        float vr[16], vi[16];
+        if (have) {
+          tmem_ld16(tbase + c, vr);
+          tmem_ld16(tbase + 128 + c, vi);
         } else {
-          out64[o] = (double)vr[i];
-          out64[o + out64_plane] = (double)vi[i];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
+        }
+        if (!row_ok) continue;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int j = c + i;
+          if (j >= ntile) break;
+          const int64_t o = task.out_off + (int64_t)gm * task.row_stride + (int64_t)(tile.n0 + j) * task.col_stride;
+          if (MODE == 1) {
+            // stage-1 output: split into the four planes stage 2 reads
+            const float hr = tf32_rna(vr[i]), hi = tf32_rna(vi[i]);
+            out32[o] = hr;
+            out32[o + out32_plane] = tf32_rna(vr[i] - hr);
+            out32[o + 2 * out32_plane] = hi;
+            out32[o + 3 * out32_plane] = tf32_rna(vi[i] - hi);
+          } else {
+            out64[o] = (double)vr[i];
+            out64[o + out64_plane] = (double)vi[i];
+          }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[buf])) : "memory");
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -298,22 +344,27 @@ int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double*
            int* d_err, cudaStream_t st) {
   if (p.tiles.empty()) return CMPS_OK;
   if (p.tiles.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many tcgen05 tiles");
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = (int)p.tiles.size();
+  const unsigned grid = (unsigned)std::min(ntiles, sms);
   if (mode == 1) {
     static bool cfg1 = false;
     if (!cfg1) {
       CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
       cfg1 = true;
     }
-    tc_split_gemm<1><<<(unsigned)p.tiles.size(), kThreads, kSmemBytes, st>>>(
-        p.d_tiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+    tc_split_gemm<1><<<grid, kThreads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
+                                                          p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
   } else {
     static bool cfg2 = false;
     if (!cfg2) {
       CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
       cfg2 = true;
     }
-    tc_split_gemm<2><<<(unsigned)p.tiles.size(), kThreads, kSmemBytes, st>>>(
-        p.d_tiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+    tc_split_gemm<2><<<grid, kThreads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
+                                                          p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
   }
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;

@@ -37,7 +37,7 @@ struct TcPlan {
   TcTile* d_tiles = nullptr;
   CUtensorMap* d_amaps = nullptr;
   CUtensorMap* d_bmaps = nullptr;
-  int upload();
+  int upload(cudaStream_t st);
   void release();
 };
 

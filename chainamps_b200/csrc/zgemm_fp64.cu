@@ -216,7 +216,7 @@ int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, co
   return launch_variant<true, true>(p, A, B, C, st);
 }
 
-int GemmPlan::upload(int bm, int bn) {
+int GemmPlan::upload(int bm, int bn, cudaStream_t st) {
   tiles.clear();
   for (size_t i = 0; i < tasks.size(); ++i) {
     const GemmTask& t = tasks[i];
@@ -224,12 +224,11 @@ int GemmPlan::upload(int bm, int bn) {
       for (int n0 = 0; n0 < t.n; n0 += bn) tiles.push_back(GemmTile{(int32_t)i, m0, n0, 0});
   }
   release();
-  auto up = [](auto& v, auto** d) -> int {
+  auto up = [st](auto& v, auto** d) -> int {
     if (v.empty()) return CMPS_OK;
     size_t bytes = v.size() * sizeof(v[0]);
     CMPS_CUDA(cudaMalloc((void**)d, bytes));
-    CMPS_CUDA(cudaMemcpy(*d, v.data(), bytes, cudaMemcpyHostToDevice));
-    return CMPS_OK;
+    return copy_wait(*d, v.data(), bytes, cudaMemcpyHostToDevice, st);
   };
   CMPS_TRY(up(tasks, &d_tasks));
   CMPS_TRY(up(terms, &d_terms));

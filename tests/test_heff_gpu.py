@@ -152,3 +152,47 @@ def test_ground_state_svd_and_blocks(ctx, name, steps, chi):
     assert np.max(np.abs(Lg.data.reshape(-1) - Lnew_ref.data.reshape(-1))) <= 1e-12 * sl
     sr = np.max(np.abs(Rnew_ref.data))
     assert np.max(np.abs(Rg.data.reshape(-1) - Rnew_ref.data.reshape(-1))) <= 1e-12 * sr
+
+
+def test_svd_large_sectors(ctx):
+    """Sectors of >= 192 rows and columns take the Gram-matrix route when
+    the bond-dimension cap decides the kept count; values, per-sector kept
+    counts and the truncated wavefunction must match the oracle's SVD."""
+    from chainamps_b200 import TwoVertexComponents
+    from tests.helpers import random_bond, random_left_block, random_right_block
+    H = ZOO["xxz"]
+    rng = np.random.default_rng(21)
+    pool = [(0,), (1,), (2,)]
+    bq = H.indices[1].charges
+    L = random_left_block(rng, H.rules, random_bond(rng, 320, pool), bq)
+    R = random_right_block(rng, H.rules, random_bond(rng, 300, pool), bq)
+    ref = od.TwoVertexComponents(L, H, R)
+    gpu = TwoVertexComponents(ctx, H.rules, to_tensor(L), to_tensor(H), to_tensor(R))
+    x = rng.standard_normal(gpu.n) + 1j * rng.standard_normal(gpu.n)
+    x /= np.linalg.norm(x)
+    full = np.zeros(ref.length, complex)
+    full[ref.allowed] = x
+    theta = from_matrix(H.rules, ref.indices, 2, full.reshape((ref.vrows, ref.vcols), order="F"))
+    for chi in (150, 400):
+        dref = od.block_svd(theta, chi, 1e-16)
+        gpu.set_theta(x)
+        s = gpu.SVD(chi, 1e-16)
+        assert s.kept == len(dref.values)
+        out = s.copy(ref.vrows, ref.vcols)
+        np.testing.assert_allclose(out["values"], dref.values, rtol=1e-10, atol=1e-14)
+        keys, cnt = np.unique(out["charges"], axis=0, return_counts=True)
+        rkeys, rcnt = np.unique(dref.U.indices[2].charges, axis=0, return_counts=True)
+        np.testing.assert_array_equal(keys, rkeys)
+        np.testing.assert_array_equal(cnt, rcnt)
+        ucp, uri, uv = out["u"]
+        U = np.zeros((ref.vrows, s.kept), complex)
+        for c in range(s.kept):
+            U[uri[ucp[c]:ucp[c + 1]], c] = uv[ucp[c]:ucp[c + 1]]
+        vcp, vri, vv = out["vd"]
+        Vd = np.zeros((s.kept, ref.vcols), complex)
+        for c in range(ref.vcols):
+            Vd[vri[vcp[c]:vcp[c + 1]], c] = vv[vcp[c]:vcp[c + 1]]
+        rec = U @ np.diag(out["values"]) @ Vd
+        rec_ref = dref.U.matrix() @ np.diag(dref.values) @ dref.Vd.matrix()
+        assert np.max(np.abs(rec - rec_ref)) <= 1e-10
+        assert abs(s.discarded - dref.truncation) <= 1e-12
