@@ -87,6 +87,8 @@ _SIGS = {
     "cmps_heff_status": (C.c_int, [C.c_void_p]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
                                  C.POINTER(C.c_int)]),
+    "cmps_heff_eigs_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       c_dblp]),
     "cmps_heff_set_theta": (C.c_int, [C.c_void_p, c_dblp]),
     "cmps_heff_theta_svd": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]),
     "cmps_svd_destroy": (C.c_int, [C.c_void_p]),
@@ -104,6 +106,7 @@ _SIGS = {
     "cmps_dmrg_set_solver": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
     "cmps_dmrg_grow": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
     "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
+    "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -285,6 +288,15 @@ class TwoVertexComponents:
                                   None if vec is None else _p(vec.view(np.float64), C.c_double), C.byref(mv)))
         return ev.value, vec, mv.value
 
+    def eigs_stats(self):
+        """Work of the last HED: dict(split_matvecs, fp64_matvecs, cycles,
+        ms_split, ms_fp64, ms_total) (device time, CUDA events)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        ms = np.zeros(3, np.float64)
+        _check(lib.cmps_heff_eigs_stats(self.h, C.byref(a), C.byref(b), C.byref(c), _p(ms, C.c_double)))
+        return dict(split_matvecs=a.value, fp64_matvecs=b.value, cycles=c.value, ms_split=ms[0], ms_fp64=ms[1],
+                    ms_total=ms[2])
+
     def set_theta(self, theta):
         t = np.ascontiguousarray(np.asarray(theta, np.complex128))
         _check(lib.cmps_heff_set_theta(self.h, _p(t.view(np.float64), C.c_double)))
@@ -412,6 +424,16 @@ class iDMRG:
         self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
                          chi=bd.value, matvecs=mv.value, ms=ms)
         return self.last
+
+    def profile(self):
+        """Breakdown of the last step: dict(env_ms, build_ms, eig_ms, svd_ms,
+        total_ms, split_matvecs, fp64_matvecs, cycles, split_mv_ms,
+        fp64_mv_ms) (device time, CUDA events)."""
+        v = np.zeros(10, np.float64)
+        _check(lib.cmps_dmrg_profile(self.h, _p(v, C.c_double)))
+        keys = ("env_ms", "build_ms", "eig_ms", "svd_ms", "total_ms", "split_matvecs", "fp64_matvecs", "cycles",
+                "split_mv_ms", "fp64_mv_ms")
+        return {k: (int(x) if k in ("split_matvecs", "fp64_matvecs", "cycles") else float(x)) for k, x in zip(keys, v)}
 
     def values(self):
         v = np.zeros(self.last["chi"], np.float64)

@@ -240,6 +240,20 @@ int cmps_heff_eigs(cmps_heff* h, const double* guess, double tol, int max_restar
   return h->impl->eigs(guess, tol, max_restarts, krylov_dim, eval, evec, matvecs);
 }
 
+int cmps_heff_eigs_stats(const cmps_heff* h, int* split_matvecs, int* fp64_matvecs, int* cycles, double* ms3) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  const Heff::EigStats& s = h->impl->eig_stats;
+  if (split_matvecs) *split_matvecs = s.mv_split;
+  if (fp64_matvecs) *fp64_matvecs = s.mv_fp64;
+  if (cycles) *cycles = s.cycles;
+  if (ms3) {
+    ms3[0] = s.ms_split;
+    ms3[1] = s.ms_fp64;
+    ms3[2] = s.ms_total;
+  }
+  return CMPS_OK;
+}
+
 int cmps_heff_set_theta(cmps_heff* h, const double* theta) {
   if (!h || !h->impl || !theta) return fail(CMPS_ERR_ARG, "null argument");
   Heff& H = *h->impl;

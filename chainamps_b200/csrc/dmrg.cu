@@ -68,7 +68,8 @@ struct Dmrg {
   double tol = 1e-10;
   int restarts = 50, kdim = 24;
   int last_matvecs = 0;
-  double last_ms[4] = {0, 0, 0, 0};  // env update, eigensolve, svd, total
+  double last_ms[4] = {0, 0, 0, 0};  // env update + H_eff build + prediction, eigensolve, svd, total
+  double last_profile[10] = {0};     // cmps_dmrg_profile layout
 
   ~Dmrg() {
     if (svd) {
@@ -224,7 +225,14 @@ int Dmrg::predict(Heff& next, bool* ok) {
 
 int Dmrg::grow(int64_t chi, double trunc, double* out) {
   cudaStream_t st = ctx->stream;
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 5; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } ev_guard{ev};
   for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));
   cudaEventRecord(ev[0], st);
   Env L, R;
@@ -234,6 +242,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
     CMPS_TRY(left_update(*heff, *svd, L));
     CMPS_TRY(right_update(*heff, *svd, R));
   }
+  cudaEventRecord(ev[4], st);
   auto next = std::unique_ptr<Heff>(new Heff());
   next->ctx = ctx;
   next->device = ctx->device;
@@ -264,15 +273,19 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   CMPS_TRY(theta_svd(*heff, chi, trunc, *svd));
   cudaEventRecord(ev[3], st);
   cudaEventSynchronize(ev[3]);
-  float t01 = 0, t12 = 0, t23 = 0;
+  float t01 = 0, t12 = 0, t23 = 0, t0e = 0;
   cudaEventElapsedTime(&t01, ev[0], ev[1]);
   cudaEventElapsedTime(&t12, ev[1], ev[2]);
   cudaEventElapsedTime(&t23, ev[2], ev[3]);
+  cudaEventElapsedTime(&t0e, ev[0], ev[4]);
   last_ms[0] = t01;
   last_ms[1] = t12;
   last_ms[2] = t23;
   last_ms[3] = t01 + t12 + t23;
-  for (auto& ee : ev) cudaEventDestroy(ee);
+  const Heff::EigStats& es = heff->eig_stats;
+  const double prof[10] = {t0e, t01 - t0e, t12, t23, t01 + t12 + t23, (double)es.mv_split, (double)es.mv_fp64,
+                           (double)es.cycles, es.ms_split, es.ms_fp64};
+  for (int i = 0; i < 10; ++i) last_profile[i] = prof[i];
   // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
   std::vector<double> v = svd->values;
   double sq = 0.0;
@@ -376,6 +389,12 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
   if (ms4)
     for (int i = 0; i < 4; ++i) ms4[i] = D.last_ms[i];
   return rc;
+}
+
+int cmps_dmrg_profile(const cmps_dmrg* d, double* out10) {
+  if (!d || !d->impl || !out10) return fail(CMPS_ERR_ARG, "null argument");
+  for (int i = 0; i < 10; ++i) out10[i] = d->impl->last_profile[i];
+  return CMPS_OK;
 }
 
 int cmps_dmrg_values(const cmps_dmrg* d, double* values) {

@@ -73,10 +73,17 @@ struct Heff {
   double* d_io = nullptr;        // interleaved staging (2 * n_allowed doubles)
   bool have_theta = false;
   Planar theta;                  // last eigenvector (theta space)
-  // Krylov basis
-  Planar kv;                     // kdim vectors of length th.total (planar, stride th.total)
+  // Krylov basis: vector j at kv.d + 2 j n (n = th.total), its real plane
+  // then its imaginary plane, so each basis vector is itself a Planar view
+  Planar kv;
   int kv_dim = 0;
   VecOps ops;
+  double* h_ab = nullptr;        // pinned: alpha_j, beta_j of the current Lanczos step
+  // Work of the last eigs() call.
+  struct EigStats {
+    int mv_split = 0, mv_fp64 = 0, cycles = 0;
+    double ms_split = 0.0, ms_fp64 = 0.0, ms_total = 0.0;
+  } eig_stats;
 
   ~Heff();
   int build(cmps_context* c, const Rules& r, const cmps_mpx_desc* Ld, const cmps_mpx_desc* Wd,
@@ -118,6 +125,11 @@ int right_update(Heff& H, const SvdResult& s, Env& out);
 int prepare_precision(Heff* h, int precision);
 void release_split(Heff* h);
 int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st);
+// The same matvec without a host synchronisation; a pipeline time-out is
+// recorded in the handle's error word, cleared by split_reset_error() and
+// read by split_error().
+int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st);
+int split_reset_error(Heff& H, cudaStream_t st);
 int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
 int split_error(Heff& H);
 // cuSOLVER handle owned by the context (svd.cu).

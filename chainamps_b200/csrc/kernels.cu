@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "internal.h"
 #include "kernels.h"
 
@@ -222,6 +224,132 @@ __global__ void k_combine(const double* __restrict__ Vr, const double* __restric
   }
 }
 
+// ---- Krylov kernels with device-resident coefficients ----------------------
+// The Lanczos loop keeps its coefficients on the device: a projection's
+// coefficients are reduced into device memory and read back by the update
+// kernel, so one iteration needs no host round trip.
+constexpr int KR_THREADS = 256;
+constexpr int KR_E = 8;  // elements per thread per tile: w is read once, into registers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// partial[r][blk]: r = 2j, 2j+1 -> <V_j, w> (re, im) for j < k; r = 2k -> |w|^2.
+// One pass over w (held in registers per tile) and one over each V_j.
+__global__ void __launch_bounds__(KR_THREADS)
+k_mdot(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k,
+       const double* __restrict__ wr, const double* __restrict__ wi, int64_t n, double* __restrict__ partial) {
+  extern __shared__ double acc[];  // [warps][2k + 1], one row per warp: no shared-memory atomics
+  const int nw = KR_THREADS / 32, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rows = 2 * k + 1;
+  for (int t = threadIdx.x; t < nw * rows; t += blockDim.x) acc[t] = 0.0;
+  __syncthreads();
+  const int64_t tile = (int64_t)KR_THREADS * KR_E;
+  for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+    double xr[KR_E], xi[KR_E];
+    double s = 0.0;
+#pragma unroll
+    for (int e = 0; e < KR_E; ++e) {
+      const int64_t i = base + (int64_t)e * KR_THREADS + threadIdx.x;
+      xr[e] = i < n ? wr[i] : 0.0;
+      xi[e] = i < n ? wi[i] : 0.0;
+      s += xr[e] * xr[e] + xi[e] * xi[e];
+    }
+    s = warp_sum(s);
+    if (lane == 0) acc[warp * rows + 2 * k] += s;
+    for (int j = 0; j < k; ++j) {
+      const double* vr = Vr + (int64_t)j * ldv;
+      const double* vi = Vi + (int64_t)j * ldv;
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int e = 0; e < KR_E; ++e) {
+        const int64_t i = base + (int64_t)e * KR_THREADS + threadIdx.x;
+        if (i < n) {
+          const double ar = vr[i], ai = vi[i];
+          sr += ar * xr[e] + ai * xi[e];
+          si += ar * xi[e] - ai * xr[e];
+        }
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (lane == 0) {
+        acc[warp * rows + 2 * j] += sr;
+        acc[warp * rows + 2 * j + 1] += si;
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += acc[w * rows + r];
+    partial[(int64_t)r * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// w -= sum_j h_j V_j (h complex, on the device); partial[blk] = |w|^2 over
+// this CTA's elements afterwards.
+__global__ void __launch_bounds__(KR_THREADS)
+k_maxpy_norm(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k,
+             const double* __restrict__ h, double* __restrict__ wr, double* __restrict__ wi, int64_t n,
+             double* __restrict__ partial) {
+  __shared__ double hs[2 * 128];
+  __shared__ double red[KR_THREADS / 32];
+  for (int j = threadIdx.x; j < 2 * k; j += blockDim.x) hs[j] = h[j];
+  __syncthreads();
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double xr = wr[i], xi = wi[i];
+#pragma unroll 4
+    for (int j = 0; j < k; ++j) {
+      const double hr = hs[2 * j], hi = hs[2 * j + 1];
+      const double vr = Vr[(int64_t)j * ldv + i], vi = Vi[(int64_t)j * ldv + i];
+      xr -= hr * vr - hi * vi;
+      xi -= hr * vi + hi * vr;
+    }
+    wr[i] = xr;
+    wi[i] = xi;
+    s += xr * xr + xi * xi;
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < KR_THREADS / 32; ++w) t += red[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
+// Lanczos coefficients of step j after two projection passes:
+// alpha_j = Re(hA_j + hB_j), beta_j = |w|; scale = 1 / beta_j, or 0 when the
+// Krylov space is exhausted (the next basis vector is then zero).
+__global__ void k_lanczos_coef(const double* __restrict__ hA, const double* __restrict__ hB,
+                               const double* __restrict__ nrm2, int j, double* __restrict__ alpha,
+                               double* __restrict__ beta, double* __restrict__ scale) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double a = hA[2 * j] + hB[2 * j];
+  const double b = sqrt(fmax(0.0, *nrm2));
+  alpha[j] = a;
+  beta[j] = b;
+  *scale = b > 1e-14 * fmax(1.0, fabs(a)) ? 1.0 / b : 0.0;
+}
+
+// y = s * x with s read from the device; `inv_sqrt` takes s = 1 / sqrt(*p)
+// (0 when *p is not positive).
+__global__ void k_scale_dev(const double* __restrict__ xr, const double* __restrict__ xi,
+                            const double* __restrict__ p, int inv_sqrt, double* __restrict__ yr,
+                            double* __restrict__ yi, int64_t n) {
+  const double v = *p;
+  const double s = inv_sqrt ? (v > 0.0 ? 1.0 / sqrt(v) : 0.0) : v;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    yr[i] = s * xr[i];
+    yi[i] = s * xi[i];
+  }
+}
+
 }  // namespace
 
 int launch_pack(const double* in, const int64_t* pos, int64_t n, Planar& dst, cudaStream_t st) {
@@ -251,7 +379,8 @@ int VecOps::init(int64_t n_) {
   n = n_;
   nb = grid_for(n, RED_THREADS);
   if (nb > 1024) nb = 1024;
-  CMPS_CUDA(cudaMalloc(&d_partial, sizeof(double) * 2 * 128 * nb));
+  CMPS_CUDA(cudaMalloc(&d_partial, sizeof(double) * (2 * 128 + 2) * nb));
+  CMPS_CUDA(cudaMalloc(&d_coef, sizeof(double) * kCoefDoubles));
   CMPS_CUDA(cudaMalloc(&d_small, sizeof(double) * 2 * 128 * 2));
   CMPS_CUDA(cudaMalloc(&d_pidx, sizeof(int64_t) * nb));
   return CMPS_OK;
@@ -261,7 +390,8 @@ void VecOps::release() {
   if (d_partial) cudaFree(d_partial);
   if (d_small) cudaFree(d_small);
   if (d_pidx) cudaFree(d_pidx);
-  d_partial = d_small = nullptr;
+  if (d_coef) cudaFree(d_coef);
+  d_partial = d_small = d_coef = nullptr;
   d_pidx = nullptr;
 }
 
@@ -338,6 +468,45 @@ int VecOps::absmax(const double* re, const double* im, double* val, int64_t* idx
 
 int VecOps::phase_drop(double* re, double* im, double pr, double pi, double thr, cudaStream_t st) {
   k_phase_drop<<<grid_for(n, 256), 256, 0, st>>>(re, im, n, pr, pi, thr);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::mdot_dev(const double* Vr, const double* Vi, int64_t ldv, int k, const double* wr, const double* wi,
+                     double* d_out, cudaStream_t st) {
+  if (k < 0 || k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  const int64_t tile = (int64_t)KR_THREADS * KR_E;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(nb, (n + tile - 1) / tile));
+  const int rows = 2 * k + 1;
+  const size_t smem = sizeof(double) * (KR_THREADS / 32) * rows;
+  k_mdot<<<g, KR_THREADS, smem, st>>>(Vr, Vi, ldv, k, wr, wi, n, d_partial);
+  CMPS_CUDA(cudaGetLastError());
+  k_reduce_rows<<<rows, RED_THREADS, 0, st>>>(d_partial, g, rows, d_out);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::maxpy_norm_dev(const double* Vr, const double* Vi, int64_t ldv, int k, const double* d_h, double* wr,
+                           double* wi, double* d_nrm2, cudaStream_t st) {
+  if (k < 0 || k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  const int g = std::min(nb, grid_for(n, KR_THREADS));
+  k_maxpy_norm<<<g, KR_THREADS, 0, st>>>(Vr, Vi, ldv, k, d_h, wr, wi, n, d_partial);
+  CMPS_CUDA(cudaGetLastError());
+  k_reduce_rows<<<1, RED_THREADS, 0, st>>>(d_partial, g, 1, d_nrm2);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::lanczos_coef(const double* d_hA, const double* d_hB, const double* d_nrm2, int j, double* d_alpha,
+                         double* d_beta, double* d_scale, cudaStream_t st) {
+  k_lanczos_coef<<<1, 32, 0, st>>>(d_hA, d_hB, d_nrm2, j, d_alpha, d_beta, d_scale);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::scale_dev(const double* xr, const double* xi, const double* d_s, bool inv_sqrt, double* yr, double* yi,
+                      cudaStream_t st) {
+  k_scale_dev<<<grid_for(n, 256), 256, 0, st>>>(xr, xi, d_s, inv_sqrt ? 1 : 0, yr, yi, n);
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }

@@ -30,6 +30,22 @@ struct VecOps {
   int combine(const double* Vr, const double* Vi, int64_t ldv, int k, const double* c_host, double* yr,
               double* yi, cudaStream_t st);
   int absmax(const double* re, const double* im, double* val_sq, int64_t* idx, cudaStream_t st);
+
+  // Krylov steps whose coefficients stay on the device (no host round trip).
+  double* d_coef = nullptr;  // coefficient scratch, kCoefDoubles
+  static constexpr int kCoefDoubles = 2048;
+  // d_out[2j], d_out[2j+1] = <V_j, w> for j < k (k <= 128); d_out[2k] = |w|^2.
+  int mdot_dev(const double* Vr, const double* Vi, int64_t ldv, int k, const double* wr, const double* wi,
+               double* d_out, cudaStream_t st);
+  // w -= sum_j h_j V_j with h = d_h (2k doubles); *d_nrm2 = |w|^2 afterwards.
+  int maxpy_norm_dev(const double* Vr, const double* Vi, int64_t ldv, int k, const double* d_h, double* wr,
+                     double* wi, double* d_nrm2, cudaStream_t st);
+  // alpha_j, beta_j of a Lanczos step and the scale of the next basis vector.
+  int lanczos_coef(const double* d_hA, const double* d_hB, const double* d_nrm2, int j, double* d_alpha,
+                   double* d_beta, double* d_scale, cudaStream_t st);
+  // y = s x with s = *d_s, or s = 1 / sqrt(*d_s) when inv_sqrt.
+  int scale_dev(const double* xr, const double* xi, const double* d_s, bool inv_sqrt, double* yr, double* yi,
+                cudaStream_t st);
   int phase_drop(double* re, double* im, double pr, double pi, double thr, cudaStream_t st);
 };
 

@@ -442,12 +442,17 @@ int prepare_precision(Heff* h, int precision) {
   return st;
 }
 
-// theta-space matvec in split precision: FP64 planar in -> FP64 planar out.
-int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
+int split_reset_error(Heff& H, cudaStream_t st) {
+  SplitState* S = H.split;
+  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
+  CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
+  return CMPS_OK;
+}
+
+int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   const int64_t n = H.th.total;
-  CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
   int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
   if (n > 0) {
     k_split_theta<<<std::max(grid, 1), 256, 0, st>>>(in.re(), in.im(), S->d_theta_map, n, S->buf + S->s1a_off,
@@ -456,6 +461,14 @@ int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   }
   CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st));
   CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st));
+  return CMPS_OK;
+}
+
+// theta-space matvec in split precision: FP64 planar in -> FP64 planar out.
+int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
+  CMPS_TRY(split_reset_error(H, st));
+  CMPS_TRY(apply_split_async(H, in, out, st));
+  SplitState* S = H.split;
   CMPS_CUDA(cudaMemcpyAsync(S->h_err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
   if (*S->h_err) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(*S->h_err) + ")");

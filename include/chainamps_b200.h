@@ -153,6 +153,12 @@ int cmps_heff_set_precision(cmps_heff* h, int precision);
  * cmps_heff_theta_svd either way).  tol: residual norm / |eigenvalue|. */
 int cmps_heff_eigs(cmps_heff* h, const double* guess, double tol, int max_restarts,
                    int krylov_dim, double* eval, double* evec, int* matvecs);
+/* Work of the last cmps_heff_eigs call on this handle (no reference
+ * counterpart; diagnostics).  With CMPS_SPLIT_TF32 each restart cycle opens
+ * with one FP64 matvec and continues with split-TF32 ones; with CMPS_FP64
+ * every matvec is FP64.  ms3 = device time of {split matvecs, FP64 matvecs,
+ * whole solve} (CUDA events).  Any output pointer may be NULL. */
+int cmps_heff_eigs_stats(const cmps_heff* h, int* split_matvecs, int* fp64_matvecs, int* cycles, double* ms3);
 
 /* ---- charge-block SVD of the two-vertex wavefunction ------------------
  * Replaces TwoVertexSVD -> MPX_matrix::SVD -> SparseMatrix::SVD
@@ -213,6 +219,12 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
                    int* matvecs, double* ms4);
 /* The current (rescaled) singular values, bond_dim of them, descending. */
 int cmps_dmrg_values(const cmps_dmrg* d, double* values);
+/* Breakdown of the last growth step (no reference counterpart;
+ * diagnostics).  out10 = {environment update ms, H_eff build + prediction
+ * ms, eigensolve ms, SVD ms, total ms, split matvecs, FP64 matvecs, restart
+ * cycles, split matvec ms, FP64 matvec ms}; times are device time (CUDA
+ * events). */
+int cmps_dmrg_profile(const cmps_dmrg* d, double* out10);
 
 #ifdef __cplusplus
 }
