@@ -16,6 +16,11 @@ flush is needed between steps.
   (``cmps_heff_apply``: H2D, matvec, D2H inside the timed region);
 * roofline: the grouped FP64 GEMM stages against a live cuBLAS complex128
   GEMM measurement (the FP64 tensor-path ceiling for a library GEMM);
+* idmrg: the iDMRG growth step itself on the same model (real MPO, real
+  environments grown from the dummy blocks up to chi = 512; Arnoldi
+  tolerance 1e-10): device time per step at full chi in FP64 and in mixed
+  precision (split-TF32 matvecs, FP64 Krylov/SVD/energies), the per-phase
+  profile, and the largest relative energy difference between the two runs;
 * cpu_baseline: the oracle's block-sparse numpy port of the same matvec on
   the host cores (one full matvec);
 * --impl reference: the CPU port timed as the reference arm.
@@ -48,6 +53,7 @@ def parse():
     p.add_argument("--chi", type=int, default=512)
     p.add_argument("--precision", default="both", choices=["both", "fp64", "split_tf32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--idmrg-steps", type=int, default=4, help="timed iDMRG steps at full chi (0: skip)")
     return p.parse_args()
 
 
@@ -290,6 +296,8 @@ def main():
                                           "scatter": f["st"][3]},
                              "roofline_frac_vs_zgemm": canonical / ((f["st"][1] + f["st"][2]) * 1e-3) / 1e12 / zgemm}
         line["speedup_mixed_vs_fp64"] = f["ms"] / r["ms"]
+    if a.idmrg_steps > 0:
+        line["idmrg"] = idmrg_bench(ctx, wl, a.chi, a.idmrg_steps, dist)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t, setup, cores, _ = cpu_port(wl, 1)
         line["cpu_baseline"] = {"value": canonical / t / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
@@ -301,6 +309,44 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10):
+    """iDMRG growth on the ladder MPO in FP64 and in mixed precision: `warm`
+    untimed steps bring the bond dimension to chi, then `steps` timed ones.
+    Step time is the library's device time of the whole step (environment
+    update, H_eff build, prediction, eigensolve, SVD; CUDA events), max over
+    ranks."""
+    import torch
+    from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32
+    out = {"chi": chi, "warmup_steps": warm, "timed_steps": steps, "arnoldi_tol": tol, "krylov_dim": 24}
+    energies = {}
+    for name, prec in (("fp64", CMPS_FP64), ("mixed", CMPS_SPLIT_TF32)):
+        run = iDMRG(ctx, wl["rules"], wl["Wt"], precision=prec, tol=tol, krylov_dim=24)
+        e, prof, wall = [], [], []
+        for i in range(warm + steps):
+            t0 = time.perf_counter()
+            r = run.grow(chi, 1e-16)
+            dt = time.perf_counter() - t0
+            e.append(r["energy"])
+            if i >= warm:
+                prof.append(run.profile())
+                wall.append(dt)
+        run.close()
+        torch.cuda.empty_cache()
+        ms = float(np.mean([p["total_ms"] for p in prof]))
+        ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        if dist:
+            dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        keys = [k for k in prof[0] if k != "total_ms"]
+        out[name] = {"ms_per_step": float(ms_t.item()), "host_ms_per_step": 1e3 * float(np.mean(wall)),
+                     "chi": r["chi"], "energy_last": e[-1],
+                     "profile_mean": {k: float(np.mean([p[k] for p in prof])) for k in keys}}
+        energies[name] = np.array(e)
+    rel = np.abs(energies["mixed"] - energies["fp64"]) / np.abs(energies["fp64"])
+    out["max_rel_dE_mixed_vs_fp64"] = float(rel.max())
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
 
 
 def canonical_flops_cpu(wl):

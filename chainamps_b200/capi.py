@@ -106,7 +106,7 @@ _SIGS = {
     "cmps_dmrg_set_solver": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int]),
     "cmps_dmrg_grow": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
     "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
-    "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp]),
+    "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp, C.c_int]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -426,13 +426,14 @@ class iDMRG:
         return self.last
 
     def profile(self):
-        """Breakdown of the last step: dict(env_ms, build_ms, eig_ms, svd_ms,
-        total_ms, split_matvecs, fp64_matvecs, cycles, split_mv_ms,
-        fp64_mv_ms) (device time, CUDA events)."""
-        v = np.zeros(10, np.float64)
-        _check(lib.cmps_dmrg_profile(self.h, _p(v, C.c_double)))
+        """Breakdown of the last step: device times (CUDA events) of the
+        environment update, H_eff build, eigensolve, SVD and whole step; the
+        eigensolver's matvec counts and times; host wall times per phase."""
         keys = ("env_ms", "build_ms", "eig_ms", "svd_ms", "total_ms", "split_matvecs", "fp64_matvecs", "cycles",
-                "split_mv_ms", "fp64_mv_ms")
+                "split_mv_ms", "fp64_mv_ms", "host_env_ms", "host_build_ms", "host_split_ms", "host_predict_ms",
+                "host_release_ms", "host_svd_ms", "host_total_ms")
+        v = np.zeros(len(keys), np.float64)
+        _check(lib.cmps_dmrg_profile(self.h, _p(v, C.c_double), len(keys)))
         return {k: (int(x) if k in ("split_matvecs", "fp64_matvecs", "cycles") else float(x)) for k, x in zip(keys, v)}
 
     def values(self):

@@ -3,8 +3,10 @@
 // failure is an int status plus cmps_last_error().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -25,6 +27,39 @@ int copy_wait(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cud
   CMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
   return CMPS_OK;
+}
+
+static std::mutex g_pool_mu;
+static bool g_pool_ready[64] = {false};
+
+static cudaError_t pool_setup(int dev) {
+  if (dev < 0 || dev >= 64) return cudaSuccess;  // beyond the table: default pool settings
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (g_pool_ready[dev]) return cudaSuccess;
+  cudaMemPool_t pool;
+  cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, dev);
+  if (e != cudaSuccess) return e;
+  uint64_t keep = UINT64_MAX;
+  e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e == cudaSuccess) g_pool_ready[dev] = true;
+  return e;
+}
+
+cudaError_t dmalloc(void** p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = pool_setup(dev);
+  if (e == cudaSuccess) e = cudaMallocAsync(p, std::max<size_t>(bytes, 1), cudaStreamLegacy);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+  return e;
+}
+
+cudaError_t dfree(void* p) {
+  if (!p) return cudaSuccess;
+  cudaError_t e = cudaDeviceSynchronize();
+  cudaError_t f = cudaFreeAsync(p, cudaStreamLegacy);
+  return e != cudaSuccess ? e : f;
 }
 
 int zero_wait(void* dst, size_t bytes, cudaStream_t st) {
@@ -160,8 +195,8 @@ int cmps_heff_length(const cmps_heff* h, int64_t* n_allowed, int64_t* full_lengt
 
 int cmps_heff_allowed_indices(const cmps_heff* h, int64_t* out) {
   if (!h || !h->impl || !out) return fail(CMPS_ERR_ARG, "null argument");
-  std::memcpy(out, h->impl->allowed.data(), sizeof(int64_t) * h->impl->allowed.size());
-  return CMPS_OK;
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->allowed_indices(out);
 }
 
 int cmps_heff_apply(cmps_heff* h, const double* in, double* out) {

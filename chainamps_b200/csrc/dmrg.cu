@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -69,7 +70,8 @@ struct Dmrg {
   int restarts = 50, kdim = 24;
   int last_matvecs = 0;
   double last_ms[4] = {0, 0, 0, 0};  // env update + H_eff build + prediction, eigensolve, svd, total
-  double last_profile[10] = {0};     // cmps_dmrg_profile layout
+  static constexpr int kProfile = 17;
+  double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
 
   ~Dmrg() {
     if (svd) {
@@ -150,7 +152,7 @@ int Dmrg::predict(Heff& next, bool* ok) {
     hostbuf.insert(hostbuf.end(), urow.begin(), urow.end());
     hostbuf.insert(hostbuf.end(), colsc.begin(), colsc.end());
     hostbuf.insert(hostbuf.end(), colsc.begin(), colsc.end());
-    if (cudaMalloc(&d_scale, sizeof(double) * nb) != cudaSuccess) {
+    if (dmalloc(&d_scale, sizeof(double) * nb) != cudaSuccess) {
       status = fail(CMPS_ERR_NOMEM, "prediction scale allocation failed");
       break;
     }
@@ -166,7 +168,7 @@ int Dmrg::predict(Heff& next, bool* ok) {
                                                           to.ncols[m], d_vrow, nullptr, Vs.re() + S.voff[m],
                                                           Vs.im() + S.voff[m]);
     cudaStreamSynchronize(st);
-    cudaFree(d_scale);
+    dfree(d_scale);
     d_scale = nullptr;
   }
   // grouped GEMM plan into the next theta blocks
@@ -234,6 +236,11 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
     }
   } ev_guard{ev};
   for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));
+  using clock = std::chrono::steady_clock;
+  auto ms_since = [](clock::time_point a, clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  const auto h0 = clock::now();
   cudaEventRecord(ev[0], st);
   Env L, R;
   if (size == 0) {
@@ -243,6 +250,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
     CMPS_TRY(right_update(*heff, *svd, R));
   }
   cudaEventRecord(ev[4], st);
+  const auto h_env = clock::now();
   auto next = std::unique_ptr<Heff>(new Heff());
   next->ctx = ctx;
   next->device = ctx->device;
@@ -251,10 +259,13 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   next->L = L;   // ownership of the device blocks moves to `next`
   next->R = R;
   CMPS_TRY(next->finish());
+  const auto h_fin = clock::now();
   CMPS_TRY(prepare_precision(next.get(), precision));
   next->precision = precision;
+  const auto h_split = clock::now();
   bool have_guess = false;
   CMPS_TRY(predict(*next, &have_guess));
+  const auto h_pred = clock::now();
   // the previous step's factors and H_eff are no longer needed
   if (svd) {
     svd->U.release();
@@ -262,17 +273,20 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
     svd.reset();
   }
   heff = std::move(next);
+  const auto h_rel = clock::now();
   cudaEventRecord(ev[1], st);
   double e = 0.0;
   int nmv = 0;
   int rc = heff->eigs(nullptr, tol, restarts, kdim, &e, nullptr, &nmv, have_guess);
   if (rc != CMPS_OK && rc != CMPS_ERR_SOLVER) return rc;
   last_matvecs = nmv;
+  const auto h_eig = clock::now();
   cudaEventRecord(ev[2], st);
   svd.reset(new SvdResult());
   CMPS_TRY(theta_svd(*heff, chi, trunc, *svd));
   cudaEventRecord(ev[3], st);
   cudaEventSynchronize(ev[3]);
+  const auto h_svd = clock::now();
   float t01 = 0, t12 = 0, t23 = 0, t0e = 0;
   cudaEventElapsedTime(&t01, ev[0], ev[1]);
   cudaEventElapsedTime(&t12, ev[1], ev[2]);
@@ -283,9 +297,24 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   last_ms[2] = t23;
   last_ms[3] = t01 + t12 + t23;
   const Heff::EigStats& es = heff->eig_stats;
-  const double prof[10] = {t0e, t01 - t0e, t12, t23, t01 + t12 + t23, (double)es.mv_split, (double)es.mv_fp64,
-                           (double)es.cycles, es.ms_split, es.ms_fp64};
-  for (int i = 0; i < 10; ++i) last_profile[i] = prof[i];
+  const double prof[kProfile] = {t0e,
+                                 t01 - t0e,
+                                 t12,
+                                 t23,
+                                 t01 + t12 + t23,
+                                 (double)es.mv_split,
+                                 (double)es.mv_fp64,
+                                 (double)es.cycles,
+                                 es.ms_split,
+                                 es.ms_fp64,
+                                 ms_since(h0, h_env),
+                                 ms_since(h_env, h_fin),
+                                 ms_since(h_fin, h_split),
+                                 ms_since(h_split, h_pred),
+                                 ms_since(h_pred, h_rel),
+                                 ms_since(h_eig, h_svd),
+                                 ms_since(h0, h_svd)};
+  for (int i = 0; i < kProfile; ++i) last_profile[i] = prof[i];
   // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
   std::vector<double> v = svd->values;
   double sq = 0.0;
@@ -391,10 +420,10 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
   return rc;
 }
 
-int cmps_dmrg_profile(const cmps_dmrg* d, double* out10) {
-  if (!d || !d->impl || !out10) return fail(CMPS_ERR_ARG, "null argument");
-  for (int i = 0; i < 10; ++i) out10[i] = d->impl->last_profile[i];
-  return CMPS_OK;
+int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n) {
+  if (!d || !d->impl || !out || n < 0) return fail(CMPS_ERR_ARG, "null argument");
+  for (int i = 0; i < n && i < Dmrg::kProfile; ++i) out[i] = d->impl->last_profile[i];
+  return std::min(n, Dmrg::kProfile) == n ? CMPS_OK : fail(CMPS_ERR_ARG, "profile has 17 entries");
 }
 
 int cmps_dmrg_values(const cmps_dmrg* d, double* values) {

@@ -77,7 +77,7 @@ int Planar::alloc(int64_t n) {
   release();
   len = n;
   if (n == 0) return CMPS_OK;
-  cudaError_t e = cudaMalloc(&d, sizeof(double) * 2 * (size_t)n);
+  cudaError_t e = dmalloc(&d, sizeof(double) * 2 * (size_t)n);
   if (e != cudaSuccess) {
     d = nullptr;
     len = 0;
@@ -88,7 +88,7 @@ int Planar::alloc(int64_t n) {
 }
 
 void Planar::release() {
-  if (d) cudaFree(d);
+  if (d) dfree(d);
   d = nullptr;
   len = 0;
 }
@@ -237,21 +237,21 @@ Heff::~Heff() {
   stage1.release();
   stage2.release();
   ops.release();
-  if (d_pos) cudaFree(d_pos);
-  if (d_io) cudaFree(d_io);
+  if (d_pos) dfree(d_pos);
+  if (d_io) dfree(d_io);
   if (h_ab) cudaFreeHost(h_ab);
-  if (d_lp_blocks) cudaFree(d_lp_blocks);
-  if (d_lp_terms) cudaFree(d_lp_terms);
-  if (d_rp_blocks) cudaFree(d_rp_blocks);
-  if (d_rp_terms) cudaFree(d_rp_terms);
+  if (d_lp_blocks) dfree(d_lp_blocks);
+  if (d_lp_terms) dfree(d_lp_terms);
+  if (d_rp_blocks) dfree(d_rp_blocks);
+  if (d_rp_terms) dfree(d_rp_terms);
 }
 
 template <typename T>
 static int upload_vec(const std::vector<T>& v, T** d, cudaStream_t st) {
-  if (*d) cudaFree(*d);
+  if (*d) dfree(*d);
   *d = nullptr;
   if (v.empty()) return CMPS_OK;
-  CMPS_CUDA(cudaMalloc((void**)d, sizeof(T) * v.size()));
+  CMPS_CUDA(dmalloc((void**)d, sizeof(T) * v.size()));
   return copy_wait(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
 }
 
@@ -319,6 +319,56 @@ int Heff::parse_mpo(const cmps_mpx_desc* Wd) {
   return CMPS_OK;
 }
 
+// One CTA per ARPACK column: out[start + i] for the i-th allowed row of the
+// column's sector block (mode 0: theta offset, mode 1: full linear index).
+__global__ void k_arpack_map(const Heff::MapCol* __restrict__ cols, const Heff::MapSec* __restrict__ secs,
+                             const int64_t* __restrict__ rowlin, const int64_t* __restrict__ rowth, int64_t dchiL,
+                             int mode, int64_t* __restrict__ out) {
+  const Heff::MapCol c = cols[blockIdx.x];
+  const Heff::MapSec s = secs[c.m];
+  for (int64_t i = threadIdx.x; i < s.nrows; i += blockDim.x) {
+    const int64_t r = s.rowstart + i;
+    out[c.start + i] = mode == 0 ? s.base + rowth[r] * s.ncols + c.colth : rowlin[r] + dchiL * c.colpart;
+  }
+}
+
+int Heff::arpack_map(int mode, int64_t* d_out, cudaStream_t st) const {
+  if (map_cols.empty() || n_allowed == 0) return CMPS_OK;
+  if (map_cols.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many wavefunction columns");
+  MapCol* dc = nullptr;
+  MapSec* ds = nullptr;
+  int64_t *drl = nullptr, *drt = nullptr;
+  int rc = CMPS_OK;
+  auto up = [&](auto& v, auto** d) -> int {
+    const size_t bytes = sizeof(v[0]) * std::max<size_t>(1, v.size());
+    CMPS_CUDA(dmalloc((void**)d, bytes));
+    return copy_wait(*d, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice, st);
+  };
+  if ((rc = up(map_cols, &dc)) == CMPS_OK && (rc = up(map_secs, &ds)) == CMPS_OK &&
+      (rc = up(map_rowlin, &drl)) == CMPS_OK && (rc = up(map_rowth, &drt)) == CMPS_OK) {
+    const int64_t dchiL = (int64_t)d * L.a.size();
+    k_arpack_map<<<(unsigned)map_cols.size(), 256, 0, st>>>(dc, ds, drl, drt, dchiL, mode, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail(CMPS_ERR_CUDA, std::string("ARPACK index map: ") + cudaGetErrorString(e));
+  }
+  if (dc) dfree(dc);
+  if (ds) dfree(ds);
+  if (drl) dfree(drl);
+  if (drt) dfree(drt);
+  return rc;
+}
+
+int Heff::allowed_indices(int64_t* host_out) const {
+  if (n_allowed == 0) return CMPS_OK;
+  int64_t* tmp = nullptr;
+  CMPS_CUDA(dmalloc(&tmp, sizeof(int64_t) * n_allowed));
+  int rc = arpack_map(1, tmp, ctx->stream);
+  if (rc == CMPS_OK) rc = copy_wait(host_out, tmp, sizeof(int64_t) * n_allowed, cudaMemcpyDeviceToHost, ctx->stream);
+  dfree(tmp);
+  return rc;
+}
+
 int Heff::finish() {
   const Rules& r = rules;
   const Bond& A0 = L.a;
@@ -360,37 +410,44 @@ int Heff::finish() {
     th.total += th.nrows[m] * th.ncols[m];
   }
   // ---- allowed indices, ARPACK order (DMRG_routines.cpp:808-824) ----
+  // ARPACK order = ascending s1 + d a0 + d chiL (s2 + d a2).  Every entry of
+  // sector block m is allowed, so a column (s2, a2) holds exactly the rows of
+  // block m = q(a2) - q(s2), in ascending s1 + d a0 order: the maps follow
+  // from one row list per block and one descriptor per column.
   full_length = (int64_t)d * A0.size() * d * A2.size();
-  std::map<QKey, std::vector<int>> sig_by_q;
-  for (int s1 = 0; s1 < d; ++s1) sig_by_q[sigq[s1]].push_back(s1);
-  allowed.clear();
-  allowed.reserve(th.total);
-  std::vector<int64_t> pos;
-  pos.reserve(th.total);
   const int64_t chiL = A0.size();
+  map_secs.assign(nm, MapSec{0, 0, 0, 0});
+  map_rowlin.clear();
+  map_rowth.clear();
+  for (int m = 0; m < nm; ++m) {
+    map_secs[m].rowstart = (int64_t)map_rowlin.size();
+    for (int64_t a0 = 0; a0 < chiL; ++a0)
+      for (int s1 = 0; s1 < d; ++s1) {
+        if (r.add(sigq[s1], A0.sq[A0.esec[a0]]) != th.mq[m]) continue;
+        map_rowlin.push_back(s1 + (int64_t)d * a0);
+        map_rowth.push_back(th.rowoff[m][s1] + A0.epos[a0]);
+      }
+    map_secs[m].nrows = (int64_t)map_rowlin.size() - map_secs[m].rowstart;
+    map_secs[m].base = th.base[m];
+    map_secs[m].ncols = th.ncols[m];
+    if (map_secs[m].nrows != th.nrows[m]) return fail(CMPS_ERR_STATE, "internal: sector row count mismatch");
+  }
+  map_cols.clear();
+  n_allowed = 0;
   for (int64_t a2 = 0; a2 < A2.size(); ++a2) {
     const QKey qa2 = A2.sq[A2.esec[a2]];
     for (int s2 = 0; s2 < d; ++s2) {
-      QKey m = r.sub(qa2, sigq[s2]);
-      int im = th.find(m);
+      const int im = th.find(r.sub(qa2, sigq[s2]));
       if (im < 0) continue;
-      const int64_t colpart = s2 + (int64_t)d * a2;
-      const int64_t col = th.coloff[im][s2] + A2.epos[a2];
-      for (int64_t a0 = 0; a0 < chiL; ++a0) {
-        QKey need = r.sub(m, A0.sq[A0.esec[a0]]);
-        auto it = sig_by_q.find(need);
-        if (it == sig_by_q.end()) continue;
-        for (int s1 : it->second) {
-          allowed.push_back(s1 + (int64_t)d * a0 + (int64_t)d * chiL * colpart);
-          int64_t row = th.rowoff[im][s1] + A0.epos[a0];
-          pos.push_back(th.base[im] + row * th.ncols[im] + col);
-        }
-      }
+      map_cols.push_back(MapCol{s2 + (int64_t)d * a2, th.coloff[im][s2] + A2.epos[a2], n_allowed, im});
+      n_allowed += th.nrows[im];
     }
   }
-  n_allowed = (int64_t)allowed.size();
   if (n_allowed != th.total) return fail(CMPS_ERR_STATE, "internal: allowed count differs from sector total");
-  CMPS_TRY(upload_vec(pos, &d_pos, ctx->stream));
+  if (d_pos) dfree(d_pos);
+  d_pos = nullptr;
+  CMPS_CUDA(dmalloc(&d_pos, sizeof(int64_t) * std::max<int64_t>(1, n_allowed)));
+  CMPS_TRY(arpack_map(0, d_pos, ctx->stream));
 
   // ---- LeftPart blocks: key (b1, s1', s1, a0-sector s) ----
   lp_off.clear();
@@ -562,8 +619,15 @@ int Heff::finish() {
     for (int q = b.t0; q < b.t1; ++q)
       if (b.dst_off + b.len > rp_total || rp_terms[q].src_off + b.len > R.data.len)
         return fail(CMPS_ERR_STATE, "RightPart block range outside its buffer");
-  for (int64_t p : pos)
-    if (p < 0 || p >= th.total) return fail(CMPS_ERR_STATE, "pack map entry outside the sector blocks");
+  // pack map: every column and row index inside its sector block
+  for (const MapCol& c : map_cols)
+    if (c.m < 0 || c.m >= nm || c.colth < 0 || c.colth >= th.ncols[c.m])
+      return fail(CMPS_ERR_STATE, "pack map column outside the sector blocks");
+  for (int m = 0; m < nm; ++m)
+    for (int64_t i = 0; i < map_secs[m].nrows; ++i) {
+      const int64_t rt = map_rowth[map_secs[m].rowstart + i];
+      if (rt < 0 || rt >= th.nrows[m]) return fail(CMPS_ERR_STATE, "pack map row outside the sector blocks");
+    }
   CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   cudaStream_t st = ctx->stream;
@@ -614,7 +678,7 @@ int Heff::finish() {
   }
   CMPS_TRY(x.alloc(th.total));
   CMPS_TRY(y.alloc(th.total));
-  CMPS_CUDA(cudaMalloc(&d_io, sizeof(double) * 2 * std::max<int64_t>(1, n_allowed)));
+  CMPS_CUDA(dmalloc(&d_io, sizeof(double) * 2 * std::max<int64_t>(1, n_allowed)));
   CMPS_TRY(ops.init(th.total));
   CMPS_CUDA(cudaStreamSynchronize(st));
   return CMPS_OK;

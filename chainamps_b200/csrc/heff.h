@@ -51,8 +51,22 @@ struct Heff {
   std::vector<int16_t> bq_raw;  // as given (for export)
   ThetaSpace th;
   int64_t n_allowed = 0, full_length = 0;
-  std::vector<int64_t> allowed;  // ARPACK order -> full linear index
   int64_t* d_pos = nullptr;      // ARPACK order -> theta block offset
+  // ARPACK-order maps, generated on the device from per-column and per-sector
+  // descriptors (a few thousand entries instead of n host-side ones)
+  struct MapCol {
+    int64_t colpart, colth, start;  // s2 + d a2; theta column in its block; first ARPACK index
+    int64_t m;
+  };
+  struct MapSec {
+    int64_t rowstart, nrows, base, ncols;  // rows of block m in ARPACK row order
+  };
+  std::vector<MapCol> map_cols;
+  std::vector<MapSec> map_secs;
+  std::vector<int64_t> map_rowlin, map_rowth;  // per allowed row: s1 + d a0, theta row
+  // mode 0: ARPACK index -> theta offset (d_pos); mode 1: -> full linear index
+  int arpack_map(int mode, int64_t* d_out, cudaStream_t st) const;
+  int allowed_indices(int64_t* host_out) const;
   // LeftPart / RightPart sector blocks
   Planar LP, RP;
   std::vector<AxpyBlock> lp_blocks, rp_blocks;

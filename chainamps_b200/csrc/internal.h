@@ -41,6 +41,21 @@ int fail(int code, const std::string& msg);
 int copy_wait(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st);
 int zero_wait(void* dst, size_t bytes, cudaStream_t st);
 
+// Device memory of the library.  A DMRG step frees and re-allocates buffers
+// of several GB (Krylov basis, LeftPart/RightPart, T, split operands, SVD
+// work); plain cudaMalloc / cudaFree map and unmap that memory every step,
+// which costs up to hundreds of ms at unpredictable points.  These take it
+// from the current device's stream-ordered pool instead, whose release
+// threshold is raised so freed memory stays mapped for the next step.  Both
+// keep the synchronisation of cudaMalloc / cudaFree: dmalloc returns memory
+// usable from any stream, dfree waits for the device before releasing.
+cudaError_t dmalloc(void** p, size_t bytes);
+cudaError_t dfree(void* p);
+template <class T>
+inline cudaError_t dmalloc(T** p, size_t bytes) {
+  return dmalloc(reinterpret_cast<void**>(p), bytes);
+}
+
 // Charge arithmetic of State (states.hpp:176-206).
 struct Rules {
   int nq = 0;

@@ -379,18 +379,18 @@ int VecOps::init(int64_t n_) {
   n = n_;
   nb = grid_for(n, RED_THREADS);
   if (nb > 1024) nb = 1024;
-  CMPS_CUDA(cudaMalloc(&d_partial, sizeof(double) * (2 * 128 + 2) * nb));
-  CMPS_CUDA(cudaMalloc(&d_coef, sizeof(double) * kCoefDoubles));
-  CMPS_CUDA(cudaMalloc(&d_small, sizeof(double) * 2 * 128 * 2));
-  CMPS_CUDA(cudaMalloc(&d_pidx, sizeof(int64_t) * nb));
+  CMPS_CUDA(dmalloc(&d_partial, sizeof(double) * (2 * 128 + 2) * nb));
+  CMPS_CUDA(dmalloc(&d_coef, sizeof(double) * kCoefDoubles));
+  CMPS_CUDA(dmalloc(&d_small, sizeof(double) * 2 * 128 * 2));
+  CMPS_CUDA(dmalloc(&d_pidx, sizeof(int64_t) * nb));
   return CMPS_OK;
 }
 
 void VecOps::release() {
-  if (d_partial) cudaFree(d_partial);
-  if (d_small) cudaFree(d_small);
-  if (d_pidx) cudaFree(d_pidx);
-  if (d_coef) cudaFree(d_coef);
+  if (d_partial) dfree(d_partial);
+  if (d_small) dfree(d_small);
+  if (d_pidx) dfree(d_pidx);
+  if (d_coef) dfree(d_coef);
   d_partial = d_small = d_coef = nullptr;
   d_pidx = nullptr;
 }

@@ -31,7 +31,10 @@ struct SplitState {
   std::vector<int64_t> ncols_pad;               // per m
   float* buf = nullptr;                         // one allocation for S1A, LPS, TS, RPTS
   int64_t s1a_off = 0, s1a_len = 0, lps_off = 0, lps_len = 0, ts_off = 0, ts_len = 0, rpt_off = 0, rpt_len = 0;
-  int64_t* d_theta_map = nullptr;
+  // theta -> S1A: one descriptor per (m, sigma1, sigma2) chunk, one per 32x32 tile
+  void* d_theta_chunks = nullptr;
+  void* d_theta_tiles = nullptr;
+  int64_t n_theta_tiles = 0;
   int* d_err = nullptr;
   int* h_err = nullptr;  // pinned
   tc::TcPlan p1, p2;
@@ -73,11 +76,48 @@ __global__ void k_split_blocks(const SplitBlock* __restrict__ blocks, const doub
   }
 }
 
-__global__ void k_split_theta(const double* __restrict__ re, const double* __restrict__ im,
-                              const int64_t* __restrict__ map, int64_t n, float* __restrict__ dst, int64_t plane) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t o = map[e];
-    split4(re[e], im[e], dst + o, dst + o + plane, dst + o + 2 * plane, dst + o + 3 * plane);
+// A (m, sigma1, sigma2) chunk of theta: rows a0 (sector dim), columns a2,
+// row-major inside its sector block; its S1A image is the transpose [a2][a0].
+struct ThetaChunk {
+  int64_t src_off, src_ld, dst_off, dst_ld;
+  int32_t rows, cols;
+};
+struct ThetaTile {
+  int32_t chunk, r0, c0, pad;
+};
+
+// theta -> split S1A, one 32 x 32 tile per CTA, transposed through shared
+// memory so that both the FP64 reads and the FP32 plane writes coalesce.
+__global__ void __launch_bounds__(256) k_split_theta_t(const ThetaTile* __restrict__ tiles,
+                                                       const ThetaChunk* __restrict__ chunks,
+                                                       const double* __restrict__ re, const double* __restrict__ im,
+                                                       float* __restrict__ dst, int64_t plane) {
+  __shared__ float4 t[32][33];
+  const ThetaTile tl = tiles[blockIdx.x];
+  const ThetaChunk c = chunks[tl.chunk];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = tl.r0 + ty + 8 * k, col = tl.c0 + tx;
+    if (r < c.rows && col < c.cols) {
+      const int64_t o = c.src_off + (int64_t)r * c.src_ld + col;
+      float4 v;
+      split4(re[o], im[o], &v.x, &v.y, &v.z, &v.w);
+      t[ty + 8 * k][tx] = v;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int col = tl.c0 + ty + 8 * k, r = tl.r0 + tx;
+    if (r < c.rows && col < c.cols) {
+      const float4 v = t[tx][ty + 8 * k];
+      const int64_t o = c.dst_off + (int64_t)col * c.dst_ld + r;
+      dst[o] = v.x;
+      dst[o + plane] = v.y;
+      dst[o + 2 * plane] = v.z;
+      dst[o + 3 * plane] = v.w;
+    }
   }
 }
 
@@ -126,7 +166,7 @@ int TcPlan::upload(cudaStream_t st) {
   auto up = [st](auto& v, auto** d) -> int {
     if (v.empty()) return CMPS_OK;
     size_t bytes = v.size() * sizeof(v[0]);
-    CMPS_CUDA(cudaMalloc((void**)d, bytes));
+    CMPS_CUDA(dmalloc((void**)d, bytes));
     return copy_wait(*d, v.data(), bytes, cudaMemcpyHostToDevice, st);
   };
   CMPS_TRY(up(tasks, &d_tasks));
@@ -137,11 +177,11 @@ int TcPlan::upload(cudaStream_t st) {
   return CMPS_OK;
 }
 void TcPlan::release() {
-  if (d_tasks) cudaFree(d_tasks);
-  if (d_terms) cudaFree(d_terms);
-  if (d_tiles) cudaFree(d_tiles);
-  if (d_amaps) cudaFree(d_amaps);
-  if (d_bmaps) cudaFree(d_bmaps);
+  if (d_tasks) dfree(d_tasks);
+  if (d_terms) dfree(d_terms);
+  if (d_tiles) dfree(d_tiles);
+  if (d_amaps) dfree(d_amaps);
+  if (d_bmaps) dfree(d_bmaps);
   d_tasks = nullptr;
   d_terms = nullptr;
   d_tiles = nullptr;
@@ -155,9 +195,10 @@ void release_split(Heff* h) {
   SplitState* s = h->split;
   s->p1.release();
   s->p2.release();
-  if (s->buf) cudaFree(s->buf);
-  if (s->d_theta_map) cudaFree(s->d_theta_map);
-  if (s->d_err) cudaFree(s->d_err);
+  if (s->buf) dfree(s->buf);
+  if (s->d_theta_chunks) dfree(s->d_theta_chunks);
+  if (s->d_theta_tiles) dfree(s->d_theta_tiles);
+  if (s->d_err) dfree(s->d_err);
   if (s->h_err) cudaFreeHost(s->h_err);
   delete s;
   h->split = nullptr;
@@ -239,11 +280,11 @@ static int build_split(Heff& H) {
   S->rpt_off = S->ts_off + 4 * S->ts_len;
   S->rpt_len = align32(std::max<int64_t>(rpt, 32));
   const int64_t total = S->rpt_off + 4 * S->rpt_len;
-  if (cudaMalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
+  if (dmalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
     return fail(CMPS_ERR_NOMEM, "split-TF32 operand allocation failed");
   // zero fill: padding rows and columns of every operand must read as zero
   CMPS_TRY(zero_wait(S->buf, sizeof(float) * total, H.ctx->stream));
-  CMPS_CUDA(cudaMalloc(&S->d_err, sizeof(int)));
+  CMPS_CUDA(dmalloc(&S->d_err, sizeof(int)));
   CMPS_TRY(zero_wait(S->d_err, sizeof(int), H.ctx->stream));
   CMPS_CUDA(cudaMallocHost(&S->h_err, sizeof(int)));
   // ---- split LeftPart / RightPart ----
@@ -259,7 +300,7 @@ static int build_split(Heff& H) {
         if (b.dst_off + (rows - 1) * b.ld_dst + cols > len || b.ld_dst < cols)
           return fail(CMPS_ERR_STATE, "split block outside its buffer");
       }
-      CMPS_CUDA(cudaMalloc(&d, sizeof(SplitBlock) * v.size()));
+      CMPS_CUDA(dmalloc(&d, sizeof(SplitBlock) * v.size()));
       CMPS_TRY(copy_wait(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice, H.ctx->stream));
       const Planar& src = pass == 0 ? H.LP : H.RP;
       float* dst = S->buf + (pass == 0 ? S->lps_off : S->rpt_off);
@@ -267,12 +308,13 @@ static int build_split(Heff& H) {
       k_split_blocks<<<(unsigned)v.size(), 256, 0, H.ctx->stream>>>(d, src.re(), src.im(), dst, plane);
       CMPS_CUDA(cudaGetLastError());
       CMPS_CUDA(cudaStreamSynchronize(H.ctx->stream));
-      cudaFree(d);
+      dfree(d);
     }
   }
-  // ---- theta -> S1A map ----
+  // ---- theta -> S1A chunk and tile descriptors ----
   {
-    std::vector<int64_t> map(th.total, -1);
+    std::vector<ThetaChunk> chunks;
+    std::vector<ThetaTile> tiles;
     for (int m = 0; m < nm; ++m)
       for (int s1 = 0; s1 < d; ++s1) {
         if (th.rowoff[m][s1] < 0) continue;
@@ -281,18 +323,32 @@ static int build_split(Heff& H) {
         for (int s2 = 0; s2 < d; ++s2) {
           if (th.coloff[m][s2] < 0) continue;
           int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
-          for (int64_t p = 0; p < A0.sdim[s]; ++p)
-            for (int64_t c = 0; c < A2.sdim[t]; ++c) {
-              const int64_t src = th.base[m] + (th.rowoff[m][s1] + p) * th.ncols[m] + th.coloff[m][s2] + c;
-              map[src] = ch + (S->coloff_pad[m][s2] + c) * S->ldS[s] + p;
-            }
+          ThetaChunk c{};
+          c.src_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m] + th.coloff[m][s2];
+          c.src_ld = th.ncols[m];
+          c.dst_off = ch + S->coloff_pad[m][s2] * S->ldS[s];
+          c.dst_ld = S->ldS[s];
+          c.rows = (int32_t)A0.sdim[s];
+          c.cols = (int32_t)A2.sdim[t];
+          // both images inside their buffers
+          if (c.src_off + (int64_t)(c.rows - 1) * c.src_ld + c.cols > th.total ||
+              c.dst_off + (int64_t)(c.cols - 1) * c.dst_ld + c.rows > S->s1a_len || c.dst_ld < c.rows)
+            return fail(CMPS_ERR_STATE, "theta split chunk outside its buffer");
+          for (int32_t r0 = 0; r0 < c.rows; r0 += 32)
+            for (int32_t c0 = 0; c0 < c.cols; c0 += 32) tiles.push_back(ThetaTile{(int32_t)chunks.size(), r0, c0, 0});
+          chunks.push_back(c);
         }
       }
-    for (int64_t v : map)
-      if (v < 0 || v >= S->s1a_len) return fail(CMPS_ERR_STATE, "theta split map incomplete");
-    CMPS_CUDA(cudaMalloc(&S->d_theta_map, sizeof(int64_t) * std::max<int64_t>(1, th.total)));
-    CMPS_TRY(copy_wait(S->d_theta_map, map.data(), sizeof(int64_t) * th.total, cudaMemcpyHostToDevice,
-                       H.ctx->stream));
+    if (tiles.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many theta tiles");
+    S->n_theta_tiles = (int64_t)tiles.size();
+    if (!chunks.empty()) {
+      CMPS_CUDA(dmalloc(&S->d_theta_chunks, sizeof(ThetaChunk) * chunks.size()));
+      CMPS_TRY(copy_wait(S->d_theta_chunks, chunks.data(), sizeof(ThetaChunk) * chunks.size(), cudaMemcpyHostToDevice,
+                         H.ctx->stream));
+      CMPS_CUDA(dmalloc(&S->d_theta_tiles, sizeof(ThetaTile) * tiles.size()));
+      CMPS_TRY(copy_wait(S->d_theta_tiles, tiles.data(), sizeof(ThetaTile) * tiles.size(), cudaMemcpyHostToDevice,
+                         H.ctx->stream));
+    }
   }
   // ---- stage 1 plan: C1[r_pad, a0'] = sum S1A[r_pad, a0] LPS[a0', a0] ----
   tc::TcPlan& p1 = S->p1;
@@ -442,6 +498,15 @@ int prepare_precision(Heff* h, int precision) {
   return st;
 }
 
+static int split_theta(const SplitState& S, const Planar& in, cudaStream_t st) {
+  if (S.n_theta_tiles == 0) return CMPS_OK;
+  k_split_theta_t<<<(unsigned)S.n_theta_tiles, 256, 0, st>>>((const ThetaTile*)S.d_theta_tiles,
+                                                             (const ThetaChunk*)S.d_theta_chunks, in.re(), in.im(),
+                                                             S.buf + S.s1a_off, S.s1a_len);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
 int split_reset_error(Heff& H, cudaStream_t st) {
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
@@ -453,12 +518,8 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   const int64_t n = H.th.total;
-  int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
-  if (n > 0) {
-    k_split_theta<<<std::max(grid, 1), 256, 0, st>>>(in.re(), in.im(), S->d_theta_map, n, S->buf + S->s1a_off,
-                                                     S->s1a_len);
-    CMPS_CUDA(cudaGetLastError());
-  }
+  (void)n;
+  CMPS_TRY(split_theta(*S, in, st));
   CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st));
   CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st));
   return CMPS_OK;
@@ -481,10 +542,7 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   const int64_t n = H.th.total;
   if (which == 1) {
     CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
-    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
-    k_split_theta<<<std::max(grid, 1), 256, 0, st>>>(in.re(), in.im(), S->d_theta_map, n, S->buf + S->s1a_off,
-                                                     S->s1a_len);
-    CMPS_CUDA(cudaGetLastError());
+    CMPS_TRY(split_theta(*S, in, st));
     return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st);
   }
   return tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st);

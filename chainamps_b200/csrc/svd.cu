@@ -204,25 +204,25 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
   double* dS = nullptr;
   int* dinfo = nullptr;
   auto cleanup = [&]() {
-    if (dflags) cudaFree(dflags);
-    if (dweight) cudaFree(dweight);
-    if (dA) cudaFree(dA);
-    if (dS) cudaFree(dS);
-    if (dinfo) cudaFree(dinfo);
+    if (dflags) dfree(dflags);
+    if (dweight) dfree(dweight);
+    if (dA) dfree(dA);
+    if (dS) dfree(dS);
+    if (dinfo) dfree(dinfo);
     for (auto& b : blk) {
-      if (b.dU) cudaFree(b.dU);
-      if (b.dV) cudaFree(b.dV);
-      if (b.drows) cudaFree(b.drows);
-      if (b.dcols) cudaFree(b.dcols);
+      if (b.dU) dfree(b.dU);
+      if (b.dV) dfree(b.dV);
+      if (b.drows) dfree(b.drows);
+      if (b.dcols) dfree(b.dcols);
     }
   };
   int status = CMPS_OK;
   do {
-    if (cudaMalloc(&dflags, sizeof(int) * (maxr + maxc)) != cudaSuccess ||
-        cudaMalloc(&dweight, sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&dA, sizeof(double2) * maxr * maxc) != cudaSuccess ||
-        cudaMalloc(&dS, sizeof(double) * std::min(maxr, maxc)) != cudaSuccess ||
-        cudaMalloc(&dinfo, sizeof(int)) != cudaSuccess) {
+    if (dmalloc(&dflags, sizeof(int) * (maxr + maxc)) != cudaSuccess ||
+        dmalloc(&dweight, sizeof(double)) != cudaSuccess ||
+        dmalloc(&dA, sizeof(double2) * maxr * maxc) != cudaSuccess ||
+        dmalloc(&dS, sizeof(double) * std::min(maxr, maxc)) != cudaSuccess ||
+        dmalloc(&dinfo, sizeof(int)) != cudaSuccess) {
       status = fail(CMPS_ERR_NOMEM, "SVD workspace allocation failed");
       break;
     }
@@ -253,10 +253,10 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       for (int64_t j = 0; j < C; ++j) if (fl[R + j]) b.cols.push_back(j);
       const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
       const int64_t mn = std::min(nr, nc);
-      if (cudaMalloc(&b.drows, sizeof(int64_t) * nr) != cudaSuccess ||
-          cudaMalloc(&b.dcols, sizeof(int64_t) * nc) != cudaSuccess ||
-          cudaMalloc(&b.dU, sizeof(double2) * nr * mn) != cudaSuccess ||
-          cudaMalloc(&b.dV, sizeof(double2) * nc * mn) != cudaSuccess) {
+      if (dmalloc(&b.drows, sizeof(int64_t) * nr) != cudaSuccess ||
+          dmalloc(&b.dcols, sizeof(int64_t) * nc) != cudaSuccess ||
+          dmalloc(&b.dU, sizeof(double2) * nr * mn) != cudaSuccess ||
+          dmalloc(&b.dV, sizeof(double2) * nc * mn) != cudaSuccess) {
         status = fail(CMPS_ERR_NOMEM, "SVD block allocation failed");
         break;
       }
@@ -289,7 +289,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
                                          (int)nc, &lwork, params) != CUSOLVER_STATUS_SUCCESS)
           return fail(CMPS_ERR_SOLVER, "gesvdj buffer query failed");
         cuDoubleComplex* work = nullptr;
-        if (cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+        if (dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
           return fail(CMPS_ERR_NOMEM, "SVD work allocation failed");
         cusolverStatus_t cs = cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                                 (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr,
@@ -298,7 +298,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t ce = cudaStreamSynchronize(st);
-        cudaFree(work);
+        dfree(work);
         if (cs != CUSOLVER_STATUS_SUCCESS || ce != cudaSuccess) return fail(CMPS_ERR_SOLVER, "gesvdj failed");
         if (info < 0) return fail(CMPS_ERR_SOLVER, "gesvdj: invalid argument");
         return CMPS_OK;  // info > 0: not converged to tolerance within max sweeps; values still usable
@@ -309,9 +309,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       double2* G = nullptr;   // Gram matrix, then its eigenvectors
       double* W = nullptr;
       int lwork = 0;
-      if (cudaMalloc(&G, sizeof(double2) * (size_t)p * p) != cudaSuccess ||
-          cudaMalloc(&W, sizeof(double) * p) != cudaSuccess) {
-        if (G) cudaFree(G);
+      if (dmalloc(&G, sizeof(double2) * (size_t)p * p) != cudaSuccess ||
+          dmalloc(&W, sizeof(double) * p) != cudaSuccess) {
+        if (G) dfree(G);
         return fail(CMPS_ERR_NOMEM, "Gram matrix allocation failed");
       }
       const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
@@ -328,7 +328,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (rc == CMPS_OK && cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
                                                        (cuDoubleComplex*)G, p, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
         rc = fail(CMPS_ERR_SOLVER, "zheevd buffer query failed");
-      if (rc == CMPS_OK && cudaMalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+      if (rc == CMPS_OK && dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
         rc = fail(CMPS_ERR_NOMEM, "zheevd work allocation failed");
       if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
                                             (cuDoubleComplex*)G, p, W, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
@@ -356,9 +356,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         k_scale_cols_inv<<<grid_of((left ? nc : nr) * (int64_t)p), 256, 0, st>>>(O, left ? nc : nr, p, dS);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(CMPS_ERR_CUDA, "eigen-route SVD failed");
       }
-      if (work) cudaFree(work);
-      cudaFree(G);
-      cudaFree(W);
+      if (work) dfree(work);
+      dfree(G);
+      dfree(W);
       return rc;
     };
     for (int m = 0; m < nm && status == CMPS_OK; ++m)

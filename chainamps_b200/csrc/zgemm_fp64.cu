@@ -227,7 +227,7 @@ int GemmPlan::upload(int bm, int bn, cudaStream_t st) {
   auto up = [st](auto& v, auto** d) -> int {
     if (v.empty()) return CMPS_OK;
     size_t bytes = v.size() * sizeof(v[0]);
-    CMPS_CUDA(cudaMalloc((void**)d, bytes));
+    CMPS_CUDA(dmalloc((void**)d, bytes));
     return copy_wait(*d, v.data(), bytes, cudaMemcpyHostToDevice, st);
   };
   CMPS_TRY(up(tasks, &d_tasks));
@@ -259,9 +259,9 @@ int GemmPlan::validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t
 }
 
 void GemmPlan::release() {
-  if (d_tasks) cudaFree(d_tasks);
-  if (d_terms) cudaFree(d_terms);
-  if (d_tiles) cudaFree(d_tiles);
+  if (d_tasks) dfree(d_tasks);
+  if (d_terms) dfree(d_terms);
+  if (d_tiles) dfree(d_tiles);
   d_tasks = nullptr;
   d_terms = nullptr;
   d_tiles = nullptr;

@@ -220,11 +220,13 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
 /* The current (rescaled) singular values, bond_dim of them, descending. */
 int cmps_dmrg_values(const cmps_dmrg* d, double* values);
 /* Breakdown of the last growth step (no reference counterpart;
- * diagnostics).  out10 = {environment update ms, H_eff build + prediction
- * ms, eigensolve ms, SVD ms, total ms, split matvecs, FP64 matvecs, restart
- * cycles, split matvec ms, FP64 matvec ms}; times are device time (CUDA
- * events). */
-int cmps_dmrg_profile(const cmps_dmrg* d, double* out10);
+ * diagnostics).  Writes the first n (<= 17) of: {environment update ms, H_eff
+ * build + prediction ms, eigensolve ms, SVD ms, total ms (device time, CUDA
+ * events); split matvecs, FP64 matvecs, restart cycles, split matvec ms,
+ * FP64 matvec ms; host wall ms of environment update, H_eff build, split
+ * operand preparation, prediction, release of the previous step, SVD, whole
+ * step}. */
+int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n);
 
 #ifdef __cplusplus
 }
