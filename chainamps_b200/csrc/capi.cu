@@ -223,13 +223,13 @@ int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void*
   int status = CMPS_OK;
   for (int r = 0; r < reps && status == CMPS_OK; ++r) {
     cudaEventRecord(ev[0], st);
-    status = launch_pack(d_in, H.d_pos, H.n_allowed, H.x, st);
+    status = H.pack(d_in, H.x, st);
     cudaEventRecord(ev[1], st);
     if (status == CMPS_OK) status = H.apply_stage(1, H.x, H.y, st);
     cudaEventRecord(ev[2], st);
     if (status == CMPS_OK) status = H.apply_stage(2, H.x, H.y, st);
     cudaEventRecord(ev[3], st);
-    if (status == CMPS_OK) status = launch_unpack(H.y, H.d_pos, H.n_allowed, d_out, st);
+    if (status == CMPS_OK) status = H.unpack(H.y, d_out, st);
     cudaEventRecord(ev[4], st);
     if (cudaEventSynchronize(ev[4]) != cudaSuccess) status = fail(CMPS_ERR_CUDA, "stage timing failed");
     for (int k = 0; k < 4 && status == CMPS_OK; ++k) {
@@ -296,7 +296,7 @@ int cmps_heff_set_theta(cmps_heff* h, const double* theta) {
   cudaStream_t st = H.ctx->stream;
   CMPS_CUDA(cudaMemcpyAsync(H.d_io, theta, sizeof(double) * 2 * H.n_allowed, cudaMemcpyHostToDevice, st));
   if (H.theta.len != H.th.total) CMPS_TRY(H.theta.alloc(H.th.total));
-  CMPS_TRY(launch_pack(H.d_io, H.d_pos, H.n_allowed, H.theta, st));
+  CMPS_TRY(H.pack(H.d_io, H.theta, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
   H.have_theta = true;
   return CMPS_OK;

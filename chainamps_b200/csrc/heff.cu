@@ -237,7 +237,7 @@ Heff::~Heff() {
   stage1.release();
   stage2.release();
   ops.release();
-  if (d_pos) dfree(d_pos);
+  if (d_pack) dfree(d_pack);
   if (d_io) dfree(d_io);
   if (h_ab) cudaFreeHost(h_ab);
   if (d_lp_blocks) dfree(d_lp_blocks);
@@ -369,6 +369,137 @@ int Heff::allowed_indices(int64_t* host_out) const {
   return rc;
 }
 
+// ARPACK order -> sector blocks: CTA = (group of <= 32 columns, 32 rows).
+// Reads run down each ARPACK column (contiguous), writes along theta rows
+// (the group's columns are consecutive theta columns).
+template <bool PACK>
+__global__ void __launch_bounds__(256) k_pack_tiles(const Heff::PackTile* __restrict__ tiles,
+                                                    const Heff::PackGroup* __restrict__ groups,
+                                                    const int32_t* __restrict__ gcols,
+                                                    const Heff::MapCol* __restrict__ cols,
+                                                    const Heff::MapSec* __restrict__ secs,
+                                                    const int64_t* __restrict__ rowth, double2* __restrict__ arp,
+                                                    double* __restrict__ re, double* __restrict__ im) {
+  __shared__ double2 t[32][33];  // [column j][row r]
+  const Heff::PackTile tl = tiles[blockIdx.x];
+  const Heff::PackGroup g = groups[tl.group];
+  const Heff::MapSec s = secs[g.m];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t left = s.nrows - tl.r0;
+  const int nr = left < 32 ? (int)left : 32;
+  if (PACK) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int j = ty + 8 * k, r = tx;
+      if (j < g.cnt && r < nr) t[j][r] = arp[cols[gcols[g.off + j]].start + tl.r0 + r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = ty + 8 * k, j = tx;
+      if (j < g.cnt && r < nr) {
+        const int64_t p = s.base + rowth[s.rowstart + tl.r0 + r] * s.ncols + cols[gcols[g.off + j]].colth;
+        const double2 v = t[j][r];
+        re[p] = v.x;
+        im[p] = v.y;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = ty + 8 * k, j = tx;
+      if (j < g.cnt && r < nr) {
+        const int64_t p = s.base + rowth[s.rowstart + tl.r0 + r] * s.ncols + cols[gcols[g.off + j]].colth;
+        t[j][r] = make_double2(re[p], im[p]);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int j = ty + 8 * k, r = tx;
+      if (j < g.cnt && r < nr) arp[cols[gcols[g.off + j]].start + tl.r0 + r] = t[j][r];
+    }
+  }
+}
+
+int Heff::build_pack(cudaStream_t st) {
+  // ARPACK column index of (a2, s2), then groups per (m, s2) in a2-sector order
+  const Bond& A2 = R.a;
+  std::vector<int32_t> col_of((size_t)A2.size() * d, -1);
+  for (size_t c = 0; c < map_cols.size(); ++c) {
+    const int64_t s2 = map_cols[c].colpart % d, a2 = map_cols[c].colpart / d;
+    col_of[(size_t)a2 * d + s2] = (int32_t)c;
+  }
+  std::vector<std::vector<int64_t>> elems(A2.nsec());
+  for (int64_t a2 = 0; a2 < A2.size(); ++a2) elems[A2.esec[a2]].push_back(a2);
+  std::vector<int32_t> gcols;
+  std::vector<PackGroup> groups;
+  std::vector<PackTile> tiles;
+  for (int m = 0; m < (int)th.mq.size(); ++m)
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      const int t = A2.find(rules.add(th.mq[m], sigq[s2]));
+      const std::vector<int64_t>& el = elems[t];
+      for (size_t e0 = 0; e0 < el.size(); e0 += 32) {
+        PackGroup g{(int64_t)gcols.size(), (int32_t)std::min<size_t>(32, el.size() - e0), m};
+        for (int j = 0; j < g.cnt; ++j) {
+          const int32_t c = col_of[(size_t)el[e0 + j] * d + s2];
+          if (c < 0 || map_cols[c].m != m || map_cols[c].colth != th.coloff[m][s2] + (int64_t)(e0 + j))
+            return fail(CMPS_ERR_STATE, "internal: pack group columns not consecutive");
+          gcols.push_back(c);
+        }
+        for (int64_t r0 = 0; r0 < th.nrows[m]; r0 += 32) tiles.push_back(PackTile{(int32_t)groups.size(), (int32_t)r0});
+        groups.push_back(g);
+      }
+    }
+  if (tiles.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many pack tiles");
+  n_pack_tiles = 0;
+  if (tiles.empty()) return CMPS_OK;
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t b_cols = al(sizeof(MapCol) * map_cols.size()), b_secs = al(sizeof(MapSec) * map_secs.size()),
+               b_rowth = al(sizeof(int64_t) * map_rowth.size()), b_gcols = al(sizeof(int32_t) * gcols.size()),
+               b_groups = al(sizeof(PackGroup) * groups.size()), b_tiles = al(sizeof(PackTile) * tiles.size());
+  if (d_pack) dfree(d_pack);
+  d_pack = nullptr;
+  CMPS_CUDA(dmalloc(&d_pack, b_cols + b_secs + b_rowth + b_gcols + b_groups + b_tiles));
+  char* p = (char*)d_pack;
+  d_map_cols = (const MapCol*)p;
+  CMPS_TRY(copy_wait(p, map_cols.data(), sizeof(MapCol) * map_cols.size(), cudaMemcpyHostToDevice, st));
+  p += b_cols;
+  d_map_secs = (const MapSec*)p;
+  CMPS_TRY(copy_wait(p, map_secs.data(), sizeof(MapSec) * map_secs.size(), cudaMemcpyHostToDevice, st));
+  p += b_secs;
+  d_map_rowth = (const int64_t*)p;
+  CMPS_TRY(copy_wait(p, map_rowth.data(), sizeof(int64_t) * map_rowth.size(), cudaMemcpyHostToDevice, st));
+  p += b_rowth;
+  d_pack_gcols = (const int32_t*)p;
+  CMPS_TRY(copy_wait(p, gcols.data(), sizeof(int32_t) * gcols.size(), cudaMemcpyHostToDevice, st));
+  p += b_gcols;
+  d_pack_groups = (const PackGroup*)p;
+  CMPS_TRY(copy_wait(p, groups.data(), sizeof(PackGroup) * groups.size(), cudaMemcpyHostToDevice, st));
+  p += b_groups;
+  d_pack_tiles = (const PackTile*)p;
+  CMPS_TRY(copy_wait(p, tiles.data(), sizeof(PackTile) * tiles.size(), cudaMemcpyHostToDevice, st));
+  n_pack_tiles = (int64_t)tiles.size();
+  return CMPS_OK;
+}
+
+int Heff::pack(const double* in, const Planar& out, cudaStream_t st) const {
+  if (n_pack_tiles == 0) return CMPS_OK;
+  k_pack_tiles<true><<<(unsigned)n_pack_tiles, 256, 0, st>>>(d_pack_tiles, d_pack_groups, d_pack_gcols, d_map_cols,
+                                                             d_map_secs, d_map_rowth, (double2*)in, out.re(), out.im());
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int Heff::unpack(const Planar& in, double* out, cudaStream_t st) const {
+  if (n_pack_tiles == 0) return CMPS_OK;
+  k_pack_tiles<false><<<(unsigned)n_pack_tiles, 256, 0, st>>>(d_pack_tiles, d_pack_groups, d_pack_gcols, d_map_cols,
+                                                              d_map_secs, d_map_rowth, (double2*)out, in.re(), in.im());
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
 int Heff::finish() {
   const Rules& r = rules;
   const Bond& A0 = L.a;
@@ -444,10 +575,6 @@ int Heff::finish() {
     }
   }
   if (n_allowed != th.total) return fail(CMPS_ERR_STATE, "internal: allowed count differs from sector total");
-  if (d_pos) dfree(d_pos);
-  d_pos = nullptr;
-  CMPS_CUDA(dmalloc(&d_pos, sizeof(int64_t) * std::max<int64_t>(1, n_allowed)));
-  CMPS_TRY(arpack_map(0, d_pos, ctx->stream));
 
   // ---- LeftPart blocks: key (b1, s1', s1, a0-sector s) ----
   lp_off.clear();
@@ -628,6 +755,7 @@ int Heff::finish() {
       const int64_t rt = map_rowth[map_secs[m].rowstart + i];
       if (rt < 0 || rt >= th.nrows[m]) return fail(CMPS_ERR_STATE, "pack map row outside the sector blocks");
     }
+  CMPS_TRY(build_pack(ctx->stream));
   CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   cudaStream_t st = ctx->stream;
@@ -704,14 +832,14 @@ int Heff::apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
-  CMPS_TRY(launch_pack(din, d_pos, n_allowed, x, st));
+  CMPS_TRY(pack(din, x, st));
   if (precision == CMPS_SPLIT_TF32) {
     CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
     CMPS_TRY(apply_split_stage(*this, 2, x, y, st));
   } else {
     CMPS_TRY(apply_theta(x, y, st));
   }
-  CMPS_TRY(launch_unpack(y, d_pos, n_allowed, dout, st));
+  CMPS_TRY(unpack(y, dout, st));
   return CMPS_OK;
 }
 
@@ -817,9 +945,9 @@ static void tridiag_lowest(int k, const double* a, const double* b, double* lam,
   y = z;
 }
 
-// Restarted Lanczos with full re-orthogonalisation (classical Gram-Schmidt,
-// two passes per step), coefficients kept on the device and a convergence
-// check after every step.
+// Restarted Lanczos with full re-orthogonalisation (the local three-term
+// step, then one classical Gram-Schmidt pass against the whole basis),
+// coefficients kept on the device and a convergence check after every step.
 //
 // FP64 operator: every step uses the FP64 matvec; the run ends when the Ritz
 // residual estimate |beta_j y_j| falls below tol |lambda|.
@@ -874,7 +1002,7 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   // start vector into x
   if (guess) {
     CMPS_CUDA(cudaMemcpyAsync(d_io, guess, sizeof(double) * 2 * n_allowed, cudaMemcpyHostToDevice, st));
-    CMPS_TRY(launch_pack(d_io, d_pos, n_allowed, x, st));
+    CMPS_TRY(pack(d_io, x, st));
   }
   double nrm0 = 0.0;
   const bool have_start = guess || start_in_x;
@@ -913,12 +1041,16 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
       }
       CMPS_CUDA(cudaEventRecord(ev[1], st));
       ++nmv;
-      // two classical Gram-Schmidt passes against v_0..v_j
-      CMPS_TRY(ops.mdot_dev(kv.d, kv.d + n, ldv, j + 1, y.re(), y.im(), hA, st));
-      CMPS_TRY(ops.maxpy_norm_dev(kv.d, kv.d + n, ldv, j + 1, hA, y.re(), y.im(), nrm, st));
-      CMPS_TRY(ops.mdot_dev(kv.d, kv.d + n, ldv, j + 1, y.re(), y.im(), hB, st));
+      // local three-term step (y -= beta_{j-1} v_{j-1}, alpha = <v_j, y>,
+      // y -= alpha v_j), then one full classical Gram-Schmidt pass against
+      // v_0..v_j that removes what rounding and the split operator's
+      // non-Hermitian error leave behind
+      const double* vp = j > 0 ? vre(j - 1) : nullptr;
+      CMPS_TRY(ops.axpy_dot_dev(vp, vp ? vp + n : nullptr, beta_d + (j > 0 ? j - 1 : 0), vre(j), vre(j) + n, y.re(),
+                                y.im(), hA, st));
+      CMPS_TRY(ops.update_mdot_dev(hA, vre(j), vre(j) + n, kv.d, kv.d + n, ldv, j + 1, y.re(), y.im(), hB, st));
       CMPS_TRY(ops.maxpy_norm_dev(kv.d, kv.d + n, ldv, j + 1, hB, y.re(), y.im(), nrm, st));
-      CMPS_TRY(ops.lanczos_coef(hA, hB, nrm, j, alpha_d, beta_d, scale_d, st));
+      CMPS_TRY(ops.lanczos_coef(hA, hB + 2 * j, nrm, j, alpha_d, beta_d, scale_d, st));
       if (j + 1 < kdim) CMPS_TRY(ops.scale_dev(y.re(), y.im(), scale_d, false, vre(j + 1), vre(j + 1) + n, st));
       CMPS_CUDA(cudaMemcpyAsync(h_ab, alpha_d + j, sizeof(double), cudaMemcpyDeviceToHost, st));
       CMPS_CUDA(cudaMemcpyAsync(h_ab + 1, beta_d + j, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -995,7 +1127,7 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   CMPS_CUDA(cudaMemcpyAsync(theta.d, x.d, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, st));
   have_theta = true;
   if (evec) {
-    CMPS_TRY(launch_unpack(theta, d_pos, n_allowed, d_io, st));
+    CMPS_TRY(unpack(theta, d_io, st));
     CMPS_CUDA(cudaMemcpyAsync(evec, d_io, sizeof(double) * 2 * n_allowed, cudaMemcpyDeviceToHost, st));
   }
   CMPS_CUDA(cudaStreamSynchronize(st));

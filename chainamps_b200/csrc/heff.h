@@ -51,7 +51,6 @@ struct Heff {
   std::vector<int16_t> bq_raw;  // as given (for export)
   ThetaSpace th;
   int64_t n_allowed = 0, full_length = 0;
-  int64_t* d_pos = nullptr;      // ARPACK order -> theta block offset
   // ARPACK-order maps, generated on the device from per-column and per-sector
   // descriptors (a few thousand entries instead of n host-side ones)
   struct MapCol {
@@ -64,9 +63,31 @@ struct Heff {
   std::vector<MapCol> map_cols;
   std::vector<MapSec> map_secs;
   std::vector<int64_t> map_rowlin, map_rowth;  // per allowed row: s1 + d a0, theta row
-  // mode 0: ARPACK index -> theta offset (d_pos); mode 1: -> full linear index
+  // mode 0: ARPACK index -> theta offset; mode 1: -> full linear index
   int arpack_map(int mode, int64_t* d_out, cudaStream_t st) const;
   int allowed_indices(int64_t* host_out) const;
+  // ARPACK order <-> sector blocks as 32 x 32 transpose tiles: a group is up
+  // to 32 ARPACK columns of one (block m, sigma2) with consecutive a2
+  // positions, i.e. consecutive theta columns.
+  struct PackGroup {
+    int64_t off;  // into the group column list
+    int32_t cnt, m;
+  };
+  struct PackTile {
+    int32_t group, r0;
+  };
+  void* d_pack = nullptr;        // one allocation: cols, secs, rowth, group columns, groups, tiles
+  const MapCol* d_map_cols = nullptr;
+  const MapSec* d_map_secs = nullptr;
+  const int64_t* d_map_rowth = nullptr;
+  const int32_t* d_pack_gcols = nullptr;
+  const PackGroup* d_pack_groups = nullptr;
+  const PackTile* d_pack_tiles = nullptr;
+  int64_t n_pack_tiles = 0;
+  int build_pack(cudaStream_t st);
+  // in: n_allowed interleaved complex (ARPACK order) -> theta blocks, and back
+  int pack(const double* in, const Planar& out, cudaStream_t st) const;
+  int unpack(const Planar& in, double* out, cudaStream_t st) const;
   // LeftPart / RightPart sector blocks
   Planar LP, RP;
   std::vector<AxpyBlock> lp_blocks, rp_blocks;

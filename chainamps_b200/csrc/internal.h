@@ -158,10 +158,6 @@ struct AxpyTerm {
 // ---- kernels (launchers) ---------------------------------------------------
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
                       Planar& C, cudaStream_t st);
-int launch_pack(const double* in_interleaved, const int64_t* pos, int64_t n, Planar& dst,
-                cudaStream_t st);
-int launch_unpack(const Planar& src, const int64_t* pos, int64_t n, double* out_interleaved,
-                  cudaStream_t st);
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,
                       const Planar& src, Planar& dst, cudaStream_t st);
 

@@ -1,7 +1,6 @@
-// Memory-bound kernels of the hot path: ARPACK-order <-> sector-block
-// gathers/scatters, block AXPY lists (LeftPart / RightPart formation), and
-// the FP64 vector kernels of the device Krylov solver.  All are
-// grid-stride loops sized to a multiple of the SM count.
+// Memory-bound kernels of the hot path: block AXPY lists (LeftPart /
+// RightPart formation) and the FP64 vector kernels of the device Krylov
+// solver.  All are grid-stride loops sized to a multiple of the SM count.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -22,24 +21,6 @@ int grid_for(int64_t n, int threads) {
   int64_t cap = (int64_t)sms * 8;
   if (want < 1) want = 1;
   return (int)(want < cap ? want : cap);
-}
-
-__global__ void k_pack(const double2* __restrict__ in, const int64_t* __restrict__ pos, int64_t n,
-                       double* __restrict__ re, double* __restrict__ im) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double2 v = in[i];
-    int64_t p = pos[i];
-    re[p] = v.x;
-    im[p] = v.y;
-  }
-}
-
-__global__ void k_unpack(const double* __restrict__ re, const double* __restrict__ im,
-                         const int64_t* __restrict__ pos, int64_t n, double2* __restrict__ out) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t p = pos[i];
-    out[i] = make_double2(re[p], im[p]);
-  }
 }
 
 // One CTA per destination block; dst = sum_t w_t src_t.
@@ -239,9 +220,12 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // partial[r][blk]: r = 2j, 2j+1 -> <V_j, w> (re, im) for j < k; r = 2k -> |w|^2.
 // One pass over w (held in registers per tile) and one over each V_j.
+// With `uc` set, w -= c u (c = uc[0] + i uc[1], u = (ur, ui)) first, written
+// back, and the products are taken with the updated w.
 __global__ void __launch_bounds__(KR_THREADS)
-k_mdot(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k,
-       const double* __restrict__ wr, const double* __restrict__ wi, int64_t n, double* __restrict__ partial) {
+k_mdot(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv, int k, double* __restrict__ wr,
+       double* __restrict__ wi, int64_t n, const double* __restrict__ uc, const double* __restrict__ ur,
+       const double* __restrict__ ui, double* __restrict__ partial) {
   extern __shared__ double acc[];  // [warps][2k + 1], one row per warp: no shared-memory atomics
   const int nw = KR_THREADS / 32, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rows = 2 * k + 1;
@@ -256,6 +240,13 @@ k_mdot(const double* __restrict__ Vr, const double* __restrict__ Vi, int64_t ldv
       const int64_t i = base + (int64_t)e * KR_THREADS + threadIdx.x;
       xr[e] = i < n ? wr[i] : 0.0;
       xi[e] = i < n ? wi[i] : 0.0;
+      if (uc && i < n) {
+        const double cr = uc[0], ci = uc[1], a = ur[i], b = ui[i];
+        xr[e] -= cr * a - ci * b;
+        xi[e] -= cr * b + ci * a;
+        wr[i] = xr[e];
+        wi[i] = xi[e];
+      }
       s += xr[e] * xr[e] + xi[e] * xi[e];
     }
     s = warp_sum(s);
@@ -323,14 +314,49 @@ k_maxpy_norm(const double* __restrict__ Vr, const double* __restrict__ Vi, int64
   }
 }
 
-// Lanczos coefficients of step j after two projection passes:
-// alpha_j = Re(hA_j + hB_j), beta_j = |w|; scale = 1 / beta_j, or 0 when the
+// Local Lanczos step: w -= beta v_prev (beta = *pb, skipped when v_prev is
+// null), then partial[0|1][blk] = <v, w> (re | im) over this CTA's elements.
+__global__ void __launch_bounds__(KR_THREADS)
+k_axpy_dot(const double* __restrict__ pr, const double* __restrict__ pi, const double* __restrict__ pb,
+           const double* __restrict__ vr, const double* __restrict__ vi, double* __restrict__ wr,
+           double* __restrict__ wi, int64_t n, double* __restrict__ partial) {
+  __shared__ double red[2][KR_THREADS / 32];
+  const double b = pr ? *pb : 0.0;
+  double sr = 0.0, si = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double xr = wr[i], xi = wi[i];
+    if (pr) {
+      xr -= b * pr[i];
+      xi -= b * pi[i];
+      wr[i] = xr;
+      wi[i] = xi;
+    }
+    const double ar = vr[i], ai = vi[i];
+    sr += ar * xr + ai * xi;
+    si += ar * xi - ai * xr;
+  }
+  sr = warp_sum(sr);
+  si = warp_sum(si);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = sr;
+    red[1][threadIdx.x >> 5] = si;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double t = 0.0;
+    for (int w = 0; w < KR_THREADS / 32; ++w) t += red[threadIdx.x][w];
+    partial[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// Lanczos coefficients of step j: alpha_j = *a1 + *a2 (the real parts of the
+// two projections on v_j), beta_j = |w|; scale = 1 / beta_j, or 0 when the
 // Krylov space is exhausted (the next basis vector is then zero).
-__global__ void k_lanczos_coef(const double* __restrict__ hA, const double* __restrict__ hB,
+__global__ void k_lanczos_coef(const double* __restrict__ a1, const double* __restrict__ a2,
                                const double* __restrict__ nrm2, int j, double* __restrict__ alpha,
                                double* __restrict__ beta, double* __restrict__ scale) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const double a = hA[2 * j] + hB[2 * j];
+  const double a = *a1 + *a2;
   const double b = sqrt(fmax(0.0, *nrm2));
   alpha[j] = a;
   beta[j] = b;
@@ -351,20 +377,6 @@ __global__ void k_scale_dev(const double* __restrict__ xr, const double* __restr
 }
 
 }  // namespace
-
-int launch_pack(const double* in, const int64_t* pos, int64_t n, Planar& dst, cudaStream_t st) {
-  if (n == 0) return CMPS_OK;
-  k_pack<<<grid_for(n, 256), 256, 0, st>>>((const double2*)in, pos, n, dst.re(), dst.im());
-  CMPS_CUDA(cudaGetLastError());
-  return CMPS_OK;
-}
-
-int launch_unpack(const Planar& src, const int64_t* pos, int64_t n, double* out, cudaStream_t st) {
-  if (n == 0) return CMPS_OK;
-  k_unpack<<<grid_for(n, 256), 256, 0, st>>>(src.re(), src.im(), pos, n, (double2*)out);
-  CMPS_CUDA(cudaGetLastError());
-  return CMPS_OK;
-}
 
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms, const Planar& src,
                       Planar& dst, cudaStream_t st) {
@@ -479,9 +491,34 @@ int VecOps::mdot_dev(const double* Vr, const double* Vi, int64_t ldv, int k, con
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>(nb, (n + tile - 1) / tile));
   const int rows = 2 * k + 1;
   const size_t smem = sizeof(double) * (KR_THREADS / 32) * rows;
-  k_mdot<<<g, KR_THREADS, smem, st>>>(Vr, Vi, ldv, k, wr, wi, n, d_partial);
+  k_mdot<<<g, KR_THREADS, smem, st>>>(Vr, Vi, ldv, k, const_cast<double*>(wr), const_cast<double*>(wi), n, nullptr,
+                                      nullptr, nullptr, d_partial);
   CMPS_CUDA(cudaGetLastError());
   k_reduce_rows<<<rows, RED_THREADS, 0, st>>>(d_partial, g, rows, d_out);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::update_mdot_dev(const double* d_c, const double* ur, const double* ui, const double* Vr, const double* Vi,
+                            int64_t ldv, int k, double* wr, double* wi, double* d_out, cudaStream_t st) {
+  if (k < 0 || k > 128) return fail(CMPS_ERR_ARG, "krylov dimension above 128");
+  const int64_t tile = (int64_t)KR_THREADS * KR_E;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(nb, (n + tile - 1) / tile));
+  const int rows = 2 * k + 1;
+  const size_t smem = sizeof(double) * (KR_THREADS / 32) * rows;
+  k_mdot<<<g, KR_THREADS, smem, st>>>(Vr, Vi, ldv, k, wr, wi, n, d_c, ur, ui, d_partial);
+  CMPS_CUDA(cudaGetLastError());
+  k_reduce_rows<<<rows, RED_THREADS, 0, st>>>(d_partial, g, rows, d_out);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
+}
+
+int VecOps::axpy_dot_dev(const double* pr, const double* pi, const double* d_beta, const double* vr, const double* vi,
+                         double* wr, double* wi, double* d_out, cudaStream_t st) {
+  const int g = std::min(nb, grid_for(n, KR_THREADS));
+  k_axpy_dot<<<g, KR_THREADS, 0, st>>>(pr, pi, d_beta, vr, vi, wr, wi, n, d_partial);
+  CMPS_CUDA(cudaGetLastError());
+  k_reduce_rows<<<2, RED_THREADS, 0, st>>>(d_partial, g, 2, d_out);
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }
@@ -497,9 +534,9 @@ int VecOps::maxpy_norm_dev(const double* Vr, const double* Vi, int64_t ldv, int 
   return CMPS_OK;
 }
 
-int VecOps::lanczos_coef(const double* d_hA, const double* d_hB, const double* d_nrm2, int j, double* d_alpha,
+int VecOps::lanczos_coef(const double* d_a1, const double* d_a2, const double* d_nrm2, int j, double* d_alpha,
                          double* d_beta, double* d_scale, cudaStream_t st) {
-  k_lanczos_coef<<<1, 32, 0, st>>>(d_hA, d_hB, d_nrm2, j, d_alpha, d_beta, d_scale);
+  k_lanczos_coef<<<1, 32, 0, st>>>(d_a1, d_a2, d_nrm2, j, d_alpha, d_beta, d_scale);
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }

@@ -40,8 +40,15 @@ struct VecOps {
   // w -= sum_j h_j V_j with h = d_h (2k doubles); *d_nrm2 = |w|^2 afterwards.
   int maxpy_norm_dev(const double* Vr, const double* Vi, int64_t ldv, int k, const double* d_h, double* wr,
                      double* wi, double* d_nrm2, cudaStream_t st);
-  // alpha_j, beta_j of a Lanczos step and the scale of the next basis vector.
-  int lanczos_coef(const double* d_hA, const double* d_hB, const double* d_nrm2, int j, double* d_alpha,
+  // w -= c u (c = d_c[0] + i d_c[1]), then as mdot_dev with the updated w.
+  int update_mdot_dev(const double* d_c, const double* ur, const double* ui, const double* Vr, const double* Vi,
+                      int64_t ldv, int k, double* wr, double* wi, double* d_out, cudaStream_t st);
+  // w -= (*d_beta) p (skipped when pr is null), then d_out[0..1] = <v, w>.
+  int axpy_dot_dev(const double* pr, const double* pi, const double* d_beta, const double* vr, const double* vi,
+                   double* wr, double* wi, double* d_out, cudaStream_t st);
+  // alpha_j = *d_a1 + *d_a2, beta_j = sqrt(*d_nrm2), and the scale of the next
+  // basis vector (0 when the Krylov space is exhausted).
+  int lanczos_coef(const double* d_a1, const double* d_a2, const double* d_nrm2, int j, double* d_alpha,
                    double* d_beta, double* d_scale, cudaStream_t st);
   // y = s x with s = *d_s, or s = 1 / sqrt(*d_s) when inv_sqrt.
   int scale_dev(const double* xr, const double* xi, const double* d_s, bool inv_sqrt, double* yr, double* yi,

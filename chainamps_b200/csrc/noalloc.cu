@@ -77,9 +77,9 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
   t.len = H.T.len;
   y.d = t.d + 2 * H.T.len;
   y.len = H.th.total;
-  CMPS_TRY(launch_pack(d_in, H.d_pos, H.n_allowed, x, st));
+  CMPS_TRY(H.pack(d_in, x, st));
   CMPS_TRY(launch_zgemm_fp64(H.stage1, false, false, H.LP, x, t, st));
   CMPS_TRY(launch_zgemm_fp64(H.stage2, false, false, t, H.RP, y, st));
-  CMPS_TRY(launch_unpack(y, H.d_pos, H.n_allowed, d_out, st));
+  CMPS_TRY(H.unpack(y, d_out, st));
   return CMPS_OK;
 }
