@@ -107,6 +107,9 @@ _SIGS = {
     "cmps_dmrg_grow": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
     "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
     "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp, C.c_int]),
+    "cmps_heff_adjoint": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc), C.c_void_p, C.c_void_p, c_dblp]),
+    "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
+    "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -306,6 +309,15 @@ class TwoVertexComponents:
         _check(lib.cmps_heff_theta_svd(self.h, chi, max_trunc, C.byref(s)))
         return SVDResult(s, self.nq)
 
+    def adjoint(self, dW: MPXTensor, dL: "Block" = None, dR: "Block" = None):
+        """dE/dlambda = Re <theta|dH_eff|theta> / <theta|theta> for W = W0 +
+        lambda dW, with optional environment derivatives dL / dR."""
+        d, keep = dW._desc()
+        g = C.c_double()
+        _check(lib.cmps_heff_adjoint(self.h, C.byref(d), dL.h if dL is not None else None,
+                                     dR.h if dR is not None else None, C.byref(g)))
+        return g.value
+
     def make_left_block(self, svd: "SVDResult"):
         b = C.c_void_p()
         _check(lib.cmps_heff_left_block(self.h, svd.h, C.byref(b)))
@@ -398,7 +410,9 @@ class iDMRG:
     DMRG_routines.cpp:346-374; iDMRG::run, iDMRG_routines.cpp:19-33)."""
 
     def __init__(self, ctx: Context, rules, W: MPXTensor, target=None, precision=CMPS_FP64, tol=1e-10,
-                 max_restarts=50, krylov_dim=24):
+                 max_restarts=50, krylov_dim=24, gradient=None):
+        """gradient: optional dW (MPXTensor, the MPO's derivative with respect
+        to one coupling); each grow() then also returns dE/dlambda."""
         self.ctx = ctx
         cr, self._r = _rules(rules)
         dw, kw = W._desc()
@@ -410,6 +424,10 @@ class iDMRG:
         _check(lib.cmps_dmrg_create(ctx.h, C.byref(cr), C.byref(dw), t, precision, C.byref(h)))
         self.h = h
         _check(lib.cmps_dmrg_set_solver(h, tol, max_restarts, krylov_dim))
+        self._grad = gradient is not None
+        if self._grad:
+            gd, gk = gradient._desc()
+            _check(lib.cmps_dmrg_set_gradient(h, C.byref(gd)))
         self.last = None
 
     def grow(self, chi=0, max_trunc=0.0):
@@ -423,6 +441,10 @@ class iDMRG:
                                   _p(ms, C.c_double)))
         self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
                          chi=bd.value, matvecs=mv.value, ms=ms)
+        if self._grad:
+            g = C.c_double()
+            _check(lib.cmps_dmrg_gradient(self.h, C.byref(g)))
+            self.last["gradient"] = g.value
         return self.last
 
     def profile(self):

@@ -70,6 +70,12 @@ struct Dmrg {
   int restarts = 50, kdim = 24;
   int last_matvecs = 0;
   double last_ms[4] = {0, 0, 0, 0};  // env update + H_eff build + prediction, eigensolve, svd, total
+  // coupling gradient: dW and the derivative environments carried along
+  bool grad_on = false;
+  std::vector<WEntry> dW;
+  Env dL, dR;
+  bool have_dlr = false;
+  double last_grad = std::nan("");
   static constexpr int kProfile = 17;
   double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
 
@@ -78,6 +84,8 @@ struct Dmrg {
       svd->U.release();
       svd->Vd.release();
     }
+    dL.data.release();
+    dR.data.release();
   }
   int dummy_blocks(Env& L, Env& R);
   int predict(Heff& next, bool* ok);
@@ -248,6 +256,21 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   } else {
     CMPS_TRY(left_update(*heff, *svd, L));
     CMPS_TRY(right_update(*heff, *svd, R));
+    if (grad_on) {
+      // derivative environments with the same truncation factors
+      Env nl, nr;
+      int rc = derivative_envs(*heff, *svd, dW, have_dlr ? &dL : nullptr, have_dlr ? &dR : nullptr, nl, nr);
+      if (rc != CMPS_OK) {
+        nl.data.release();
+        nr.data.release();
+        return rc;
+      }
+      dL.data.release();
+      dR.data.release();
+      dL = nl;
+      dR = nr;
+      have_dlr = true;
+    }
   }
   cudaEventRecord(ev[4], st);
   const auto h_env = clock::now();
@@ -280,6 +303,9 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   int rc = heff->eigs(nullptr, tol, restarts, kdim, &e, nullptr, &nmv, have_guess);
   if (rc != CMPS_OK && rc != CMPS_ERR_SOLVER) return rc;
   last_matvecs = nmv;
+  last_grad = std::nan("");
+  if (grad_on && rc == CMPS_OK)
+    CMPS_TRY(heff_adjoint(*heff, dW, have_dlr ? &dL : nullptr, have_dlr ? &dR : nullptr, &last_grad));
   const auto h_eig = clock::now();
   cudaEventRecord(ev[2], st);
   svd.reset(new SvdResult());
@@ -418,6 +444,31 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
   if (ms4)
     for (int i = 0; i < 4; ++i) ms4[i] = D.last_ms[i];
   return rc;
+}
+
+int cmps_dmrg_set_gradient(cmps_dmrg* d, const cmps_mpx_desc* dW) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  Dmrg& D = *d->impl;
+  if (D.size != 0) return fail(CMPS_ERR_STATE, "set the gradient direction before the first growth step");
+  CMPS_CUDA(cudaSetDevice(D.device));
+  if (!dW) {
+    D.grad_on = false;
+    D.dW.clear();
+    return CMPS_OK;
+  }
+  Heff ref;
+  ref.rules = D.rules;
+  CMPS_TRY(ref.parse_mpo(&D.W));
+  CMPS_TRY(parse_derivative_mpo(ref, dW, D.dW));
+  D.grad_on = true;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_gradient(const cmps_dmrg* d, double* grad) {
+  if (!d || !d->impl || !grad) return fail(CMPS_ERR_ARG, "null argument");
+  if (!d->impl->grad_on) return fail(CMPS_ERR_STATE, "no gradient direction set");
+  *grad = d->impl->last_grad;
+  return CMPS_OK;
 }
 
 int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n) {

@@ -153,8 +153,15 @@ struct SvdResult {
 };
 
 int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out);
+// adjoint.cu: derivative of the contraction with respect to a vertex coupling
+int parse_derivative_mpo(const Heff& H, const cmps_mpx_desc* dW, std::vector<WEntry>& out);
+int derivative_parts(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, Planar& LPd,
+                     Planar& RPd);
+int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad);
 int left_update(Heff& H, const SvdResult& s, Env& out);
 int right_update(Heff& H, const SvdResult& s, Env& out);
+int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, const Env* dL, const Env* dR,
+                    Env& dLn, Env& dRn);
 
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);

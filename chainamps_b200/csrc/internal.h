@@ -159,6 +159,6 @@ struct AxpyTerm {
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
                       Planar& C, cudaStream_t st);
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,
-                      const Planar& src, Planar& dst, cudaStream_t st);
+                      const Planar& src, Planar& dst, cudaStream_t st, bool accumulate = false);
 
 }  // namespace cmps

@@ -23,10 +23,11 @@ int grid_for(int64_t n, int threads) {
   return (int)(want < cap ? want : cap);
 }
 
-// One CTA per destination block; dst = sum_t w_t src_t.
+// One CTA per destination block; dst = sum_t w_t src_t (dst += ... when
+// `accumulate`).
 __global__ void k_block_axpy(const AxpyBlock* __restrict__ blocks, const AxpyTerm* __restrict__ terms,
                              const double* __restrict__ sr, const double* __restrict__ si,
-                             double* __restrict__ dr, double* __restrict__ di) {
+                             double* __restrict__ dr, double* __restrict__ di, int accumulate) {
   const AxpyBlock b = blocks[blockIdx.x];
   for (int64_t e = threadIdx.x; e < b.len; e += blockDim.x) {
     double xr = 0.0, xi = 0.0;
@@ -35,6 +36,10 @@ __global__ void k_block_axpy(const AxpyBlock* __restrict__ blocks, const AxpyTer
       double vr = sr[tm.src_off + e], vi = si[tm.src_off + e];
       xr += tm.wr * vr - tm.wi * vi;
       xi += tm.wr * vi + tm.wi * vr;
+    }
+    if (accumulate) {
+      xr += dr[b.dst_off + e];
+      xi += di[b.dst_off + e];
     }
     dr[b.dst_off + e] = xr;
     di[b.dst_off + e] = xi;
@@ -379,9 +384,9 @@ __global__ void k_scale_dev(const double* __restrict__ xr, const double* __restr
 }  // namespace
 
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms, const Planar& src,
-                      Planar& dst, cudaStream_t st) {
+                      Planar& dst, cudaStream_t st, bool accumulate) {
   if (nblocks == 0) return CMPS_OK;
-  k_block_axpy<<<nblocks, 256, 0, st>>>(d_blocks, d_terms, src.re(), src.im(), dst.re(), dst.im());
+  k_block_axpy<<<nblocks, 256, 0, st>>>(d_blocks, d_terms, src.re(), src.im(), dst.re(), dst.im(), accumulate ? 1 : 0);
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }

@@ -196,6 +196,20 @@ int cmps_block_info(const cmps_block* b, int64_t* chi, int64_t* mpo_dim, int64_t
 int cmps_block_copy(const cmps_block* b, int16_t* a_charges, int64_t* colptr,
                     int64_t* rowind, double* values);
 
+/* ---- adjoint of the H_eff contraction (no reference counterpart) -------
+ * Derivative of the variational energy E = <theta|H_eff|theta>/<theta|theta>
+ * with respect to one coupling lambda of the vertex MPO, W = W0 + lambda dW
+ * (an interchain coupling, a field).  theta is the wavefunction last produced
+ * by cmps_heff_eigs (or set by cmps_heff_set_theta).  dW has the MPO's
+ * indices and charges; its non-zero entries must lie inside the non-zero
+ * pattern of W (evaluate at a non-zero coupling).  dL / dR are the
+ * environments' own derivatives (dW inserted at one earlier vertex; layout of
+ * the handle's L / R), or NULL for zero.  grad = Re <theta|dH_eff|theta> /
+ * <theta|theta>, contracted in FP64 through the matvec's own grouped-GEMM
+ * plans (two matvecs). */
+int cmps_heff_adjoint(cmps_heff* h, const cmps_mpx_desc* dW, const cmps_block* dL,
+                      const cmps_block* dR, double* grad);
+
 /* ---- device-resident iDMRG growth (SuperBlock) -------------------------
  * Replaces SuperBlock::grow_two_vertex (DMRG_routines.cpp:346-374) with
  * everything on the device: the new environments come from the previous
@@ -219,6 +233,14 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
                    int* matvecs, double* ms4);
 /* The current (rescaled) singular values, bond_dim of them, descending. */
 int cmps_dmrg_values(const cmps_dmrg* d, double* values);
+/* Coupling gradient along the growth (no reference counterpart).  Set before
+ * the first growth step: dW as for cmps_heff_adjoint (NULL turns it off).
+ * Each step then carries the derivative environments dL, dR (the environment
+ * update with LeftPart / RightPart replaced by their derivatives, the step's
+ * truncation factors held fixed) and cmps_dmrg_gradient returns dE/dlambda of
+ * the last step's energy (cmps_heff_adjoint with those environments). */
+int cmps_dmrg_set_gradient(cmps_dmrg* d, const cmps_mpx_desc* dW);
+int cmps_dmrg_gradient(const cmps_dmrg* d, double* grad);
 /* Breakdown of the last growth step (no reference counterpart;
  * diagnostics).  Writes the first n (<= 17) of: {environment update ms, H_eff
  * build + prediction ms, eigensolve ms, SVD ms, total ms (device time, CUDA
