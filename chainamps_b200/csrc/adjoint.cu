@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <set>
 #include <vector>
 
 #include "heff.h"
@@ -120,6 +121,13 @@ int parse_derivative_mpo(const Heff& H, const cmps_mpx_desc* dW, std::vector<WEn
     return fail(CMPS_ERR_ARG, "adjoint: dW indices differ from the MPO's");
   out = tmp.W;
   return CMPS_OK;
+}
+
+void extend_pattern(std::vector<WEntry>& W, const std::vector<WEntry>& dW) {
+  std::set<std::array<int, 4>> have;
+  for (const WEntry& w : W) have.insert({w.sp, w.bl, w.s, w.br});
+  for (const WEntry& w : dW)
+    if (have.insert({w.sp, w.bl, w.s, w.br}).second) W.push_back(WEntry{w.sp, w.bl, w.s, w.br, 0.0, 0.0});
 }
 
 int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad) {

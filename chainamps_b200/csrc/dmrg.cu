@@ -279,6 +279,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   next->device = ctx->device;
   next->rules = rules;
   CMPS_TRY(next->parse_mpo(&W));
+  if (grad_on) extend_pattern(next->W, dW);
   next->L = L;   // ownership of the device blocks moves to `next`
   next->R = R;
   CMPS_TRY(next->finish());

@@ -155,6 +155,9 @@ struct SvdResult {
 int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out);
 // adjoint.cu: derivative of the contraction with respect to a vertex coupling
 int parse_derivative_mpo(const Heff& H, const cmps_mpx_desc* dW, std::vector<WEntry>& out);
+// W gains a zero-weight entry at every position where dW is non-zero and W
+// is not, so that LeftPart / RightPart blocks exist for every dW term.
+void extend_pattern(std::vector<WEntry>& W, const std::vector<WEntry>& dW);
 int derivative_parts(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, Planar& LPd,
                      Planar& RPd);
 int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad);

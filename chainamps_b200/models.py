@@ -184,6 +184,77 @@ def ladder_model(legs=4, j=1.0, j_perp=0.5):
     return (0,), ch, W, bq
 
 
+def ising_chain_vertex(sites=12, g=1.2, keep=64, g_basis=None):
+    """One vertex = a periodic transverse-field Ising chain
+    H(g) = -sum_i X_i X_{i+1} - g sum_i Z_i, reduced to its `keep` lowest
+    eigenstates (computed at g_basis, default g) with their Z2 parity
+    (prod_i Z_i) as the charge, rules (2,).
+
+    Returns (charges (keep, 1), ops {"X0".."X{sites-1}": keep x keep
+    sigma^x_i in the kept basis (parity odd)}, H (keep x keep, the vertex
+    Hamiltonian at g in that basis), dH_dg (keep x keep), gap at the cut).
+    The basis is built per parity sector in the sigma^z product basis with bit
+    operations; each eigenvector's sign makes its largest component positive.
+    Near-degenerate states (momentum pairs) are kept or cut together only if
+    the cut falls in a gap; the gap at the cut is returned."""
+    gb = g if g_basis is None else g_basis
+    n = 1 << sites
+    s = np.arange(n, dtype=np.int64)
+    bits = (s[:, None] >> np.arange(sites)[None, :]) & 1            # 1 = spin down
+    z = 1 - 2 * bits                                                  # Z_i eigenvalue
+    zsum = z.sum(axis=1).astype(np.float64)
+    parity = (bits.sum(axis=1) & 1)                                   # 0: even, 1: odd
+    evals, vecs, labels = [], [], []
+    for par in (0, 1):
+        sel = np.nonzero(parity == par)[0]
+        pos = -np.ones(n, np.int64)
+        pos[sel] = np.arange(sel.size)
+        Hs = np.zeros((sel.size, sel.size))
+        Hs[np.arange(sel.size), np.arange(sel.size)] = -gb * zsum[sel]
+        for i in range(sites):
+            flip = (1 << i) | (1 << ((i + 1) % sites))
+            Hs[np.arange(sel.size), pos[sel ^ flip]] -= 1.0
+        w, v = np.linalg.eigh(Hs)
+        for k in range(w.size):
+            vec = np.zeros(n)
+            vec[sel] = v[:, k]
+            j = int(np.argmax(np.abs(vec)))
+            if vec[j] < 0:
+                vec = -vec
+            evals.append(w[k])
+            vecs.append(vec)
+            labels.append(par)
+    order = np.argsort(np.asarray(evals), kind="stable")
+    ev = np.asarray(evals)[order]
+    gap = float(ev[keep] - ev[keep - 1]) if keep < ev.size else float("inf")
+    order = order[:keep]
+    V = np.stack([vecs[i] for i in order], axis=1)                   # n x keep, real
+    ch = np.asarray([[labels[i]] for i in order], np.int64)
+    ops = {}
+    for i in range(sites):
+        ops[f"X{i}"] = (V.T @ V[s ^ (1 << i)]).astype(np.complex128)
+    Hxx = np.zeros((keep, keep))
+    for i in range(sites):
+        flip = (1 << i) | (1 << ((i + 1) % sites))
+        Hxx -= V.T @ V[s ^ flip]
+    Hz = -(V * zsum[:, None]).T @ V
+    H = (Hxx + g * Hz).astype(np.complex128)
+    H = 0.5 * (H + H.conj().T)
+    return ch, ops, H, Hz.astype(np.complex128), gap
+
+
+def coupled_ising_model(sites=12, g=1.2, keep=64, j_perp=0.05, g_basis=None):
+    """Coupled transverse-field Ising chains: each vertex is the chain of
+    ising_chain_vertex, neighbouring vertices coupled by
+    j_perp * sum_i X_i X_i (chain-basis matrix elements, parity odd, so only
+    the total Z2 parity is conserved).  Returns (rules, charges, W, bq) of
+    the reference's MakeGeneralHMPO layout."""
+    ch, ops, H, _, _ = ising_chain_vertex(sites, g, keep, g_basis)
+    cps = [(f"X{i}", f"X{i}", j_perp) for i in range(sites)]
+    W, bq = general_hmpo(ch, (2,), H, ops, cps)
+    return (2,), ch, W, bq
+
+
 def gaussian_bond(chi, step=2, width=3.5, offset=0):
     """Bond charges with a discretised Gaussian sector-size profile (the
     shape of a converged total-Sz distribution), ``chi`` elements, charges

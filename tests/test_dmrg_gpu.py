@@ -68,3 +68,25 @@ def test_split_precision_idmrg_energies(ctx):
         rb = b.grow(40, 1e-16)
         assert abs(ra["energy"] - rb["energy"]) <= 1e-9 * abs(ra["energy"]), (ra, rb)
         assert ra["chi"] == rb["chi"]
+
+
+def test_coupled_ising_idmrg_matches_oracle(ctx):
+    """Coupled transverse-field Ising chains (each vertex a 4-site periodic
+    chain cut to its 8 lowest states, Z2 parity only): device iDMRG in FP64
+    and mixed precision against the oracle's SuperBlock, step by step."""
+    from chainamps_b200 import iDMRG, CMPS_SPLIT_TF32, models
+    from oracle import model as om
+    ch, ops, Hv, _, _ = models.ising_chain_vertex(4, 1.2, 8)
+    H = om.make_general_hmpo(om.Vertex((2,), ch, ops, Hv),
+                             [om.Coupling(f"J{i}", f"X{i}", f"X{i}", 0.05) for i in range(4)])
+    sb = od.SuperBlock(H)
+    run = iDMRG(ctx, H.rules, to_tensor(H), tol=1e-12, krylov_dim=32)
+    mixed = iDMRG(ctx, H.rules, to_tensor(H), precision=CMPS_SPLIT_TF32, tol=1e-12, krylov_dim=32)
+    for _ in range(4):
+        ref = sb.grow(24, 1e-16)
+        got = run.grow(24, 1e-16)
+        mx = mixed.grow(24, 1e-16)
+        assert got["chi"] == ref["chi"]
+        assert abs(got["energy"] - ref["energy"]) <= 1e-9 * abs(ref["energy"]), (got, ref)
+        assert abs(got["entropy"] - ref["entropy"]) <= 1e-8
+        assert abs(mx["energy"] - got["energy"]) <= 1e-9 * abs(got["energy"]), (mx, got)
