@@ -21,6 +21,12 @@ flush is needed between steps.
   tolerance 1e-10): device time per step at full chi in FP64 and in mixed
   precision (split-TF32 matvecs, FP64 Krylov/SVD/energies), the per-phase
   profile, and the largest relative energy difference between the two runs;
+* idmrg_coupled_ising: the same FP64-vs-mixed iDMRG step on the
+  coupled transverse-field Ising chain config (each vertex a periodic
+  12-site chain at g = 1.2 cut by exact diagonalisation to its 64 lowest
+  states with Z2 parity, interchain J_perp = 0.05 sum_i X_i X_i, MPO D = 26)
+  at chi = 64, the largest bond dimension whose FP64 step fits the bench's
+  time budget (the config's chi = 2048 needs a 137 GB wavefunction);
 * cpu_baseline: the oracle's block-sparse numpy port of the same matvec on
   the host cores (one full matvec);
 * --impl reference: the CPU port timed as the reference arm.
@@ -54,6 +60,8 @@ def parse():
     p.add_argument("--precision", default="both", choices=["both", "fp64", "split_tf32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--idmrg-steps", type=int, default=4, help="timed iDMRG steps at full chi (0: skip)")
+    p.add_argument("--ising-steps", type=int, default=2, help="timed coupled-Ising iDMRG steps (0: skip)")
+    p.add_argument("--ising-chi", type=int, default=64)
     return p.parse_args()
 
 
@@ -298,6 +306,13 @@ def main():
         line["speedup_mixed_vs_fp64"] = f["ms"] / r["ms"]
     if a.idmrg_steps > 0:
         line["idmrg"] = idmrg_bench(ctx, wl, a.chi, a.idmrg_steps, dist)
+    if a.ising_steps > 0:
+        from chainamps_b200 import models
+        rules, ch, W, bq = models.coupled_ising_model(12, 1.2, 64, 0.05)
+        iw = dict(rules=rules, Wt=models.mpo_tensor(ch, W, bq))
+        line["idmrg_coupled_ising"] = idmrg_bench(ctx, iw, a.ising_chi, a.ising_steps, dist, warm=2)
+        line["idmrg_coupled_ising"]["model"] = ("coupled TFIM chains: 12-site periodic chain vertex, g=1.2, 64 "
+                                                "lowest states (Z2), J_perp=0.05 sum X_i X_i, MPO D=26")
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t, setup, cores, _ = cpu_port(wl, 1)
         line["cpu_baseline"] = {"value": canonical / t / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",

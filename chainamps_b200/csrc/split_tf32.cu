@@ -133,10 +133,11 @@ int encoder() {
   return CMPS_OK;
 }
 
-// 3-D map over one operand block: (K, rows, 4 planes); box (16, 128, 4).
+// 3-D map over one operand block: (K, rows, 4 planes); box (16, box_rows, 4).
 // `base_off` is the block's element offset inside its plane of `plane`
 // elements; the block must lie inside the plane.
-int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t ld, int64_t plane, CUtensorMap* out) {
+int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t ld, int64_t plane, CUtensorMap* out,
+             int box_rows = 128) {
   float* base = plane0 + base_off;
   if (((uintptr_t)base & 15) || (ld * 4) % 16 || (plane * 4) % 16 || K < 1 || rows < 1 || K > ld)
     return fail(CMPS_ERR_STATE, "tensor map: misaligned operand block");
@@ -144,7 +145,8 @@ int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t l
     return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
   cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, 4};
   cuuint64_t strides[2] = {(cuuint64_t)(ld * 4), (cuuint64_t)(plane * 4)};
-  cuuint32_t box[3] = {16, 128, 4};
+  if (box_rows < 16 || box_rows > 128 || (box_rows & 15)) return fail(CMPS_ERR_STATE, "tensor map: bad box height");
+  cuuint32_t box[3] = {16, (cuuint32_t)box_rows, 4};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = g_encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -155,7 +157,7 @@ int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t l
 
 void add_tiles(tc::TcPlan& p, int32_t task, int32_t m, int32_t n) {
   for (int32_t m0 = 0; m0 < m; m0 += 128)
-    for (int32_t n0 = 0; n0 < n; n0 += 128) p.tiles.push_back(tc::TcTile{task, m0, n0, 0});
+    for (int32_t n0 = 0; n0 < n; n0 += 128) p.tiles.push_back(tc::TcTile{task, m0, n0, tc::b_box_rows(n)});
 }
 
 }  // namespace
@@ -362,11 +364,14 @@ static int build_split(Heff& H) {
     p1.amaps.push_back(cm);
   }
   std::map<std::array<int, 4>, int32_t> bmap1;
+  std::vector<int32_t> b1_rows, b2_rows;  // row extent of every B map (= its task's N)
   for (size_t i = 0; i < lpsb.size(); ++i) {
     const SplitBlock& b = lpsb[i];
     CUtensorMap cm;
-    CMPS_TRY(make_map(S->buf + S->lps_off, b.dst_off, b.cols, b.rows, b.ld_dst, S->lps_len, &cm));
+    CMPS_TRY(make_map(S->buf + S->lps_off, b.dst_off, b.cols, b.rows, b.ld_dst, S->lps_len, &cm,
+                      tc::b_box_rows(b.rows)));
     p1.bmaps.push_back(cm);
+    b1_rows.push_back(b.rows);
   }
   {
     int32_t i = 0;
@@ -423,8 +428,10 @@ static int build_split(Heff& H) {
       const SplitBlock& b = rptb[i];
       CUtensorMap cm;
       // destination layout [a2'][a2]: rows = dim t', K = dim t
-      CMPS_TRY(make_map(S->buf + S->rpt_off, b.dst_off, b.rows, b.cols, b.ld_dst, S->rpt_len, &cm));
+      CMPS_TRY(make_map(S->buf + S->rpt_off, b.dst_off, b.rows, b.cols, b.ld_dst, S->rpt_len, &cm,
+                        tc::b_box_rows(b.cols)));
       p2.bmaps.push_back(cm);
+      b2_rows.push_back(b.cols);
       bmap2[kv.first] = i++;
     }
   }
@@ -483,6 +490,18 @@ static int build_split(Heff& H) {
         return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
     for (const tc::TcTile& tl : p->tiles)
       if (tl.task < 0 || tl.task >= (int32_t)p->tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
+  }
+  // every B map of a task has the task's N rows, so the tile's B box height
+  // (and the transaction bytes the producer expects) matches each map
+  for (int stage = 0; stage < 2; ++stage) {
+    const tc::TcPlan& p = stage == 0 ? p1 : p2;
+    const std::vector<int32_t>& rows = stage == 0 ? b1_rows : b2_rows;
+    if (rows.size() != p.bmaps.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map count");
+    for (const tc::TcTask& t : p.tasks)
+      for (int q = t.t0; q < t.t1; ++q)
+        if (rows[p.terms[q].b_map] != t.n) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map rows differ from N");
+    for (const tc::TcTile& tl : p.tiles)
+      if (tl.b_rows != tc::b_box_rows(p.tasks[tl.task].n)) return fail(CMPS_ERR_STATE, "tcgen05 plan: B box height");
   }
   CMPS_TRY(p1.upload(H.ctx->stream));
   CMPS_TRY(p2.upload(H.ctx->stream));

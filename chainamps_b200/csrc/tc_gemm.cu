@@ -197,7 +197,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
             }
             uint8_t* sa = smem + s * kStageBytes;
             uint8_t* sb = sa + kOperandBytes;
-            mbar_expect_tx(&full[s], kStageBytes);
+            // A: 128-row box; B: the task's b_rows-row box (both four planes)
+            mbar_expect_tx(&full[s], (uint32_t)kOperandBytes + 4u * 64u * (uint32_t)tile.b_rows);
             tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
             tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
           }
@@ -231,6 +232,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d_re = tmem + (uint32_t)(buf * 256), d_im = d_re + 128;
+        const uint32_t b_plane = 64u * (uint32_t)tile.b_rows;  // bytes per B plane in shared memory
         bool first = true;
         for (int t = task.t0; t < task.t1 && ok; ++t) {
           const int kt = terms[t].k;
@@ -251,7 +253,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
 #pragma unroll
               for (int p = 0; p < 4; ++p) {
                 A[p] = smem_desc_sw64(a0 + p * kPlaneTileBytes + kk * 32);
-                B[p] = smem_desc_sw64(b0 + p * kPlaneTileBytes + kk * 32);
+                B[p] = smem_desc_sw64(b0 + p * b_plane + kk * 32);
               }
               const uint32_t acc = first ? 0u : 1u;
               first = false;

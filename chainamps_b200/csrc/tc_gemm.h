@@ -23,9 +23,13 @@ struct TcTask {
 struct TcTerm {
   int32_t a_map, b_map, a_x0, k;
 };
+// b_rows: row count of the B boxes of this tile's task (its N rounded up to
+// 16, at most 128); the B tensor maps of that task are encoded with it.
 struct TcTile {
-  int32_t task, m0, n0, pad;
+  int32_t task, m0, n0, b_rows;
 };
+// B box rows for a task of N columns.
+inline int32_t b_box_rows(int32_t n) { return n >= 128 ? 128 : ((n + 15) & ~15); }
 
 struct TcPlan {
   std::vector<TcTask> tasks;
