@@ -107,6 +107,10 @@ _SIGS = {
     "cmps_dmrg_grow": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
     "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
     "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp, C.c_int]),
+    "cmps_dmrg_keep_blocks": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_dmrg_move": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int),
+                                 c_dblp]),
+    "cmps_dmrg_position": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),
     "cmps_heff_adjoint": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc), C.c_void_p, C.c_void_p, c_dblp]),
     "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
     "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
@@ -473,6 +477,61 @@ class iDMRG:
             self.close()
         except Exception:
             pass
+
+
+class fDMRG(iDMRG):
+    """Finite DMRG on the device: fDMRG_DRV's growth to `nvertices`, then
+    FiniteDMRG::run's sweeps (fDMRG_routines.cpp:19-66) with every block kept
+    in device memory."""
+
+    def __init__(self, ctx: Context, rules, W: MPXTensor, nvertices, target=None, precision=CMPS_FP64, tol=1e-10,
+                 max_restarts=50, krylov_dim=24):
+        super().__init__(ctx, rules, W, target, precision, tol, max_restarts, krylov_dim)
+        _check(lib.cmps_dmrg_keep_blocks(self.h, 1))
+        self.nvertices = int(nvertices)
+
+    def position(self):
+        """(vertices left of the two-vertex window, chain length)."""
+        nl, n = C.c_int64(), C.c_int64()
+        _check(lib.cmps_dmrg_position(self.h, C.byref(nl), C.byref(n)))
+        return nl.value, n.value
+
+    def move(self, direction, chi=0, max_trunc=0.0):
+        """One sweep step, +1 right / -1 left (move_{right,left}_two_vertex)."""
+        row = np.zeros(5, np.float64)
+        bd = C.c_int64()
+        mv = C.c_int()
+        ms = np.zeros(4, np.float64)
+        _check(lib.cmps_dmrg_move(self.h, int(direction), chi, max_trunc, _p(row, C.c_double), C.byref(bd),
+                                  C.byref(mv), _p(ms, C.c_double)))
+        self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
+                         chi=bd.value, matvecs=mv.value, ms=ms)
+        return self.last
+
+    def run(self, sweeps, chi, max_trunc=1e-16):
+        """Growth rows, then the rows written when the window passes the
+        middle of the chain (twice per sweep): the rows of the energies file."""
+        rows = [self.grow(chi, max_trunc) for _ in range(self.nvertices // 2)]
+        nl, n = self.position()
+        if n <= 2:
+            return rows
+        for _ in range(sweeps):
+            nl, n = self.position()
+            for _ in range(n - nl - 2):
+                self.move(+1, chi, max_trunc)
+            nl, n = self.position()
+            for _ in range(nl):
+                r = self.move(-1, chi, max_trunc)
+                a, b = self.position()
+                if a == b - a - 2:
+                    rows.append(r)
+            nl, n = self.position()
+            for _ in range((n - nl - 2) - nl):
+                r = self.move(+1, chi, max_trunc)
+                a, b = self.position()
+                if a == b - a - 2:
+                    rows.append(r)
+        return rows
 
 
 def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: bool):

@@ -86,10 +86,29 @@ struct Dmrg {
     }
     dL.data.release();
     dR.data.release();
+    for (auto& kv : lblocks) kv.second.data.release();
+    for (auto& kv : rblocks) kv.second.data.release();
   }
+  // finite sweeps: the blocks of every length, kept when keep_blocks is set
+  // before growth; key = number of vertices the block covers
+  bool keep_blocks = false;
+  std::map<int64_t, Env> lblocks, rblocks;
+  int64_t nleft = 0;  // vertices left of the two-vertex window
+
   int dummy_blocks(Env& L, Env& R);
   int predict(Heff& next, bool* ok);
-  int grow(int64_t chi, double trunc, double* out);
+  // dir 0: iDMRG growth step (grow_two_vertex); +1 / -1: finite sweep step
+  // to the right / left (move_{right,left}_two_vertex)
+  int step(int dir, int64_t chi, double trunc, double* out);
+  int grow(int64_t chi, double trunc, double* out) { return step(0, chi, trunc, out); }
+  static int store(std::map<int64_t, Env>& m, int64_t k, const Env& e, cudaStream_t st) {
+    auto it = m.find(k);
+    if (it != m.end()) it->second.data.release();
+    Env c;
+    CMPS_TRY(copy_env(e, c, st));
+    m[k] = c;
+    return CMPS_OK;
+  }
 };
 
 int Dmrg::dummy_blocks(Env& L, Env& R) {
@@ -233,8 +252,15 @@ int Dmrg::predict(Heff& next, bool* ok) {
   return status;
 }
 
-int Dmrg::grow(int64_t chi, double trunc, double* out) {
+int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   cudaStream_t st = ctx->stream;
+  if (dir != 0) {
+    if (!keep_blocks || !heff || !svd) return fail(CMPS_ERR_STATE, "finite sweep: grow with kept blocks first");
+    if (grad_on) return fail(CMPS_ERR_STATE, "the coupling gradient is carried through growth steps only");
+    const int64_t nright = size - nleft - 2;
+    if (dir > 0 && nright < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the right end");
+    if (dir < 0 && nleft < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the left end");
+  }
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   struct EvGuard {
     cudaEvent_t* e;
@@ -251,7 +277,31 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   const auto h0 = clock::now();
   cudaEventRecord(ev[0], st);
   Env L, R;
-  if (size == 0) {
+  if (dir > 0) {
+    // MakeLeftBlock with A = U of this window; the right block of the new
+    // window was stored by the growth or the previous sweep
+    Env nl;
+    CMPS_TRY(left_update(*heff, *svd, nl));
+    int rc = store(lblocks, nleft + 1, nl, st);
+    nl.data.release();
+    CMPS_TRY(rc);
+    nleft += 1;
+    auto ir = rblocks.find(size - nleft - 2);
+    if (ir == rblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: right block missing");
+    CMPS_TRY(copy_env(lblocks[nleft], L, st));
+    CMPS_TRY(copy_env(ir->second, R, st));
+  } else if (dir < 0) {
+    Env nr;
+    CMPS_TRY(right_update(*heff, *svd, nr));
+    int rc = store(rblocks, size - nleft - 1, nr, st);
+    nr.data.release();
+    CMPS_TRY(rc);
+    nleft -= 1;
+    auto il = lblocks.find(nleft);
+    if (il == lblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: left block missing");
+    CMPS_TRY(copy_env(il->second, L, st));
+    CMPS_TRY(copy_env(rblocks[size - nleft - 2], R, st));
+  } else if (size == 0) {
     CMPS_TRY(dummy_blocks(L, R));
   } else {
     CMPS_TRY(left_update(*heff, *svd, L));
@@ -272,6 +322,13 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
       have_dlr = true;
     }
   }
+  if (dir == 0) {
+    if (size > 0) nleft += 1;
+    if (keep_blocks) {
+      CMPS_TRY(store(lblocks, nleft, L, st));
+      CMPS_TRY(store(rblocks, nleft, R, st));
+    }
+  }
   cudaEventRecord(ev[4], st);
   const auto h_env = clock::now();
   auto next = std::unique_ptr<Heff>(new Heff());
@@ -288,7 +345,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   next->precision = precision;
   const auto h_split = clock::now();
   bool have_guess = false;
-  CMPS_TRY(predict(*next, &have_guess));
+  if (dir == 0) CMPS_TRY(predict(*next, &have_guess));
   const auto h_pred = clock::now();
   // the previous step's factors and H_eff are no longer needed
   if (svd) {
@@ -310,7 +367,11 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   const auto h_eig = clock::now();
   cudaEventRecord(ev[2], st);
   svd.reset(new SvdResult());
-  CMPS_TRY(theta_svd(*heff, chi, trunc, *svd));
+  // sweep steps next to an end keep every state up to chi (no weight cut),
+  // as move_{right,left}_two_vertex do
+  const int64_t nright_now = (dir == 0 ? size + 2 : size) - nleft - 2;
+  const double cut = (dir > 0 && nright_now <= 1) || (dir < 0 && nleft <= 1) ? -0.0 : trunc;
+  CMPS_TRY(theta_svd(*heff, chi, cut, *svd));
   cudaEventRecord(ev[3], st);
   cudaEventSynchronize(ev[3]);
   const auto h_svd = clock::now();
@@ -351,7 +412,7 @@ int Dmrg::grow(int64_t chi, double trunc, double* out) {
   for (double& x : v) x *= f;
   prev_lambda = size == 0 ? std::vector<double>(1, 1.0) : lambda;
   lambda = v;
-  size += 2;
+  if (dir == 0) size += 2;
   out[0] = e;
   out[1] = e / (double)size;
   out[2] = entropy_of(lambda);
@@ -434,17 +495,42 @@ int cmps_dmrg_set_solver(cmps_dmrg* d, double tol, int max_restarts, int krylov_
   return CMPS_OK;
 }
 
-int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
-                   double* ms4) {
+static int dmrg_step(cmps_dmrg* d, int dir, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim,
+                     int* matvecs, double* ms4) {
   if (!d || !d->impl || !row5) return fail(CMPS_ERR_ARG, "null argument");
   Dmrg& D = *d->impl;
   CMPS_CUDA(cudaSetDevice(D.device));
-  int rc = D.grow(chi, max_trunc, row5);
+  int rc = D.step(dir, chi, max_trunc, row5);
   if (bond_dim) *bond_dim = (int64_t)D.lambda.size();
   if (matvecs) *matvecs = D.last_matvecs;
   if (ms4)
     for (int i = 0; i < 4; ++i) ms4[i] = D.last_ms[i];
   return rc;
+}
+
+int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
+                   double* ms4) {
+  return dmrg_step(d, 0, chi, max_trunc, row5, bond_dim, matvecs, ms4);
+}
+
+int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (d->impl->size != 0) return fail(CMPS_ERR_STATE, "choose block keeping before the first growth step");
+  d->impl->keep_blocks = keep != 0;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim,
+                   int* matvecs, double* ms4) {
+  if (direction != 1 && direction != -1) return fail(CMPS_ERR_ARG, "direction must be +1 (right) or -1 (left)");
+  return dmrg_step(d, direction, chi, max_trunc, row5, bond_dim, matvecs, ms4);
+}
+
+int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (nleft) *nleft = d->impl->nleft;
+  if (size) *size = d->impl->size;
+  return CMPS_OK;
 }
 
 int cmps_dmrg_set_gradient(cmps_dmrg* d, const cmps_mpx_desc* dW) {

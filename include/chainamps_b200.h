@@ -233,6 +233,23 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
                    int* matvecs, double* ms4);
 /* The current (rescaled) singular values, bond_dim of them, descending. */
 int cmps_dmrg_values(const cmps_dmrg* d, double* values);
+/* ---- finite sweeps (FiniteDMRG, fDMRG_routines.cpp:19-66) ---------------
+ * cmps_dmrg_keep_blocks(d, 1) before the first growth step keeps the left
+ * and right blocks of every length (BlocksStructure, kept in device memory
+ * instead of the reference's .BLOCK files).  After growth to the chain
+ * length, cmps_dmrg_move(d, +1 / -1, ...) is move_right_two_vertex /
+ * move_left_two_vertex (DMRG_routines.cpp:376-444): the block of the side
+ * the window leaves is updated with this window's U or V^dagger, the new
+ * window is solved and truncated (no weight cut next to an end), and row5 is
+ * the reference's energies row (fidelity NaN).  The start vector of a sweep
+ * step is the fixed pseudo-random one (the finite predictions,
+ * MakeL/RFinitePrediction :709-716, are not built).  cmps_dmrg_position
+ * returns the number of vertices left of the window and the chain length. */
+int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep);
+int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, double* row5,
+                   int64_t* bond_dim, int* matvecs, double* ms4);
+int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);
+
 /* Coupling gradient along the growth (no reference counterpart).  Set before
  * the first growth step: dW as for cmps_heff_adjoint (NULL turns it off).
  * Each step then carries the derivative environments dL, dR (the environment

@@ -90,3 +90,39 @@ def test_coupled_ising_idmrg_matches_oracle(ctx):
         assert abs(got["energy"] - ref["energy"]) <= 1e-9 * abs(ref["energy"]), (got, ref)
         assert abs(got["entropy"] - ref["entropy"]) <= 1e-8
         assert abs(mx["energy"] - got["energy"]) <= 1e-9 * abs(got["energy"]), (mx, got)
+
+
+def test_device_fdmrg_reproduces_spin_half_example(ctx):
+    """fDMRG_DRV -B 50 -F 2 on 10 vertices, entirely on the device: the 5
+    growth rows and the 4 sweep rows of the reference's example README
+    (energy 1e-10 relative, entropy 1e-8, truncation 1e-12)."""
+    from chainamps_b200 import fDMRG
+    k = json.load(open(GOLD))["spin_half_fdmrg"]
+    v = parse_user_vertex(k["basis"], k["hamiltonian"], k["operators"])
+    H = make_general_hmpo(v, parse_couplings(k["input"].splitlines()[2]))
+    run = fDMRG(ctx, H.rules, to_tensor(H), k["vertices"], tol=1e-12, krylov_dim=32)
+    rows = run.run(k["sweeps"], k["chi"], k["trunc"])
+    assert len(rows) == len(k["energies"])
+    for r, e in zip(rows, k["energies"]):
+        assert abs(r["energy"] - e[1]) <= 1e-10 * abs(e[1]), (r, e)
+        assert abs(r["energy_per"] - e[2]) <= 1e-10 * abs(e[2])
+        assert abs(r["entropy"] - e[3]) <= 1e-8, (r, e)
+        assert abs(r["truncation"] - e[4]) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_fdmrg_matches_oracle_with_truncation(ctx, precision):
+    """XXZ chain of 16 vertices at chi = 12 (truncating): every energies-file
+    row of the device sweeps against the oracle's run_fdmrg."""
+    from chainamps_b200 import fDMRG, CMPS_FP64, CMPS_SPLIT_TF32
+    H = model_zoo()["xxz"]
+    _, ref = od.run_fdmrg(H, 16, 2, 12, 1e-16, tol=1e-13)
+    prec = CMPS_FP64 if precision == "fp64" else CMPS_SPLIT_TF32
+    run = fDMRG(ctx, H.rules, to_tensor(H), 16, precision=prec, tol=1e-12, krylov_dim=32)
+    rows = run.run(2, 12, 1e-16)
+    assert len(rows) == len(ref)
+    for r, e in zip(rows, ref):
+        assert r["chi"] == e["chi"]
+        assert abs(r["energy"] - e["energy"]) <= 1e-9 * abs(e["energy"]), (r, e)
+        assert abs(r["entropy"] - e["entropy"]) <= 1e-7, (r, e)
+        assert abs(r["truncation"] - e["truncation"]) <= 1e-11
