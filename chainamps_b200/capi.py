@@ -108,6 +108,7 @@ _SIGS = {
     "cmps_dmrg_values": (C.c_int, [C.c_void_p, c_dblp]),
     "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp, C.c_int]),
     "cmps_dmrg_keep_blocks": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_dmrg_set_fidelity": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_dmrg_move": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int),
                                  c_dblp]),
     "cmps_dmrg_position": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),

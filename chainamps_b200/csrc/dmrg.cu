@@ -92,6 +92,7 @@ struct Dmrg {
   // finite sweeps: the blocks of every length, kept when keep_blocks is set
   // before growth; key = number of vertices the block covers
   bool keep_blocks = false;
+  bool want_fidelity = true;  // CheckConvergence on growth steps
   std::map<int64_t, Env> lblocks, rblocks;
   int64_t nleft = 0;  // vertices left of the two-vertex window
 
@@ -372,6 +373,18 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   const int64_t nright_now = (dir == 0 ? size + 2 : size) - nleft - 2;
   const double cut = (dir > 0 && nright_now <= 1) || (dir < 0 && nleft <= 1) ? -0.0 : trunc;
   CMPS_TRY(theta_svd(*heff, chi, cut, *svd));
+  // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
+  std::vector<double> v = svd->values;
+  double sq = 0.0;
+  for (double x : v) sq += x * x;
+  if (!(sq > 0.0)) return fail(CMPS_ERR_SOLVER, "square sum error: no weight kept");
+  const double f = std::sqrt(1.0 / sq);
+  for (double& x : v) x *= f;
+  prev_lambda = size == 0 ? std::vector<double>(1, 1.0) : lambda;
+  lambda = v;
+  // growth steps report CheckConvergence, timed with the SVD phase
+  double fid = std::nan("");
+  if (dir == 0 && want_fidelity) CMPS_TRY(growth_fidelity(*heff, *svd, lambda, prev_lambda, &fid));
   cudaEventRecord(ev[3], st);
   cudaEventSynchronize(ev[3]);
   const auto h_svd = clock::now();
@@ -403,21 +416,12 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
                                  ms_since(h_eig, h_svd),
                                  ms_since(h0, h_svd)};
   for (int i = 0; i < kProfile; ++i) last_profile[i] = prof[i];
-  // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
-  std::vector<double> v = svd->values;
-  double sq = 0.0;
-  for (double x : v) sq += x * x;
-  if (!(sq > 0.0)) return fail(CMPS_ERR_SOLVER, "square sum error: no weight kept");
-  const double f = std::sqrt(1.0 / sq);
-  for (double& x : v) x *= f;
-  prev_lambda = size == 0 ? std::vector<double>(1, 1.0) : lambda;
-  lambda = v;
   if (dir == 0) size += 2;
   out[0] = e;
   out[1] = e / (double)size;
   out[2] = entropy_of(lambda);
   out[3] = svd->discarded;
-  out[4] = std::nan("");
+  out[4] = fid;
   return rc;
 }
 
@@ -511,6 +515,12 @@ static int dmrg_step(cmps_dmrg* d, int dir, int64_t chi, double max_trunc, doubl
 int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
                    double* ms4) {
   return dmrg_step(d, 0, chi, max_trunc, row5, bond_dim, matvecs, ms4);
+}
+
+int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  d->impl->want_fidelity = on != 0;
+  return CMPS_OK;
 }
 
 int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep) {

@@ -161,6 +161,8 @@ void extend_pattern(std::vector<WEntry>& W, const std::vector<WEntry>& dW);
 int derivative_parts(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, Planar& LPd,
                      Planar& RPd);
 int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad);
+int growth_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, const std::vector<double>& prev,
+                    double* out);
 int left_update(Heff& H, const SvdResult& s, Env& out);
 int right_update(Heff& H, const SvdResult& s, Env& out);
 int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, const Env* dL, const Env* dR,

@@ -142,6 +142,19 @@ __global__ void k_scale_cols_inv(double2* __restrict__ G, int64_t rows, int64_t 
   }
 }
 
+// M[r + R c] = rs[r] cs[c] Vd[src[r] + c]  (column-major gather of
+// Lambda V^dagger diag(prev_lambda) restricted to one a2 sector)
+__global__ void k_gather_fid(const double* __restrict__ vr, const double* __restrict__ vi,
+                             const int64_t* __restrict__ src, const double* __restrict__ rs,
+                             const double* __restrict__ cs, int64_t R, int64_t Cn, double2* __restrict__ M) {
+  const int64_t n = R * Cn;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % R, c = e / R;
+    const double f = rs[r] * cs[c];
+    M[e] = make_double2(f * vr[src[r] + c], f * vi[src[r] + c]);
+  }
+}
+
 int grid_of(int64_t n) {
   int64_t g = (n + 255) / 256;
   if (g < 1) g = 1;
@@ -436,6 +449,102 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
   } while (false);
   cleanup();
   return status;
+}
+
+// CheckConvergence (DMRG_routines.cpp:769-771) for a growth step:
+// 1 - sum of the singular values of Aux diag(prev_lambda), where MakePrediction
+// (:693-707) takes Aux = diag(s~) V~^dagger from the SVD of Lambda V^dagger
+// reshaped to rows (sigma2, a1) and columns a2.  Aux^H Aux equals
+// (Lambda V^dagger)^H (Lambda V^dagger), so the singular values of
+// Aux diag(prev_lambda) are those of (Lambda V^dagger) diag(prev_lambda)
+// itself; that matrix is block diagonal in the a2 charge, and each block's
+// values come from a values-only one-sided Jacobi SVD (not the Gram matrix,
+// whose small eigenvalues would carry an error ~ sqrt(eps) s_max).
+int growth_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, const std::vector<double>& prev,
+                    double* out) {
+  const Rules& r = H.rules;
+  const ThetaSpace& th = s.th;
+  const Bond& A2 = s.a2;
+  if ((int64_t)prev.size() != A2.size()) return fail(CMPS_ERR_STATE, "fidelity: previous values do not match the bond");
+  cudaStream_t st = H.ctx->stream;
+  cusolverDnHandle_t sol;
+  CMPS_TRY(get_solver(H.ctx, &sol));
+  gesvdjInfo_t params;
+  if (cusolverDnCreateGesvdjInfo(&params) != CUSOLVER_STATUS_SUCCESS) return fail(CMPS_ERR_SOLVER, "gesvdj info");
+  cusolverDnXgesvdjSetTolerance(params, 0.0);
+  cusolverDnXgesvdjSetMaxSweeps(params, 100);
+  double total = 0.0;
+  int status = CMPS_OK;
+  for (int t = 0; t < A2.nsec() && status == CMPS_OK; ++t) {
+    const int64_t Cn = A2.sdim[t];
+    std::vector<int64_t> src;
+    std::vector<double> rs, cs(Cn);
+    for (int64_t c = 0; c < Cn; ++c) cs[c] = prev[A2.selem[t][c]];
+    for (int s2 = 0; s2 < H.d; ++s2) {
+      const int m = th.find(r.sub(A2.sq[t], H.sigq[s2]));
+      if (m < 0 || s.kept[m] == 0 || th.coloff[m][s2] < 0) continue;
+      for (int64_t j = 0; j < s.kept[m]; ++j) {
+        src.push_back(s.voff[m] + j * th.ncols[m] + th.coloff[m][s2]);
+        rs.push_back(lam[s.gidx[m][j]]);
+      }
+    }
+    const int64_t R = (int64_t)src.size();
+    if (R == 0 || Cn == 0) continue;
+    if (R > 0x7fffffff || Cn > 0x7fffffff) { status = fail(CMPS_ERR_ARG, "fidelity: block too large"); break; }
+    int64_t* dsrc = nullptr;
+    double *drs = nullptr, *dcs = nullptr, *dS = nullptr;
+    double2 *dM = nullptr, *dU = nullptr, *dV = nullptr;
+    cuDoubleComplex* work = nullptr;
+    int* dinfo = nullptr;
+    const int64_t mn = std::min(R, Cn);
+    do {
+      if (dmalloc(&dsrc, sizeof(int64_t) * R) != cudaSuccess || dmalloc(&drs, sizeof(double) * R) != cudaSuccess ||
+          dmalloc(&dcs, sizeof(double) * Cn) != cudaSuccess || dmalloc(&dM, sizeof(double2) * R * Cn) != cudaSuccess ||
+          dmalloc(&dS, sizeof(double) * mn) != cudaSuccess || dmalloc(&dU, sizeof(double2) * R * mn) != cudaSuccess ||
+          dmalloc(&dV, sizeof(double2) * Cn * mn) != cudaSuccess || dmalloc(&dinfo, sizeof(int)) != cudaSuccess) {
+        status = fail(CMPS_ERR_NOMEM, "fidelity: allocation failed");
+        break;
+      }
+      if ((status = copy_wait(dsrc, src.data(), sizeof(int64_t) * R, cudaMemcpyHostToDevice, st)) != CMPS_OK) break;
+      if ((status = copy_wait(drs, rs.data(), sizeof(double) * R, cudaMemcpyHostToDevice, st)) != CMPS_OK) break;
+      if ((status = copy_wait(dcs, cs.data(), sizeof(double) * Cn, cudaMemcpyHostToDevice, st)) != CMPS_OK) break;
+      k_gather_fid<<<grid_of(R * Cn), 256, 0, st>>>(s.Vd.re(), s.Vd.im(), dsrc, drs, dcs, R, Cn, dM);
+      int lwork = 0;
+      // the solver checks ldu >= rows and ldv >= columns even without vectors
+      if (cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_NOVECTOR, 1, (int)R, (int)Cn, (cuDoubleComplex*)dM,
+                                       (int)R, dS, (cuDoubleComplex*)dU, (int)R, (cuDoubleComplex*)dV, (int)Cn,
+                                       &lwork, params) != CUSOLVER_STATUS_SUCCESS) {
+        status = fail(CMPS_ERR_SOLVER, "fidelity: gesvdj buffer query failed");
+        break;
+      }
+      if (dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess) {
+        status = fail(CMPS_ERR_NOMEM, "fidelity: work allocation failed");
+        break;
+      }
+      if (cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_NOVECTOR, 1, (int)R, (int)Cn, (cuDoubleComplex*)dM, (int)R, dS,
+                            (cuDoubleComplex*)dU, (int)R, (cuDoubleComplex*)dV, (int)Cn, work, lwork, dinfo,
+                            params) != CUSOLVER_STATUS_SUCCESS) {
+        status = fail(CMPS_ERR_SOLVER, "fidelity: gesvdj failed");
+        break;
+      }
+      std::vector<double> sv(mn);
+      if ((status = copy_wait(sv.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st)) != CMPS_OK) break;
+      for (double v : sv) total += v;
+    } while (false);
+    dfree(dsrc);
+    dfree(drs);
+    dfree(dcs);
+    dfree(dM);
+    dfree(dS);
+    dfree(dU);
+    dfree(dV);
+    dfree(work);
+    dfree(dinfo);
+  }
+  cusolverDnDestroyGesvdjInfo(params);
+  CMPS_TRY(status);
+  *out = 1.0 - total;
+  return CMPS_OK;
 }
 
 // New bond built from the kept singular vectors, in the reference's element

@@ -225,10 +225,12 @@ int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cm
 int cmps_dmrg_destroy(cmps_dmrg* d);
 int cmps_dmrg_set_solver(cmps_dmrg* d, double tol, int max_restarts, int krylov_dim);
 /* One growth step.  row5 = {energy, energy / vertices, entropy, truncation,
- * fidelity (NaN: not computed)} -- the Data row of iDMRG_DRV's energies
- * file; bond_dim = kept states; matvecs = H_eff applications; ms4 = device
- * time of {environment update + H_eff build + prediction, eigensolve, SVD,
- * total} in ms (CUDA events).  Any output pointer but row5 may be NULL. */
+ * fidelity} -- the Data row of iDMRG_DRV's energies file (fidelity =
+ * CheckConvergence, DMRG_routines.cpp:769-771, on by default; NaN when
+ * turned off with cmps_dmrg_set_fidelity(d, 0)); bond_dim = kept states;
+ * matvecs = H_eff applications; ms4 = device time of {environment update +
+ * H_eff build + prediction, eigensolve, SVD (+ fidelity), total} in ms (CUDA
+ * events).  Any output pointer but row5 may be NULL. */
 int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim,
                    int* matvecs, double* ms4);
 /* The current (rescaled) singular values, bond_dim of them, descending. */
@@ -246,6 +248,7 @@ int cmps_dmrg_values(const cmps_dmrg* d, double* values);
  * MakeL/RFinitePrediction :709-716, are not built).  cmps_dmrg_position
  * returns the number of vertices left of the window and the chain length. */
 int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep);
+int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on);
 int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, double* row5,
                    int64_t* bond_dim, int* matvecs, double* ms4);
 int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);

@@ -40,6 +40,7 @@ def test_device_growth_reproduces_spin_half_example(ctx):
         assert abs(r["energy"] - row[1]) <= 1e-10 * abs(row[1]), (r, row)
         assert abs(r["entropy"] - row[3]) <= 1e-8, (r, row)
         assert abs(r["truncation"] - row[4]) <= 1e-12
+        assert abs(r["fidelity"] - row[5]) <= 1e-10, (r, row)      # CheckConvergence
 
 
 @pytest.mark.parametrize("name,chi,steps", [("xxz", 32, 10), ("tfim", 24, 5)])
@@ -55,6 +56,7 @@ def test_device_idmrg_matches_oracle(ctx, name, chi, steps):
         assert abs(got["energy"] - ref["energy"]) <= 1e-9 * abs(ref["energy"]), (got, ref)
         assert abs(got["entropy"] - ref["entropy"]) <= 1e-8
         assert abs(got["truncation"] - ref["truncation"]) <= 1e-12
+        assert abs(got["fidelity"] - ref["fidelity"]) <= 1e-9, (got, ref)
         np.testing.assert_allclose(run.values(), sb.dec.values, rtol=1e-7, atol=1e-10)
 
 
