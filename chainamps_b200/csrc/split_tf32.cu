@@ -157,7 +157,8 @@ int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t l
 
 void add_tiles(tc::TcPlan& p, int32_t task, int32_t m, int32_t n) {
   for (int32_t m0 = 0; m0 < m; m0 += 128)
-    for (int32_t n0 = 0; n0 < n; n0 += 128) p.tiles.push_back(tc::TcTile{task, m0, n0, tc::b_box_rows(n)});
+    for (int32_t n0 = 0; n0 < n; n0 += 128)
+      p.tiles.push_back(tc::TcTile{task, m0, n0, tc::b_box_rows(n), 0, ((std::min(128, n - n0)) + 15) & ~15});
 }
 
 }  // namespace
@@ -466,15 +467,20 @@ static int build_split(Heff& H) {
       add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
       p2.tasks.push_back(task);
     }
+  // k-steps per tile (the MMA warp walks them without term lookups)
+  for (tc::TcPlan* p : {&p1, &p2})
+    for (tc::TcTile& t : p->tiles) {
+      const tc::TcTask& k = p->tasks[t.task];
+      int64_t it = 0;
+      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + 15) / 16;
+      if (it > 0x7fffffff) return fail(CMPS_ERR_ARG, "tcgen05 plan: too many k-steps in one tile");
+      t.kiters = (int32_t)it;
+    }
   // heaviest tiles first: the persistent kernel deals tiles round-robin to
   // the SMs, so this ordering balances the per-SM work
   for (tc::TcPlan* p : {&p1, &p2}) {
     auto cost = [&](const tc::TcTile& t) {
-      const tc::TcTask& k = p->tasks[t.task];
-      int64_t it = 0;
-      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + 15) / 16;
-      const int64_t n = std::min<int64_t>(128, k.n - t.n0);
-      return (it + 2) * ((n + 15) / 16);  // +2: fixed per-tile cost (epilogue)
+      return (int64_t)(t.kiters + 2) * (t.nmma / 16);  // +2: fixed per-tile cost (epilogue)
     };
     std::stable_sort(p->tiles.begin(), p->tiles.end(),
                      [&](const tc::TcTile& a, const tc::TcTile& b) { return cost(a) > cost(b); });
@@ -500,8 +506,15 @@ static int build_split(Heff& H) {
     for (const tc::TcTask& t : p.tasks)
       for (int q = t.t0; q < t.t1; ++q)
         if (rows[p.terms[q].b_map] != t.n) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map rows differ from N");
-    for (const tc::TcTile& tl : p.tiles)
-      if (tl.b_rows != tc::b_box_rows(p.tasks[tl.task].n)) return fail(CMPS_ERR_STATE, "tcgen05 plan: B box height");
+    for (const tc::TcTile& tl : p.tiles) {
+      const tc::TcTask& t = p.tasks[tl.task];
+      if (tl.b_rows != tc::b_box_rows(t.n)) return fail(CMPS_ERR_STATE, "tcgen05 plan: B box height");
+      if (tl.nmma < 16 || tl.nmma > 128 || tl.nmma != ((std::min(128, t.n - tl.n0) + 15) & ~15) || tl.nmma > tl.b_rows)
+        return fail(CMPS_ERR_STATE, "tcgen05 plan: tile N");
+      int64_t it = 0;
+      for (int q = t.t0; q < t.t1; ++q) it += (p.terms[q].k + 15) / 16;
+      if (it != tl.kiters) return fail(CMPS_ERR_STATE, "tcgen05 plan: tile k-steps");
+    }
   }
   CMPS_TRY(p1.upload(H.ctx->stream));
   CMPS_TRY(p2.upload(H.ctx->stream));

@@ -218,11 +218,11 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
     if (lane == 0) {
       int it = 0, tc = 0;
       bool ok = true;
+      TcTile nxt = blockIdx.x < (unsigned)ntiles ? tiles[blockIdx.x] : TcTile{};
       for (int ti = blockIdx.x; ti < ntiles && ok; ti += gridDim.x, ++tc) {
-        const TcTile tile = tiles[ti];
-        const TcTask task = tasks[tile.task];
-        const int ntile = min(kBN, task.n - tile.n0);
-        const int nmma = (ntile + 15) & ~15;  // multiple of 16 for M = 128
+        const TcTile tile = nxt;
+        if (ti + (int)gridDim.x < ntiles) nxt = tiles[ti + gridDim.x];  // in flight during this tile
+        const int nmma = tile.nmma;  // multiple of 16 for M = 128
         const uint32_t id_pos = idesc_tf32(nmma, false), id_neg = idesc_tf32(nmma, true);
         const int buf = tc & 1;
         const uint32_t use = (uint32_t)(tc >> 1);
@@ -234,9 +234,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         const uint32_t d_re = tmem + (uint32_t)(buf * 256), d_im = d_re + 128;
         const uint32_t b_plane = 64u * (uint32_t)tile.b_rows;  // bytes per B plane in shared memory
         bool first = true;
-        for (int t = task.t0; t < task.t1 && ok; ++t) {
-          const int kt = terms[t].k;
-          for (int k0 = 0; k0 < kt; k0 += kBK, ++it) {
+        {
+          for (int kst = 0; kst < tile.kiters; ++kst, ++it) {
             const int s = it % kStages;
             const uint32_t ph = (uint32_t)((it / kStages) & 1);
             if (!mbar_wait(&full[s], ph, err, 2)) {
@@ -281,11 +280,18 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = quad * 32 + lane;
     int tc = 0;
+    // the next tile's records are loaded while this tile waits and drains
+    TcTile nt = blockIdx.x < (unsigned)ntiles ? tiles[blockIdx.x] : TcTile{};
+    TcTask nk = blockIdx.x < (unsigned)ntiles ? tasks[nt.task] : TcTask{};
     for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x, ++tc) {
-      const TcTile tile = tiles[ti];
-      const TcTask task = tasks[tile.task];
+      const TcTile tile = nt;
+      const TcTask task = nk;
+      if (ti + (int)gridDim.x < ntiles) {
+        nt = tiles[ti + gridDim.x];
+        nk = tasks[nt.task];
+      }
       const int ntile = min(kBN, task.n - tile.n0);
-      const int nmma = (ntile + 15) & ~15;
+      const int nmma = tile.nmma;
       const int buf = tc & 1;
       const uint32_t use = (uint32_t)(tc >> 1);
       int have = task.t1 > task.t0 ? 1 : 0;

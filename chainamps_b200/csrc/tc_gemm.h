@@ -25,8 +25,10 @@ struct TcTerm {
 };
 // b_rows: row count of the B boxes of this tile's task (its N rounded up to
 // 16, at most 128); the B tensor maps of that task are encoded with it.
+// kiters: 16-wide k-steps of the task's terms; nmma: the tile's N rounded up
+// to 16 (the MMA N) -- so the MMA warp needs no task or term lookups.
 struct TcTile {
-  int32_t task, m0, n0, b_rows;
+  int32_t task, m0, n0, b_rows, kiters, nmma;
 };
 // B box rows for a task of N columns.
 inline int32_t b_box_rows(int32_t n) { return n >= 128 ? 128 : ((n + 15) & ~15); }
