@@ -1,12 +1,15 @@
 // Split-precision (3-term TF32 on tcgen05, FP32 accumulate) form of the
 // H_eff matvec: operand preparation, tensor maps and the two stage plans.
 //
-// Layouts (FP32, four planes re_hi, re_lo, im_hi, im_lo per buffer):
+// Layouts (FP32; S1A, LPS and RPTS as four planes re_hi, re_lo, im_hi, im_lo,
+// TS as two planes re, im):
 //  * S1A  -- stage-1 A operand: theta transposed per (m, sigma1) chunk,
 //            [r][a0] with r running over the padded right index of m (each
 //            sigma2 chunk starts on a 4-element boundary) and ld = pad4(dim a0);
 //  * LPS  -- stage-1 B operand: LeftPart blocks [a0'][a0], ld = pad4(dim a0);
-//  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad];
+//  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad], the
+//            FP32 accumulator; stage 2 splits it into TF32 hi / lo in shared
+//            memory, so T crosses HBM at 8 bytes per complex entry each way;
 //  * RPTS -- stage-2 B operand: RightPart blocks transposed, [a2'][a2].
 // Every block base is 128-byte aligned and every leading dimension a multiple
 // of 4 floats, as the TMA requires; the K tail of every operand is zero-filled
@@ -177,9 +180,12 @@ int TcPlan::upload(cudaStream_t st) {
   CMPS_TRY(up(tiles, &d_tiles));
   CMPS_TRY(up(amaps, &d_amaps));
   CMPS_TRY(up(bmaps, &d_bmaps));
+  CMPS_TRY(up(adescs, &d_adescs));
   return CMPS_OK;
 }
 void TcPlan::release() {
+  if (d_adescs) dfree(d_adescs);
+  d_adescs = nullptr;
   if (d_tasks) dfree(d_tasks);
   if (d_terms) dfree(d_terms);
   if (d_tiles) dfree(d_tiles);
@@ -280,7 +286,7 @@ static int build_split(Heff& H) {
   S->lps_len = align32(std::max<int64_t>(lps, 32));
   S->ts_off = S->lps_off + 4 * S->lps_len;
   S->ts_len = align32(std::max<int64_t>(ts, 32));
-  S->rpt_off = S->ts_off + 4 * S->ts_len;
+  S->rpt_off = S->ts_off + 2 * S->ts_len;  // T: two FP32 planes (re, im)
   S->rpt_len = align32(std::max<int64_t>(rpt, 32));
   const int64_t total = S->rpt_off + 4 * S->rpt_len;
   if (dmalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
@@ -417,10 +423,12 @@ static int build_split(Heff& H) {
       const int64_t tb = ts_base[(size_t)b1 * nm + m];
       if (tb < 0) continue;
       int mp = th.find(r.add(th.mq[m], H.bq[b1]));
-      CUtensorMap cm;
-      CMPS_TRY(make_map(S->buf + S->ts_off, tb, S->ncols_pad[m], th.nrows[mp], S->ncols_pad[m], S->ts_len, &cm));
-      amap2[(size_t)b1 * nm + m] = (int32_t)p2.amaps.size();
-      p2.amaps.push_back(cm);
+      // T^{b1}_m as two FP32 planes, read and split by the converter warps
+      tc::TcADesc ad{tb, S->ncols_pad[m], (int32_t)th.nrows[mp], (int32_t)S->ncols_pad[m]};
+      if (tb < 0 || tb % 4 || ad.ld % 4 || tb + (ad.rows - 1) * ad.ld + ad.cols > S->ts_len)
+        return fail(CMPS_ERR_STATE, "stage-2 A block outside T");
+      amap2[(size_t)b1 * nm + m] = (int32_t)p2.adescs.size();
+      p2.adescs.push_back(ad);
     }
   std::map<std::array<int, 4>, int32_t> bmap2;
   {
@@ -487,10 +495,14 @@ static int build_split(Heff& H) {
   }
   // plan integrity: every term names an existing map, every tile an existing task
   for (const tc::TcPlan* p : {&p1, &p2}) {
+    const int32_t na = (int32_t)(p == &p1 ? p->amaps.size() : p->adescs.size());
     for (const tc::TcTerm& tm : p->terms)
-      if (tm.a_map < 0 || tm.a_map >= (int32_t)p->amaps.size() || tm.b_map < 0 ||
-          tm.b_map >= (int32_t)p->bmaps.size() || tm.k < 1 || (tm.a_x0 & 3))
+      if (tm.a_map < 0 || tm.a_map >= na || tm.b_map < 0 || tm.b_map >= (int32_t)p->bmaps.size() || tm.k < 1 ||
+          (tm.a_x0 & 3))
         return fail(CMPS_ERR_STATE, "tcgen05 plan: bad term");
+    if (p == &p2)
+      for (const tc::TcTerm& tm : p->terms)
+        if (tm.a_x0 + tm.k > p->adescs[tm.a_map].cols) return fail(CMPS_ERR_STATE, "tcgen05 plan: term past its T block");
     for (const tc::TcTask& t : p->tasks)
       if (t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)p->terms.size() || t.m < 1 || t.n < 1 || t.out_off < 0)
         return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
@@ -552,8 +564,8 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   const int64_t n = H.th.total;
   (void)n;
   CMPS_TRY(split_theta(*S, in, st));
-  CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st));
-  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st));
+  CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st));
+  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->buf + S->ts_off, S->ts_len, S->d_err, st));
   return CMPS_OK;
 }
 
@@ -575,9 +587,9 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   if (which == 1) {
     CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
     CMPS_TRY(split_theta(*S, in, st));
-    return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, S->d_err, st);
+    return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st);
   }
-  return tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->d_err, st);
+  return tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->buf + S->ts_off, S->ts_len, S->d_err, st);
 }
 
 int split_error(Heff& H) {

@@ -10,7 +10,11 @@
 // carried by the instruction descriptor's negate-A bit.  Both operands are
 // K-major (C[m,n] = sum_k A[m,k] B[n,k]); each operand block has its own 3-D
 // tensor map (K, rows, 4 planes) and one TMA load brings all four planes of a
-// 128-row x 16-column tile (SWIZZLE_64B).
+// 128-row x 16-column tile (SWIZZLE_64B).  Mode 2 (stage 2 of the matvec)
+// takes its A operand, the stage-1 intermediate T, as the raw FP32
+// accumulator in two planes: four converter warps load it and write the four
+// TF32 planes into shared memory in the same swizzled layout, which halves
+// T's HBM traffic in both stages.
 //
 // Persistent: one CTA per SM walks a list of 128 x N (N <= 128) output tiles
 // (tile i of CTA b is tiles[b + i * gridDim]; the host orders tiles by
@@ -32,7 +36,12 @@
 namespace cmps {
 namespace tc {
 
-constexpr int kThreads = 192;
+// warps 0 producer, 1 MMA, 2-5 epilogue; mode 2 adds warps 6-9, which load
+// the A tiles from global memory and split them into TF32 planes
+template <int MODE>
+constexpr int threads_of() {
+  return MODE == 2 ? 320 : 192;
+}
 constexpr int kStages = 3;
 constexpr int kBN = 128, kBK = 16;
 constexpr int kPlaneTileBytes = 128 * kBK * 4;          // 8 KB: 128 rows x 64 B
@@ -140,10 +149,11 @@ __device__ __forceinline__ float tf32_rna(float x) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(threads_of<MODE>(), 1)
 tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __restrict__ tasks,
               const TcTerm* __restrict__ terms, const CUtensorMap* __restrict__ amaps,
-              const CUtensorMap* __restrict__ bmaps, float* __restrict__ out32, int64_t out32_plane,
+              const CUtensorMap* __restrict__ bmaps, const TcADesc* __restrict__ adescs,
+              const float* __restrict__ ain, int64_t a_plane, float* __restrict__ out32, int64_t out32_plane,
               double* __restrict__ out64, int64_t out64_plane, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -157,7 +167,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 1);
+      mbar_init(&full[s], MODE == 2 ? 5 : 1);  // mode 2: the B copy plus one arrival per converter warp
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -186,7 +196,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         const TcTask task = tasks[tile.task];
         for (int t = task.t0; t < task.t1 && ok; ++t) {
           const TcTerm tm = terms[t];
-          tensormap_acquire(amaps + tm.a_map);
+          if (MODE == 1) tensormap_acquire(amaps + tm.a_map);
           tensormap_acquire(bmaps + tm.b_map);
           for (int k0 = 0; k0 < tm.k; k0 += kBK, ++it) {
             const int s = it % kStages;
@@ -197,9 +207,11 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
             }
             uint8_t* sa = smem + s * kStageBytes;
             uint8_t* sb = sa + kOperandBytes;
-            // A: 128-row box; B: the task's b_rows-row box (both four planes)
-            mbar_expect_tx(&full[s], (uint32_t)kOperandBytes + 4u * 64u * (uint32_t)tile.b_rows);
-            tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
+            // A: 128-row box (mode 1; written by the converter warps in mode 2);
+            // B: the task's b_rows-row box; both four planes
+            const uint32_t bbytes = 4u * 64u * (uint32_t)tile.b_rows;
+            mbar_expect_tx(&full[s], (MODE == 1 ? (uint32_t)kOperandBytes : 0u) + bbytes);
+            if (MODE == 1) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
             tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
           }
         }
@@ -275,7 +287,122 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         umma_commit(&tfull[buf]);  // arrives at once for a tile without terms
       }
     }
-  } else {
+  } else if (MODE == 2 && warp >= 6) {
+    // ---------------- A converters (mode 2): warps 6..9, one A row per thread ----------------
+    // Each k-step: this row's 16 K columns of the re and im planes are loaded,
+    // split into TF32 hi / lo and stored into the four A planes of the slot in
+    // the SWIZZLE_64B K-major layout the MMA descriptors read (16-byte chunk c
+    // of row r at r * 64 + ((c ^ ((r >> 1) & 3)) << 4)), made visible to the
+    // tensor core's async proxy and signalled on the slot's full barrier.  A
+    // cursor over this CTA's k-steps (tile, term, k0) runs one step ahead of
+    // the stores, so each row's global load is in flight while the previous
+    // k-step is converted and waits for its slot.
+    const int row = (warp - 6) * 32 + lane;
+    const uint32_t sw = (uint32_t)((row >> 1) & 3);
+    struct Cur {
+      int ti, t, t1, k0, k, a_x0, m0;
+      TcADesc ad;
+      bool valid;
+    };
+    auto first_term = [&](Cur& c) {
+      // from term c.t of tile c.ti onwards, skipping tiles without terms
+      while (c.valid && c.t >= c.t1) {
+        c.ti += gridDim.x;
+        if (c.ti >= ntiles) {
+          c.valid = false;
+          return;
+        }
+        const TcTile tl = tiles[c.ti];
+        const TcTask tk = tasks[tl.task];
+        c.m0 = tl.m0;
+        c.t = tk.t0;
+        c.t1 = tk.t1;
+      }
+      if (!c.valid) return;
+      const TcTerm tm = terms[c.t];
+      c.ad = adescs[tm.a_map];
+      c.k = tm.k;
+      c.a_x0 = tm.a_x0;
+      c.k0 = 0;
+    };
+    auto advance = [&](Cur& c) {
+      c.k0 += kBK;
+      if (c.k0 < c.k) return;
+      ++c.t;
+      first_term(c);
+    };
+    auto load = [&](const Cur& c, float* xr, float* xi) {
+      const int gr = c.m0 + row;
+      const bool rok = gr < c.ad.rows;
+      const float* pre = ain + c.ad.off + (int64_t)(rok ? gr : 0) * c.ad.ld;
+      const float* pim = pre + a_plane;
+      const int x0 = c.a_x0 + c.k0;
+      if (rok && x0 + 16 <= c.ad.cols) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 a = *(const float4*)(pre + x0 + 4 * q);
+          const float4 b = *(const float4*)(pim + x0 + 4 * q);
+          xr[4 * q] = a.x; xr[4 * q + 1] = a.y; xr[4 * q + 2] = a.z; xr[4 * q + 3] = a.w;
+          xi[4 * q] = b.x; xi[4 * q + 1] = b.y; xi[4 * q + 2] = b.z; xi[4 * q + 3] = b.w;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const bool in = rok && x0 + q < c.ad.cols;
+          xr[q] = in ? pre[x0 + q] : 0.f;
+          xi[q] = in ? pim[x0 + q] : 0.f;
+        }
+      }
+    };
+    Cur cur;
+    cur.ti = (int)blockIdx.x - (int)gridDim.x;  // first_term steps to this CTA's first tile
+    cur.t = cur.t1 = 0;
+    cur.valid = true;
+    first_term(cur);
+    float ar[16], ai[16], br[16], bi[16];
+    if (cur.valid) load(cur, ar, ai);
+    int it = 0;
+    while (cur.valid) {
+      Cur nxt = cur;
+      advance(nxt);
+      if (nxt.valid) load(nxt, br, bi);  // next k-step's row, in flight during this one
+      const int s = it % kStages;
+      const uint32_t ph = (uint32_t)((it / kStages) & 1);
+      int go = 1;
+      if (lane == 0) go = mbar_wait(&empty[s], ph ^ 1u, err, 5) ? 1 : 0;
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
+      uint8_t* sa = smem + s * kStageBytes + row * 64;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float4 h_r, l_r, h_i, l_i;
+        float* hr = &h_r.x; float* lr = &l_r.x; float* hi = &h_i.x; float* li = &l_i.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float a = ar[4 * q + e], b = ai[4 * q + e];
+          hr[e] = tf32_rna(a);
+          lr[e] = tf32_rna(a - hr[e]);
+          hi[e] = tf32_rna(b);
+          li[e] = tf32_rna(b - hi[e]);
+        }
+        const uint32_t off = ((uint32_t)q ^ sw) << 4;
+        *(float4*)(sa + 0 * kPlaneTileBytes + off) = h_r;
+        *(float4*)(sa + 1 * kPlaneTileBytes + off) = l_r;
+        *(float4*)(sa + 2 * kPlaneTileBytes + off) = h_i;
+        *(float4*)(sa + 3 * kPlaneTileBytes + off) = l_i;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[s])) : "memory");
+      ++it;
+      cur = nxt;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        ar[q] = br[q];
+        ai[q] = bi[q];
+      }
+    }
+  } else if (warp >= 2 && warp < 6) {
     // ---------------- epilogue: warps 2..5 ----------------
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = quad * 32 + lane;
@@ -322,12 +449,10 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
           if (j >= ntile) break;
           const int64_t o = task.out_off + (int64_t)gm * task.row_stride + (int64_t)(tile.n0 + j) * task.col_stride;
           if (MODE == 1) {
-            // stage-1 output: split into the four planes stage 2 reads
-            const float hr = tf32_rna(vr[i]), hi = tf32_rna(vi[i]);
-            out32[o] = hr;
-            out32[o + out32_plane] = tf32_rna(vr[i] - hr);
-            out32[o + 2 * out32_plane] = hi;
-            out32[o + 3 * out32_plane] = tf32_rna(vi[i] - hi);
+            // stage-1 output: the FP32 accumulator, re and im planes (the
+            // stage-2 converter warps split it into TF32 hi / lo)
+            out32[o] = vr[i];
+            out32[o + out32_plane] = vi[i];
           } else {
             out64[o] = (double)vr[i];
             out64[o + out64_plane] = (double)vi[i];
@@ -349,7 +474,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
 int smem_bytes() { return kSmemBytes; }
 
 int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double* out64, int64_t out64_plane,
-           int* d_err, cudaStream_t st) {
+           const float* ain, int64_t a_plane, int* d_err, cudaStream_t st) {
   if (p.tiles.empty()) return CMPS_OK;
   if (p.tiles.size() > 0x7fffffffull) return fail(CMPS_ERR_ARG, "too many tcgen05 tiles");
   int dev = 0, sms = 148;
@@ -363,16 +488,19 @@ int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double*
       CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
       cfg1 = true;
     }
-    tc_split_gemm<1><<<grid, kThreads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
-                                                          p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+    tc_split_gemm<1><<<grid, threads_of<1>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
+                                                                 p.d_bmaps, nullptr, nullptr, 0, out32, out32_plane,
+                                                                 out64, out64_plane, d_err);
   } else {
+    if (!ain || !p.d_adescs) return fail(CMPS_ERR_STATE, "tcgen05 mode 2: no A operand");
     static bool cfg2 = false;
     if (!cfg2) {
       CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
       cfg2 = true;
     }
-    tc_split_gemm<2><<<grid, kThreads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
-                                                          p.d_bmaps, out32, out32_plane, out64, out64_plane, d_err);
+    tc_split_gemm<2><<<grid, threads_of<2>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, nullptr,
+                                                                 p.d_bmaps, p.d_adescs, ain, a_plane, out32,
+                                                                 out32_plane, out64, out64_plane, d_err);
   }
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;

@@ -23,6 +23,12 @@ struct TcTask {
 struct TcTerm {
   int32_t a_map, b_map, a_x0, k;
 };
+// A operand read by the converter warps (mode 2): element (i, j) of the block
+// at off + i * ld + j in each of two FP32 planes (re, im); rows x cols.
+struct TcADesc {
+  int64_t off, ld;
+  int32_t rows, cols;
+};
 // b_rows: row count of the B boxes of this tile's task (its N rounded up to
 // 16, at most 128); the B tensor maps of that task are encoded with it.
 // kiters: 16-wide k-steps of the task's terms; nmma: the tile's N rounded up
@@ -38,6 +44,8 @@ struct TcPlan {
   std::vector<TcTerm> terms;
   std::vector<TcTile> tiles;
   std::vector<CUtensorMap> amaps, bmaps;
+  std::vector<TcADesc> adescs;  // mode 2: A blocks in two FP32 planes
+  TcADesc* d_adescs = nullptr;
   TcTask* d_tasks = nullptr;
   TcTerm* d_terms = nullptr;
   TcTile* d_tiles = nullptr;
@@ -48,10 +56,13 @@ struct TcPlan {
 };
 
 int smem_bytes();
-// mode 1: FP32 split output (four planes, plane stride out32_plane);
-// mode 2: FP64 planar output (re, im; plane stride out64_plane).
+// mode 1: A and B by TMA (four TF32 planes each); FP32 output in two planes
+//         (re, im; plane stride out32_plane), the raw accumulator.
+// mode 2: A read from two FP32 planes (ain, plane stride a_plane; blocks
+//         described by p.adescs) and split to TF32 hi/lo in shared memory;
+//         B by TMA; FP64 planar output (re, im; plane stride out64_plane).
 int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double* out64, int64_t out64_plane,
-           int* d_err, cudaStream_t st);
+           const float* ain, int64_t a_plane, int* d_err, cudaStream_t st);
 
 }  // namespace tc
 }  // namespace cmps
