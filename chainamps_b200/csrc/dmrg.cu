@@ -64,7 +64,14 @@ struct Dmrg {
   std::vector<QKey> bq;
   int64_t size = 0;
   std::unique_ptr<Heff> heff;
-  std::unique_ptr<SvdResult> svd;
+  std::shared_ptr<SvdResult> svd;  // factors of the current window (shared with lsvd / rsvd)
+  static std::shared_ptr<SvdResult> new_svd() {
+    return std::shared_ptr<SvdResult>(new SvdResult(), [](SvdResult* s) {
+      s->U.release();
+      s->Vd.release();
+      delete s;
+    });
+  }
   std::vector<double> lambda, prev_lambda;
   double tol = 1e-10;
   int restarts = 50, kdim = 24;
@@ -80,10 +87,6 @@ struct Dmrg {
   double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
 
   ~Dmrg() {
-    if (svd) {
-      svd->U.release();
-      svd->Vd.release();
-    }
     dL.data.release();
     dR.data.release();
     for (auto& kv : lblocks) kv.second.data.release();
@@ -94,10 +97,15 @@ struct Dmrg {
   bool keep_blocks = false;
   bool want_fidelity = true;  // CheckConvergence on growth steps
   std::map<int64_t, Env> lblocks, rblocks;
+  // the factors each kept block was built with: lsvd[k]'s U made lblocks[k]
+  // (the left MPS tensor of vertex k), rsvd[k]'s V^dagger made rblocks[k]
+  // (the right MPS tensor of the k-th vertex from the right end)
+  std::map<int64_t, std::shared_ptr<SvdResult>> lsvd, rsvd;
   int64_t nleft = 0;  // vertices left of the two-vertex window
 
   int dummy_blocks(Env& L, Env& R);
   int predict(Heff& next, bool* ok);
+  int finite_predict(Heff& next, int dir, bool* ok);
   // dir 0: iDMRG growth step (grow_two_vertex); +1 / -1: finite sweep step
   // to the right / left (move_{right,left}_two_vertex)
   int step(int dir, int64_t chi, double trunc, double* out);
@@ -253,6 +261,133 @@ int Dmrg::predict(Heff& next, bool* ok) {
   return status;
 }
 
+// MakeRFinitePrediction / MakeLFinitePrediction (DMRG_routines.cpp:709-716):
+// the start vector of a sweep step.
+//  moving right: theta'[(s2, a1), (s3, a3)] = sum_a2 (Lambda V^dagger)[a1, (s2, a2)] B[a2, (s3, a3)],
+//                B = the right MPS tensor of the vertex entering the window (rsvd);
+//  moving left:  theta'[(s0, a_), (s1, a1)] = sum_a0 A[(s0, a_), a0] (U Lambda)[(s1, a0), a1],
+//                A = the left MPS tensor of the vertex entering the window (lsvd).
+// One grouped FP64 GEMM from the sector blocks of the two factors into the new
+// theta blocks; a block whose sectors do not line up is left out (zero).
+int Dmrg::finite_predict(Heff& next, int dir, bool* ok) {
+  *ok = false;
+  if (!svd) return CMPS_OK;
+  const int64_t nright = size - nleft - 2;
+  auto& store_map = dir > 0 ? rsvd : lsvd;
+  auto it = store_map.find(dir > 0 ? nright + 1 : nleft + 1);
+  if (it == store_map.end() || !it->second) return CMPS_OK;
+  const SvdResult& C = *svd;         // this window's factors (before the move)
+  const SvdResult& O = *it->second;  // the stored tensor's factors
+  cudaStream_t st = ctx->stream;
+  const ThetaSpace& tc = C.th;
+  const ThetaSpace& to = O.th;
+  const ThetaSpace& tn = next.th;
+  const Rules& r = next.rules;
+  const int d = next.d;
+  // Lambda on the current factor: rows of V^dagger (right) or columns of U (left)
+  Planar S;
+  const Planar& src = dir > 0 ? C.Vd : C.U;
+  CMPS_TRY(S.alloc(std::max<int64_t>(1, src.len)));
+  int status = CMPS_OK;
+  for (int m = 0; m < (int)tc.mq.size() && status == CMPS_OK; ++m) {
+    const int64_t k = C.kept[m];
+    if (!k) continue;
+    std::vector<double> lam(k);
+    for (int64_t j = 0; j < k; ++j) lam[j] = lambda[C.gidx[m][j]];
+    double* dl = nullptr;
+    if (dmalloc(&dl, sizeof(double) * k) != cudaSuccess) {
+      status = fail(CMPS_ERR_NOMEM, "finite prediction: scale allocation failed");
+      break;
+    }
+    status = copy_wait(dl, lam.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
+    if (status == CMPS_OK) {
+      if (dir > 0)
+        k_scale_block<<<grid_n(k * tc.ncols[m]), 256, 0, st>>>(C.Vd.re() + C.voff[m], C.Vd.im() + C.voff[m], k,
+                                                              tc.ncols[m], dl, nullptr, S.re() + C.voff[m],
+                                                              S.im() + C.voff[m]);
+      else
+        k_scale_block<<<grid_n(tc.nrows[m] * k), 256, 0, st>>>(C.U.re() + C.uoff[m], C.U.im() + C.uoff[m],
+                                                              tc.nrows[m], k, nullptr, dl, S.re() + C.uoff[m],
+                                                              S.im() + C.uoff[m]);
+      if (cudaStreamSynchronize(st) != cudaSuccess) status = fail(CMPS_ERR_CUDA, "finite prediction: scaling failed");
+    }
+    dfree(dl);
+  }
+  GemmPlan p;
+  for (int mn = 0; mn < (int)tn.mq.size() && status == CMPS_OK; ++mn)
+    for (int a = 0; a < d; ++a) {
+      if (tn.rowoff[mn][a] < 0) continue;
+      for (int b = 0; b < d; ++b) {
+        if (tn.coloff[mn][b] < 0) continue;
+        GemmTask task{};
+        GemmTerm tm{};
+        task.c_off = tn.base[mn] + tn.rowoff[mn][a] * tn.ncols[mn] + tn.coloff[mn][b];
+        task.ldc = (int32_t)tn.ncols[mn];
+        if (dir > 0) {
+          // rows: new left bond sector q(mn) - q(a) = a current window block
+          const int mc = tc.find(r.sub(tn.mq[mn], next.sigq[a]));
+          if (mc < 0 || !C.kept[mc] || tc.coloff[mc][a] < 0) continue;
+          const QKey t2 = r.add(tc.mq[mc], C.sigq[a]);  // a2 sector = the stored factor's block
+          const int mo = to.find(t2);
+          const int s2 = C.a2.find(t2);
+          if (mo < 0 || s2 < 0 || O.kept[mo] != C.a2.sdim[s2] || to.coloff[mo][b] < 0) continue;
+          const int sr = next.L.a.find(tc.mq[mc]);
+          const int t3 = O.a2.find(r.add(t2, O.sigq[b]));
+          const int sc = next.R.a.find(r.add(tn.mq[mn], next.sigq[b]));
+          if (sr < 0 || t3 < 0 || sc < 0 || next.L.a.sdim[sr] != C.kept[mc] || next.R.a.sdim[sc] != O.a2.sdim[t3])
+            continue;
+          task.m = (int32_t)C.kept[mc];
+          task.n = (int32_t)O.a2.sdim[t3];
+          tm.a_off = C.voff[mc] + tc.coloff[mc][a];
+          tm.lda = (int32_t)tc.ncols[mc];
+          tm.k = (int32_t)O.kept[mo];
+          tm.b_off = O.voff[mo] + to.coloff[mo][b];
+          tm.ldb = (int32_t)to.ncols[mo];
+        } else {
+          // contraction over a0 of charge q(mn): the stored factor's block
+          const int mo = to.find(tn.mq[mn]);
+          if (mo < 0 || !O.kept[mo] || to.rowoff[mo][a] < 0) continue;
+          const int mc = tc.find(r.add(tn.mq[mn], next.sigq[b]));
+          if (mc < 0 || !C.kept[mc] || tc.rowoff[mc][b] < 0) continue;
+          const int s0 = C.a0.find(tn.mq[mn]);
+          if (s0 < 0 || C.a0.sdim[s0] != O.kept[mo]) continue;
+          const int sr = next.L.a.find(r.sub(tn.mq[mn], next.sigq[a]));
+          const int ro = O.a0.find(r.sub(tn.mq[mn], O.sigq[a]));
+          const int sc = next.R.a.find(tc.mq[mc]);
+          if (sr < 0 || ro < 0 || sc < 0 || next.L.a.sdim[sr] != O.a0.sdim[ro] || next.R.a.sdim[sc] != C.kept[mc])
+            continue;
+          task.m = (int32_t)O.a0.sdim[ro];
+          task.n = (int32_t)C.kept[mc];
+          tm.a_off = O.uoff[mo] + to.rowoff[mo][a] * O.kept[mo];
+          tm.lda = (int32_t)O.kept[mo];
+          tm.k = (int32_t)O.kept[mo];
+          tm.b_off = C.uoff[mc] + tc.rowoff[mc][b] * C.kept[mc];
+          tm.ldb = (int32_t)C.kept[mc];
+        }
+        task.t0 = (int32_t)p.terms.size();
+        p.terms.push_back(tm);
+        task.t1 = (int32_t)p.terms.size();
+        p.tasks.push_back(task);
+      }
+    }
+  if (status == CMPS_OK && !p.tasks.empty()) {
+    const Planar& A = dir > 0 ? S : O.U;
+    const Planar& B = dir > 0 ? O.Vd : S;
+    status = p.validate(false, false, A.len, B.len, tn.total, "finite prediction");
+    if (status == CMPS_OK) status = p.upload(64, 64, st);
+    if (status == CMPS_OK) {
+      cudaMemsetAsync(next.x.d, 0, sizeof(double) * 2 * tn.total, st);
+      status = launch_zgemm_fp64(p, false, false, A, B, next.x, st);
+    }
+    if (status == CMPS_OK && cudaStreamSynchronize(st) != cudaSuccess)
+      status = fail(CMPS_ERR_CUDA, "finite prediction GEMM failed");
+    if (status == CMPS_OK) *ok = true;
+  }
+  p.release();
+  S.release();
+  return status;
+}
+
 int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   cudaStream_t st = ctx->stream;
   if (dir != 0) {
@@ -286,6 +421,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     int rc = store(lblocks, nleft + 1, nl, st);
     nl.data.release();
     CMPS_TRY(rc);
+    lsvd[nleft + 1] = svd;
     nleft += 1;
     auto ir = rblocks.find(size - nleft - 2);
     if (ir == rblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: right block missing");
@@ -297,6 +433,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     int rc = store(rblocks, size - nleft - 1, nr, st);
     nr.data.release();
     CMPS_TRY(rc);
+    rsvd[size - nleft - 1] = svd;
     nleft -= 1;
     auto il = lblocks.find(nleft);
     if (il == lblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: left block missing");
@@ -328,6 +465,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (keep_blocks) {
       CMPS_TRY(store(lblocks, nleft, L, st));
       CMPS_TRY(store(rblocks, nleft, R, st));
+      if (svd) lsvd[nleft] = rsvd[nleft] = svd;  // the previous window's U and V^dagger made them
     }
   }
   cudaEventRecord(ev[4], st);
@@ -347,13 +485,10 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   const auto h_split = clock::now();
   bool have_guess = false;
   if (dir == 0) CMPS_TRY(predict(*next, &have_guess));
+  else CMPS_TRY(finite_predict(*next, dir, &have_guess));
   const auto h_pred = clock::now();
-  // the previous step's factors and H_eff are no longer needed
-  if (svd) {
-    svd->U.release();
-    svd->Vd.release();
-    svd.reset();
-  }
+  // the previous step's factors are released here unless a kept block needs them
+  svd.reset();
   heff = std::move(next);
   const auto h_rel = clock::now();
   cudaEventRecord(ev[1], st);
@@ -367,7 +502,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     CMPS_TRY(heff_adjoint(*heff, dW, have_dlr ? &dL : nullptr, have_dlr ? &dR : nullptr, &last_grad));
   const auto h_eig = clock::now();
   cudaEventRecord(ev[2], st);
-  svd.reset(new SvdResult());
+  svd = new_svd();
   // sweep steps next to an end keep every state up to chi (no weight cut),
   // as move_{right,left}_two_vertex do
   const int64_t nright_now = (dir == 0 ? size + 2 : size) - nleft - 2;

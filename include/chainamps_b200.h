@@ -244,8 +244,9 @@ int cmps_dmrg_values(const cmps_dmrg* d, double* values);
  * the window leaves is updated with this window's U or V^dagger, the new
  * window is solved and truncated (no weight cut next to an end), and row5 is
  * the reference's energies row (fidelity NaN).  The start vector of a sweep
- * step is the fixed pseudo-random one (the finite predictions,
- * MakeL/RFinitePrediction :709-716, are not built).  cmps_dmrg_position
+ * step is MakeRFinitePrediction / MakeLFinitePrediction (:709-716): this
+ * window's Lambda V^dagger (U Lambda) times the stored right (left) MPS
+ * tensor of the vertex entering the window.  cmps_dmrg_position
  * returns the number of vertices left of the window and the chain length. */
 int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep);
 int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on);
