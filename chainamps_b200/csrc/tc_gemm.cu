@@ -32,6 +32,7 @@
 #include <algorithm>
 
 #include "tc_gemm.h"
+#include "tf32_round.cuh"
 
 namespace cmps {
 namespace tc {
@@ -141,11 +142,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
 }
 
 template <int MODE>
