@@ -115,6 +115,11 @@ _SIGS = {
     "cmps_heff_adjoint": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc), C.c_void_p, C.c_void_p, c_dblp]),
     "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
     "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
+    "cmps_heff_sector_table": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_dblp]),
+    "cmps_heff_set_owned": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cmps_heff_theta_from_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cmps_heff_theta_to_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -261,6 +266,34 @@ class TwoVertexComponents:
         """Device pointers (ints) to n complex doubles each."""
         _check(lib.cmps_heff_apply_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
                                           C.c_void_p(stream) if stream else None))
+
+    def sector_table(self):
+        """theta layout: (offsets[n_sectors + 1], flops[n_sectors]); output
+        sector m occupies elements offsets[m]:offsets[m + 1] of each plane."""
+        n = C.c_int64(0)
+        _check(lib.cmps_heff_sector_table(self.h, C.byref(n), None, None))
+        off = np.zeros(n.value + 1, np.int64)
+        fl = np.zeros(max(1, n.value), np.float64)
+        _check(lib.cmps_heff_sector_table(self.h, C.byref(n), _p(off, C.c_int64), _p(fl, C.c_double)))
+        return off, fl[:n.value]
+
+    def set_owned(self, owned):
+        """Compute only the output sectors with owned[m] true (sharded matvec)."""
+        mask = np.ascontiguousarray(np.asarray(owned, bool).astype(np.uint8))
+        _check(lib.cmps_heff_set_owned(self.h, _p(mask, C.c_uint8)))
+
+    def multiply_theta_device(self, d_in, d_out, stream=None):
+        """theta-layout matvec on device pointers (2 * total doubles, planar)."""
+        _check(lib.cmps_heff_apply_theta_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
+                                                C.c_void_p(stream) if stream else None))
+
+    def theta_from_arpack_device(self, d_arpack, d_theta, stream=None):
+        _check(lib.cmps_heff_theta_from_arpack(self.h, C.c_void_p(d_arpack), C.c_void_p(d_theta),
+                                               C.c_void_p(stream) if stream else None))
+
+    def theta_to_arpack_device(self, d_theta, d_arpack, stream=None):
+        _check(lib.cmps_heff_theta_to_arpack(self.h, C.c_void_p(d_theta), C.c_void_p(d_arpack),
+                                             C.c_void_p(stream) if stream else None))
 
     def time_stages(self, d_in, d_out, stream=None, reps=3):
         """Average ms of [gather, stage 1, stage 2, scatter] (CUDA events)."""

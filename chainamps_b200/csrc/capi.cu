@@ -212,10 +212,81 @@ int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void
   return h->impl->apply_device(d_in, d_out, st);
 }
 
+int cmps_heff_sector_table(const cmps_heff* h, int64_t* n_sectors, int64_t* offsets, double* flops) {
+  if (!h || !h->impl || !n_sectors) return fail(CMPS_ERR_ARG, "null argument");
+  const Heff& H = *h->impl;
+  const int64_t nm = (int64_t)H.th.mq.size();
+  if (offsets || flops) {
+    if (*n_sectors != nm) return fail(CMPS_ERR_ARG, "sector table: *n_sectors differs from the sector count");
+    if (offsets) {
+      for (int64_t m = 0; m < nm; ++m) offsets[m] = H.th.base[m];
+      offsets[nm] = H.th.total;
+    }
+    if (flops)
+      for (int64_t m = 0; m < nm; ++m) flops[m] = (int64_t)H.sector_flops.size() == nm ? H.sector_flops[m] : 0.0;
+  }
+  *n_sectors = nm;
+  return CMPS_OK;
+}
+
+int cmps_heff_set_owned(cmps_heff* h, const uint8_t* owned) {
+  if (!h || !h->impl || !owned) return fail(CMPS_ERR_ARG, "null argument");
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->set_owned(owned);
+}
+
+int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out, void* stream) {
+  if (!h || !h->impl || !d_in || !d_out) return fail(CMPS_ERR_ARG, "null argument");
+  if (d_in == d_out) return fail(CMPS_ERR_ARG, "theta-layout apply: in and out must be different arrays");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
+  // views of the caller's arrays (planar: re plane, then im plane)
+  Planar in, out;
+  in.d = const_cast<double*>(d_in);
+  in.len = H.th.total;
+  out.d = d_out;
+  out.len = H.th.total;
+  int rc;
+  if (H.precision == CMPS_SPLIT_TF32) {
+    rc = apply_split_stage(H, 1, in, out, st);
+    if (rc == CMPS_OK) rc = apply_split_stage(H, 2, in, out, st);
+  } else {
+    rc = H.apply_theta_fp64(in, out, st);
+  }
+  in.d = out.d = nullptr;
+  return rc;
+}
+
+int cmps_heff_theta_from_arpack(cmps_heff* h, const double* d_arpack, double* d_theta, void* stream) {
+  if (!h || !h->impl || !d_arpack || !d_theta) return fail(CMPS_ERR_ARG, "null argument");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  Planar out;
+  out.d = d_theta;
+  out.len = H.th.total;
+  const int rc = H.pack(d_arpack, out, stream ? (cudaStream_t)stream : H.ctx->stream);
+  out.d = nullptr;
+  return rc;
+}
+
+int cmps_heff_theta_to_arpack(cmps_heff* h, const double* d_theta, double* d_arpack, void* stream) {
+  if (!h || !h->impl || !d_arpack || !d_theta) return fail(CMPS_ERR_ARG, "null argument");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  Planar in;
+  in.d = const_cast<double*>(d_theta);
+  in.len = H.th.total;
+  const int rc = H.unpack(in, d_arpack, stream ? (cudaStream_t)stream : H.ctx->stream);
+  in.d = nullptr;
+  return rc;
+}
+
 int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void* stream, int reps, double* ms) {
   if (!h || !h->impl || !d_in || !d_out || !ms || reps < 1) return fail(CMPS_ERR_ARG, "bad argument");
   Heff& H = *h->impl;
   CMPS_TRY(use_device(H.ctx));
+  if (!H.all_owned()) return fail(CMPS_ERR_STATE, "stage timing: the matvec is sharded");
   cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
   cudaEvent_t ev[5];
   for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));

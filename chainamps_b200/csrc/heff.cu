@@ -639,105 +639,8 @@ int Heff::finish() {
   CMPS_TRY(upload_vec(rp_blocks, &d_rp_blocks, ctx->stream));
   CMPS_TRY(upload_vec(rp_terms, &d_rp_terms, ctx->stream));
 
-  // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
-  std::set<int> b1s;
-  for (auto& kv2 : lp_off) b1s.insert(kv2.first[0]);
-  std::set<int> b1r;
-  for (auto& kv2 : rp_off) b1r.insert(kv2.first[0]);
-  t_base.assign((size_t)D * nm, -1);
-  stage1 = GemmPlan();
-  int64_t t_total = 0;
-  flops_executed = 0.0;
-  for (int b1 : b1s) {
-    if (!b1r.count(b1)) continue;
-    for (int m = 0; m < nm; ++m) {
-      int mp = th.find(r.add(th.mq[m], bq[b1]));
-      if (mp < 0) continue;
-      std::vector<GemmTask> tasks;
-      std::vector<GemmTerm> terms;
-      int64_t ldc = th.ncols[m];
-      for (int s1p = 0; s1p < d; ++s1p) {
-        if (th.rowoff[mp][s1p] < 0) continue;
-        int sp = A0.find(r.sub(th.mq[mp], sigq[s1p]));
-        GemmTask task{};
-        task.c_off = th.rowoff[mp][s1p] * ldc;  // relative to T block base, fixed below
-        task.m = (int32_t)A0.sdim[sp];
-        task.n = (int32_t)th.ncols[m];
-        task.ldc = (int32_t)ldc;
-        task.t0 = (int32_t)terms.size();
-        for (int s1 = 0; s1 < d; ++s1) {
-          if (th.rowoff[m][s1] < 0) continue;
-          int s = A0.find(r.sub(th.mq[m], sigq[s1]));
-          auto it = lp_off.find({b1, s1p, s1, s});
-          if (it == lp_off.end()) continue;
-          GemmTerm tm{};
-          tm.a_off = it->second;
-          tm.lda = (int32_t)A0.sdim[s];
-          tm.k = (int32_t)A0.sdim[s];
-          tm.b_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m];
-          tm.ldb = (int32_t)th.ncols[m];
-          terms.push_back(tm);
-        }
-        task.t1 = (int32_t)terms.size();
-        tasks.push_back(task);
-      }
-      if (terms.empty()) continue;
-      int64_t tb = t_total;
-      t_base[(size_t)b1 * nm + m] = tb;
-      t_total += th.nrows[mp] * th.ncols[m];
-      int32_t term_base = (int32_t)stage1.terms.size();
-      for (auto& tm : terms) {
-        stage1.terms.push_back(tm);
-      }
-      for (auto& task : tasks) {
-        task.c_off += tb;
-        task.t0 += term_base;
-        task.t1 += term_base;
-        for (int q = task.t0; q < task.t1; ++q)
-          flops_executed += 8.0 * task.m * (double)task.n * stage1.terms[q].k;
-        stage1.tasks.push_back(task);
-      }
-    }
-  }
-  CMPS_TRY(T.alloc(t_total));
-  // ---- stage 2: Theta'_m' = sum_b1 T^{b1}_{m'-q(b1)} . RightPart^{b1} ----
-  stage2 = GemmPlan();
-  for (int mp = 0; mp < nm; ++mp) {
-    for (int s2p = 0; s2p < d; ++s2p) {
-      if (th.coloff[mp][s2p] < 0) continue;
-      int tp = A2.find(r.add(th.mq[mp], sigq[s2p]));
-      GemmTask task{};
-      task.c_off = th.base[mp] + th.coloff[mp][s2p];
-      task.m = (int32_t)th.nrows[mp];
-      task.n = (int32_t)A2.sdim[tp];
-      task.ldc = (int32_t)th.ncols[mp];
-      task.t0 = (int32_t)stage2.terms.size();
-      for (int b1 = 0; b1 < D; ++b1) {
-        int m = th.find(r.sub(th.mq[mp], bq[b1]));
-        if (m < 0) continue;
-        int64_t tb = t_base[(size_t)b1 * nm + m];
-        if (tb < 0) continue;
-        for (int s2 = 0; s2 < d; ++s2) {
-          if (th.coloff[m][s2] < 0) continue;
-          int t = A2.find(r.add(th.mq[m], sigq[s2]));
-          auto it = rp_off.find({b1, s2, s2p, t});
-          if (it == rp_off.end()) continue;
-          GemmTerm tm{};
-          tm.a_off = tb + th.coloff[m][s2];
-          tm.lda = (int32_t)th.ncols[m];
-          tm.k = (int32_t)A2.sdim[t];
-          tm.b_off = it->second;
-          tm.ldb = (int32_t)A2.sdim[tp];
-          stage2.terms.push_back(tm);
-          flops_executed += 8.0 * task.m * (double)task.n * tm.k;
-        }
-      }
-      task.t1 = (int32_t)stage2.terms.size();
-      stage2.tasks.push_back(task);
-    }
-  }
-  CMPS_TRY(stage1.validate(false, false, lp_total, th.total, t_total, "stage 1"));
-  CMPS_TRY(stage2.validate(false, false, t_total, rp_total, th.total, "stage 2"));
+  owned.assign(nm, 1);
+  CMPS_TRY(build_plans());
   for (const AxpyBlock& b : lp_blocks)
     for (int q = b.t0; q < b.t1; ++q)
       if (b.dst_off + b.len > lp_total || lp_terms[q].src_off + b.len > L.data.len)
@@ -756,8 +659,6 @@ int Heff::finish() {
       if (rt < 0 || rt >= th.nrows[m]) return fail(CMPS_ERR_STATE, "pack map row outside the sector blocks");
     }
   CMPS_TRY(build_pack(ctx->stream));
-  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
-  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
   cudaStream_t st = ctx->stream;
   CMPS_TRY(launch_block_axpy(d_lp_blocks, (int)lp_blocks.size(), d_lp_terms, L.data, LP, st));
   CMPS_TRY(launch_block_axpy(d_rp_blocks, (int)rp_blocks.size(), d_rp_terms, R.data, RP, st));
@@ -812,6 +713,143 @@ int Heff::finish() {
   return CMPS_OK;
 }
 
+// The two grouped-GEMM plans of the matvec and the intermediate T, for the
+// output sectors marked in `owned` (all of them unless the matvec is
+// sharded): stage-2 tasks of owned output sectors only, and stage-1 tasks
+// only for the blocks T^{b1}_m those read (m + q(b1) owned).
+int Heff::build_plans() {
+  const Rules& r = rules;
+  const Bond& A0 = L.a;
+  const Bond& A2 = R.a;
+  const int nm = (int)th.mq.size();
+  if ((int)owned.size() != nm) return fail(CMPS_ERR_STATE, "owned-sector mask size");
+  stage1.release();
+  stage2.release();
+  T.release();
+  // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
+  std::set<int> b1s;
+  for (auto& kv2 : lp_off) b1s.insert(kv2.first[0]);
+  std::set<int> b1r;
+  for (auto& kv2 : rp_off) b1r.insert(kv2.first[0]);
+  t_base.assign((size_t)D * nm, -1);
+  stage1 = GemmPlan();
+  int64_t t_total = 0;
+  flops_executed = 0.0;
+  std::vector<double> fl(nm, 0.0);  // executed flops per output sector
+  for (int b1 : b1s) {
+    if (!b1r.count(b1)) continue;
+    for (int m = 0; m < nm; ++m) {
+      int mp = th.find(r.add(th.mq[m], bq[b1]));
+      if (mp < 0 || !owned[mp]) continue;  // T^{b1}_m only feeds output sector mp
+      std::vector<GemmTask> tasks;
+      std::vector<GemmTerm> terms;
+      int64_t ldc = th.ncols[m];
+      for (int s1p = 0; s1p < d; ++s1p) {
+        if (th.rowoff[mp][s1p] < 0) continue;
+        int sp = A0.find(r.sub(th.mq[mp], sigq[s1p]));
+        GemmTask task{};
+        task.c_off = th.rowoff[mp][s1p] * ldc;  // relative to T block base, fixed below
+        task.m = (int32_t)A0.sdim[sp];
+        task.n = (int32_t)th.ncols[m];
+        task.ldc = (int32_t)ldc;
+        task.t0 = (int32_t)terms.size();
+        for (int s1 = 0; s1 < d; ++s1) {
+          if (th.rowoff[m][s1] < 0) continue;
+          int s = A0.find(r.sub(th.mq[m], sigq[s1]));
+          auto it = lp_off.find({b1, s1p, s1, s});
+          if (it == lp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = it->second;
+          tm.lda = (int32_t)A0.sdim[s];
+          tm.k = (int32_t)A0.sdim[s];
+          tm.b_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m];
+          tm.ldb = (int32_t)th.ncols[m];
+          terms.push_back(tm);
+        }
+        task.t1 = (int32_t)terms.size();
+        tasks.push_back(task);
+      }
+      if (terms.empty()) continue;
+      int64_t tb = t_total;
+      t_base[(size_t)b1 * nm + m] = tb;
+      t_total += th.nrows[mp] * th.ncols[m];
+      int32_t term_base = (int32_t)stage1.terms.size();
+      for (auto& tm : terms) {
+        stage1.terms.push_back(tm);
+      }
+      for (auto& task : tasks) {
+        task.c_off += tb;
+        task.t0 += term_base;
+        task.t1 += term_base;
+        for (int q = task.t0; q < task.t1; ++q) {
+          flops_executed += 8.0 * task.m * (double)task.n * stage1.terms[q].k;
+          fl[mp] += 8.0 * task.m * (double)task.n * stage1.terms[q].k;
+        }
+        stage1.tasks.push_back(task);
+      }
+    }
+  }
+  CMPS_TRY(T.alloc(t_total));
+  // ---- stage 2: Theta'_m' = sum_b1 T^{b1}_{m'-q(b1)} . RightPart^{b1} ----
+  stage2 = GemmPlan();
+  for (int mp = 0; mp < nm; ++mp) {
+    if (!owned[mp]) continue;
+    for (int s2p = 0; s2p < d; ++s2p) {
+      if (th.coloff[mp][s2p] < 0) continue;
+      int tp = A2.find(r.add(th.mq[mp], sigq[s2p]));
+      GemmTask task{};
+      task.c_off = th.base[mp] + th.coloff[mp][s2p];
+      task.m = (int32_t)th.nrows[mp];
+      task.n = (int32_t)A2.sdim[tp];
+      task.ldc = (int32_t)th.ncols[mp];
+      task.t0 = (int32_t)stage2.terms.size();
+      for (int b1 = 0; b1 < D; ++b1) {
+        int m = th.find(r.sub(th.mq[mp], bq[b1]));
+        if (m < 0) continue;
+        int64_t tb = t_base[(size_t)b1 * nm + m];
+        if (tb < 0) continue;
+        for (int s2 = 0; s2 < d; ++s2) {
+          if (th.coloff[m][s2] < 0) continue;
+          int t = A2.find(r.add(th.mq[m], sigq[s2]));
+          auto it = rp_off.find({b1, s2, s2p, t});
+          if (it == rp_off.end()) continue;
+          GemmTerm tm{};
+          tm.a_off = tb + th.coloff[m][s2];
+          tm.lda = (int32_t)th.ncols[m];
+          tm.k = (int32_t)A2.sdim[t];
+          tm.b_off = it->second;
+          tm.ldb = (int32_t)A2.sdim[tp];
+          stage2.terms.push_back(tm);
+          flops_executed += 8.0 * task.m * (double)task.n * tm.k;
+          fl[mp] += 8.0 * task.m * (double)task.n * tm.k;
+        }
+      }
+      task.t1 = (int32_t)stage2.terms.size();
+      stage2.tasks.push_back(task);
+    }
+  }
+  CMPS_TRY(stage1.validate(false, false, LP.len, th.total, t_total, "stage 1"));
+  CMPS_TRY(stage2.validate(false, false, t_total, RP.len, th.total, "stage 2"));
+  if (all_owned()) sector_flops = fl;
+  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
+  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
+  return CMPS_OK;
+}
+
+int Heff::set_owned(const uint8_t* mask) {
+  const int nm = (int)th.mq.size();
+  CMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int m = 0; m < nm; ++m) owned[m] = mask[m] ? 1 : 0;
+  release_split(this);
+  CMPS_TRY(build_plans());
+  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(prepare_precision(this, CMPS_SPLIT_TF32));
+  return CMPS_OK;
+}
+
+bool Heff::all_owned() const {
+  return std::all_of(owned.begin(), owned.end(), [](uint8_t o) { return o != 0; });
+}
+
 int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
   if (precision == CMPS_SPLIT_TF32) return apply_split_stage(*this, which, in, out, st);
   if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
@@ -832,6 +870,7 @@ int Heff::apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
+  if (!all_owned()) return fail(CMPS_ERR_STATE, "matvec is sharded: use the theta-layout entry point");
   CMPS_TRY(pack(din, x, st));
   if (precision == CMPS_SPLIT_TF32) {
     CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
@@ -966,6 +1005,7 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   cudaStream_t st = ctx->stream;
   const int64_t n = th.total;
   if (n == 0) return fail(CMPS_ERR_STATE, "empty effective Hamiltonian");
+  if (!all_owned()) return fail(CMPS_ERR_STATE, "matvec is sharded: the single-GPU eigensolver needs every sector");
   if (kdim < 2) kdim = 2;
   if (kdim > 96) kdim = 96;
   if ((int64_t)kdim > n) kdim = (int)n;

@@ -100,6 +100,15 @@ struct Heff {
   std::vector<int64_t> t_base;   // [b1 * nm + m] -> offset into T, -1 if absent
   Planar T;                      // stage-1 intermediate
   GemmPlan stage1, stage2;
+  // Output sectors this matvec computes (1 = owned).  All of them, unless the
+  // matvec is sharded across GPUs by output sector; then the output blocks
+  // of the other sectors are left unwritten and only the theta-layout entry
+  // points apply.  sector_flops: executed flops per output sector.
+  std::vector<uint8_t> owned;
+  std::vector<double> sector_flops;
+  int build_plans();
+  int set_owned(const uint8_t* mask);
+  bool all_owned() const;
   double flops_canonical = 0.0, flops_executed = 0.0;
   int precision = CMPS_FP64;
   SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)

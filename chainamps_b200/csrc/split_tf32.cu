@@ -446,7 +446,7 @@ static int build_split(Heff& H) {
   }
   for (int mp = 0; mp < nm; ++mp)
     for (int s2p = 0; s2p < d; ++s2p) {
-      if (th.coloff[mp][s2p] < 0) continue;
+      if (th.coloff[mp][s2p] < 0 || !H.owned[mp]) continue;  // output sectors of this shard only
       int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
       tc::TcTask task{};
       task.out_off = th.base[mp] + th.coloff[mp][s2p];

@@ -128,6 +128,35 @@ int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
  * first call before any stream capture.  All calls share the array: calls
  * that overlap on the GPU race.  Nothing in it needs to start at zero. */
 int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, double* d_out, void* stream);
+/* Sharding the matvec by output sector (no reference counterpart: the
+ * reference matvec runs on one host).  In the theta layout a vector is
+ * planar -- `total` real parts, then `total` imaginary parts -- and output
+ * sector m of H_eff occupies elements [offsets[m], offsets[m+1]) of each
+ * plane.  Each GPU of a sharded run holds the same handle (the environments
+ * and the MPO are replicated), computes the output sectors it owns from the
+ * whole input vector, and exchanges its slice with the others (an
+ * all-gather per matvec, done by the caller).
+ *
+ * cmps_heff_sector_table: call with offsets = flops = NULL to read the
+ * sector count into *n_sectors, then with arrays of *n_sectors + 1 offsets
+ * and *n_sectors flops (the executed flops of the full FP64 matvec that
+ * produce output sector m, the cost model for balancing the shards). */
+int cmps_heff_sector_table(const cmps_heff* h, int64_t* n_sectors, int64_t* offsets, double* flops);
+/* Restrict the matvec to the output sectors with owned[m] != 0 (n_sectors
+ * bytes): the GEMM plans keep only the tasks that produce them, and the
+ * other output blocks are left unwritten.  A handle that does not own every
+ * sector accepts only cmps_heff_apply_theta_device (the ARPACK-order apply,
+ * the eigensolver, the adjoint and the stage timing return CMPS_ERR_STATE);
+ * owning every sector again restores them. */
+int cmps_heff_set_owned(cmps_heff* h, const uint8_t* owned);
+/* theta-layout matvec on DEVICE arrays, stream-ordered: d_in holds the whole
+ * input vector (2 * total doubles, planar), d_out receives the owned output
+ * sectors (same layout; d_out != d_in). */
+int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out, void* stream);
+/* ARPACK order (n_allowed interleaved complex) <-> theta layout, on DEVICE
+ * arrays.  theta_to_arpack reads every sector of its input. */
+int cmps_heff_theta_from_arpack(cmps_heff* h, const double* d_arpack, double* d_theta, void* stream);
+int cmps_heff_theta_to_arpack(cmps_heff* h, const double* d_theta, double* d_arpack, void* stream);
 /* Stage timing for roofline accounting: runs `reps` device applies on
  * `stream` (cudaStream_t or NULL) and returns the average duration in ms of
  * each launch, measured with CUDA events on that stream:
