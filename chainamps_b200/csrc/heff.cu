@@ -996,7 +996,8 @@ static void tridiag_lowest(int k, const double* a, const double* b, double* lam,
 // Rayleigh quotient alpha_0 and the true residual beta_0 = |H x - alpha_0 x|;
 // the run ends there once beta_0 <= tol |alpha_0|, with energy alpha_0.  The
 // remaining steps of a cycle use the split operator and stop once the Ritz
-// estimate has dropped by a factor eta below beta_0.  A cycle therefore
+// estimate has dropped by the cycle's factor eta_c below beta_0 (adapted
+// from cycle to cycle, as described where it is declared).  A cycle therefore
 // contracts the error of x by about max(eta, |dH| / gap) at the cost of one
 // FP64 matvec, as in mixed-precision iterative refinement; if two cycles in a
 // row fail to halve beta_0, the remaining cycles run in FP64.
@@ -1055,7 +1056,14 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   if (mixed) CMPS_TRY(split_reset_error(*this, st));
   bool all_fp64 = !mixed;
   const int max_cycles = std::max(1, max_restarts) * (mixed ? 4 : 1);
-  double eta = 1e-3;                    // per-cycle reduction asked of the split steps
+  // Per-cycle contraction asked of the split steps.  A cycle's FP64 residual
+  // shows what the previous cycle's split steps achieved: if they reached
+  // their request, the next request is 30x stronger; if not, they met the
+  // floor |dH|/gap of the split operator (or the Krylov cap), and the next
+  // request is what they achieved.  No cycle asks for more than the
+  // tolerance still needs (with a margin of 10).
+  double eta = 1e-3;
+  double eta_c = eta, prev_eta_c = eta;
   double prev_beta0 = HUGE_VAL;
   int stalls = 0, nmv = 0;
   double lam = 0.0;
@@ -1125,7 +1133,19 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
           lam = a;
           break;
         }
-      } else if (exhausted || resid <= eta * beta0) {
+        if (prev_beta0 < HUGE_VAL) {
+          const double got = b / prev_beta0;
+          if (got > 0.5) {
+            if (++stalls >= 2) all_fp64 = true;
+          } else {
+            stalls = 0;
+          }
+          eta = got <= 2.0 * prev_eta_c ? std::max(1e-10, prev_eta_c * 0.03) : std::min(0.1, got);
+        }
+        eta_c = std::min(0.5, std::max(eta, 0.1 * tol * std::max(1.0, std::fabs(a)) / b));
+        prev_beta0 = b;
+        prev_eta_c = eta_c;
+      } else if (exhausted || resid <= eta_c * beta0) {
         break;
       }
     }
@@ -1135,20 +1155,6 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
     CMPS_TRY(ops.combine(kv.d, kv.d + n, ldv, k, ycoef.data(), x.re(), x.im(), st));
     CMPS_TRY(ops.mdot_dev(nullptr, nullptr, 0, 0, x.re(), x.im(), nrm, st));
     CMPS_TRY(ops.scale_dev(x.re(), x.im(), nrm, true, x.re(), x.im(), st));
-    if (!all_fp64) {
-      // the split steps cannot contract x by more than about |dH| / gap a cycle:
-      // ask no more of them than the last cycle delivered
-      if (prev_beta0 < HUGE_VAL && beta0 >= 0.0) {
-        const double got = beta0 / prev_beta0;
-        eta = std::min(0.1, std::max(1e-4, got));
-        if (got > 0.5) {
-          if (++stalls >= 2) all_fp64 = true;
-        } else {
-          stalls = 0;
-        }
-      }
-      prev_beta0 = beta0;
-    }
   }
   CMPS_CUDA(cudaEventRecord(ev[3], st));
   // HED post-processing (DMRG_routines.cpp:870-889)
