@@ -14,6 +14,7 @@ struct cmps_context {
   cudaStream_t stream = nullptr;
   void* solver = nullptr;  // cusolverDnHandle_t, created on first SVD
   void* blas = nullptr;    // cublasHandle_t, created on first SVD (Gram matrices of big sectors)
+  void* svd_pool = nullptr;  // worker streams and handles of the block SVD, created on first use
 };
 
 namespace cmps {

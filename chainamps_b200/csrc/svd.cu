@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <set>
 
 #include "heff.h"
@@ -30,7 +31,48 @@ namespace cmps {
 
 static const double kEps = 2.220446049250313e-16;
 
+// Worker streams and handles for factoring the SVD's sectors concurrently:
+// cuSOLVER's dense eigensolver runs one sector far below the GPU's capacity,
+// so independent sectors run side by side, one host thread per worker.
+struct SvdWorker {
+  cudaStream_t st = nullptr;
+  cusolverDnHandle_t sol = nullptr;
+  cublasHandle_t blas = nullptr;
+};
+struct SvdPool {
+  std::vector<SvdWorker> w;
+};
+constexpr int kSvdWorkers = 4;
+
+static int get_pool(cmps_context* ctx, SvdPool** out) {
+  if (!ctx->svd_pool) {
+    auto* p = new SvdPool();
+    ctx->svd_pool = p;
+    p->w.resize(kSvdWorkers);
+    for (SvdWorker& w : p->w) {
+      if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(CMPS_ERR_CUDA, "SVD worker stream creation failed");
+      if (cusolverDnCreate(&w.sol) != CUSOLVER_STATUS_SUCCESS) return fail(CMPS_ERR_CUDA, "cusolverDnCreate failed");
+      if (cublasCreate(&w.blas) != CUBLAS_STATUS_SUCCESS) return fail(CMPS_ERR_CUDA, "cublasCreate failed");
+      cusolverDnSetStream(w.sol, w.st);
+      cublasSetStream(w.blas, w.st);
+    }
+  }
+  *out = (SvdPool*)ctx->svd_pool;
+  return CMPS_OK;
+}
+
 void release_solver(cmps_context* ctx) {
+  if (ctx && ctx->svd_pool) {
+    auto* p = (SvdPool*)ctx->svd_pool;
+    for (SvdWorker& w : p->w) {
+      if (w.sol) cusolverDnDestroy(w.sol);
+      if (w.blas) cublasDestroy(w.blas);
+      if (w.st) cudaStreamDestroy(w.st);
+    }
+    delete p;
+    ctx->svd_pool = nullptr;
+  }
   if (ctx && ctx->solver) {
     cusolverDnDestroy((cusolverDnHandle_t)ctx->solver);
     ctx->solver = nullptr;
@@ -285,7 +327,33 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     // accepted below when the bond-dimension cap, not the weight cut, decides
     // the kept count and every kept value is far above that floor.
     const int64_t kEigMin = 192;
-    auto factor = [&](int m, bool exact) -> int {
+    // Streams, handles and workspaces of one factoring thread.  Buffers with
+    // capacity 0 are allocated per sector (the sequential path); the
+    // concurrent workers get them sized up front, so that no allocation (and
+    // no device-wide synchronisation of a free) happens while they run.
+    struct FW {
+      cudaStream_t st;
+      cusolverDnHandle_t sol;
+      cublasHandle_t blas;
+      gesvdjInfo_t params;
+      double2* dA;
+      double* dS;
+      int* dinfo;
+      double2* G = nullptr;
+      size_t Gcap = 0;
+      double* W = nullptr;
+      size_t Wcap = 0;
+      cuDoubleComplex* work = nullptr;
+      size_t workcap = 0;
+    };
+    auto factor = [&](int m, bool exact, FW& fw) -> int {
+      const cudaStream_t st = fw.st;
+      const cusolverDnHandle_t sol = fw.sol;
+      const cublasHandle_t blas = fw.blas;
+      const gesvdjInfo_t params = fw.params;
+      double2* const dA = fw.dA;
+      double* const dS = fw.dS;
+      int* const dinfo = fw.dinfo;
       Blk& b = blk[m];
       const int64_t C = th.ncols[m];
       const double* bre = H.theta.re() + th.base[m];
@@ -301,8 +369,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
                                          (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr, (cuDoubleComplex*)b.dV,
                                          (int)nc, &lwork, params) != CUSOLVER_STATUS_SUCCESS)
           return fail(CMPS_ERR_SOLVER, "gesvdj buffer query failed");
-        cuDoubleComplex* work = nullptr;
-        if (dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+        cuDoubleComplex* work = fw.work;
+        const bool own = (size_t)lwork > fw.workcap;
+        if (own && dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
           return fail(CMPS_ERR_NOMEM, "SVD work allocation failed");
         cusolverStatus_t cs = cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                                 (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)b.dU, (int)nr,
@@ -311,7 +380,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * mn, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t ce = cudaStreamSynchronize(st);
-        dfree(work);
+        if (own) dfree(work);
         if (cs != CUSOLVER_STATUS_SUCCESS || ce != cudaSuccess) return fail(CMPS_ERR_SOLVER, "gesvdj failed");
         if (info < 0) return fail(CMPS_ERR_SOLVER, "gesvdj: invalid argument");
         return CMPS_OK;  // info > 0: not converged to tolerance within max sweeps; values still usable
@@ -319,11 +388,12 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       b.eig = true;
       const bool left = nr <= nc;  // eigenvectors of A A^H give U; of A^H A give V
       const int p = (int)(left ? nr : nc);
-      double2* G = nullptr;   // Gram matrix, then its eigenvectors
-      double* W = nullptr;
+      const bool ownG = (size_t)p * p > fw.Gcap || (size_t)p > fw.Wcap;
+      double2* G = ownG ? nullptr : fw.G;   // Gram matrix, then its eigenvectors
+      double* W = ownG ? nullptr : fw.W;
       int lwork = 0;
-      if (dmalloc(&G, sizeof(double2) * (size_t)p * p) != cudaSuccess ||
-          dmalloc(&W, sizeof(double) * p) != cudaSuccess) {
+      if (ownG && (dmalloc(&G, sizeof(double2) * (size_t)p * p) != cudaSuccess ||
+                   dmalloc(&W, sizeof(double) * p) != cudaSuccess)) {
         if (G) dfree(G);
         return fail(CMPS_ERR_NOMEM, "Gram matrix allocation failed");
       }
@@ -341,7 +411,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (rc == CMPS_OK && cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
                                                        (cuDoubleComplex*)G, p, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
         rc = fail(CMPS_ERR_SOLVER, "zheevd buffer query failed");
-      if (rc == CMPS_OK && dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
+      const bool ownW = (size_t)lwork > fw.workcap;
+      if (!ownW) work = fw.work;
+      if (rc == CMPS_OK && ownW && dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lwork)) != cudaSuccess)
         rc = fail(CMPS_ERR_NOMEM, "zheevd work allocation failed");
       if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, p,
                                             (cuDoubleComplex*)G, p, W, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
@@ -369,13 +441,139 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         k_scale_cols_inv<<<grid_of((left ? nc : nr) * (int64_t)p), 256, 0, st>>>(O, left ? nc : nr, p, dS);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(CMPS_ERR_CUDA, "eigen-route SVD failed");
       }
-      if (work) dfree(work);
-      dfree(G);
-      dfree(W);
+      if (work && ownW) dfree(work);
+      if (ownG) {
+        dfree(G);
+        dfree(W);
+      }
       return rc;
     };
-    for (int m = 0; m < nm && status == CMPS_OK; ++m)
-      if (!blk[m].rows.empty()) status = factor(m, false);
+    FW main_fw{st, sol, blas, params, dA, dS, dinfo};
+    std::vector<int> todo;
+    int n_eig = 0;
+    for (int m = 0; m < nm; ++m) {
+      if (blk[m].rows.empty()) continue;
+      todo.push_back(m);
+      if (std::min(blk[m].rows.size(), blk[m].cols.size()) >= (size_t)kEigMin) ++n_eig;
+    }
+    // Concurrent factoring when at least two sectors take the Gram route:
+    // sectors dealt largest first to the least-loaded worker, one host thread
+    // per worker, workspaces sized for the worker's largest sector and
+    // bounded in total; otherwise the sectors run one by one.
+    bool done = false;
+    SvdPool* pool = nullptr;
+    if (n_eig >= 2 && get_pool(H.ctx, &pool) == CMPS_OK) {
+      const int K = std::min<int>((int)pool->w.size(), n_eig);
+      std::vector<int> order = todo;
+      auto cost = [&](int m) {
+        const double nr = (double)blk[m].rows.size(), nc = (double)blk[m].cols.size();
+        return nr * nc * std::min(nr, nc);
+      };
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+      std::vector<std::vector<int>> lists(K);
+      std::vector<double> load(K, 0.0);
+      for (int m : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        lists[k].push_back(m);
+        load[k] += cost(m);
+      }
+      std::vector<FW> fws(K);
+      std::vector<size_t> nA(K, 1), nS(K, 1), nG(K, 0), nW(K, 0), nwork(K, 1);
+      bool ok = true;
+      for (int k = 0; k < K && ok; ++k) {
+        SvdWorker& w = pool->w[k];
+        fws[k] = FW{w.st, w.sol, w.blas, nullptr, nullptr, nullptr, nullptr};
+        if (cusolverDnCreateGesvdjInfo(&fws[k].params) != CUSOLVER_STATUS_SUCCESS) {
+          fws[k].params = nullptr;
+          ok = false;
+          break;
+        }
+        cusolverDnXgesvdjSetTolerance(fws[k].params, 0.0);
+        cusolverDnXgesvdjSetMaxSweeps(fws[k].params, 100);
+        cusolverDnXgesvdjSetSortEig(fws[k].params, 1);
+        for (int m : lists[k]) {
+          const int64_t nr = (int64_t)blk[m].rows.size(), nc = (int64_t)blk[m].cols.size();
+          const int64_t mn = std::min(nr, nc);
+          nA[k] = std::max(nA[k], (size_t)(nr * nc));
+          nS[k] = std::max(nS[k], (size_t)mn);
+          int lwork = 0;
+          if (mn < kEigMin) {
+            if (cusolverDnZgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
+                                             (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)blk[m].dU, (int)nr,
+                                             (cuDoubleComplex*)blk[m].dV, (int)nc, &lwork,
+                                             fws[k].params) != CUSOLVER_STATUS_SUCCESS)
+              ok = false;
+          } else {
+            const int pp = (int)mn;
+            nG[k] = std::max(nG[k], (size_t)pp * pp);
+            nW[k] = std::max(nW[k], (size_t)pp);
+            if (cusolverDnZheevd_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, pp,
+                                            (cuDoubleComplex*)dA, pp, dS, &lwork) != CUSOLVER_STATUS_SUCCESS)
+              ok = false;
+          }
+          nwork[k] = std::max(nwork[k], (size_t)std::max(1, lwork));
+        }
+      }
+      double bytes = 0.0;
+      for (int k = 0; k < K; ++k)
+        bytes += 16.0 * (nA[k] + nG[k] + nwork[k]) + 8.0 * (nS[k] + nW[k]) + 4.0;
+      if (ok && bytes <= 8e9) {
+        for (int k = 0; k < K && ok; ++k) {
+          FW& fw = fws[k];
+          if (dmalloc(&fw.dA, sizeof(double2) * nA[k]) != cudaSuccess ||
+              dmalloc(&fw.dS, sizeof(double) * nS[k]) != cudaSuccess ||
+              dmalloc(&fw.dinfo, sizeof(int)) != cudaSuccess ||
+              dmalloc(&fw.work, sizeof(cuDoubleComplex) * nwork[k]) != cudaSuccess ||
+              (nG[k] && dmalloc(&fw.G, sizeof(double2) * nG[k]) != cudaSuccess) ||
+              (nW[k] && dmalloc(&fw.W, sizeof(double) * nW[k]) != cudaSuccess)) {
+            ok = false;
+            break;
+          }
+          fw.workcap = nwork[k];
+          fw.Gcap = nG[k];
+          fw.Wcap = nW[k];
+        }
+        if (ok) {
+          // theta and the block descriptors were written on the handle's stream
+          cudaStreamSynchronize(st);
+          std::vector<int> code(K, CMPS_OK);
+          std::vector<std::string> msg(K);
+          std::vector<std::thread> th_w;
+          const int dev = H.ctx->device;
+          for (int k = 0; k < K; ++k)
+            th_w.emplace_back([&, k]() {
+              cudaSetDevice(dev);
+              for (int m : lists[k]) {
+                const int rc = factor(m, false, fws[k]);
+                if (rc != CMPS_OK) {
+                  code[k] = rc;
+                  msg[k] = cmps_last_error();
+                  break;
+                }
+              }
+              cudaStreamSynchronize(fws[k].st);
+            });
+          for (auto& t : th_w) t.join();
+          for (int k = 0; k < K; ++k)
+            if (code[k] != CMPS_OK && status == CMPS_OK) status = fail(code[k], msg[k]);
+          done = true;
+        }
+      }
+      for (FW& fw : fws) {
+        if (fw.dA) dfree(fw.dA);
+        if (fw.dS) dfree(fw.dS);
+        if (fw.dinfo) dfree(fw.dinfo);
+        if (fw.work) dfree(fw.work);
+        if (fw.G) dfree(fw.G);
+        if (fw.W) dfree(fw.W);
+        if (fw.params) cusolverDnDestroyGesvdjInfo(fw.params);
+      }
+    }
+    if (!done)
+      for (int m : todo) {
+        if (status != CMPS_OK) break;
+        status = factor(m, false, main_fw);
+      }
     // ---- global selection (redone with exact factors where the Gram route is not accurate enough) ----
     struct SV { double v; int m; int64_t j; };
     std::vector<SV> all;
@@ -400,7 +598,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           if (all[g].m == m && all[g].v * all[g].v < floor2) low = true;
         if (weight_decided || low) {
           redo = true;
-          if ((status = factor(m, true)) != CMPS_OK) break;
+          if ((status = factor(m, true, main_fw)) != CMPS_OK) break;
         }
       }
       if (!redo) break;
