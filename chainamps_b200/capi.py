@@ -115,6 +115,7 @@ _SIGS = {
     "cmps_heff_adjoint": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc), C.c_void_p, C.c_void_p, c_dblp]),
     "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
     "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
+    "cmps_dmrg_unit_cell": (C.c_int, [C.c_void_p, C.c_double, C.c_int, c_dblp]),
     "cmps_heff_sector_table": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_dblp]),
     "cmps_heff_set_owned": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -500,6 +501,16 @@ class iDMRG:
         v = np.zeros(self.last["chi"], np.float64)
         _check(lib.cmps_dmrg_values(self.h, _p(v, C.c_double)))
         return v
+
+    def unit_cell(self, tol=1e-12, krylov_dim=30):
+        """Orthogonalise + iTwoVertexEnergy of the last growth step
+        (iDMRG_DRV.cpp:71-77): energy per vertex of the translation-invariant
+        cell, entropy of its boundary values, the dominant transfer-matrix
+        eigenvalues and the number of boundary values."""
+        v = np.zeros(6, np.float64)
+        _check(lib.cmps_dmrg_unit_cell(self.h, tol, krylov_dim, _p(v, C.c_double)))
+        return dict(energy=float(v[0]), entropy=float(v[1]), eta_left=float(v[2]), eta_right=float(v[3]),
+                    chi=int(v[4]), energy_imag=float(v[5]))
 
     def close(self):
         if getattr(self, "h", None):

@@ -709,6 +709,24 @@ int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n) {
   return std::min(n, Dmrg::kProfile) == n ? CMPS_OK : fail(CMPS_ERR_ARG, "profile has 17 entries");
 }
 
+int cmps_dmrg_unit_cell(cmps_dmrg* d, double tol, int krylov_dim, double* out6) {
+  if (!d || !d->impl || !out6) return fail(CMPS_ERR_ARG, "null argument");
+  Dmrg& D = *d->impl;
+  CMPS_CUDA(cudaSetDevice(D.device));
+  if (!D.svd || !D.heff || D.prev_lambda.empty() || D.size < 4)
+    return fail(CMPS_ERR_STATE, "unit cell: needs two growth steps or more");
+  if (!(tol > 0.0)) return fail(CMPS_ERR_ARG, "unit cell: tolerance must be positive");
+  UnitCellMeasure m;
+  CMPS_TRY(unit_cell_measure(D.ctx, *D.svd, D.lambda, D.prev_lambda, D.heff->W, D.heff->D, tol, krylov_dim, &m));
+  out6[0] = m.energy;
+  out6[1] = m.entropy;
+  out6[2] = m.eta_left;
+  out6[3] = m.eta_right;
+  out6[4] = (double)m.chi;
+  out6[5] = m.energy_imag;
+  return CMPS_OK;
+}
+
 int cmps_dmrg_values(const cmps_dmrg* d, double* values) {
   if (!d || !d->impl || !values) return fail(CMPS_ERR_ARG, "null argument");
   std::memcpy(values, d->impl->lambda.data(), sizeof(double) * d->impl->lambda.size());

@@ -191,6 +191,22 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
 int split_error(Heff& H);
 // cuSOLVER handle owned by the context (svd.cu).
 void release_solver(cmps_context* ctx);
+// The context's cuBLAS / cuSOLVER handles, bound to its stream (svd.cu).
+int context_blas(cmps_context* ctx, void** out);
+int context_solver(cmps_context* ctx, void** out);
+
+// iDMRG unit cell of a growth step (unitcell.cu): Orthogonalise +
+// iTwoVertexEnergy from the step's factors U, s, V^dagger (S, lam: the
+// rescaled values) and the previous step's values lam_prev.
+struct UnitCellMeasure {
+  double energy = 0.0, energy_imag = 0.0;  // per vertex
+  double entropy = 0.0;                     // of the new boundary values Lambda'
+  double eta_left = 0.0, eta_right = 0.0;   // dominant transfer-matrix eigenvalues
+  int64_t chi = 0;                          // Lambda' values above 1e-14 of the largest (squared)
+};
+int unit_cell_measure(cmps_context* ctx, const SvdResult& S, const std::vector<double>& lam,
+                      const std::vector<double>& lam_prev, const std::vector<WEntry>& W, int D, double tol, int kdim,
+                      UnitCellMeasure* out);
 
 int copy_env(const Env& src, Env& dst, cudaStream_t st);
 

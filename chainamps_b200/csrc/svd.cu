@@ -105,6 +105,20 @@ static int get_solver(cmps_context* ctx, cusolverDnHandle_t* out) {
   return CMPS_OK;
 }
 
+int context_blas(cmps_context* ctx, void** out) {
+  cublasHandle_t h;
+  CMPS_TRY(get_blas(ctx, &h));
+  *out = h;
+  return CMPS_OK;
+}
+
+int context_solver(cmps_context* ctx, void** out) {
+  cusolverDnHandle_t h;
+  CMPS_TRY(get_solver(ctx, &h));
+  *out = h;
+  return CMPS_OK;
+}
+
 namespace {
 
 __global__ void k_nzflags(const double* __restrict__ re, const double* __restrict__ im, int64_t rows,

@@ -1,0 +1,639 @@
+// The iDMRG unit cell of the last growth step, its orthogonalisation and the
+// energy per vertex: what the iDMRG driver measures after every step
+// (iDMRG_DRV.cpp:71-77: Orthogonalise, then iTwoVertexEnergy).
+//
+// The cell (UnitCell(MPSDecomposition, PreviousLambda), UnitCell.hpp:42-47)
+// is A0[s1] = U[s1] and A1[s2] = diag(s) V^dagger[s2] diag(1/lambda_prev),
+// its right bond identified element by element with its left bond.  With
+// M[s1,s2] = A0[s1] A1[s2], the left transfer map is L(l) = sum M^dag l M
+// (l indexed [bra, ket]) and the right map R(r) = sum M r M^dag (r indexed
+// [ket, bra]); LeftED / RightED (measurement.cpp:456-575) are their
+// dominant eigenpairs, made Hermitian.  Orthogonalise (measurement.cpp:
+// 180-246) factors them (SqrtDR, MPX_matrix.cpp:829-911: l = X^dag X with
+// eigenvalues |w| <= 100 eps max|w| dropped, mixed signs a failure), takes
+// the new boundary values Lambda' from the SVD of X Y (r = Y Y^dag) and
+// regauges the cell; iTwoVertexEnergy (measurement.cpp:371-397) then traces
+// the on-vertex term H1 = W[D-1, 0] of both sites, the bond
+// sum_k RowX_k ColX_k (RowX_k = W[D-1, k], ColX_k = W[k, 0]) inside the cell
+// and the bond into the next cell against Lambda'^2.
+//
+// Here the same numbers come from the fixed points directly, which the
+// regauging leaves invariant: <O> = Tr[T_O(l) r] / (eta Tr[l r]) for an
+// operator on one cell (T_O the left map with O inserted) and
+// Tr[T_O2(T_O1(l)) r] / (eta^2 Tr[l r]) for the bond between two cells;
+// Lambda'^2 are the eigenvalues of X r X^dag, normalised.  All operators act
+// on the dense cell: cuBLAS ZGEMMs on the column-major A0[s] (chi0 x chi1)
+// and A1[s] (chi1 x chi0).  The dominant eigenpairs come from a restarted
+// Arnoldi iteration on chi0 x chi0 matrices with two classical Gram-Schmidt
+// passes; its small Hessenberg eigenproblem is solved on the host (power
+// iteration, then inverse iteration at the Rayleigh quotient).
+#include <cublas_v2.h>
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <vector>
+
+#include "heff.h"
+
+namespace cmps {
+
+namespace {
+
+using cplx = cuDoubleComplex;
+using zc = std::complex<double>;
+constexpr double kEps = 2.220446049250313e-16;
+
+int grid_of(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
+
+// Scatter one row-major planar block into a stack of column-major matrices:
+// entry (r, c) lands in matrix sig (from the row map, or from the column map
+// when rsig is null) at (rdst[r], cdst[c]), scaled by rscale[r] * cscale[c].
+__global__ void k_scatter_cell(const double* __restrict__ re, const double* __restrict__ im, int64_t nr, int64_t nc,
+                               const int32_t* __restrict__ rsig, const int32_t* __restrict__ csig,
+                               const int64_t* __restrict__ rdst, const int64_t* __restrict__ cdst,
+                               const double* __restrict__ rscale, const double* __restrict__ cscale,
+                               cplx* __restrict__ dst, int64_t ld, int64_t stride) {
+  const int64_t n = nr * nc;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / nc, c = e % nc;
+    const int64_t sig = rsig ? rsig[r] : csig[c];
+    const double f = (rscale ? rscale[r] : 1.0) * (cscale ? cscale[c] : 1.0);
+    dst[sig * stride + rdst[r] + ld * cdst[c]] = make_cuDoubleComplex(re[e] * f, im[e] * f);
+  }
+}
+
+// v <- Hermitian part of (phase * v), in place (n x n, column-major).
+__global__ void k_hermitize(cplx* __restrict__ v, int64_t n, cplx phase) {
+  const int64_t tot = n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % n, j = e / n;
+    if (i > j) continue;
+    const cplx a = cuCmul(phase, v[i + n * j]);
+    const cplx b = cuCmul(phase, v[j + n * i]);
+    const cplx h = make_cuDoubleComplex(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    v[i + n * j] = h;
+    v[j + n * i] = cuConj(h);
+  }
+}
+
+// out (m x m) = in (m x m) transposed, for `count` matrices of stride m*m.
+__global__ void k_transpose_stack(const cplx* __restrict__ in, cplx* __restrict__ out, int64_t m, int64_t count) {
+  const int64_t tot = m * m * count;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = e / (m * m), w = e % (m * m), i = w % m, j = w / m;
+    out[q * m * m + j + m * i] = in[e];
+  }
+}
+
+// X[k, j] = root[k] * conj(E[j, keep[k]]): (kL x n), column-major.
+__global__ void k_make_x(const cplx* __restrict__ E, int64_t n, const int32_t* __restrict__ keep,
+                         const double* __restrict__ root, int64_t kl, cplx* __restrict__ X) {
+  const int64_t tot = kl * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = e % kl, j = e / kl;
+    const cplx v = E[j + n * keep[k]];
+    X[e] = make_cuDoubleComplex(root[k] * v.x, -root[k] * v.y);
+  }
+}
+
+struct Cell {
+  int d = 0;
+  int64_t c0 = 0, c1 = 0;
+  cplx* A0 = nullptr;  // d x (c0 x c1)
+  cplx* A1 = nullptr;  // d x (c1 x c0)
+  cplx* a0(int s) const { return A0 + (int64_t)s * c0 * c1; }
+  cplx* a1(int s) const { return A1 + (int64_t)s * c1 * c0; }
+};
+
+struct Blas {
+  cublasHandle_t h;
+  int st = CMPS_OK;
+  void gemm(cublasOperation_t ta, cublasOperation_t tb, int64_t m, int64_t n, int64_t k, cplx alpha, const cplx* A,
+            int64_t lda, const cplx* B, int64_t ldb, cplx beta, cplx* C, int64_t ldc) {
+    if (st != CMPS_OK) return;
+    if (cublasZgemm(h, ta, tb, (int)m, (int)n, (int)k, &alpha, A, (int)lda, B, (int)ldb, &beta, C, (int)ldc) !=
+        CUBLAS_STATUS_SUCCESS)
+      st = fail(CMPS_ERR_CUDA, "unit cell: cublasZgemm failed");
+  }
+};
+
+const cplx kOne = {1.0, 0.0}, kZero = {0.0, 0.0};
+
+// out = L(in) (left) or R(in) (right); w01: c0 x c1, w11: c1 x c1, w10: c1 x c0.
+void transfer(Blas& b, const Cell& c, bool left, const cplx* in, cplx* out, cplx* w01, cplx* w11, cplx* w10) {
+  const int64_t c0 = c.c0, c1 = c.c1;
+  if (left) {
+    for (int s = 0; s < c.d; ++s) {
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c0, kOne, in, c0, c.a0(s), c0, kZero, w01, c0);
+      b.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c1, c1, c0, kOne, c.a0(s), c0, w01, c0, s ? kOne : kZero, w11, c1);
+    }
+    for (int s = 0; s < c.d; ++s) {
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c1, kOne, w11, c1, c.a1(s), c1, kZero, w10, c1);
+      b.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c0, c0, c1, kOne, c.a1(s), c1, w10, c1, s ? kOne : kZero, out, c0);
+    }
+  } else {
+    for (int s = 0; s < c.d; ++s) {
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c0, kOne, c.a1(s), c1, in, c0, kZero, w10, c1);
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c1, c1, c0, kOne, w10, c1, c.a1(s), c1, s ? kOne : kZero, w11, c1);
+    }
+    for (int s = 0; s < c.d; ++s) {
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c1, kOne, c.a0(s), c0, w11, c1, kZero, w01, c0);
+      b.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c0, c0, c1, kOne, w01, c0, c.a0(s), c0, s ? kOne : kZero, out, c0);
+    }
+  }
+}
+
+// Dominant eigenpair of a small complex matrix H (k x k, column-major):
+// power iteration from a fixed start, then inverse iteration at the
+// Rayleigh quotient.  Returns false when no iterate is finite.
+bool small_dominant(int k, const std::vector<zc>& H, zc* theta, std::vector<zc>& y) {
+  auto mul = [&](const std::vector<zc>& x) {
+    std::vector<zc> o(k, 0.0);
+    for (int j = 0; j < k; ++j)
+      for (int i = 0; i < k; ++i) o[i] += H[i + (size_t)k * j] * x[j];
+    return o;
+  };
+  auto normalise = [&](std::vector<zc>& x) {
+    double s = 0.0;
+    for (auto& v : x) s += std::norm(v);
+    s = std::sqrt(s);
+    if (!(s > 0.0) || !std::isfinite(s)) return false;
+    for (auto& v : x) v /= s;
+    return true;
+  };
+  auto rayleigh = [&](const std::vector<zc>& x) {
+    const std::vector<zc> hx = mul(x);
+    zc num = 0.0;
+    for (int i = 0; i < k; ++i) num += std::conj(x[i]) * hx[i];
+    return num;
+  };
+  y.assign(k, zc(1.0, 0.0));
+  for (int i = 0; i < k; ++i) y[i] = zc(1.0 + 0.01 * i, 0.0);
+  if (!normalise(y)) return false;
+  for (int it = 0; it < 400; ++it) {
+    y = mul(y);
+    if (!normalise(y)) return false;
+  }
+  zc mu = rayleigh(y);
+  for (int it = 0; it < 4; ++it) {
+    // solve (H - mu I) z = y by Gaussian elimination with partial pivoting
+    std::vector<zc> A(H);
+    const zc shift = mu + zc(1e-13 * std::max(1.0, std::abs(mu)), 0.0);
+    for (int i = 0; i < k; ++i) A[i + (size_t)k * i] -= shift;
+    std::vector<zc> z(y);
+    bool ok = true;
+    for (int col = 0; col < k && ok; ++col) {
+      int p = col;
+      for (int r = col + 1; r < k; ++r)
+        if (std::abs(A[r + (size_t)k * col]) > std::abs(A[p + (size_t)k * col])) p = r;
+      if (std::abs(A[p + (size_t)k * col]) == 0.0) {
+        ok = false;
+        break;
+      }
+      if (p != col) {
+        for (int j = 0; j < k; ++j) std::swap(A[col + (size_t)k * j], A[p + (size_t)k * j]);
+        std::swap(z[col], z[p]);
+      }
+      for (int r = col + 1; r < k; ++r) {
+        const zc f = A[r + (size_t)k * col] / A[col + (size_t)k * col];
+        if (f == zc(0.0)) continue;
+        for (int j = col; j < k; ++j) A[r + (size_t)k * j] -= f * A[col + (size_t)k * j];
+        z[r] -= f * z[col];
+      }
+    }
+    if (!ok) break;
+    for (int r = k - 1; r >= 0; --r) {
+      zc s = z[r];
+      for (int j = r + 1; j < k; ++j) s -= A[r + (size_t)k * j] * z[j];
+      z[r] = s / A[r + (size_t)k * r];
+    }
+    if (!normalise(z)) break;
+    y = z;
+    mu = rayleigh(y);
+  }
+  *theta = rayleigh(y);
+  return std::isfinite(theta->real()) && std::isfinite(theta->imag());
+}
+
+// Dominant eigenpair of L or R by restarted Arnoldi; x (n = c0^2) holds the
+// start vector and receives the eigenvector.  V: (kdim + 1) x n workspace.
+int dominant(Blas& b, cudaStream_t st, const Cell& c, bool left, double tol, int kdim, int max_restarts, cplx* x,
+             cplx* V, cplx* hvec, cplx* w01, cplx* w11, cplx* w10, zc* eta) {
+  const int64_t n = c.c0 * c.c0;
+  kdim = std::max(2, std::min<int>(kdim, (int)std::min<int64_t>(n, 64)));
+  zc theta = 0.0;
+  bool converged = false;
+  for (int restart = 0; restart < std::max(1, max_restarts) && !converged; ++restart) {
+    double nrm = 0.0;
+    if (cublasDznrm2(b.h, (int)n, x, 1, &nrm) != CUBLAS_STATUS_SUCCESS || !(nrm > 0.0))
+      return fail(CMPS_ERR_SOLVER, "unit cell: zero Arnoldi start vector");
+    const double inv = 1.0 / nrm;
+    cudaMemcpyAsync(V, x, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st);
+    cublasZdscal(b.h, (int)n, &inv, V, 1);
+    std::vector<zc> H((size_t)(kdim + 1) * kdim, 0.0);  // column-major (kdim+1) x kdim
+    std::vector<zc> y;
+    int k = 0;
+    for (int j = 0; j < kdim; ++j) {
+      cplx* vj = V + (int64_t)j * n;
+      cplx* w = V + (int64_t)(j + 1) * n;
+      transfer(b, c, left, vj, w, w01, w11, w10);
+      if (b.st != CMPS_OK) return b.st;
+      for (int pass = 0; pass < 2; ++pass) {
+        const cplx mone = {-1.0, 0.0};
+        if (cublasZgemv(b.h, CUBLAS_OP_C, (int)n, j + 1, &kOne, V, (int)n, w, 1, &kZero, hvec, 1) !=
+                CUBLAS_STATUS_SUCCESS ||
+            cublasZgemv(b.h, CUBLAS_OP_N, (int)n, j + 1, &mone, V, (int)n, hvec, 1, &kOne, w, 1) !=
+                CUBLAS_STATUS_SUCCESS)
+          return fail(CMPS_ERR_CUDA, "unit cell: Gram-Schmidt failed");
+        std::vector<cplx> hh(j + 1);
+        cudaMemcpyAsync(hh.data(), hvec, sizeof(cplx) * (j + 1), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return fail(CMPS_ERR_CUDA, "unit cell: Arnoldi step failed");
+        for (int i = 0; i <= j; ++i) H[i + (size_t)(kdim + 1) * j] += zc(hh[i].x, hh[i].y);
+      }
+      double beta = 0.0;
+      cublasDznrm2(b.h, (int)n, w, 1, &beta);
+      H[(j + 1) + (size_t)(kdim + 1) * j] = beta;
+      k = j + 1;
+      std::vector<zc> Hk((size_t)k * k);
+      for (int jj = 0; jj < k; ++jj)
+        for (int ii = 0; ii < k; ++ii) Hk[ii + (size_t)k * jj] = H[ii + (size_t)(kdim + 1) * jj];
+      if (!small_dominant(k, Hk, &theta, y)) return fail(CMPS_ERR_SOLVER, "unit cell: Hessenberg eigenproblem failed");
+      const double resid = beta * std::abs(y[k - 1]);
+      if (resid <= tol * std::abs(theta) || !(beta > 1e-300)) {
+        converged = true;
+        break;
+      }
+      if (j + 1 < kdim) {
+        const double ib = 1.0 / beta;
+        cublasZdscal(b.h, (int)n, &ib, w, 1);
+      }
+    }
+    // Ritz vector x = V_k y
+    std::vector<cplx> yc(k);
+    for (int i = 0; i < k; ++i) yc[i] = make_cuDoubleComplex(y[i].real(), y[i].imag());
+    cudaMemcpyAsync(hvec, yc.data(), sizeof(cplx) * k, cudaMemcpyHostToDevice, st);
+    if (cublasZgemv(b.h, CUBLAS_OP_N, (int)n, k, &kOne, V, (int)n, hvec, 1, &kZero, x, 1) != CUBLAS_STATUS_SUCCESS)
+      return fail(CMPS_ERR_CUDA, "unit cell: Ritz vector failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(CMPS_ERR_CUDA, "unit cell: Ritz vector failed");
+  }
+  if (!converged) return fail(CMPS_ERR_SOLVER, "unit cell: transfer-matrix eigensolver did not converge");
+  *eta = theta;
+  return CMPS_OK;
+}
+
+// trace of a column-major n x n matrix, on the host
+zc trace_of(const cplx* dA, int64_t n, cudaStream_t st) {
+  std::vector<cplx> h((size_t)n * n);
+  cudaMemcpyAsync(h.data(), dA, sizeof(cplx) * n * n, cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  zc t = 0.0;
+  for (int64_t i = 0; i < n; ++i) t += zc(h[i + n * i].x, h[i + n * i].y);
+  return t;
+}
+
+}  // namespace
+
+int unit_cell_measure(cmps_context* ctx, const SvdResult& S, const std::vector<double>& lam,
+                      const std::vector<double>& lam_prev, const std::vector<WEntry>& W, int D, double tol, int kdim,
+                      UnitCellMeasure* out) {
+  cudaStream_t st = ctx->stream;
+  const int d = S.d;
+  const int64_t c0 = S.a0.size(), c1 = (int64_t)S.values.size();
+  if (S.a0.element_charges() != S.a2.element_charges() || (int64_t)lam_prev.size() != c0 ||
+      (int64_t)lam.size() != c1 || c0 < 1 || c1 < 1)
+    return fail(CMPS_ERR_STATE, "unit cell: the step's end bonds differ (no previous step to pair them)");
+  if (D < 3) return fail(CMPS_ERR_STATE, "unit cell: MPO bond dimension below 3");
+  const ThetaSpace& th = S.th;
+  const int nm = (int)th.mq.size();
+  void* blas_v = nullptr;
+  void* sol_v = nullptr;
+  CMPS_TRY(context_blas(ctx, &blas_v));
+  CMPS_TRY(context_solver(ctx, &sol_v));
+  Blas bl{(cublasHandle_t)blas_v};
+  cusolverDnHandle_t sol = (cusolverDnHandle_t)sol_v;
+
+  std::vector<void*> allocs;
+  auto alloc = [&](auto** p, size_t bytes) -> int {
+    if (dmalloc((void**)p, std::max<size_t>(bytes, 16)) != cudaSuccess)
+      return fail(CMPS_ERR_NOMEM, "unit cell: device allocation failed");
+    allocs.push_back((void*)*p);
+    return CMPS_OK;
+  };
+  struct Free {
+    std::vector<void*>& a;
+    ~Free() {
+      for (void* p : a) dfree(p);
+    }
+  } free_guard{allocs};
+
+  // ---- dense cell ----
+  Cell c{d, c0, c1, nullptr, nullptr};
+  CMPS_TRY(alloc(&c.A0, sizeof(cplx) * d * c0 * c1));
+  CMPS_TRY(alloc(&c.A1, sizeof(cplx) * d * c1 * c0));
+  CMPS_CUDA(cudaMemsetAsync(c.A0, 0, sizeof(cplx) * d * c0 * c1, st));
+  CMPS_CUDA(cudaMemsetAsync(c.A1, 0, sizeof(cplx) * d * c1 * c0, st));
+  std::vector<double> inv_prev(c0);
+  for (int64_t j = 0; j < c0; ++j) inv_prev[j] = lam_prev[j] != 0.0 ? 1.0 / lam_prev[j] : 0.0;
+  for (int m = 0; m < nm; ++m) {
+    const int64_t k = S.kept[m];
+    if (!k) continue;
+    const int64_t R = th.nrows[m], C = th.ncols[m];
+    std::vector<int32_t> rsig(R, -1), csig(C, -1);
+    std::vector<int64_t> rdst(R, -1), cdst_c(C, -1), kcol(k);
+    std::vector<double> kscale(k), cscale(C, 0.0);
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (th.rowoff[m][s1] < 0) continue;
+      const int sa = S.a0.find(S.rules.sub(th.mq[m], S.sigq[s1]));
+      for (int64_t p = 0; p < S.a0.sdim[sa]; ++p) {
+        rsig[th.rowoff[m][s1] + p] = s1;
+        rdst[th.rowoff[m][s1] + p] = S.a0.selem[sa][p];
+      }
+    }
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      const int t = S.a2.find(S.rules.add(th.mq[m], S.sigq[s2]));
+      for (int64_t p = 0; p < S.a2.sdim[t]; ++p) {
+        const int64_t j = S.a2.selem[t][p];
+        csig[th.coloff[m][s2] + p] = s2;
+        cdst_c[th.coloff[m][s2] + p] = j;
+        cscale[th.coloff[m][s2] + p] = inv_prev[j];
+      }
+    }
+    for (int64_t j = 0; j < k; ++j) {
+      kcol[j] = S.gidx[m][j];
+      kscale[j] = lam[S.gidx[m][j]];
+    }
+    for (int64_t r = 0; r < R; ++r)
+      if (rsig[r] < 0 || rdst[r] < 0 || rdst[r] >= c0) return fail(CMPS_ERR_STATE, "unit cell: row map");
+    for (int64_t q = 0; q < C; ++q)
+      if (csig[q] < 0 || cdst_c[q] < 0 || cdst_c[q] >= c0) return fail(CMPS_ERR_STATE, "unit cell: column map");
+    for (int64_t j = 0; j < k; ++j)
+      if (kcol[j] < 0 || kcol[j] >= c1) return fail(CMPS_ERR_STATE, "unit cell: bond map");
+    int32_t *d_rsig, *d_csig;
+    int64_t *d_rdst, *d_cdst, *d_kcol;
+    double *d_kscale, *d_cscale;
+    CMPS_TRY(alloc(&d_rsig, sizeof(int32_t) * R));
+    CMPS_TRY(alloc(&d_csig, sizeof(int32_t) * C));
+    CMPS_TRY(alloc(&d_rdst, sizeof(int64_t) * R));
+    CMPS_TRY(alloc(&d_cdst, sizeof(int64_t) * C));
+    CMPS_TRY(alloc(&d_kcol, sizeof(int64_t) * k));
+    CMPS_TRY(alloc(&d_kscale, sizeof(double) * k));
+    CMPS_TRY(alloc(&d_cscale, sizeof(double) * C));
+    CMPS_TRY(copy_wait(d_rsig, rsig.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_csig, csig.data(), sizeof(int32_t) * C, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_rdst, rdst.data(), sizeof(int64_t) * R, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_cdst, cdst_c.data(), sizeof(int64_t) * C, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_kcol, kcol.data(), sizeof(int64_t) * k, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_kscale, kscale.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_cscale, cscale.data(), sizeof(double) * C, cudaMemcpyHostToDevice, st));
+    // A0[s1][a0, a1] = U_m[(s1, a0), j]
+    k_scatter_cell<<<grid_of(R * k), 256, 0, st>>>(S.U.re() + S.uoff[m], S.U.im() + S.uoff[m], R, k, d_rsig,
+                                                   nullptr, d_rdst, d_kcol, nullptr, nullptr, c.A0, c0, c0 * c1);
+    // A1[s2][a1, a2] = s[a1] V^dagger_m[j, (s2, a2)] / lambda_prev[a2]
+    k_scatter_cell<<<grid_of(k * C), 256, 0, st>>>(S.Vd.re() + S.voff[m], S.Vd.im() + S.voff[m], k, C, nullptr,
+                                                   d_csig, d_kcol, d_cdst, d_kscale, d_cscale, c.A1, c1, c1 * c0);
+    CMPS_CUDA(cudaGetLastError());
+  }
+
+  // ---- dominant fixed points ----
+  const int64_t n = c0 * c0;
+  const int kd = std::max(2, std::min<int>(kdim, (int)std::min<int64_t>(n, 64)));
+  cplx *V, *hvec, *w01, *w11, *w10, *lft, *rgt;
+  CMPS_TRY(alloc(&V, sizeof(cplx) * (kd + 1) * n));
+  CMPS_TRY(alloc(&hvec, sizeof(cplx) * (kd + 1)));
+  CMPS_TRY(alloc(&w01, sizeof(cplx) * c0 * c1));
+  CMPS_TRY(alloc(&w11, sizeof(cplx) * c1 * c1));
+  CMPS_TRY(alloc(&w10, sizeof(cplx) * c1 * c0));
+  CMPS_TRY(alloc(&lft, sizeof(cplx) * n));
+  CMPS_TRY(alloc(&rgt, sizeof(cplx) * n));
+  {
+    // start: the identity (the fixed point of a canonical cell)
+    std::vector<cplx> id((size_t)n, kZero);
+    for (int64_t i = 0; i < c0; ++i) id[i + c0 * i] = kOne;
+    CMPS_TRY(copy_wait(lft, id.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(rgt, id.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
+  }
+  zc eta_l = 0.0, eta_r = 0.0;
+  CMPS_TRY(dominant(bl, st, c, true, tol, kd, 200, lft, V, hvec, w01, w11, w10, &eta_l));
+  CMPS_TRY(dominant(bl, st, c, false, tol, kd, 200, rgt, V, hvec, w01, w11, w10, &eta_r));
+  for (zc e : {eta_l, eta_r})
+    if (std::abs(e.imag()) >= 1e-10 * std::abs(e.real()) || !(e.real() > 0.0))
+      return fail(CMPS_ERR_SOLVER, "unit cell: dominant transfer-matrix eigenvalue is not real and positive");
+  for (cplx* v : {lft, rgt}) {
+    const zc tr = trace_of(v, c0, st);
+    if (!(std::abs(tr) > 0.0)) return fail(CMPS_ERR_SOLVER, "unit cell: traceless fixed point");
+    const zc ph = std::conj(tr) / std::abs(tr);
+    k_hermitize<<<grid_of(n), 256, 0, st>>>(v, c0, make_cuDoubleComplex(ph.real(), ph.imag()));
+  }
+
+  // ---- SqrtDR of the left fixed point; Lambda'^2 = eig(X r X^dag) ----
+  {
+    cplx* E;
+    double* w;
+    int* dinfo;
+    CMPS_TRY(alloc(&E, sizeof(cplx) * n));
+    CMPS_TRY(alloc(&w, sizeof(double) * c0));
+    CMPS_TRY(alloc(&dinfo, sizeof(int)));
+    CMPS_CUDA(cudaMemcpyAsync(E, lft, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+    cusolverDnSetStream(sol, st);
+    int lwork = 0;
+    if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)c0, E, (int)c0, w,
+                                    &lwork) != CUSOLVER_STATUS_SUCCESS)
+      return fail(CMPS_ERR_SOLVER, "unit cell: zheevd buffer query failed");
+    cplx* work;
+    CMPS_TRY(alloc(&work, sizeof(cplx) * std::max(1, lwork)));
+    if (cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)c0, E, (int)c0, w, work, lwork,
+                         dinfo) != CUSOLVER_STATUS_SUCCESS)
+      return fail(CMPS_ERR_SOLVER, "unit cell: zheevd failed");
+    std::vector<double> hw(c0);
+    int info = 0;
+    cudaMemcpyAsync(hw.data(), w, sizeof(double) * c0, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+    CMPS_CUDA(cudaStreamSynchronize(st));
+    if (info != 0) return fail(CMPS_ERR_SOLVER, "unit cell: zheevd did not converge");
+    double mx = 0.0;
+    for (double x : hw) mx = std::max(mx, std::fabs(x));
+    const double cut = mx * 100.0 * kEps;
+    std::vector<int32_t> keep;
+    std::vector<double> root;
+    int neg = 0;
+    for (int64_t i = 0; i < c0; ++i)
+      if (std::fabs(hw[i]) > cut) {
+        keep.push_back((int32_t)i);
+        root.push_back(std::sqrt(std::fabs(hw[i])));
+        if (hw[i] < 0.0) ++neg;
+      }
+    if (keep.empty() || (neg != 0 && neg != (int)keep.size()))
+      return fail(CMPS_ERR_SOLVER, "unit cell: SqrtDR failure (eigenvalues of both signs)");
+    const int64_t kl = (int64_t)keep.size();
+    int32_t* d_keep;
+    double* d_root;
+    cplx *X, *XR, *B;
+    CMPS_TRY(alloc(&d_keep, sizeof(int32_t) * kl));
+    CMPS_TRY(alloc(&d_root, sizeof(double) * kl));
+    CMPS_TRY(alloc(&X, sizeof(cplx) * kl * c0));
+    CMPS_TRY(alloc(&XR, sizeof(cplx) * kl * c0));
+    CMPS_TRY(alloc(&B, sizeof(cplx) * kl * kl));
+    CMPS_TRY(copy_wait(d_keep, keep.data(), sizeof(int32_t) * kl, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(d_root, root.data(), sizeof(double) * kl, cudaMemcpyHostToDevice, st));
+    k_make_x<<<grid_of(kl * c0), 256, 0, st>>>(E, c0, d_keep, d_root, kl, X);
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, kl, c0, c0, kOne, X, kl, rgt, c0, kZero, XR, kl);
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_C, kl, kl, c0, kOne, XR, kl, X, kl, kZero, B, kl);
+    if (bl.st != CMPS_OK) return bl.st;
+    double* wb;
+    CMPS_TRY(alloc(&wb, sizeof(double) * kl));
+    int lw2 = 0;
+    if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, (int)kl, B, (int)kl, wb,
+                                    &lw2) != CUSOLVER_STATUS_SUCCESS)
+      return fail(CMPS_ERR_SOLVER, "unit cell: zheevd buffer query failed");
+    cplx* work2;
+    CMPS_TRY(alloc(&work2, sizeof(cplx) * std::max(1, lw2)));
+    if (cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_NOVECTOR, CUBLAS_FILL_MODE_LOWER, (int)kl, B, (int)kl, wb, work2, lw2,
+                         dinfo) != CUSOLVER_STATUS_SUCCESS)
+      return fail(CMPS_ERR_SOLVER, "unit cell: zheevd failed");
+    std::vector<double> hb(kl);
+    cudaMemcpyAsync(hb.data(), wb, sizeof(double) * kl, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+    CMPS_CUDA(cudaStreamSynchronize(st));
+    if (info != 0) return fail(CMPS_ERR_SOLVER, "unit cell: zheevd did not converge");
+    double sum = 0.0, bmax = 0.0;
+    for (double x : hb) {
+      if (x > 0.0) sum += x;
+      bmax = std::max(bmax, x);
+    }
+    if (!(sum > 0.0)) return fail(CMPS_ERR_SOLVER, "unit cell: no weight in the new boundary values");
+    double ent = 0.0;
+    int64_t chi_new = 0;
+    for (double x : hb) {
+      if (!(x > 0.0)) continue;
+      const double p = x / sum;
+      ent -= p * std::log(p);
+      if (x > 1e-14 * bmax) ++chi_new;
+    }
+    out->entropy = ent;
+    out->chi = chi_new;
+  }
+
+  // ---- energy per vertex from trace tables ----
+  // F[s1',s1] = A0[s1']^H l A0[s1] (c1 x c1), G[s2,s2'] = A1[s2] r A1[s2']^H,
+  // T1[(s1',s1),(s2,s2')] = Tr[F G]; P[s2',s2] = A1[s2']^H K A1[s2] with
+  // K = sum F[s1,s1], Q[s1,s1'] = A0[s1] Gs A0[s1']^H with Gs = sum G[s2,s2],
+  // T2[(s2',s2),(s1,s1')] = Tr[P Q].  Pair index (a, b) -> a + d b.
+  const int64_t dd = (int64_t)d * d;
+  cplx *F, *G, *FT, *P, *Q, *PT, *T1, *T2, *K, *Gs;
+  CMPS_TRY(alloc(&F, sizeof(cplx) * dd * c1 * c1));
+  CMPS_TRY(alloc(&G, sizeof(cplx) * dd * c1 * c1));
+  CMPS_TRY(alloc(&FT, sizeof(cplx) * dd * c1 * c1));
+  CMPS_TRY(alloc(&P, sizeof(cplx) * dd * c0 * c0));
+  CMPS_TRY(alloc(&Q, sizeof(cplx) * dd * c0 * c0));
+  CMPS_TRY(alloc(&PT, sizeof(cplx) * dd * c0 * c0));
+  CMPS_TRY(alloc(&T1, sizeof(cplx) * dd * dd));
+  CMPS_TRY(alloc(&T2, sizeof(cplx) * dd * dd));
+  CMPS_TRY(alloc(&K, sizeof(cplx) * c1 * c1));
+  CMPS_TRY(alloc(&Gs, sizeof(cplx) * c1 * c1));
+  for (int s1 = 0; s1 < d; ++s1) {
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c0, kOne, lft, c0, c.a0(s1), c0, kZero, w01, c0);  // l A0[s1]
+    for (int s1p = 0; s1p < d; ++s1p)
+      bl.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c1, c1, c0, kOne, c.a0(s1p), c0, w01, c0, kZero,
+              F + (s1p + (int64_t)d * s1) * c1 * c1, c1);
+  }
+  for (int s2 = 0; s2 < d; ++s2) {
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c0, kOne, c.a1(s2), c1, rgt, c0, kZero, w10, c1);  // A1[s2] r
+    for (int s2p = 0; s2p < d; ++s2p)
+      bl.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c1, c1, c0, kOne, w10, c1, c.a1(s2p), c1, kZero,
+              G + (s2 + (int64_t)d * s2p) * c1 * c1, c1);
+  }
+  if (bl.st != CMPS_OK) return bl.st;
+  CMPS_CUDA(cudaMemsetAsync(K, 0, sizeof(cplx) * c1 * c1, st));
+  CMPS_CUDA(cudaMemsetAsync(Gs, 0, sizeof(cplx) * c1 * c1, st));
+  for (int s = 0; s < d; ++s) {
+    if (cublasZaxpy(bl.h, (int)(c1 * c1), &kOne, F + (s + (int64_t)d * s) * c1 * c1, 1, K, 1) !=
+            CUBLAS_STATUS_SUCCESS ||
+        cublasZaxpy(bl.h, (int)(c1 * c1), &kOne, G + (s + (int64_t)d * s) * c1 * c1, 1, Gs, 1) !=
+            CUBLAS_STATUS_SUCCESS)
+      return fail(CMPS_ERR_CUDA, "unit cell: axpy failed");
+  }
+  for (int s2 = 0; s2 < d; ++s2) {
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c1, kOne, K, c1, c.a1(s2), c1, kZero, w10, c1);  // K A1[s2]
+    for (int s2p = 0; s2p < d; ++s2p)
+      bl.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c0, c0, c1, kOne, c.a1(s2p), c1, w10, c1, kZero,
+              P + (s2p + (int64_t)d * s2) * c0 * c0, c0);
+  }
+  for (int s1 = 0; s1 < d; ++s1) {
+    bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c1, kOne, c.a0(s1), c0, Gs, c1, kZero, w01, c0);  // A0[s1] Gs
+    for (int s1p = 0; s1p < d; ++s1p)
+      bl.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c0, c0, c1, kOne, w01, c0, c.a0(s1p), c0, kZero,
+              Q + (s1 + (int64_t)d * s1p) * c0 * c0, c0);
+  }
+  if (bl.st != CMPS_OK) return bl.st;
+  // Tr[F G] = vec(F^T) . vec(G): T1 = FT_mat^T G_mat over the stacked matrices
+  k_transpose_stack<<<grid_of(dd * c1 * c1), 256, 0, st>>>(F, FT, c1, dd);
+  k_transpose_stack<<<grid_of(dd * c0 * c0), 256, 0, st>>>(P, PT, c0, dd);
+  bl.gemm(CUBLAS_OP_T, CUBLAS_OP_N, dd, dd, c1 * c1, kOne, FT, c1 * c1, G, c1 * c1, kZero, T1, dd);
+  bl.gemm(CUBLAS_OP_T, CUBLAS_OP_N, dd, dd, c0 * c0, kOne, PT, c0 * c0, Q, c0 * c0, kZero, T2, dd);
+  if (bl.st != CMPS_OK) return bl.st;
+  std::vector<cplx> h1((size_t)dd * dd), h2((size_t)dd * dd);
+  cudaMemcpyAsync(h1.data(), T1, sizeof(cplx) * dd * dd, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(h2.data(), T2, sizeof(cplx) * dd * dd, cudaMemcpyDeviceToHost, st);
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  auto t1 = [&](int s1p, int s1, int s2, int s2p) {
+    const cplx v = h1[(s1p + (size_t)d * s1) + (size_t)dd * (s2 + (size_t)d * s2p)];
+    return zc(v.x, v.y);
+  };
+  auto t2 = [&](int s2p, int s2, int s1, int s1p) {
+    const cplx v = h2[(s2p + (size_t)d * s2) + (size_t)dd * (s1 + (size_t)d * s1p)];
+    return zc(v.x, v.y);
+  };
+  // MPO blocks as d x d operators O[s', s]
+  auto block = [&](int bl_, int br_) {
+    std::vector<zc> O((size_t)d * d, 0.0);
+    for (const WEntry& e : W)
+      if (e.bl == bl_ && e.br == br_) O[e.sp + (size_t)d * e.s] += zc(e.wr, e.wi);
+    return O;
+  };
+  const std::vector<zc> H1 = block(D - 1, 0);
+  zc norm = 0.0, local = 0.0, bond1 = 0.0, bond2 = 0.0;
+  for (int s1 = 0; s1 < d; ++s1)
+    for (int s2 = 0; s2 < d; ++s2) norm += t1(s1, s1, s2, s2);
+  for (int a = 0; a < d; ++a)
+    for (int b = 0; b < d; ++b) {
+      const zc h = H1[a + (size_t)d * b];  // H1[s', s]
+      if (h == zc(0.0)) continue;
+      for (int s = 0; s < d; ++s) {
+        local += h * t1(a, b, s, s);  // site 0
+        local += h * t1(s, s, b, a);  // site 1
+      }
+    }
+  for (int kb = 1; kb <= D - 2; ++kb) {
+    const std::vector<zc> Rx = block(D - 1, kb), Cx = block(kb, 0);
+    bool any_r = false, any_c = false;
+    for (const zc& v : Rx) any_r |= v != zc(0.0);
+    for (const zc& v : Cx) any_c |= v != zc(0.0);
+    if (!any_r || !any_c) continue;
+    for (int a = 0; a < d; ++a)
+      for (int b = 0; b < d; ++b) {
+        const zc r = Rx[a + (size_t)d * b];
+        if (r == zc(0.0)) continue;
+        for (int e = 0; e < d; ++e)
+          for (int f = 0; f < d; ++f) {
+            const zc cc = Cx[e + (size_t)d * f];
+            if (cc == zc(0.0)) continue;
+            bond1 += r * cc * t1(a, b, f, e);   // RowX on site 0, ColX on site 1
+            bond2 += r * cc * t2(a, b, f, e);   // RowX on site 1, ColX on the next site 0
+          }
+      }
+  }
+  const double eta = eta_l.real();
+  const zc e = 0.5 * (local + bond1 + bond2 / eta) / norm;
+  out->energy = e.real();
+  out->energy_imag = e.imag();
+  out->eta_left = eta_l.real();
+  out->eta_right = eta_r.real();
+  return CMPS_OK;
+}
+
+}  // namespace cmps

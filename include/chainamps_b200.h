@@ -264,6 +264,25 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
                    int* matvecs, double* ms4);
 /* The current (rescaled) singular values, bond_dim of them, descending. */
 int cmps_dmrg_values(const cmps_dmrg* d, double* values);
+/* The translation-invariant unit cell of the last growth step and its
+ * energy per vertex: what iDMRG_DRV measures after every step
+ * (iDMRG_DRV.cpp:71-77), Orthogonalise(MPSDecomposition, PreviousLambda)
+ * (measurement.cpp:180-246, 254-257) followed by
+ * iTwoVertexEnergy(ColX, RowX, H1, UnitCell) (measurement.cpp:378-397),
+ * with H1, ColX and RowX the on-vertex, column and row blocks of the
+ * handle's MPO (measurement.cpp:371-376).  The cell is U and
+ * diag(s) V^dagger diag(1/lambda_prev) (UnitCell.hpp:42-47); the dominant
+ * left and right eigenpairs of its transfer matrix come from a restarted
+ * Arnoldi iteration to residual <= tol * |eigenvalue| (Krylov dimension
+ * krylov_dim, at most 64).  out6 = {energy per vertex, entropy of the
+ * orthogonalised boundary values, left and right dominant eigenvalues,
+ * number of boundary values (those whose square is above 1e-14 of the
+ * largest), imaginary part of the energy}.  Needs two growth steps or more
+ * (lambda_prev must live on the cell's end bonds; the reference measures
+ * after its two warm-up steps, iDMRG_DRV.cpp:46-50,64-71); CMPS_ERR_SOLVER
+ * where Orthogonalise returns an empty cell (complex dominant eigenvalue,
+ * SqrtDR with eigenvalues of both signs). */
+int cmps_dmrg_unit_cell(cmps_dmrg* d, double tol, int krylov_dim, double* out6);
 /* ---- finite sweeps (FiniteDMRG, fDMRG_routines.cpp:19-66) ---------------
  * cmps_dmrg_keep_blocks(d, 1) before the first growth step keeps the left
  * and right blocks of every length (BlocksStructure, kept in device memory
