@@ -65,7 +65,7 @@ def parse():
     p.add_argument("--precision", default="both", choices=["both", "fp64", "split_tf32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--idmrg-steps", type=int, default=4, help="timed iDMRG steps at full chi (0: skip)")
-    p.add_argument("--ising-steps", type=int, default=2, help="timed coupled-Ising iDMRG steps (0: skip)")
+    p.add_argument("--ising-steps", type=int, default=3, help="timed coupled-Ising iDMRG steps (0: skip)")
     p.add_argument("--ising-chi", type=int, default=64)
     return p.parse_args()
 
@@ -425,12 +425,13 @@ def main():
     return 0
 
 
-def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10):
+def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True):
     """iDMRG growth on the ladder MPO in FP64 and in mixed precision: `warm`
     untimed steps bring the bond dimension to chi, then `steps` timed ones.
     Step time is the library's device time of the whole step (environment
-    update, H_eff build, prediction, eigensolve, SVD; CUDA events), max over
-    ranks."""
+    update, H_eff build, prediction, eigensolve, SVD; CUDA events), the
+    median over the timed steps, max over ranks.  unit_cell: after the FP64 run, the unit cell of its last step
+    (energy per vertex, entropy, time)."""
     import torch
     from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32
     out = {"chi": chi, "warmup_steps": warm, "timed_steps": steps, "arnoldi_tol": tol, "krylov_dim": 24}
@@ -446,15 +447,25 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10):
             if i >= warm:
                 prof.append(run.profile())
                 wall.append(dt)
+        if name == "fp64" and unit_cell:
+            # Orthogonalise + iTwoVertexEnergy of the last step (iDMRG_DRV's
+            # per-step measurement), timed on the host (it synchronises)
+            t0 = time.perf_counter()
+            uc = run.unit_cell(tol=1e-12, krylov_dim=30)
+            out["unit_cell"] = dict(uc, ms=1e3 * (time.perf_counter() - t0))
         run.close()
         torch.cuda.empty_cache()
-        ms = float(np.mean([p["total_ms"] for p in prof]))
+        # median over the timed steps: a host-side stall in one step (allocator
+        # growth, a busy host) would otherwise dominate a mean over few steps
+        ms = float(np.median([p["total_ms"] for p in prof]))
         ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         if dist:
             dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
         keys = [k for k in prof[0] if k != "total_ms"]
-        out[name] = {"ms_per_step": float(ms_t.item()), "host_ms_per_step": 1e3 * float(np.mean(wall)),
+        out[name] = {"ms_per_step": float(ms_t.item()), "ms_per_step_mean": float(np.mean([p["total_ms"] for p in prof])),
+                     "host_ms_per_step": 1e3 * float(np.mean(wall)),
                      "chi": r["chi"], "energy_last": e[-1],
+                     "profile_median": {k: float(np.median([p[k] for p in prof])) for k in keys},
                      "profile_mean": {k: float(np.mean([p[k] for p in prof])) for k in keys}}
         energies[name] = np.array(e)
     rel = np.abs(energies["mixed"] - energies["fp64"]) / np.abs(energies["fp64"])

@@ -57,6 +57,31 @@ static int get_pool(cmps_context* ctx, SvdPool** out) {
       cusolverDnSetStream(w.sol, w.st);
       cublasSetStream(w.blas, w.st);
     }
+    // first use of a handle loads and sets up its kernels: do it here, once,
+    // with a 2 x 2 eigenproblem and GEMM per worker, not inside a step's SVD
+    cuDoubleComplex* a = nullptr;
+    double* wv = nullptr;
+    int* info = nullptr;
+    if (dmalloc(&a, sizeof(cuDoubleComplex) * 8) == cudaSuccess && dmalloc(&wv, sizeof(double) * 2) == cudaSuccess &&
+        dmalloc(&info, sizeof(int)) == cudaSuccess) {
+      const cuDoubleComplex id[4] = {{1, 0}, {0, 0}, {0, 0}, {1, 0}};
+      for (SvdWorker& w : p->w) {
+        cudaMemcpyAsync(a, id, sizeof(id), cudaMemcpyHostToDevice, w.st);
+        int lw = 0;
+        cusolverDnZheevd_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, 2, a, 2, wv, &lw);
+        cuDoubleComplex* work = nullptr;
+        if (dmalloc(&work, sizeof(cuDoubleComplex) * std::max(1, lw)) == cudaSuccess) {
+          cusolverDnZheevd(w.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, 2, a, 2, wv, work, lw, info);
+          const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+          cublasZgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_C, 2, 2, 2, &one, a, 2, a, 2, &zero, a + 4, 2);
+          cudaStreamSynchronize(w.st);
+          dfree(work);
+        }
+      }
+    }
+    if (a) dfree(a);
+    if (wv) dfree(wv);
+    if (info) dfree(info);
   }
   *out = (SvdPool*)ctx->svd_pool;
   return CMPS_OK;
@@ -476,7 +501,8 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     // bounded in total; otherwise the sectors run one by one.
     bool done = false;
     SvdPool* pool = nullptr;
-    if (n_eig >= 2 && get_pool(H.ctx, &pool) == CMPS_OK) {
+    const bool have_pool = get_pool(H.ctx, &pool) == CMPS_OK;  // set up on the first SVD, whatever its size
+    if (n_eig >= 2 && have_pool) {
       const int K = std::min<int>((int)pool->w.size(), n_eig);
       std::vector<int> order = todo;
       auto cost = [&](int m) {
