@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <map>
 #include <vector>
 
 #include "heff.h"
@@ -576,56 +577,69 @@ int unit_cell_measure(cmps_context* ctx, const SvdResult& S, const std::vector<d
   bl.gemm(CUBLAS_OP_T, CUBLAS_OP_N, dd, dd, c1 * c1, kOne, FT, c1 * c1, G, c1 * c1, kZero, T1, dd);
   bl.gemm(CUBLAS_OP_T, CUBLAS_OP_N, dd, dd, c0 * c0, kOne, PT, c0 * c0, Q, c0 * c0, kZero, T2, dd);
   if (bl.st != CMPS_OK) return bl.st;
-  std::vector<cplx> h1((size_t)dd * dd), h2((size_t)dd * dd);
-  cudaMemcpyAsync(h1.data(), T1, sizeof(cplx) * dd * dd, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(h2.data(), T2, sizeof(cplx) * dd * dd, cudaMemcpyDeviceToHost, st);
-  CMPS_CUDA(cudaStreamSynchronize(st));
-  auto t1 = [&](int s1p, int s1, int s2, int s2p) {
-    const cplx v = h1[(s1p + (size_t)d * s1) + (size_t)dd * (s2 + (size_t)d * s2p)];
-    return zc(v.x, v.y);
+  // Contract the tables with the MPO blocks on the device.  Operator O[s', s]
+  // as a pair vector: site 0 of a cell reads pairs (s', s) = s' + d s of the
+  // first table index; site 1 reads pairs (s, s') = s + d s' of the second.
+  // Columns of Cm: ColX_k in second-index order; of Rm: RowX_k in first-index
+  // order.  V1 = T1 [Cm | e | h'] and V2 = T2 Cm, with e the identity pairs
+  // (s, s) and h' = H1 in second-index order; everything else is dot products
+  // of these few columns on the host.
+  std::map<std::pair<int, int>, std::vector<zc>> blocks;
+  for (const WEntry& e : W) {
+    if (!((e.bl == D - 1 && e.br >= 0 && e.br <= D - 2) || (e.br == 0 && e.bl >= 1 && e.bl <= D - 1))) continue;
+    auto& O = blocks[{e.bl, e.br}];
+    if (O.empty()) O.assign((size_t)dd, 0.0);
+    O[e.sp + (size_t)d * e.s] += zc(e.wr, e.wi);  // O[s', s]
+  }
+  auto second = [&](const std::vector<zc>& O) {  // O[s', s] at s + d s'
+    std::vector<zc> v((size_t)dd);
+    for (int sp = 0; sp < d; ++sp)
+      for (int sv = 0; sv < d; ++sv) v[sv + (size_t)d * sp] = O[sp + (size_t)d * sv];
+    return v;
   };
-  auto t2 = [&](int s2p, int s2, int s1, int s1p) {
-    const cplx v = h2[(s2p + (size_t)d * s2) + (size_t)dd * (s1 + (size_t)d * s1p)];
-    return zc(v.x, v.y);
-  };
-  // MPO blocks as d x d operators O[s', s]
-  auto block = [&](int bl_, int br_) {
-    std::vector<zc> O((size_t)d * d, 0.0);
-    for (const WEntry& e : W)
-      if (e.bl == bl_ && e.br == br_) O[e.sp + (size_t)d * e.s] += zc(e.wr, e.wi);
-    return O;
-  };
-  const std::vector<zc> H1 = block(D - 1, 0);
-  zc norm = 0.0, local = 0.0, bond1 = 0.0, bond2 = 0.0;
-  for (int s1 = 0; s1 < d; ++s1)
-    for (int s2 = 0; s2 < d; ++s2) norm += t1(s1, s1, s2, s2);
-  for (int a = 0; a < d; ++a)
-    for (int b = 0; b < d; ++b) {
-      const zc h = H1[a + (size_t)d * b];  // H1[s', s]
-      if (h == zc(0.0)) continue;
-      for (int s = 0; s < d; ++s) {
-        local += h * t1(a, b, s, s);  // site 0
-        local += h * t1(s, s, b, a);  // site 1
-      }
-    }
+  std::vector<std::vector<zc>> Rcols, Ccols;
   for (int kb = 1; kb <= D - 2; ++kb) {
-    const std::vector<zc> Rx = block(D - 1, kb), Cx = block(kb, 0);
-    bool any_r = false, any_c = false;
-    for (const zc& v : Rx) any_r |= v != zc(0.0);
-    for (const zc& v : Cx) any_c |= v != zc(0.0);
-    if (!any_r || !any_c) continue;
-    for (int a = 0; a < d; ++a)
-      for (int b = 0; b < d; ++b) {
-        const zc r = Rx[a + (size_t)d * b];
-        if (r == zc(0.0)) continue;
-        for (int e = 0; e < d; ++e)
-          for (int f = 0; f < d; ++f) {
-            const zc cc = Cx[e + (size_t)d * f];
-            if (cc == zc(0.0)) continue;
-            bond1 += r * cc * t1(a, b, f, e);   // RowX on site 0, ColX on site 1
-            bond2 += r * cc * t2(a, b, f, e);   // RowX on site 1, ColX on the next site 0
-          }
-      }
+    auto r = blocks.find({D - 1, kb}), c2 = blocks.find({kb, 0});
+    if (r == blocks.end() || c2 == blocks.end()) continue;
+    Rcols.push_back(r->second);
+    Ccols.push_back(second(c2->second));
+  }
+  std::vector<zc> H1((size_t)dd, 0.0);
+  if (blocks.count({D - 1, 0})) H1 = blocks[{D - 1, 0}];
+  std::vector<zc> ess((size_t)dd, 0.0);
+  for (int sv = 0; sv < d; ++sv) ess[sv + (size_t)d * sv] = 1.0;
+  const int64_t nk = (int64_t)Rcols.size();
+  const int64_t ncol = nk + 2;
+  std::vector<cplx> rhs((size_t)dd * ncol);
+  auto put = [&](int64_t col, const std::vector<zc>& v) {
+    for (int64_t p = 0; p < dd; ++p) rhs[p + (size_t)dd * col] = make_cuDoubleComplex(v[p].real(), v[p].imag());
+  };
+  for (int64_t k = 0; k < nk; ++k) put(k, Ccols[k]);
+  put(nk, ess);
+  put(nk + 1, second(H1));
+  cplx *d_rhs, *V1, *V2;
+  CMPS_TRY(alloc(&d_rhs, sizeof(cplx) * dd * ncol));
+  CMPS_TRY(alloc(&V1, sizeof(cplx) * dd * ncol));
+  CMPS_TRY(alloc(&V2, sizeof(cplx) * dd * std::max<int64_t>(1, nk)));
+  CMPS_TRY(copy_wait(d_rhs, rhs.data(), sizeof(cplx) * dd * ncol, cudaMemcpyHostToDevice, st));
+  bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, dd, ncol, dd, kOne, T1, dd, d_rhs, dd, kZero, V1, dd);
+  if (nk) bl.gemm(CUBLAS_OP_N, CUBLAS_OP_N, dd, nk, dd, kOne, T2, dd, d_rhs, dd, kZero, V2, dd);
+  if (bl.st != CMPS_OK) return bl.st;
+  std::vector<cplx> hv1((size_t)dd * ncol), hv2((size_t)dd * std::max<int64_t>(1, nk));
+  cudaMemcpyAsync(hv1.data(), V1, sizeof(cplx) * dd * ncol, cudaMemcpyDeviceToHost, st);
+  if (nk) cudaMemcpyAsync(hv2.data(), V2, sizeof(cplx) * dd * nk, cudaMemcpyDeviceToHost, st);
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  auto dot = [&](const std::vector<zc>& u, const std::vector<cplx>& M, int64_t col) {
+    zc acc = 0.0;
+    for (int64_t p = 0; p < dd; ++p) acc += u[p] * zc(M[p + (size_t)dd * col].x, M[p + (size_t)dd * col].y);
+    return acc;
+  };
+  zc norm = dot(ess, hv1, nk);                       // sum_{s1,s2} T1[(s1,s1),(s2,s2)] = eta Tr[l r]
+  zc local = dot(H1, hv1, nk) + dot(ess, hv1, nk + 1);  // H1 on site 0, on site 1
+  zc bond1 = 0.0, bond2 = 0.0;
+  for (int64_t k = 0; k < nk; ++k) {
+    bond1 += dot(Rcols[k], hv1, k);   // RowX on site 0, ColX on site 1
+    bond2 += dot(Rcols[k], hv2, k);   // RowX on site 1, ColX on the next cell's site 0
   }
   const double eta = eta_l.real();
   const zc e = 0.5 * (local + bond1 + bond2 / eta) / norm;
