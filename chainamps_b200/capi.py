@@ -116,6 +116,7 @@ _SIGS = {
     "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
     "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
     "cmps_dmrg_unit_cell": (C.c_int, [C.c_void_p, C.c_double, C.c_int, c_dblp]),
+    "cmps_heff_set_projectors": (C.c_int, [C.c_void_p, C.c_int, c_dblp, c_dblp]),
     "cmps_heff_sector_table": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_dblp]),
     "cmps_heff_set_owned": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -267,6 +268,19 @@ class TwoVertexComponents:
         """Device pointers (ints) to n complex doubles each."""
         _check(lib.cmps_heff_apply_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
                                           C.c_void_p(stream) if stream else None))
+
+    def set_projectors(self, tensors, weights):
+        """ProjectorTensors: every application of H_eff adds
+        sum_p w_p (P_p . x) conj(P_p) (DMRG_routines.cpp:947-973).  tensors:
+        vectors of length n in ARPACK order; an empty list removes them."""
+        P = np.ascontiguousarray(np.asarray(tensors, np.complex128).reshape(-1, self.n)) if len(tensors) else \
+            np.zeros((0, self.n), np.complex128)
+        w = np.ascontiguousarray(np.asarray(weights, np.float64).reshape(-1))
+        if w.size != P.shape[0]:
+            raise ValueError("one weight per projector tensor")
+        pv = P.view(np.float64) if P.size else np.zeros(2, np.float64)
+        wv = w if w.size else np.zeros(1, np.float64)
+        _check(lib.cmps_heff_set_projectors(self.h, P.shape[0], _p(pv, C.c_double), _p(wv, C.c_double)))
 
     def sector_table(self):
         """theta layout: (offsets[n_sectors + 1], flops[n_sectors]); output

@@ -251,11 +251,18 @@ int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out
   if (H.precision == CMPS_SPLIT_TF32) {
     rc = apply_split_stage(H, 1, in, out, st);
     if (rc == CMPS_OK) rc = apply_split_stage(H, 2, in, out, st);
+    if (rc == CMPS_OK) rc = H.add_projectors(in, out, st);
   } else {
     rc = H.apply_theta_fp64(in, out, st);
   }
   in.d = out.d = nullptr;
   return rc;
+}
+
+int cmps_heff_set_projectors(cmps_heff* h, int count, const double* tensors, const double* weights) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->set_projectors(count, tensors, weights);
 }
 
 int cmps_heff_theta_from_arpack(cmps_heff* h, const double* d_arpack, double* d_theta, void* stream) {

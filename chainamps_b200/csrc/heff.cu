@@ -234,6 +234,9 @@ Heff::~Heff() {
   y.release();
   theta.release();
   kv.release();
+  proj.release();
+  if (d_proj) dfree(d_proj);
+  d_proj = nullptr;
   stage1.release();
   stage2.release();
   ops.release();
@@ -860,13 +863,78 @@ int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
   if (precision == CMPS_SPLIT_TF32) return apply_split(*this, in, out, st);
   CMPS_TRY(apply_stage(1, in, out, st));
   CMPS_TRY(apply_stage(2, in, out, st));
+  return add_projectors(in, out, st);
+}
+
+int Heff::apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st) {
+  CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
+  CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
   return CMPS_OK;
 }
 
 int Heff::apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st) {
-  CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
-  CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
+  CMPS_TRY(apply_fp64_stages(in, out, st));
+  return add_projectors(in, out, st);
+}
+
+namespace {
+// h[2p], h[2p+1] = -w_p * c_p (c_p = <phi_p, x>), for the subtracting multi-axpy
+__global__ void k_proj_coef(const double* __restrict__ c, const double* __restrict__ w, int np,
+                            double* __restrict__ h) {
+  const int p = threadIdx.x;
+  if (p < np) {
+    h[2 * p] = -w[p] * c[2 * p];
+    h[2 * p + 1] = -w[p] * c[2 * p + 1];
+  }
+}
+}  // namespace
+
+int Heff::set_projectors(int np, const double* host_arpack, const double* weights) {
+  CMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  proj.release();
+  if (d_proj) dfree(d_proj);
+  d_proj = nullptr;
+  proj_np = 0;
+  proj_w.clear();
+  if (np == 0) return CMPS_OK;
+  if (np < 0 || np > 64) return fail(CMPS_ERR_ARG, "projectors: between 0 and 64 of them");
+  if (!host_arpack || !weights) return fail(CMPS_ERR_ARG, "projectors: null argument");
+  const int64_t n = th.total;
+  CMPS_TRY(proj.alloc((int64_t)np * n));
+  CMPS_CUDA(dmalloc(&d_proj, sizeof(double) * (3 * (size_t)np + 4)));
+  cudaStream_t st = ctx->stream;
+  std::vector<double> buf(2 * (size_t)n_allowed);
+  for (int p = 0; p < np; ++p) {
+    const double* src = host_arpack + 2 * (size_t)n_allowed * p;
+    for (int64_t i = 0; i < n_allowed; ++i) {  // phi = conj(P)
+      buf[2 * i] = src[2 * i];
+      buf[2 * i + 1] = -src[2 * i + 1];
+    }
+    CMPS_TRY(copy_wait(d_io, buf.data(), sizeof(double) * 2 * n_allowed, cudaMemcpyHostToDevice, st));
+    Planar v;
+    v.d = proj.d + 2 * n * p;
+    v.len = n;
+    const int rc = pack(d_io, v, st);
+    v.d = nullptr;
+    CMPS_TRY(rc);
+  }
+  proj_w.assign(weights, weights + np);
+  CMPS_TRY(copy_wait(d_proj, proj_w.data(), sizeof(double) * np, cudaMemcpyHostToDevice, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  proj_np = np;
   return CMPS_OK;
+}
+
+int Heff::add_projectors(const Planar& in, Planar& out, cudaStream_t st) {
+  if (!proj_np) return CMPS_OK;
+  const int64_t n = th.total;
+  // d_proj: weights [0, np), then c = <phi_p, x> (2 np) and |x|^2, then one
+  // scratch norm; the coefficients are turned into -w_p c_p in place
+  double* c = d_proj + proj_np;
+  CMPS_TRY(ops.mdot_dev(proj.d, proj.d + n, 2 * n, proj_np, in.re(), in.im(), c, st));
+  k_proj_coef<<<1, 64, 0, st>>>(c, d_proj, proj_np, c);
+  CMPS_CUDA(cudaGetLastError());
+  return ops.maxpy_norm_dev(proj.d, proj.d + n, 2 * n, proj_np, c, out.re(), out.im(), c + 2 * proj_np + 1, st);
 }
 
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
@@ -875,6 +943,7 @@ int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
   if (precision == CMPS_SPLIT_TF32) {
     CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
     CMPS_TRY(apply_split_stage(*this, 2, x, y, st));
+    CMPS_TRY(add_projectors(x, y, st));
   } else {
     CMPS_TRY(apply_theta(x, y, st));
   }

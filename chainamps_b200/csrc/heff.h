@@ -110,6 +110,18 @@ struct Heff {
   int build_plans();
   int set_owned(const uint8_t* mask);
   bool all_owned() const;
+  // Excited-state projectors (TwoVertexComponents::ProjectorTensors,
+  // DMRG_routines.hpp:205): the matvec adds sum_p w_p (P_p . x) conj(P_p),
+  // the bilinear product P . x taken without conjugation
+  // (DMRG_routines.cpp:947-973).  Stored as phi_p = conj(P_p) in the theta
+  // layout (vector p: re plane at proj.d + 2 p n, im plane n further), so the
+  // term is sum_p w_p phi_p <phi_p, x>.
+  Planar proj;
+  int proj_np = 0;
+  double* d_proj = nullptr;  // weights [np], coefficients [2 np + 4]
+  std::vector<double> proj_w;
+  int set_projectors(int np, const double* host_arpack, const double* weights);
+  int add_projectors(const Planar& in, Planar& out, cudaStream_t st);
   double flops_canonical = 0.0, flops_executed = 0.0;
   int precision = CMPS_FP64;
   SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)
@@ -137,7 +149,8 @@ struct Heff {
   int parse_mpo(const cmps_mpx_desc* Wd);
   int finish();  // sector structure, LeftPart/RightPart, GEMM plans (L, R, W set)
   int apply_theta(const Planar& in, Planar& out, cudaStream_t st);  // theta-space matvec
-  int apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st);
+  int apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st);   // with the projectors
+  int apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st);  // the two GEMM stages only
   int apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st);  // 1: T = LP in, 2: out = T RP
   int apply_host(const double* in, double* out);
   int apply_device(const double* din, double* dout, cudaStream_t st);

@@ -566,7 +566,7 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   CMPS_TRY(split_theta(*S, in, st));
   CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st));
   CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->buf + S->ts_off, S->ts_len, S->d_err, st));
-  return CMPS_OK;
+  return H.add_projectors(in, out, st);
 }
 
 // theta-space matvec in split precision: FP64 planar in -> FP64 planar out.

@@ -128,6 +128,17 @@ int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
  * first call before any stream capture.  All calls share the array: calls
  * that overlap on the GPU race.  Nothing in it needs to start at zero. */
 int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, double* d_out, void* stream);
+/* Excited-state projectors: TwoVertexComponents::ProjectorTensors
+ * (DMRG_routines.hpp:205, built by ProjectorBlocks::makePTensor, :830).
+ * count tensors P_p (each n_allowed interleaved complex in ARPACK order, the
+ * layout of TwoVertexMPOMPSMultiply's vectors) with weights w_p: every
+ * application of H_eff -- cmps_heff_apply[_device], the theta-layout apply and
+ * the eigensolver's steps, FP64 and split-TF32 -- adds
+ * sum_p w_p (P_p . x) conj(P_p), with the product P_p . x taken without
+ * conjugation (DMRG_routines.cpp:947-973).  count = 0 removes them; at most
+ * 64.  The adjoint (dE/dlambda) ignores them, as they do not depend on the
+ * coupling; the no-allocation matvec refuses a handle that has them. */
+int cmps_heff_set_projectors(cmps_heff* h, int count, const double* tensors, const double* weights);
 /* Sharding the matvec by output sector (no reference counterpart: the
  * reference matvec runs on one host).  In the theta layout a vector is
  * planar -- `total` real parts, then `total` imaginary parts -- and output
