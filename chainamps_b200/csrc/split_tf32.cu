@@ -213,6 +213,16 @@ void release_split(Heff* h) {
   h->split = nullptr;
 }
 
+#ifndef CMPS_FUSE_MAX_SEG_N1
+#define CMPS_FUSE_MAX_SEG_N1 64
+#endif
+#ifndef CMPS_FUSE_MAX_SEG_N2
+#define CMPS_FUSE_MAX_SEG_N2 64
+#endif
+// widest task (column count) that is fused with others along N, per stage
+constexpr int32_t kFuseMaxSegN1 = CMPS_FUSE_MAX_SEG_N1;
+constexpr int32_t kFuseMaxSegN2 = CMPS_FUSE_MAX_SEG_N2;
+
 static int build_split(Heff& H) {
   CMPS_TRY(encoder());
   const Rules& r = H.rules;
@@ -248,17 +258,6 @@ static int build_split(Heff& H) {
       s1a_chunk[{m, s1}] = s1a;
       s1a += align32(S->ncols_pad[m] * S->ldS[s]);
     }
-  std::map<std::array<int, 4>, int64_t> lps_blk;
-  std::vector<SplitBlock> lpsb;
-  int64_t lps = 0;
-  for (auto& kv : H.lp_off) {
-    const auto& key = kv.first;  // (b1, s1', s1, s)
-    int s = key[3];
-    int sp = A0.find(r.sub(r.add(r.add(A0.sq[s], H.sigq[key[2]]), H.bq[key[0]]), H.sigq[key[1]]));
-    lps_blk[key] = lps;
-    lpsb.push_back(SplitBlock{kv.second, lps, (int32_t)A0.sdim[sp], (int32_t)A0.sdim[s], (int32_t)S->ldS[s], 0});
-    lps += align32(A0.sdim[sp] * S->ldS[s]);
-  }
   std::vector<int64_t> ts_base((size_t)H.D * nm, -1);
   int64_t ts = 0;
   for (int b1 = 0; b1 < H.D; ++b1)
@@ -268,17 +267,148 @@ static int build_split(Heff& H) {
       ts_base[(size_t)b1 * nm + m] = ts;
       ts += align32(th.nrows[mp] * S->ncols_pad[m]);
     }
-  std::map<std::array<int, 4>, int64_t> rpt_blk;
-  std::vector<SplitBlock> rptb;
-  int64_t rpt = 0;
-  for (auto& kv : H.rp_off) {
-    const auto& key = kv.first;  // (b1, s2, s2', t)
-    int t = key[3];
-    int tp = A2.find(r.sub(r.add(r.add(A2.sq[t], H.sigq[key[2]]), H.bq[key[0]]), H.sigq[key[1]]));
-    rpt_blk[key] = rpt;
-    // RP block is [a2][a2'] (dim t x dim t'); stored transposed [a2'][a2], ld = pad4(dim t)
-    rptb.push_back(SplitBlock{kv.second, rpt, (int32_t)A2.sdim[t], (int32_t)A2.sdim[tp], (int32_t)S->ldR[t], 1});
-    rpt += align32(A2.sdim[tp] * S->ldR[t]);
+  // ---- tasks, fused along N ----
+  // A stage-1 task (b1, sigma1') computes rows sigma1' of T^{b1}_m; a stage-2
+  // task (m', sigma2') columns sigma2' of theta'_m'.  Tasks of one stage whose
+  // term lists read the same A tiles (stage 1: the same m and sigma1 list;
+  // stage 2: the same m' and (b1, sigma2) list) are fused into one task of up
+  // to four column segments and N <= 128: the A tiles, the larger operand for
+  // narrow sectors, are then loaded once for all of them.  Each fused term's
+  // B rows are laid out contiguously (one tensor map per fused term), and the
+  // epilogue sends each column to its segment's output.
+  struct Seg {
+    int64_t out_off;
+    int32_t n;
+    std::vector<std::array<int, 4>> keys;  // LP / RP block of every term
+  };
+  struct Fused {
+    int m = 0;                             // stage 1: m; stage 2: m'
+    int32_t ntot = 0;
+    std::vector<std::array<int, 4>> tk;    // stage 1: (s1, s, 0, 0); stage 2: (b1, m, s2, t)
+    std::vector<Seg> segs;
+  };
+  auto fuse = [](std::vector<std::pair<std::vector<int64_t>, std::pair<Fused, Seg>>>& raw, int32_t max_seg_n) {
+    // raw: (signature, (task shape, its segment)) in creation order
+    std::map<std::vector<int64_t>, std::vector<size_t>> groups;
+    std::vector<std::vector<int64_t>> order;
+    for (size_t i = 0; i < raw.size(); ++i) {
+      auto it = groups.find(raw[i].first);
+      if (it == groups.end()) {
+        order.push_back(raw[i].first);
+        groups[raw[i].first].push_back(i);
+      } else {
+        it->second.push_back(i);
+      }
+    }
+    std::vector<Fused> out;
+    for (const auto& sig : order) {
+      Fused cur;
+      bool open = false;
+      for (size_t i : groups[sig]) {
+        Seg& sg = raw[i].second.second;
+        const bool fits = open && sg.n <= max_seg_n && cur.ntot + sg.n <= 128 && cur.segs.size() < 4 &&
+                          cur.segs[0].n <= max_seg_n;
+        if (!fits) {
+          if (open) out.push_back(std::move(cur));
+          cur = raw[i].second.first;
+          cur.ntot = 0;
+          cur.segs.clear();
+          open = true;
+        }
+        cur.ntot += sg.n;
+        cur.segs.push_back(std::move(sg));
+      }
+      if (open) out.push_back(std::move(cur));
+    }
+    return out;
+  };
+  std::vector<Fused> f1, f2;
+  {
+    std::vector<std::pair<std::vector<int64_t>, std::pair<Fused, Seg>>> raw;
+    for (int b1 = 0; b1 < H.D; ++b1)
+      for (int m = 0; m < nm; ++m) {
+        const int64_t tb = ts_base[(size_t)b1 * nm + m];
+        if (tb < 0) continue;
+        const int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+        for (int s1p = 0; s1p < d; ++s1p) {
+          if (th.rowoff[mp][s1p] < 0) continue;
+          const int sp = A0.find(r.sub(th.mq[mp], H.sigq[s1p]));
+          Fused shape;
+          shape.m = m;
+          Seg sg{tb + th.rowoff[mp][s1p] * S->ncols_pad[m], (int32_t)A0.sdim[sp], {}};
+          std::vector<int64_t> sig{(int64_t)m};
+          for (int s1 = 0; s1 < d; ++s1) {
+            if (th.rowoff[m][s1] < 0) continue;
+            const int sa = A0.find(r.sub(th.mq[m], H.sigq[s1]));
+            if (!H.lp_off.count({b1, s1p, s1, sa})) continue;
+            shape.tk.push_back({s1, sa, 0, 0});
+            sg.keys.push_back({b1, s1p, s1, sa});
+            sig.push_back(s1);
+          }
+          raw.push_back({sig, {shape, sg}});
+        }
+      }
+    f1 = fuse(raw, kFuseMaxSegN1);
+  }
+  {
+    std::vector<std::pair<std::vector<int64_t>, std::pair<Fused, Seg>>> raw;
+    for (int mp = 0; mp < nm; ++mp)
+      for (int s2p = 0; s2p < d; ++s2p) {
+        if (th.coloff[mp][s2p] < 0 || !H.owned[mp]) continue;  // output sectors of this shard only
+        const int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
+        Fused shape;
+        shape.m = mp;
+        Seg sg{th.base[mp] + th.coloff[mp][s2p], (int32_t)A2.sdim[tp], {}};
+        std::vector<int64_t> sig{(int64_t)mp};
+        for (int b1 = 0; b1 < H.D; ++b1) {
+          const int m = th.find(r.sub(th.mq[mp], H.bq[b1]));
+          if (m < 0 || ts_base[(size_t)b1 * nm + m] < 0) continue;
+          for (int s2 = 0; s2 < d; ++s2) {
+            if (th.coloff[m][s2] < 0) continue;
+            const int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
+            if (!H.rp_off.count({b1, s2, s2p, t})) continue;
+            shape.tk.push_back({b1, m, s2, t});
+            sg.keys.push_back({b1, s2, s2p, t});
+            sig.push_back((int64_t)b1 * 65536 + s2);
+          }
+        }
+        raw.push_back({sig, {shape, sg}});
+      }
+    f2 = fuse(raw, kFuseMaxSegN2);
+  }
+  // LPS / RPTS: one block per fused term, rows = the fused N (segment rows in
+  // order), ld = pad4(K); every LP / RP block is split into its segment's rows
+  std::vector<SplitBlock> lpsb, rptb;
+  std::vector<std::vector<int64_t>> f1_base(f1.size()), f2_base(f2.size());
+  int64_t lps = 0, rpt = 0;
+  for (size_t i = 0; i < f1.size(); ++i) {
+    const Fused& f = f1[i];
+    for (size_t q = 0; q < f.tk.size(); ++q) {
+      const int sa = f.tk[q][1];
+      const int64_t ld = S->ldS[sa];
+      f1_base[i].push_back(lps);
+      int64_t row = 0;
+      for (const Seg& sg : f.segs) {
+        lpsb.push_back(SplitBlock{H.lp_off.at(sg.keys[q]), lps + row * ld, sg.n, (int32_t)A0.sdim[sa], (int32_t)ld, 0});
+        row += sg.n;
+      }
+      lps += align32(f.ntot * ld);
+    }
+  }
+  for (size_t i = 0; i < f2.size(); ++i) {
+    const Fused& f = f2[i];
+    for (size_t q = 0; q < f.tk.size(); ++q) {
+      const int t = f.tk[q][3];
+      const int64_t ld = S->ldR[t];
+      f2_base[i].push_back(rpt);
+      int64_t row = 0;
+      for (const Seg& sg : f.segs) {
+        // RP block is [a2][a2'] (dim t x dim t'); stored transposed [a2'][a2]
+        rptb.push_back(SplitBlock{H.rp_off.at(sg.keys[q]), rpt + row * ld, (int32_t)A2.sdim[t], sg.n, (int32_t)ld, 1});
+        row += sg.n;
+      }
+      rpt += align32(f.ntot * ld);
+    }
   }
   S->s1a_off = 0;
   S->s1a_len = align32(std::max<int64_t>(s1a, 32));
@@ -370,51 +500,45 @@ static int build_split(Heff& H) {
     amap1[kv.first] = (int32_t)p1.amaps.size();
     p1.amaps.push_back(cm);
   }
-  std::map<std::array<int, 4>, int32_t> bmap1;
   std::vector<int32_t> b1_rows, b2_rows;  // row extent of every B map (= its task's N)
-  for (size_t i = 0; i < lpsb.size(); ++i) {
-    const SplitBlock& b = lpsb[i];
-    CUtensorMap cm;
-    CMPS_TRY(make_map(S->buf + S->lps_off, b.dst_off, b.cols, b.rows, b.ld_dst, S->lps_len, &cm,
-                      tc::b_box_rows(b.rows)));
-    p1.bmaps.push_back(cm);
-    b1_rows.push_back(b.rows);
-  }
-  {
-    int32_t i = 0;
-    for (auto& kv : lps_blk) bmap1[kv.first] = i++;  // same order as lpsb (both follow lp_off order)
-  }
-  for (int b1 = 0; b1 < H.D; ++b1)
-    for (int m = 0; m < nm; ++m) {
-      const int64_t tb = ts_base[(size_t)b1 * nm + m];
-      if (tb < 0) continue;
-      int mp = th.find(r.add(th.mq[m], H.bq[b1]));
-      for (int s1p = 0; s1p < d; ++s1p) {
-        if (th.rowoff[mp][s1p] < 0) continue;
-        int sp = A0.find(r.sub(th.mq[mp], H.sigq[s1p]));
-        tc::TcTask task{};
-        task.out_off = tb + th.rowoff[mp][s1p] * S->ncols_pad[m];
-        task.row_stride = 1;
-        task.col_stride = S->ncols_pad[m];
-        task.m = (int32_t)S->ncols_pad[m];
-        task.n = (int32_t)A0.sdim[sp];
-        task.t0 = (int32_t)p1.terms.size();
-        for (int s1 = 0; s1 < d; ++s1) {
-          if (th.rowoff[m][s1] < 0) continue;
-          int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
-          auto it = bmap1.find({b1, s1p, s1, s});
-          if (it == bmap1.end()) continue;
-          p1.terms.push_back(tc::TcTerm{amap1[{m, s1}], it->second, 0, (int32_t)A0.sdim[s]});
-        }
-        task.t1 = (int32_t)p1.terms.size();
-        // output range check (four planes of TS)
-        if (task.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(task.n - 1) * task.col_stride >=
-            S->ts_len)
-          return fail(CMPS_ERR_STATE, "stage-1 output outside TS");
-        add_tiles(p1, (int32_t)p1.tasks.size(), task.m, task.n);
-        p1.tasks.push_back(task);
-      }
+  auto set_segments = [](tc::TcTask& task, const std::vector<Seg>& segs) {
+    task.nseg = (int32_t)segs.size();
+    int32_t col = 0;
+    for (int q = 0; q < 4; ++q) {
+      task.seg_n0[q] = q < (int)segs.size() ? col : 0x7fffffff;
+      task.seg_off[q] = q < (int)segs.size() ? segs[q].out_off : 0;
+      if (q < (int)segs.size()) col += segs[q].n;
     }
+    task.out_off = segs[0].out_off;
+  };
+  for (size_t i = 0; i < f1.size(); ++i) {
+    const Fused& f = f1[i];
+    const int m = f.m;
+    tc::TcTask task{};
+    set_segments(task, f.segs);
+    task.row_stride = 1;
+    task.col_stride = S->ncols_pad[m];
+    task.m = (int32_t)S->ncols_pad[m];
+    task.n = f.ntot;
+    task.t0 = (int32_t)p1.terms.size();
+    for (size_t q = 0; q < f.tk.size(); ++q) {
+      const int s1 = f.tk[q][0], sa = f.tk[q][1];
+      CUtensorMap cm;
+      CMPS_TRY(make_map(S->buf + S->lps_off, f1_base[i][q], A0.sdim[sa], f.ntot, S->ldS[sa], S->lps_len, &cm,
+                        tc::b_box_rows(f.ntot)));
+      p1.terms.push_back(tc::TcTerm{amap1[{m, s1}], (int32_t)p1.bmaps.size(), 0, (int32_t)A0.sdim[sa]});
+      p1.bmaps.push_back(cm);
+      b1_rows.push_back(f.ntot);
+    }
+    task.t1 = (int32_t)p1.terms.size();
+    // output range check of every segment (two planes of TS)
+    for (const Seg& sg : f.segs)
+      if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
+                                S->ts_len)
+        return fail(CMPS_ERR_STATE, "stage-1 output outside TS");
+    add_tiles(p1, (int32_t)p1.tasks.size(), task.m, task.n);
+    p1.tasks.push_back(task);
+  }
   // ---- stage 2 plan: C2[l', a2'] = sum TS[l', r_pad] RPTS[a2', a2] ----
   tc::TcPlan& p2 = S->p2;
   std::vector<int32_t> amap2((size_t)H.D * nm, -1);
@@ -430,51 +554,36 @@ static int build_split(Heff& H) {
       amap2[(size_t)b1 * nm + m] = (int32_t)p2.adescs.size();
       p2.adescs.push_back(ad);
     }
-  std::map<std::array<int, 4>, int32_t> bmap2;
-  {
-    int32_t i = 0;
-    for (auto& kv : rpt_blk) {
-      const SplitBlock& b = rptb[i];
+  for (size_t i = 0; i < f2.size(); ++i) {
+    const Fused& f = f2[i];
+    const int mp = f.m;
+    tc::TcTask task{};
+    set_segments(task, f.segs);
+    task.row_stride = th.ncols[mp];
+    task.col_stride = 1;
+    task.m = (int32_t)th.nrows[mp];
+    task.n = f.ntot;
+    task.t0 = (int32_t)p2.terms.size();
+    for (size_t q = 0; q < f.tk.size(); ++q) {
+      const int b1 = f.tk[q][0], m = f.tk[q][1], s2 = f.tk[q][2], t = f.tk[q][3];
+      const int32_t am = amap2[(size_t)b1 * nm + m];
+      if (am < 0) return fail(CMPS_ERR_STATE, "stage-2 term without its T block");
       CUtensorMap cm;
-      // destination layout [a2'][a2]: rows = dim t', K = dim t
-      CMPS_TRY(make_map(S->buf + S->rpt_off, b.dst_off, b.rows, b.cols, b.ld_dst, S->rpt_len, &cm,
-                        tc::b_box_rows(b.cols)));
+      // destination layout [a2'][a2]: rows = fused N, K = dim t
+      CMPS_TRY(make_map(S->buf + S->rpt_off, f2_base[i][q], A2.sdim[t], f.ntot, S->ldR[t], S->rpt_len, &cm,
+                        tc::b_box_rows(f.ntot)));
+      p2.terms.push_back(tc::TcTerm{am, (int32_t)p2.bmaps.size(), (int32_t)S->coloff_pad[m][s2], (int32_t)A2.sdim[t]});
       p2.bmaps.push_back(cm);
-      b2_rows.push_back(b.cols);
-      bmap2[kv.first] = i++;
+      b2_rows.push_back(f.ntot);
     }
-  }
-  for (int mp = 0; mp < nm; ++mp)
-    for (int s2p = 0; s2p < d; ++s2p) {
-      if (th.coloff[mp][s2p] < 0 || !H.owned[mp]) continue;  // output sectors of this shard only
-      int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
-      tc::TcTask task{};
-      task.out_off = th.base[mp] + th.coloff[mp][s2p];
-      task.row_stride = th.ncols[mp];
-      task.col_stride = 1;
-      task.m = (int32_t)th.nrows[mp];
-      task.n = (int32_t)A2.sdim[tp];
-      task.t0 = (int32_t)p2.terms.size();
-      for (int b1 = 0; b1 < H.D; ++b1) {
-        int m = th.find(r.sub(th.mq[mp], H.bq[b1]));
-        if (m < 0) continue;
-        const int32_t am = amap2[(size_t)b1 * nm + m];
-        if (am < 0) continue;
-        for (int s2 = 0; s2 < d; ++s2) {
-          if (th.coloff[m][s2] < 0) continue;
-          int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
-          auto it = bmap2.find({b1, s2, s2p, t});
-          if (it == bmap2.end()) continue;
-          p2.terms.push_back(tc::TcTerm{am, it->second, (int32_t)S->coloff_pad[m][s2], (int32_t)A2.sdim[t]});
-        }
-      }
-      task.t1 = (int32_t)p2.terms.size();
-      if (task.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(task.n - 1) * task.col_stride >=
-          th.total)
+    task.t1 = (int32_t)p2.terms.size();
+    for (const Seg& sg : f.segs)
+      if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
+                                th.total)
         return fail(CMPS_ERR_STATE, "stage-2 output outside theta");
-      add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
-      p2.tasks.push_back(task);
-    }
+    add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
+    p2.tasks.push_back(task);
+  }
   // k-steps per tile (the MMA warp walks them without term lookups)
   for (tc::TcPlan* p : {&p1, &p2})
     for (tc::TcTile& t : p->tiles) {
@@ -506,6 +615,17 @@ static int build_split(Heff& H) {
     for (const tc::TcTask& t : p->tasks)
       if (t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)p->terms.size() || t.m < 1 || t.n < 1 || t.out_off < 0)
         return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
+    // segments: start at column 0, increase, cover N; a task wider than one
+    // 128-column tile has a single segment
+    for (const tc::TcTask& t : p->tasks) {
+      if (t.nseg < 1 || t.nseg > 4 || t.seg_n0[0] != 0 || t.seg_off[0] != t.out_off || (t.nseg > 1 && t.n > 128))
+        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
+      for (int q = 1; q < 4; ++q) {
+        if (q < t.nseg ? (t.seg_n0[q] <= t.seg_n0[q - 1] || t.seg_n0[q] >= t.n || t.seg_off[q] < 0)
+                       : t.seg_n0[q] != 0x7fffffff)
+          return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
+      }
+    }
     for (const tc::TcTile& tl : p->tiles)
       if (tl.task < 0 || tl.task >= (int32_t)p->tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
   }

@@ -443,7 +443,15 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         for (int i = 0; i < 16; ++i) {
           const int j = c + i;
           if (j >= ntile) break;
-          const int64_t o = task.out_off + (int64_t)gm * task.row_stride + (int64_t)(tile.n0 + j) * task.col_stride;
+          // the column's segment by selects (an indexed read of the task's
+          // arrays would put the task in local memory)
+          const int col = tile.n0 + j;
+          int64_t so = task.seg_off[0];
+          int n0 = 0;
+          if (col >= task.seg_n0[1]) so = task.seg_off[1], n0 = task.seg_n0[1];
+          if (col >= task.seg_n0[2]) so = task.seg_off[2], n0 = task.seg_n0[2];
+          if (col >= task.seg_n0[3]) so = task.seg_off[3], n0 = task.seg_n0[3];
+          const int64_t o = so + (int64_t)gm * task.row_stride + (int64_t)(col - n0) * task.col_stride;
           if (MODE == 1) {
             // stage-1 output: the FP32 accumulator, re and im planes (the
             // stage-2 converter warps split it into TF32 hi / lo)

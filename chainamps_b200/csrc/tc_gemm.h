@@ -12,12 +12,19 @@
 namespace cmps {
 namespace tc {
 
-// One output region: element (i, j) of C lands at out_off + i*row_stride + j*col_stride.
+// One output region of up to four column segments: column j belongs to the
+// last segment q with seg_n0[q] <= j (seg_n0[0] = 0; unused segments hold
+// INT32_MAX), and element (i, j) of C lands at
+// seg_off[q] + i*row_stride + (j - seg_n0[q])*col_stride.  out_off repeats
+// seg_off[0].
 struct TcTask {
   int64_t out_off;
   int64_t row_stride, col_stride;
   int32_t m, n;
   int32_t t0, t1;
+  int32_t nseg;
+  int32_t seg_n0[4];
+  int64_t seg_off[4];
 };
 // One K-concatenated term: A tile at (a_x0 + k, row) of map a_map, B tile at (k, row) of b_map.
 struct TcTerm {
