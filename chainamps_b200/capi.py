@@ -93,6 +93,7 @@ _SIGS = {
     "cmps_heff_theta_svd": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]),
     "cmps_svd_destroy": (C.c_int, [C.c_void_p]),
     "cmps_svd_info": (C.c_int, [C.c_void_p, c_i64p, c_dblp, c_i64p, c_i64p]),
+    "cmps_svd_routes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "cmps_svd_copy": (C.c_int, [C.c_void_p, c_dblp, C.POINTER(C.c_int16), c_i64p, c_i64p, c_dblp, c_i64p, c_i64p,
                                 c_dblp]),
     "cmps_heff_left_block": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -394,6 +395,12 @@ class SVDResult:
         self.kept = kept.value
         self.discarded = disc.value
         self._nu, self._nv = nu.value, nv.value
+
+    def routes(self):
+        """Sectors factored by each route: dict(exact, gram, randomized)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib.cmps_svd_routes(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(exact=a.value, gram=b.value, randomized=c.value)
 
     def copy(self, u_rows, vd_cols):
         k = self.kept

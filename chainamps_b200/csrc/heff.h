@@ -173,6 +173,7 @@ struct SvdResult {
   std::vector<std::pair<int, int64_t>> order;  // global index -> (m, j)
   std::vector<std::vector<int64_t>> gidx;      // [m][j] -> global index
   double discarded = 0.0;
+  int routes[3] = {0, 0, 0};  // sectors factored exactly, by the Gram matrix, by the randomized route
 };
 
 int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out);

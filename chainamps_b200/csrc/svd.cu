@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <atomic>
 #include <thread>
 #include <set>
 
@@ -42,7 +43,7 @@ struct SvdWorker {
 struct SvdPool {
   std::vector<SvdWorker> w;
 };
-constexpr int kSvdWorkers = 4;
+constexpr int kSvdWorkers = 6;
 
 static int get_pool(cmps_context* ctx, SvdPool** out) {
   if (!ctx->svd_pool) {
@@ -212,6 +213,98 @@ __global__ void k_reverse_cols(const double2* __restrict__ E, int64_t p, double2
   }
 }
 
+// X[e] = two uniform values in [-1, 1) from a counter hash (splitmix64) of
+// (seed, e): the Gaussian-free test matrix of the range finder.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+__global__ void k_fill_random(double2* __restrict__ X, int64_t n, uint64_t seed) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t h = splitmix64(seed ^ splitmix64((uint64_t)e));
+    const double a = (double)(h >> 32) * (1.0 / 4294967296.0), b = (double)(h & 0xffffffffull) * (1.0 / 4294967296.0);
+    X[e] = make_double2(2.0 * a - 1.0, 2.0 * b - 1.0);
+  }
+}
+
+// out[j] = |R[:, j] - s[j] F[:, j]|^2 (column-major rows x cols, one block per column)
+__global__ void __launch_bounds__(256) k_col_resid(const double2* __restrict__ R, const double2* __restrict__ F,
+                                                   const double* __restrict__ s, int64_t rows,
+                                                   double* __restrict__ out) {
+  __shared__ double part[8];
+  const int64_t j = blockIdx.x;
+  const double sj = s[j];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
+    const double2 r = R[i + rows * j], f = F[i + rows * j];
+    const double x = r.x - sj * f.x, y = r.y - sj * f.y;
+    acc += x * x + y * y;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += part[w];
+    out[j] = t;
+  }
+}
+
+// G[i][i] += c * trace(G) (one block): the shift of shifted Cholesky QR,
+// with the Frobenius norm squared (the trace of the Gram matrix) standing in
+// for the squared 2-norm.
+__global__ void __launch_bounds__(256) k_shift_diag(double2* __restrict__ G, int64_t n, double c) {
+  __shared__ double part[8];
+  __shared__ double tr;
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) acc += G[i + n * i].x;
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += part[w];
+    tr = t;
+  }
+  __syncthreads();
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) G[i + n * i].x += c * tr;
+}
+
+// flag |= (info != 0): a Cholesky factorisation that broke down
+__global__ void k_or_info(const int* __restrict__ info, int* __restrict__ flag) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && *info != 0) *flag = 1;
+}
+
+// Sum of |X[e]|^2 in a fixed order: kSumBlocks partial sums, then one block
+// adds them (no atomics, so the result does not depend on scheduling).
+constexpr int kSumBlocks = 512;
+__global__ void __launch_bounds__(256) k_sumsq_partial(const double2* __restrict__ X, int64_t n,
+                                                       double* __restrict__ part) {
+  __shared__ double wsum[8];
+  double acc = 0.0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = X[e];
+    acc += v.x * v.x + v.y * v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += wsum[w];
+    part[blockIdx.x] = t;
+  }
+}
+__global__ void k_sum_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < n; ++i) t += part[i];
+    *out = t;
+  }
+}
+
 // G[:, j] /= s[j]  (column-major, rows x cols); zero columns where s[j] == 0
 __global__ void k_scale_cols_inv(double2* __restrict__ G, int64_t rows, int64_t cols, const double* __restrict__ s) {
   const int64_t n = rows * cols;
@@ -281,6 +374,12 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     std::vector<int64_t> rows, cols;
     std::vector<double> s;
     bool eig = false;
+    // randomized route: only the leading s.size() triplets were computed;
+    // tail = |A - Q Q^H A|_F^2 (the weight outside the range found),
+    // resid[j] = |A v_j - s_j u_j| (or its transpose form)
+    bool rnd = false;
+    double tail = 0.0;
+    std::vector<double> resid;
     double2* dU = nullptr;
     double2* dV = nullptr;
     int64_t* drows = nullptr;
@@ -380,12 +479,182 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       int* dinfo;
       double2* G = nullptr;
       size_t Gcap = 0;
+      double2* X = nullptr;  // scratch of the randomized route
+      size_t Xcap = 0;
       double* W = nullptr;
       size_t Wcap = 0;
       cuDoubleComplex* work = nullptr;
       size_t workcap = 0;
     };
-    auto factor = [&](int m, bool exact, FW& fw) -> int {
+    // Randomized route (Halko, Martinsson and Tropp, SIAM Review 53 (2011)
+    // 217, algorithms 4.4 and 5.1) for a sector much larger than the bond
+    // dimension: no sector keeps more than chi values, so its leading
+    // bb = chi + kRandPad triplets suffice whenever the checks of the global
+    // selection pass.  Range of M (the sector, or its adjoint when it is
+    // tall) by kRandIters subspace iterations with Cholesky QR
+    // re-orthonormalisation from a random start; then the eigenpairs of the
+    // bb x bb matrix B B^H with B = Q^H M.  Besides the triplets it records
+    // every triplet's residual and the weight outside the range found.
+    const int64_t kRandPad = 32;
+    const int kRandIters = 2;
+    auto rand_b = [&](int64_t mn) -> int64_t {
+      if (chi <= 0 || mn < kEigMin) return 0;
+      const int64_t bb = std::min<int64_t>(mn, chi + kRandPad);
+      return 4 * bb <= 3 * mn ? bb : 0;
+    };
+    auto rand_scratch = [&](int64_t nr, int64_t nc, int64_t bb) -> size_t {
+      const int64_t pp = std::min(nr, nc), ll = std::max(nr, nc);
+      return (size_t)(2 * pp * bb + ll * bb + bb * bb + bb + kSumBlocks / 2 + 2);
+    };
+    auto rand_lwork = [&](cusolverDnHandle_t sol, int64_t nr, int64_t nc, int64_t bb, int* lw) -> int {
+      const int pp = (int)std::min(nr, nc), ll = (int)std::max(nr, nc), b32 = (int)bb;
+      (void)pp;
+      (void)ll;
+      int a = 0, g = 0;
+      cuDoubleComplex* any = (cuDoubleComplex*)dA;
+      if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, b32, any, b32, dS, &g) !=
+              CUSOLVER_STATUS_SUCCESS)
+        return fail(CMPS_ERR_SOLVER, "randomized SVD buffer query failed");
+      *lw = std::max(std::max(a, g), 1);
+      return CMPS_OK;
+    };
+    auto factor_rand = [&](int m, int64_t bb, FW& fw) -> int {
+      const cudaStream_t st = fw.st;
+      const cusolverDnHandle_t sol = fw.sol;
+      const cublasHandle_t blas = fw.blas;
+      double2* const dA = fw.dA;
+      double* const dS = fw.dS;
+      int* const dinfo = fw.dinfo;
+      Blk& b = blk[m];
+      const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
+      const bool left = nr <= nc;  // M = A (short side rows) or M = A^H
+      const int64_t pp = left ? nr : nc, ll = left ? nc : nr;
+      const cublasOperation_t opM = left ? CUBLAS_OP_N : CUBLAS_OP_C, opMH = left ? CUBLAS_OP_C : CUBLAS_OP_N;
+      const size_t need = rand_scratch(nr, nc, bb);
+      double2* X = fw.X;
+      const bool ownX = need > fw.Xcap;
+      if (ownX && dmalloc(&X, sizeof(double2) * need) != cudaSuccess)
+        return fail(CMPS_ERR_NOMEM, "randomized SVD scratch allocation failed");
+      int lwork = 0;
+      int rc = rand_lwork(sol, nr, nc, bb, &lwork);
+      cuDoubleComplex* work = fw.work;
+      const bool ownW = rc == CMPS_OK && (size_t)lwork > fw.workcap;
+      if (ownW && dmalloc(&work, sizeof(cuDoubleComplex) * (size_t)lwork) != cudaSuccess)
+        rc = fail(CMPS_ERR_NOMEM, "randomized SVD work allocation failed");
+      double2* const Y = X;              // pp x bb: range basis Q
+      double2* const Z = Y + pp * bb;    // ll x bb: test matrix, then M^H Q
+      double2* const R = Z + ll * bb;    // pp x bb: reversed eigenvectors, then M O
+      double2* const Gb = R + pp * bb;   // bb x bb
+      double* const W = (double*)(Gb + bb * bb);
+      double* const rs = W + bb;
+      double* const part = rs + bb;
+      double* const tailp = part + kSumBlocks;
+      int* const chol_bad = (int*)(tailp + 1);
+      const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0),
+                            mone = make_cuDoubleComplex(-1.0, 0.0);
+      auto zg = [&](cublasOperation_t ta, cublasOperation_t tb, int64_t M_, int64_t N_, int64_t K_,
+                    const cuDoubleComplex* al, const double2* A_, int64_t lda, const double2* B_, int64_t ldb,
+                    const cuDoubleComplex* be, double2* C_, int64_t ldc) {
+        if (rc != CMPS_OK) return;
+        if (cublasZgemm(blas, ta, tb, (int)M_, (int)N_, (int)K_, al, (const cuDoubleComplex*)A_, (int)lda,
+                        (const cuDoubleComplex*)B_, (int)ldb, be, (cuDoubleComplex*)C_, (int)ldc) !=
+            CUBLAS_STATUS_SUCCESS)
+          rc = fail(CMPS_ERR_CUDA, "randomized SVD GEMM failed");
+      };
+      // Orthonormal basis of the columns of A_ (rows x bb, in place): shifted
+      // Cholesky QR followed by two plain passes (shifted CholeskyQR3,
+      // Fukaya, Kannan, Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci.
+      // Comput. 42 (2020) A477), stable up to a condition number ~1/eps; a
+      // factorisation that breaks down sets chol_bad and the sector goes to
+      // the Gram route.
+      auto qr = [&](double2* A_, int64_t rows) {
+        for (int pass = 0; pass < 3 && rc == CMPS_OK; ++pass) {
+          zg(CUBLAS_OP_C, CUBLAS_OP_N, bb, bb, rows, &one, A_, rows, A_, rows, &zero, Gb, bb);
+          if (rc != CMPS_OK) return;
+          if (pass == 0)
+            k_shift_diag<<<1, 256, 0, st>>>(Gb, bb, 11.0 * ((double)rows * bb + (double)bb * (bb + 1)) * kEps);
+          if (cusolverDnZpotrf(sol, CUBLAS_FILL_MODE_UPPER, (int)bb, (cuDoubleComplex*)Gb, (int)bb, work, lwork,
+                               dinfo) != CUSOLVER_STATUS_SUCCESS) {
+            rc = fail(CMPS_ERR_SOLVER, "randomized SVD Cholesky failed");
+            return;
+          }
+          k_or_info<<<1, 32, 0, st>>>(dinfo, chol_bad);
+          if (cublasZtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)rows,
+                          (int)bb, &one, (const cuDoubleComplex*)Gb, (int)bb, (cuDoubleComplex*)A_, (int)rows) !=
+              CUBLAS_STATUS_SUCCESS)
+            rc = fail(CMPS_ERR_CUDA, "randomized SVD triangular solve failed");
+        }
+      };
+      if (rc == CMPS_OK) cudaMemsetAsync(chol_bad, 0, sizeof(int), st);
+      if (rc == CMPS_OK) k_fill_random<<<grid_of(ll * bb), 256, 0, st>>>(Z, ll * bb, 0x5eed5eedull + (uint64_t)m);
+      zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, Z, ll, &zero, Y, pp);  // Y = M Omega
+      qr(Y, pp);
+      for (int it = 0; it < kRandIters; ++it) {
+        zg(opMH, CUBLAS_OP_N, ll, bb, pp, &one, dA, nr, Y, pp, &zero, Z, ll);  // Z = M^H Q
+        qr(Z, ll);
+        zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, Z, ll, &zero, Y, pp);   // Y = M Z
+        qr(Y, pp);
+      }
+      zg(opMH, CUBLAS_OP_N, ll, bb, pp, &one, dA, nr, Y, pp, &zero, Z, ll);    // Z = M^H Q = B^H
+      zg(CUBLAS_OP_C, CUBLAS_OP_N, bb, bb, ll, &one, Z, ll, Z, ll, &zero, Gb, bb);  // B B^H
+      if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)bb,
+                                            (cuDoubleComplex*)Gb, (int)bb, W, work, lwork, dinfo) !=
+                               CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "randomized SVD zheevd failed");
+      std::vector<double> w(bb);
+      int info = 0;
+      if (rc == CMPS_OK) {
+        cudaMemcpyAsync(w.data(), W, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess || info != 0)
+          rc = fail(CMPS_ERR_SOLVER, "randomized SVD: zheevd did not converge");
+      }
+      if (rc == CMPS_OK) {
+        b.s.assign(bb, 0.0);
+        for (int64_t j = 0; j < bb; ++j) b.s[j] = std::sqrt(std::max(0.0, w[bb - 1 - j]));
+        cudaMemcpyAsync(dS, b.s.data(), sizeof(double) * bb, cudaMemcpyHostToDevice, st);
+        double2* F = left ? b.dU : b.dV;   // short-side vectors (ld pp)
+        double2* O = left ? b.dV : b.dU;   // long-side vectors (ld ll)
+        k_reverse_cols<<<grid_of(bb * bb), 256, 0, st>>>(Gb, bb, R);
+        zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);  // F = Q X
+        zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, R, bb, &zero, O, ll);  // O = M^H F
+        if (rc == CMPS_OK) k_scale_cols_inv<<<grid_of(ll * bb), 256, 0, st>>>(O, ll, bb, dS);
+        zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, O, ll, &zero, R, pp);     // M O
+        if (rc == CMPS_OK) k_col_resid<<<(unsigned)bb, 256, 0, st>>>(R, F, dS, pp, rs);
+        // A <- A - Q Q^H A (left) or A - A Q Q^H (tall): the part outside the range
+        if (left)
+          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Y, nr, Z, nc, &one, dA, nr);
+        else
+          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Z, nr, Y, nc, &one, dA, nr);
+        if (rc == CMPS_OK) {
+          k_sumsq_partial<<<kSumBlocks, 256, 0, st>>>(dA, nr * nc, part);
+          k_sum_final<<<1, 32, 0, st>>>(part, kSumBlocks, tailp);
+          std::vector<double> r2(bb);
+          double tail = 0.0;
+          int bad = 0;
+          cudaMemcpyAsync(r2.data(), rs, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(&tail, tailp, sizeof(double), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(&bad, chol_bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+          if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(CMPS_ERR_CUDA, "randomized SVD failed");
+          b.resid.assign(bb, 0.0);
+          for (int64_t j = 0; j < bb; ++j) b.resid[j] = std::sqrt(std::max(0.0, r2[j]));
+          // a broken-down factorisation leaves no usable basis: an infinite
+          // tail fails the selection's check and sends the sector to the Gram route
+          b.tail = bad ? HUGE_VAL : tail;
+        }
+      }
+      if (ownW) dfree(work);
+      if (ownX) dfree(X);
+      if (rc == CMPS_OK) {
+        b.eig = true;
+        b.rnd = true;
+      }
+      return rc;
+    };
+    // mode 0: randomized route where eligible, else by size; 1: Gram route
+    // for sectors of at least kEigMin, else exact; 2: exact
+    auto factor = [&](int m, int mode, FW& fw) -> int {
       const cudaStream_t st = fw.st;
       const cusolverDnHandle_t sol = fw.sol;
       const cublasHandle_t blas = fw.blas;
@@ -400,8 +669,12 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       const int64_t nr = (int64_t)b.rows.size(), nc = (int64_t)b.cols.size();
       const int64_t mn = std::min(nr, nc);
       k_gather_cm<<<grid_of(nr * nc), 256, 0, st>>>(bre, bim, C, b.drows, nr, b.dcols, nc, dA);
+      b.rnd = false;
+      b.tail = 0.0;
+      b.resid.clear();
+      if (mode == 0 && rand_b(mn) > 0) return factor_rand(m, rand_b(mn), fw);
       b.s.resize(mn);
-      if (exact || mn < kEigMin) {
+      if (mode == 2 || mn < kEigMin) {
         b.eig = false;
         int lwork = 0;
         if (cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc, (cuDoubleComplex*)dA,
@@ -503,22 +776,22 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     SvdPool* pool = nullptr;
     const bool have_pool = get_pool(H.ctx, &pool) == CMPS_OK;  // set up on the first SVD, whatever its size
     if (n_eig >= 2 && have_pool) {
-      const int K = std::min<int>((int)pool->w.size(), n_eig);
+      const int K = std::min<int>((int)pool->w.size(), (int)todo.size());
+      // One queue, longest sectors first; each worker takes the next sector
+      // when it is free.  Estimated milliseconds per route (measured on
+      // B200): the randomized route is bound by its FP64 GEMMs, the Gram
+      // route and the one-sided Jacobi SVD by their sequential sweeps.
       std::vector<int> order = todo;
       auto cost = [&](int m) {
         const double nr = (double)blk[m].rows.size(), nc = (double)blk[m].cols.size();
-        return nr * nc * std::min(nr, nc);
+        const int64_t mn = (int64_t)std::min(nr, nc);
+        if (rand_b(mn) > 0) return 10.0 + 2e-8 * nr * nc * (double)rand_b(mn);
+        if (mn >= kEigMin) return 0.013 * (double)mn + 2.5e-9 * (double)mn * (double)mn * (double)mn;
+        return 0.1 + 0.09 * (double)mn;
       };
       std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
-      std::vector<std::vector<int>> lists(K);
-      std::vector<double> load(K, 0.0);
-      for (int m : order) {
-        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        lists[k].push_back(m);
-        load[k] += cost(m);
-      }
       std::vector<FW> fws(K);
-      std::vector<size_t> nA(K, 1), nS(K, 1), nG(K, 0), nW(K, 0), nwork(K, 1);
+      std::vector<size_t> nA(K, 1), nS(K, 1), nG(K, 0), nW(K, 0), nX(K, 0), nwork(K, 1);
       bool ok = true;
       for (int k = 0; k < K && ok; ++k) {
         SvdWorker& w = pool->w[k];
@@ -531,13 +804,16 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         cusolverDnXgesvdjSetTolerance(fws[k].params, 0.0);
         cusolverDnXgesvdjSetMaxSweeps(fws[k].params, 100);
         cusolverDnXgesvdjSetSortEig(fws[k].params, 1);
-        for (int m : lists[k]) {
+        for (int m : order) {  // any worker may take any sector
           const int64_t nr = (int64_t)blk[m].rows.size(), nc = (int64_t)blk[m].cols.size();
           const int64_t mn = std::min(nr, nc);
           nA[k] = std::max(nA[k], (size_t)(nr * nc));
           nS[k] = std::max(nS[k], (size_t)mn);
           int lwork = 0;
-          if (mn < kEigMin) {
+          if (rand_b(mn) > 0) {
+            nX[k] = std::max(nX[k], rand_scratch(nr, nc, rand_b(mn)));
+            if (rand_lwork(w.sol, nr, nc, rand_b(mn), &lwork) != CMPS_OK) ok = false;
+          } else if (mn < kEigMin) {
             if (cusolverDnZgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)blk[m].dU, (int)nr,
                                              (cuDoubleComplex*)blk[m].dV, (int)nc, &lwork,
@@ -556,7 +832,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       }
       double bytes = 0.0;
       for (int k = 0; k < K; ++k)
-        bytes += 16.0 * (nA[k] + nG[k] + nwork[k]) + 8.0 * (nS[k] + nW[k]) + 4.0;
+        bytes += 16.0 * (nA[k] + nG[k] + nX[k] + nwork[k]) + 8.0 * (nS[k] + nW[k]) + 4.0;
       if (ok && bytes <= 8e9) {
         for (int k = 0; k < K && ok; ++k) {
           FW& fw = fws[k];
@@ -565,13 +841,15 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
               dmalloc(&fw.dinfo, sizeof(int)) != cudaSuccess ||
               dmalloc(&fw.work, sizeof(cuDoubleComplex) * nwork[k]) != cudaSuccess ||
               (nG[k] && dmalloc(&fw.G, sizeof(double2) * nG[k]) != cudaSuccess) ||
-              (nW[k] && dmalloc(&fw.W, sizeof(double) * nW[k]) != cudaSuccess)) {
+              (nW[k] && dmalloc(&fw.W, sizeof(double) * nW[k]) != cudaSuccess) ||
+              (nX[k] && dmalloc(&fw.X, sizeof(double2) * nX[k]) != cudaSuccess)) {
             ok = false;
             break;
           }
           fw.workcap = nwork[k];
           fw.Gcap = nG[k];
           fw.Wcap = nW[k];
+          fw.Xcap = nX[k];
         }
         if (ok) {
           // theta and the block descriptors were written on the handle's stream
@@ -579,16 +857,19 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           std::vector<int> code(K, CMPS_OK);
           std::vector<std::string> msg(K);
           std::vector<std::thread> th_w;
+          std::atomic<size_t> next{0};
           const int dev = H.ctx->device;
           for (int k = 0; k < K; ++k)
             th_w.emplace_back([&, k]() {
               cudaSetDevice(dev);
-              for (int m : lists[k]) {
-                const int rc = factor(m, false, fws[k]);
+              for (;;) {
+                const size_t i = next.fetch_add(1);
+                if (i >= order.size() || code[k] != CMPS_OK) break;
+                const int rc = factor(order[i], 0, fws[k]);
                 if (rc != CMPS_OK) {
                   code[k] = rc;
                   msg[k] = cmps_last_error();
-                  break;
+                  next.store(order.size());  // the others stop after their current sector
                 }
               }
               cudaStreamSynchronize(fws[k].st);
@@ -606,29 +887,89 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         if (fw.work) dfree(fw.work);
         if (fw.G) dfree(fw.G);
         if (fw.W) dfree(fw.W);
+        if (fw.X) dfree(fw.X);
         if (fw.params) cusolverDnDestroyGesvdjInfo(fw.params);
       }
     }
     if (!done)
       for (int m : todo) {
         if (status != CMPS_OK) break;
-        status = factor(m, false, main_fw);
+        status = factor(m, 0, main_fw);
       }
-    // ---- global selection (redone with exact factors where the Gram route is not accurate enough) ----
+    // ---- global selection ----
+    // Sectors of the randomized route contribute only their leading values.
+    // Their result stands when it settles the truncation of the whole
+    // spectrum: (1) the bond-dimension cap, not the weight cut, decides the
+    // kept count (the weight from index cap - 1 on, computed values plus the
+    // sectors' tails, is at least max_trunc); (2) the degeneracy extension
+    // ends inside the computed values; (3) no value left out can rank above
+    // the first discarded one (each sector's tail, which bounds its largest
+    // value left out, is below half of it); (4) every kept triplet has
+    // converged: residual <= 1e-12 s_0 + 500 eps s_0^2 / s_j, the second term
+    // being the error the Gram matrix itself leaves in a vector of value s_j.
+    // Otherwise those sectors are redone
+    // by the Gram route.  Gram-route sectors are redone exactly where that
+    // route is not accurate enough (weight-decided count, or a kept value
+    // below 1e-5 s_0).
     struct SV { double v; int m; int64_t j; };
     std::vector<SV> all;
     std::vector<double> sv;
     int64_t length = 0;
-    for (int pass = 0; pass < 2 && status == CMPS_OK; ++pass) {
+    double tail_total = 0.0;
+    bool settled = false;
+    for (int pass = 0; pass < 8 && status == CMPS_OK && !settled; ++pass) {
       all.clear();
-      for (int m = 0; m < nm; ++m)
+      int64_t n_true = 0;
+      bool any_rnd = false;
+      tail_total = 0.0;
+      for (int m = 0; m < nm; ++m) {
         for (int64_t j = 0; j < (int64_t)blk[m].s.size(); ++j) all.push_back(SV{blk[m].s[j], m, j});
+        if (!blk[m].rows.empty()) n_true += (int64_t)std::min(blk[m].rows.size(), blk[m].cols.size());
+        if (blk[m].rnd) {
+          any_rnd = true;
+          tail_total += blk[m].tail;
+        }
+      }
       if (all.empty()) { status = fail(CMPS_ERR_SOLVER, "no singular values (empty wavefunction)"); break; }
       std::stable_sort(all.begin(), all.end(), [](const SV& a, const SV& b) { return a.v > b.v; });
       sv.assign(all.size(), 0.0);
       for (size_t i = 0; i < all.size(); ++i) sv[i] = all[i].v;
       bool weight_decided = false;
-      length = truncation_length(sv, chi, max_trunc, &weight_decided);
+      if (any_rnd) {
+        const int64_t np = (int64_t)sv.size();
+        const int64_t cap = (chi > 0 && chi < n_true) ? chi : n_true;
+        bool valid = cap < n_true && cap + 1 < np && sv[0] > 0.0;
+        if (valid) {
+          double beyond = tail_total;
+          for (int64_t i = cap - 1; i < np; ++i) beyond += sv[i] * sv[i];
+          valid = beyond >= 1.01 * max_trunc;                                   // (1)
+        }
+        int64_t len = cap;
+        if (valid) {
+          while (len < n_true && len < np && (sv[len - 1] - sv[len]) / sv[len - 1] < 1.0e-3) ++len;
+          valid = len < np;                                                     // (2)
+        }
+        if (valid) {
+          const double next = sv[len];
+          std::vector<int64_t> kept(nm, 0);
+          for (int64_t g = 0; g < len; ++g) kept[all[g].m] = std::max(kept[all[g].m], all[g].j + 1);
+          for (int m = 0; m < nm && valid; ++m) {
+            if (!blk[m].rnd) continue;
+            if (!(4.0 * blk[m].tail < next * next)) valid = false;             // (3)
+            for (int64_t j = 0; j < kept[m] && valid; ++j)
+              if (!(blk[m].resid[j] <= 1e-12 * sv[0] + 500.0 * kEps * sv[0] * sv[0] / blk[m].s[j]))
+                valid = false;                                                  // (4)
+          }
+        }
+        if (!valid) {
+          for (int m = 0; m < nm && status == CMPS_OK; ++m)
+            if (blk[m].rnd) status = factor(m, 1, main_fw);
+          continue;
+        }
+        length = len;
+      } else {
+        length = truncation_length(sv, chi, max_trunc, &weight_decided);
+      }
       const double floor2 = 1e-10 * sv[0] * sv[0];
       bool redo = false;
       for (int m = 0; m < nm; ++m) {
@@ -638,15 +979,18 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           if (all[g].m == m && all[g].v * all[g].v < floor2) low = true;
         if (weight_decided || low) {
           redo = true;
-          if ((status = factor(m, true, main_fw)) != CMPS_OK) break;
+          if ((status = factor(m, 2, main_fw)) != CMPS_OK) break;
         }
       }
-      if (!redo) break;
+      settled = !redo;
     }
+    if (status == CMPS_OK && !settled) status = fail(CMPS_ERR_STATE, "SVD: truncation not settled");
     cusolverDnDestroyGesvdjInfo(params);
     if (status != CMPS_OK) break;
     out.values.assign(sv.begin(), sv.begin() + length);
-    out.discarded = 0.0;
+    for (int m = 0; m < nm; ++m)
+      if (!blk[m].rows.empty()) ++out.routes[blk[m].rnd ? 2 : blk[m].eig ? 1 : 0];
+    out.discarded = tail_total;  // the weight the randomized sectors left out
     for (size_t i = length; i < sv.size(); ++i) out.discarded += sv[i] * sv[i];
     out.kept.assign(nm, 0);
     out.order.clear();
@@ -1060,6 +1404,14 @@ int cmps_svd_info(const cmps_svd* s, int64_t* kept, double* discarded, int64_t* 
   }
   if (nnz_u) *nnz_u = nu;
   if (nnz_vd) *nnz_vd = nv;
+  return CMPS_OK;
+}
+
+int cmps_svd_routes(const cmps_svd* s, int* n_exact, int* n_gram, int* n_randomized) {
+  if (!s) return fail(CMPS_ERR_ARG, "null handle");
+  if (n_exact) *n_exact = s->r.routes[0];
+  if (n_gram) *n_gram = s->r.routes[1];
+  if (n_randomized) *n_randomized = s->r.routes[2];
   return CMPS_OK;
 }
 

@@ -216,6 +216,12 @@ int cmps_svd_destroy(cmps_svd* s);
  * cols = (sigma2, a2)). */
 int cmps_svd_info(const cmps_svd* s, int64_t* kept, double* discarded_weight,
                   int64_t* nnz_u, int64_t* nnz_vd);
+/* How the non-empty charge sectors were factored (a diagnostic; the result
+ * does not depend on it beyond rounding): one-sided Jacobi SVD, eigenpairs
+ * of the Gram matrix, or the randomized range finder (sectors much larger
+ * than the bond dimension, accepted only where its leading triplets settle
+ * the truncation of the whole spectrum). */
+int cmps_svd_routes(const cmps_svd* s, int* n_exact, int* n_gram, int* n_randomized);
 /* values[kept]; new bond charges[kept * nq]; U and V^dagger in CSC. */
 int cmps_svd_copy(const cmps_svd* s, double* values, int16_t* new_charges,
                   int64_t* u_colptr, int64_t* u_rowind, double* u_values,
