@@ -776,7 +776,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     SvdPool* pool = nullptr;
     const bool have_pool = get_pool(H.ctx, &pool) == CMPS_OK;  // set up on the first SVD, whatever its size
     if (n_eig >= 2 && have_pool) {
-      const int K = std::min<int>((int)pool->w.size(), (int)todo.size());
+      int K = std::min<int>((int)pool->w.size(), (int)todo.size());
       // One queue, longest sectors first; each worker takes the next sector
       // when it is free.  Estimated milliseconds per route (measured on
       // B200): the randomized route is bound by its FP64 GEMMs, the Gram
@@ -830,10 +830,17 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           nwork[k] = std::max(nwork[k], (size_t)std::max(1, lwork));
         }
       }
+      // every worker is sized for any sector: as many workers as 8 GB of
+      // workspace allows (fewer than two: the sequential path)
       double bytes = 0.0;
       for (int k = 0; k < K; ++k)
         bytes += 16.0 * (nA[k] + nG[k] + nX[k] + nwork[k]) + 8.0 * (nS[k] + nW[k]) + 4.0;
-      if (ok && bytes <= 8e9) {
+      if (bytes > 8e9) {
+        const double per = bytes / K;
+        K = std::min<int>(K, (int)(8e9 / per));
+        bytes = per * K;
+      }
+      if (ok && K >= 2 && bytes <= 8e9) {
         for (int k = 0; k < K && ok; ++k) {
           FW& fw = fws[k];
           if (dmalloc(&fw.dA, sizeof(double2) * nA[k]) != cudaSuccess ||
