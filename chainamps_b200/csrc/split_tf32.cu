@@ -6,11 +6,14 @@
 //  * S1A  -- stage-1 A operand: theta transposed per (m, sigma1) chunk,
 //            [r][a0] with r running over the padded right index of m (each
 //            sigma2 chunk starts on a 4-element boundary) and ld = pad4(dim a0);
-//  * LPS  -- stage-1 B operand: LeftPart blocks [a0'][a0], ld = pad4(dim a0);
+//  * LPS  -- stage-1 B operand: for every term of a (fused) task, the
+//            LeftPart blocks [a0'][a0] of its column segments stacked along
+//            a0', ld = pad4(dim a0);
 //  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad], the
 //            FP32 accumulator; stage 2 splits it into TF32 hi / lo in shared
 //            memory, so T crosses HBM at 8 bytes per complex entry each way;
-//  * RPTS -- stage-2 B operand: RightPart blocks transposed, [a2'][a2].
+//  * RPTS -- stage-2 B operand: RightPart blocks transposed, [a2'][a2], the
+//            blocks of a fused task's segments stacked along a2'.
 // Every block base is 128-byte aligned and every leading dimension a multiple
 // of 4 floats, as the TMA requires; the K tail of every operand is zero-filled
 // by the TMA (out-of-bounds fill), padding rows of S1A are zero.

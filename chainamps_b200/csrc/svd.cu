@@ -506,10 +506,8 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       const int64_t pp = std::min(nr, nc), ll = std::max(nr, nc);
       return (size_t)(2 * pp * bb + ll * bb + bb * bb + bb + kSumBlocks / 2 + 2);
     };
-    auto rand_lwork = [&](cusolverDnHandle_t sol, int64_t nr, int64_t nc, int64_t bb, int* lw) -> int {
-      const int pp = (int)std::min(nr, nc), ll = (int)std::max(nr, nc), b32 = (int)bb;
-      (void)pp;
-      (void)ll;
+    auto rand_lwork = [&](cusolverDnHandle_t sol, int64_t bb, int* lw) -> int {
+      const int b32 = (int)bb;
       int a = 0, g = 0;
       cuDoubleComplex* any = (cuDoubleComplex*)dA;
       if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
@@ -537,7 +535,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (ownX && dmalloc(&X, sizeof(double2) * need) != cudaSuccess)
         return fail(CMPS_ERR_NOMEM, "randomized SVD scratch allocation failed");
       int lwork = 0;
-      int rc = rand_lwork(sol, nr, nc, bb, &lwork);
+      int rc = rand_lwork(sol, bb, &lwork);
       cuDoubleComplex* work = fw.work;
       const bool ownW = rc == CMPS_OK && (size_t)lwork > fw.workcap;
       if (ownW && dmalloc(&work, sizeof(cuDoubleComplex) * (size_t)lwork) != cudaSuccess)
@@ -812,7 +810,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           int lwork = 0;
           if (rand_b(mn) > 0) {
             nX[k] = std::max(nX[k], rand_scratch(nr, nc, rand_b(mn)));
-            if (rand_lwork(w.sol, nr, nc, rand_b(mn), &lwork) != CMPS_OK) ok = false;
+            if (rand_lwork(w.sol, rand_b(mn), &lwork) != CMPS_OK) ok = false;
           } else if (mn < kEigMin) {
             if (cusolverDnZgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)blk[m].dU, (int)nr,
