@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchainamps_b200.so")
-SOURCES = ["capi.cu", "heff.cu", "kernels.cu", "zgemm_fp64.cu", "svd.cu", "split_tf32.cu", "tc_gemm.cu", "noalloc.cu", "dmrg.cu", "adjoint.cu", "unitcell.cu"]
+SOURCES = ["capi.cu", "heff.cu", "kernels.cu", "zgemm_fp64.cu", "svd.cu", "split_tf32.cu", "tc_gemm.cu", "noalloc.cu", "dmrg.cu", "adjoint.cu", "unitcell.cu", "mpxio.cu"]
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 

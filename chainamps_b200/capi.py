@@ -123,6 +123,11 @@ _SIGS = {
     "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_theta_from_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_theta_to_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cmps_mpx_store": (C.c_int, [C.POINTER(MpxDesc), C.c_int32, C.c_char_p]),
+    "cmps_mpx_stat": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), c_i64p, c_i64p,
+                                c_i64p, c_i64p]),
+    "cmps_mpx_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_int16), C.c_int64, C.POINTER(C.c_uint8),
+                                C.POINTER(C.c_uint8), c_i64p, C.POINTER(C.c_int16), c_i64p, c_i64p, c_dblp]),
 }
 
 for _name, (_res, _args) in _SIGS.items():
@@ -609,6 +614,48 @@ def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: boo
     h = C.c_void_p()
     _check(lib.cmps_block_create(ctx.h, C.byref(cr), C.byref(db), C.byref(dw), 1 if right else 0, C.byref(h)))
     return Block(h, len(r))
+
+
+def store_mpx(t: MPXTensor, nq: int, path):
+    """Write t as the reference writes an MPX_matrix file (MPX_matrix::store):
+    the .BLOCK / .MPS_matrix / .MPX_matrix format.  Host only."""
+    d, keep = t._desc()
+    _check(lib.cmps_mpx_store(C.byref(d), int(nq), os.fsencode(path)))
+
+
+def load_mpx(path, nq: int, basis_charges=None) -> MPXTensor:
+    """Read an MPX_matrix file (load_MPX_matrix).  basis_charges ((d, nq)
+    int) gives the charges of physical indices, which the file does not
+    store.  Host only."""
+    p = os.fsencode(path)
+    ni, nr = C.c_int32(), C.c_int32()
+    tot, rows, cols, nnz = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+    _check(lib.cmps_mpx_stat(p, int(nq), C.byref(ni), C.byref(nr), C.byref(tot), C.byref(rows), C.byref(cols),
+                             C.byref(nnz)))
+    n = ni.value
+    inward = np.zeros(max(n, 1), np.uint8)
+    phys = np.zeros(max(n, 1), np.uint8)
+    sizes = np.zeros(max(n, 1), np.int64)
+    charges = np.zeros(max(tot.value * nq, 1), np.int16)
+    colptr = np.zeros(cols.value + 1, np.int64)
+    rowind = np.zeros(max(nnz.value, 1), np.int64)
+    vals = np.zeros(max(nnz.value, 1), np.complex128)
+    if basis_charges is None:
+        bc, bsize = None, 0
+    else:
+        bc = np.ascontiguousarray(np.asarray(basis_charges, np.int16).reshape(-1, nq))
+        bsize = bc.shape[0]
+    _check(lib.cmps_mpx_load(p, int(nq), None if bc is None else _p(bc, C.c_int16), bsize, _p(inward, C.c_uint8),
+                             _p(phys, C.c_uint8), _p(sizes, C.c_int64), _p(charges, C.c_int16), _p(colptr, C.c_int64),
+                             _p(rowind, C.c_int64), _p(vals.view(np.float64), C.c_double)))
+    idx, off = [], 0
+    for i in range(n):
+        sz = int(sizes[i])
+        idx.append(MPXIndexSpec(bool(inward[i]), bool(phys[i]),
+                                charges[off * nq:(off + sz) * nq].reshape(sz, nq).astype(np.int64)))
+        off += sz
+    k = nnz.value
+    return MPXTensor(idx, nr.value, rows.value, cols.value, colptr, rowind[:k].copy(), vals[:k].copy())
 
 
 def version():

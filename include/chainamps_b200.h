@@ -336,6 +336,32 @@ int cmps_dmrg_gradient(const cmps_dmrg* d, double* grad);
  * step}. */
 int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n);
 
+/* ---- MPX_matrix files (host only) ---------------------------------------
+ * The reference's binary MPX_matrix format: MPX_matrix::store /
+ * load_MPX_matrix_binary (MPX_matrix.cpp:219-247,593-607, MPXIndex.cpp:8-23,
+ * 98-121, states.cpp:59-61, sparse_interface.cpp:727-835).  It carries the
+ * .BLOCK environment checkpoints (BlocksStructure::save_left_block etc.,
+ * DMRG_routines.cpp:65-186) and the .MPS_matrix / .MPX_matrix state files.
+ * These entry points touch no device memory and need no GPU.
+ *
+ * Store m (nq charges per state) to path, as MPX_matrix::store writes it;
+ * a physical index is written without its charges. */
+int cmps_mpx_store(const cmps_mpx_desc* m, int32_t nq, const char* path);
+/* Sizes of a stored MPX_matrix: index count, row-index count, total index
+ * elements (sum of the index sizes), CSC shape and number of entries. */
+int cmps_mpx_stat(const char* path, int32_t nq, int32_t* num_indices, int32_t* num_row_indices,
+                  int64_t* total_elements, int64_t* rows, int64_t* cols, int64_t* nnz);
+/* Read a stored MPX_matrix into caller buffers sized from cmps_mpx_stat:
+ * inward / physical / sizes [num_indices], charges [total_elements * nq],
+ * colptr [cols + 1], rowind [nnz], values [2 * nnz] interleaved complex.
+ * Physical indices take basis_charges [basis_size * nq] (the model's
+ * spectrum, as load_MPXIndex_binary does); their stored size must equal
+ * basis_size.  Of the nzmax entries stored, the first colptr[cols] are kept
+ * (load_SparseMatrix_binary). */
+int cmps_mpx_load(const char* path, int32_t nq, const int16_t* basis_charges, int64_t basis_size,
+                  uint8_t* inward, uint8_t* physical, int64_t* sizes, int16_t* charges,
+                  int64_t* colptr, int64_t* rowind, double* values);
+
 #ifdef __cplusplus
 }
 #endif

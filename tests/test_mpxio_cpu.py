@@ -1,0 +1,135 @@
+"""The reference's binary MPX_matrix file format through the C ABI (host
+only, no GPU): cmps_mpx_store writes the bytes of MPX_matrix::store, and
+cmps_mpx_load reads them back as load_MPX_matrix does.
+
+Checked against the oracle's restatement of the format (oracle/mpxio.py):
+* the library's file equals the oracle's bytes exactly, for an MPO (with
+  physical indices), a grown left environment block (the .BLOCK
+  checkpoint), an MPS tensor from the block SVD (the .MPS_matrix file), a
+  two-charge MPO, and an empty matrix;
+* loading returns the same indices, row-index count and CSC matrix;
+* the reader keeps the first colptr[cols] of nzmax stored entries, and
+  refuses a matrix not in compressed-column form, a truncated file and a
+  physical index without (or with the wrong) basis."""
+import numpy as np
+import pytest
+
+from oracle import dmrg as od, mpxio as om
+from oracle.mpx import MPX, to_csc
+from tests.helpers import to_tensor, model_zoo
+
+ZOO = model_zoo()
+
+
+def lib():
+    from chainamps_b200 import capi
+    return capi
+
+
+def oracle_bytes(A: MPX, **kw):
+    rows, cols, cp, ri, vals = to_csc(A)
+    idx = [(ix.inward, ix.physical, ix.charges) for ix in A.indices]
+    return om.mpx_bytes(idx, A.nrow, rows, cols, cp, ri, vals, len(A.rules), **kw)
+
+
+def basis_of(H: MPX):
+    return next(ix.charges for ix in H.indices if ix.physical)
+
+
+def samples():
+    H = ZOO["xxz"]
+    sb = od.SuperBlock(H, tol=1e-12)
+    for _ in range(4):
+        sb.grow(12, 1e-16)
+    out = {
+        "mpo_xxz": (H, basis_of(H)),
+        "mpo_twocharge": (ZOO["twocharge"], basis_of(ZOO["twocharge"])),
+        "left_block": (sb.left_blocks[sb.nleft], None),
+        "right_block": (sb.right_blocks[sb.nleft], None),
+        "mps_U": (sb.dec.U, basis_of(H)),
+    }
+    # an empty matrix: the zero MPO of the same indices
+    Z = MPX(H.rules, list(H.indices), H.nrow, np.zeros_like(H.data))
+    out["empty"] = (Z, basis_of(H))
+    return out
+
+
+SAMPLES = samples()
+
+
+@pytest.mark.parametrize("name", sorted(SAMPLES))
+def test_store_writes_the_reference_bytes_and_loads_back(tmp_path, name):
+    capi = lib()
+    A, basis = SAMPLES[name]
+    path = tmp_path / f"{name}.MPX_matrix"
+    capi.store_mpx(to_tensor(A), len(A.rules), path)
+    data = path.read_bytes()
+    assert data == oracle_bytes(A)
+    t = capi.load_mpx(path, len(A.rules), basis)
+    ref = to_tensor(A)
+    assert t.nrow == A.nrow and t.rows == ref.rows and t.cols == ref.cols
+    assert len(t.indices) == len(A.indices)
+    for a, b in zip(t.indices, A.indices):
+        assert a.inward == b.inward and a.physical == b.physical
+        np.testing.assert_array_equal(a.charges, np.asarray(b.charges, np.int64))
+    np.testing.assert_array_equal(t.colptr, ref.colptr)
+    np.testing.assert_array_equal(t.rowind, ref.rowind)
+    np.testing.assert_array_equal(t.values, ref.values)
+    # the oracle reads the library's file the same way
+    idx, nrow, rows, cols, cp, ri, vals = om.parse(data, len(A.rules), basis)
+    assert nrow == A.nrow and (rows, cols) == (ref.rows, ref.cols)
+    np.testing.assert_array_equal(cp, ref.colptr)
+    np.testing.assert_array_equal(vals, ref.values)
+
+
+def test_reader_keeps_the_first_colptr_entries_of_nzmax(tmp_path):
+    capi = lib()
+    A = SAMPLES["left_block"][0]
+    ref = to_tensor(A)
+    nnz = int(ref.colptr[-1])
+    path = tmp_path / "padded.BLOCK"
+    path.write_bytes(oracle_bytes(A, nzmax=nnz + 7, fill=(0, 3.0 - 1.0j)))
+    t = capi.load_mpx(path, len(A.rules))
+    np.testing.assert_array_equal(t.rowind, ref.rowind)
+    np.testing.assert_array_equal(t.values, ref.values)
+
+
+def test_reader_refuses_bad_files(tmp_path):
+    capi = lib()
+    A, basis = SAMPLES["mpo_xxz"]
+    nq = len(A.rules)
+    good = oracle_bytes(A)
+    # nz != -1 (triplet form): the reference exits, the library returns an error;
+    # the matrix header starts after the index records
+    rows, cols, cp, ri, vals = to_csc(A)
+    head = len(good) - (8 * 4 + 8 * (cols + 1) + (8 + 16) * max(int(cp[-1]), 1))
+    bad = bytearray(good)
+    bad[head + 8:head + 16] = np.int64(0).tobytes()
+    p = tmp_path / "triplet.MPX_matrix"
+    p.write_bytes(bytes(bad))
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(p, nq, basis)
+    # truncated
+    p = tmp_path / "short.MPX_matrix"
+    p.write_bytes(good[:-5])
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(p, nq, basis)
+    # physical index without the basis, and with a basis of the wrong size
+    p = tmp_path / "mpo.MPX_matrix"
+    p.write_bytes(good)
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(p, nq, None)
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(p, nq, np.vstack([basis, basis]))
+    # a missing file
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(tmp_path / "none.MPX_matrix", nq, basis)
+
+
+def test_store_refuses_inconsistent_shapes(tmp_path):
+    capi = lib()
+    A = SAMPLES["left_block"][0]
+    t = to_tensor(A)
+    t.rows += 1
+    with pytest.raises(capi.CmpsError):
+        capi.store_mpx(t, len(A.rules), tmp_path / "bad.BLOCK")
