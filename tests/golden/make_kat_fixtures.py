@@ -6,9 +6,11 @@ READMEs.  This script reads them from a checkout of the reference and stores
 them as a small fixture, so the oracle and the GPU path can be checked
 against them on machines where the reference is not present:
 
-* ``examples/user_defined/spin_half_example``: input files and the
+* ``examples/user_defined/spin_half_example``: input files, the
   ``example_input_Energies.dat`` table printed in ``README.md``
-  (``fDMRG_DRV.bin -B 50 -F 2 -X 2 example_input 10``; ground state rows);
+  (``fDMRG_DRV.bin -B 50 -F 2 -X 2 example_input 10``; ground state rows)
+  and the ``example_input_Excited_Energies.dat`` table of the two excited
+  states (README.md:58-70);
 * ``examples/user_defined/quench_example``: input files and
   ``initial_input_Energies.dat`` (``fDMRG_DRV.bin -F 1 initial_input 20``);
 * ``examples/built_in/xxx_lattice_chains/README.md``: the raw iDMRG table
@@ -55,6 +57,8 @@ def main(ref):
         "operators": [read(os.path.join(sh, n)) for n in ("Sx.in", "Sy.in", "Sz.in")],
         "energies": table_after(sh_readme, "# Index, Energy, Energy/vertices"),
         "source": "examples/user_defined/spin_half_example/README.md:28-40",
+        "excited_energies": table_after(sh_readme, "# Sweep Index, State Index, Energy"),
+        "excited_source": "examples/user_defined/spin_half_example/README.md:58-70",
     }
     q = os.path.join(ex, "user_defined", "quench_example")
     quench = {

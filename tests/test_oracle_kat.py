@@ -1,5 +1,7 @@
 """The oracle reproduces the reference's own example outputs (its only
-pinned results): spin-1/2 fDMRG and the quench example."""
+pinned results): spin-1/2 fDMRG and the quench example.  The spin-1/2
+example's excited-state rows are pinned to the exact spectrum of the
+example's Hamiltonian."""
 import json
 import os
 
@@ -42,3 +44,48 @@ def test_quench_fdmrg_kat():
     for r, e in zip(rows, ref):
         assert abs(r["energy"] - e[1]) <= 1e-12 * abs(e[1])
         assert abs(r["entropy"] - e[3]) <= 1e-12
+
+
+def _chain_hamiltonian(H, n):
+    """Dense open-chain Hamiltonian of n vertices from the MPO W[s', b_l, s,
+    b_r] in the reference's lower-triangular form: the left boundary takes
+    row D - 1, the right boundary column 0 (LeftH / RightH)."""
+    W = np.asarray(H.data)
+    d, D = W.shape[0], W.shape[1]
+    v = [W[:, D - 1, :, br] for br in range(D)]  # one operator per open MPO bond
+    for _ in range(n - 1):
+        dim = v[0].shape[0] * d
+        nv = []
+        for br in range(D):
+            acc = np.zeros((dim, dim), complex)
+            for bl in range(D):
+                if np.any(v[bl]) and np.any(W[:, bl, :, br]):
+                    acc += np.kron(v[bl], W[:, bl, :, br])
+            nv.append(acc)
+        v = nv
+    return v[0]
+
+
+def test_spin_half_excited_state_kat_is_the_exact_spectrum():
+    """The excited-state rows of the example (fDMRG_DRV -X 2) converge to the
+    second and third eigenvalues of the 10-vertex chain in the target sector
+    (total charge 0), and the ground-state rows to the first: the targets
+    for the projector path (ProjectorBlocks, DMRG_routines.cpp:446-581),
+    computed here from the oracle's own MPO of the example input."""
+    k = json.load(open(GOLD))["spin_half_fdmrg"]
+    H = _model(k)
+    n = k["vertices"]
+    Hc = _chain_hamiltonian(H, n)
+    q = np.asarray(next(ix.charges for ix in H.indices if ix.physical))[:, 0]
+    tot = np.zeros(1, np.int64)
+    for _ in range(n):
+        tot = (tot[:, None] + q[None, :]).reshape(-1)
+    sel = np.nonzero(tot == 0)[0]
+    w = np.linalg.eigvalsh(Hc[np.ix_(sel, sel)])
+    ground = k["energies"][-1][1]
+    ex = k["excited_energies"]
+    first = [r[2] for r in ex if r[1] == 1.0][-1]
+    second = [r[2] for r in ex if r[1] == 2.0][-1]
+    assert abs(w[0] - ground) <= 1e-12
+    assert abs(w[1] - first) <= 1e-12
+    assert abs(w[2] - second) <= 1e-12
