@@ -596,11 +596,13 @@ class fDMRG(iDMRG):
                 a, b = self.position()
                 if a == b - a - 2:
                     rows.append(r)
+            # back to the centre: for (r = right_size(); r > left_size(); --r)
+            # reads the left size as it grows (fDMRG_routines.cpp:52-58)
             nl, n = self.position()
-            for _ in range((n - nl - 2) - nl):
+            while n - nl - 2 > nl:
                 r = self.move(+1, chi, max_trunc)
-                a, b = self.position()
-                if a == b - a - 2:
+                nl, n = self.position()
+                if nl == n - nl - 2:
                     rows.append(r)
         return rows
 

@@ -577,7 +577,9 @@ def run_fdmrg(H, nvertices, sweeps, chi, trunc=1e-16, target=None, tol=1e-14):
             r = sb.move_left(chi, trunc)
             if sb.nleft == sb.nright:
                 rows.append(r)
-        for _ in range(sb.nright, sb.nleft, -1):
+        # for (r = right_size(); r > left_size(); --r): the condition reads the
+        # left size as it grows, so the pass stops at the centre
+        while sb.nright > sb.nleft:
             r = sb.move_right(chi, trunc)
             if sb.nleft == sb.nright:
                 rows.append(r)

@@ -89,3 +89,28 @@ def test_spin_half_excited_state_kat_is_the_exact_spectrum():
     assert abs(w[0] - ground) <= 1e-12
     assert abs(w[1] - first) <= 1e-12
     assert abs(w[2] - second) <= 1e-12
+
+
+def test_spin_half_excited_states_kat():
+    """The oracle's excited-state DMRG (oracle/excited.py: ProjectorBlocks and
+    ExcitedStateFiniteDMRG, weight 100) reproduces the example's
+    excited-state table where it is converged: the number of rows of each
+    state and each state's final row (energy 1e-10, entropy 1e-8).
+
+    Not compared: the rows between, which the reference solves with ARPACK
+    capped at two restarts and tol 0.1 (arpack_interface.cpp:28-29), and the
+    init rows.  The reference's init rows (-8.7716, -8.5906) lie below the
+    exact lowest eigenvalue of the centre window's projected operator as the
+    oracle forms it (-8.6762, -8.5892), so they are not a partial Lanczos
+    result of the same problem; the cause is not identified."""
+    from oracle.excited import run_excited_fdmrg
+    k = json.load(open(GOLD))["spin_half_fdmrg"]
+    H = _model(k)
+    gs_rows, ex_rows = run_excited_fdmrg(H, k["vertices"], k["sweeps"], k["chi"], k["trunc"], nstates=2)
+    assert abs(gs_rows[-1]["energy"] - k["energies"][-1][1]) <= 1e-12
+    ref = k["excited_energies"]
+    for s, rows in enumerate(ex_rows, start=1):
+        rr = [r for r in ref if r[1] == float(s)]
+        assert len(rows) == len(rr)
+        assert abs(rows[-1]["energy"] - rr[-1][2]) <= 1e-10
+        assert abs(rows[-1]["entropy"] - rr[-1][3]) <= 1e-8
