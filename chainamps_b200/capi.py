@@ -458,6 +458,17 @@ class Block:
         n = cp[-1]
         return ch.astype(np.int64), (cp, ri[:n], v[:n])
 
+    def to_mpx(self, bq, right, target=None) -> "MPXTensor":
+        """The block as the reference's 6-index MPX_matrix (see
+        block_mpx_tensor); bq: MPO bond charges (D, nq)."""
+        ch, csc = self.to_csc()
+        return block_mpx_tensor(ch, csc, self.D, bq, right, target)
+
+    def store(self, path, bq, right, target=None):
+        """BlocksStructure::save_left_block / save_right_block
+        (DMRG_routines.cpp:65-84): write the block as a .BLOCK file."""
+        store_mpx(self.to_mpx(bq, right, target), self.nq, path)
+
     def close(self):
         if getattr(self, "h", None):
             lib.cmps_block_destroy(self.h)
@@ -468,6 +479,35 @@ class Block:
             self.close()
         except Exception:
             pass
+
+
+def block_mpx_tensor(charges, csc, D, bq, right, target=None) -> "MPXTensor":
+    """An exported environment block (cmps_block_copy: a' charges, CSC of rows
+    a', cols b + D a) as the 6-index MPX_matrix the reference holds:
+    MakeLeftBlock's (dummy, a', dummy, b, dummy, a; 3 row indices) or
+    MakeRightBlock's (a', dummy, b, dummy, a, dummy; 2 row indices)
+    (DMRG_routines.cpp:594-611).  The matrix is the export itself: the dummy
+    indices have size 1.  The right block's first and last dummies carry the
+    target charge (from MakeDummyRightBlock, :634-653), every other dummy zero."""
+    ch = np.asarray(charges, np.int64)
+    nq = ch.shape[1]
+    bq = np.asarray(bq, np.int64).reshape(-1, nq)
+    if bq.shape[0] != D:
+        raise ValueError("bq must have one charge per MPO bond state")
+    z = np.zeros((1, nq), np.int64)
+    t = z if target is None else np.asarray(target, np.int64).reshape(1, nq)
+    if not right:
+        idx = [MPXIndexSpec(False, False, z), MPXIndexSpec(True, False, ch), MPXIndexSpec(True, False, z),
+               MPXIndexSpec(False, False, bq), MPXIndexSpec(True, False, z), MPXIndexSpec(False, False, ch)]
+        nrow = 3
+    else:
+        idx = [MPXIndexSpec(False, False, ch), MPXIndexSpec(True, False, t), MPXIndexSpec(True, False, bq),
+               MPXIndexSpec(False, False, z), MPXIndexSpec(True, False, ch), MPXIndexSpec(False, False, t)]
+        nrow = 2
+    cp, ri, v = csc
+    chi = ch.shape[0]
+    return MPXTensor(idx, nrow, chi, D * chi, np.asarray(cp, np.int64), np.asarray(ri, np.int64),
+                     np.asarray(v, np.complex128))
 
 
 class iDMRG:

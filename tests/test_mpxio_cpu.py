@@ -8,6 +8,8 @@ Checked against the oracle's restatement of the format (oracle/mpxio.py):
   checkpoint), an MPS tensor from the block SVD (the .MPS_matrix file), a
   two-charge MPO, and an empty matrix;
 * loading returns the same indices, row-index count and CSC matrix;
+* an exported device block converts to the reference's 6-index block layout
+  (block_mpx_tensor) with the same bytes as the oracle's block;
 * the reader keeps the first colptr[cols] of nzmax stored entries, and
   refuses a matrix not in compressed-column form, a truncated file and a
   physical index without (or with the wrong) basis."""
@@ -133,3 +135,32 @@ def test_store_refuses_inconsistent_shapes(tmp_path):
     t.rows += 1
     with pytest.raises(capi.CmpsError):
         capi.store_mpx(t, len(A.rules), tmp_path / "bad.BLOCK")
+
+
+@pytest.mark.parametrize("target", [(0,), (2,)])
+@pytest.mark.parametrize("right", [False, True])
+def test_block_layout_from_the_export(tmp_path, target, right):
+    """block_mpx_tensor turns a block in cmps_block_copy's export layout (a'
+    charges; CSC rows a', cols b + D a) into the reference's 6-index block:
+    the same indices, charges and matrix as the oracle's MakeLeftBlock /
+    MakeRightBlock result, hence the same .BLOCK bytes."""
+    capi = lib()
+    H = ZOO["xxz"]
+    sb = od.SuperBlock(H, target=list(target), tol=1e-12)
+    for _ in range(4):
+        sb.grow(12, 1e-16)
+    B = (sb.right_blocks if right else sb.left_blocks)[sb.nleft]
+    bond = B.indices[0 if right else 1].charges
+    rows, cols, cp, ri, vals = to_csc(B)        # rows a', cols b + D a: the export layout
+    D = H.indices[1].size
+    assert (rows, cols) == (bond.shape[0], D * bond.shape[0])
+    t = capi.block_mpx_tensor(bond, (cp, ri, vals), D, H.indices[1].charges, right, target)
+    ref = to_tensor(B)
+    assert t.nrow == ref.nrow
+    for a, b in zip(t.indices, ref.indices):
+        assert a.inward == b.inward and a.physical == b.physical
+        np.testing.assert_array_equal(a.charges, np.asarray(b.charges, np.int64))
+    p1, p2 = tmp_path / "mine.BLOCK", tmp_path / "ref.BLOCK"
+    capi.store_mpx(t, 1, p1)
+    capi.store_mpx(ref, 1, p2)
+    assert p1.read_bytes() == p2.read_bytes() == oracle_bytes(B)
