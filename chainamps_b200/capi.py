@@ -658,6 +658,13 @@ def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: boo
     return Block(h, len(r))
 
 
+def load_block(ctx: Context, rules, path, W: MPXTensor, right: bool):
+    """BlocksStructure::load_left_block / load_right_block
+    (DMRG_routines.cpp:89-101): a .BLOCK file (written by the reference or by
+    Block.store) as a device Block."""
+    return upload_block(ctx, rules, load_mpx(path, len(rules)), W, right)
+
+
 def store_mpx(t: MPXTensor, nq: int, path):
     """Write t as the reference writes an MPX_matrix file (MPX_matrix::store):
     the .BLOCK / .MPS_matrix / .MPX_matrix format.  Host only."""
