@@ -424,6 +424,19 @@ class SVDResult:
         return dict(values=vals, charges=ch.astype(np.int64), u=(ucp, uri[:nu], uv[:nu]),
                     vd=(vcp, vri[:nv], vv[:nv]))
 
+    def store(self, name, nl, nr, basis_charges, a0_charges, a2_charges, store_lambda=True):
+        """MPSDecomposition::store (MPS_matrix.cpp:151-165): <name>_Left_<nl>
+        and <name>_Right_<nr>.MPS_matrix, and <name>_Lambda_<nl>_<nr>
+        .MPX_matrix if store_lambda.  basis_charges: the vertex basis (d, nq);
+        a0 / a2: the charges of the left / right environment bonds."""
+        d = np.asarray(basis_charges).reshape(-1, self.nq).shape[0]
+        out = self.copy(d * len(a0_charges), d * len(a2_charges))
+        U, Vd, Lam = mps_decomposition_tensors(out, basis_charges, a0_charges, a2_charges)
+        store_mpx(U, self.nq, f"{name}_Left_{nl}.MPS_matrix")
+        store_mpx(Vd, self.nq, f"{name}_Right_{nr}.MPS_matrix")
+        if store_lambda:
+            store_mpx(Lam, self.nq, f"{name}_Lambda_{nl}_{nr}.MPX_matrix")
+
     def close(self):
         if getattr(self, "h", None):
             lib.cmps_svd_destroy(self.h)
@@ -656,6 +669,33 @@ def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: boo
     h = C.c_void_p()
     _check(lib.cmps_block_create(ctx.h, C.byref(cr), C.byref(db), C.byref(dw), 1 if right else 0, C.byref(h)))
     return Block(h, len(r))
+
+
+def mps_decomposition_tensors(svd_copy, basis_charges, a0_charges, a2_charges):
+    """The MPSDecomposition of a device SVD (SVDResult.copy) as the reference
+    holds it (MPX_matrix.cpp:174-191): LeftMatrix (sigma1 in, a0 in, a1 out;
+    2 row indices), RightMatrix (a1 in, sigma2 in, a2 out; 1 row index) and
+    the diagonal Lambda MPX_matrix(spectrum, LeftMatrix.Index(2), values)
+    (a1 in, a1 out; MPX_matrix.cpp:55-60).  The physical indices carry the
+    basis charges; the matrices are the copy's CSC arrays."""
+    ch = np.asarray(svd_copy["charges"], np.int64)
+    nq = ch.shape[1]
+    basis = np.asarray(basis_charges, np.int64).reshape(-1, nq)
+    a0 = np.asarray(a0_charges, np.int64).reshape(-1, nq)
+    a2 = np.asarray(a2_charges, np.int64).reshape(-1, nq)
+    d, k = basis.shape[0], ch.shape[0]
+    ucp, uri, uv = svd_copy["u"]
+    vcp, vri, vv = svd_copy["vd"]
+    U = MPXTensor([MPXIndexSpec(True, True, basis), MPXIndexSpec(True, False, a0), MPXIndexSpec(False, False, ch)],
+                  2, d * a0.shape[0], k, np.asarray(ucp, np.int64), np.asarray(uri, np.int64),
+                  np.asarray(uv, np.complex128))
+    Vd = MPXTensor([MPXIndexSpec(True, False, ch), MPXIndexSpec(True, True, basis), MPXIndexSpec(False, False, a2)],
+                   1, k, d * a2.shape[0], np.asarray(vcp, np.int64), np.asarray(vri, np.int64),
+                   np.asarray(vv, np.complex128))
+    vals = np.asarray(svd_copy["values"], np.float64)
+    Lam = MPXTensor([MPXIndexSpec(True, False, ch), MPXIndexSpec(False, False, ch)], 1, k, k,
+                    np.arange(k + 1, dtype=np.int64), np.arange(k, dtype=np.int64), vals.astype(np.complex128))
+    return U, Vd, Lam
 
 
 def load_block(ctx: Context, rules, path, W: MPXTensor, right: bool):

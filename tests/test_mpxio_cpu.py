@@ -164,3 +164,31 @@ def test_block_layout_from_the_export(tmp_path, target, right):
     capi.store_mpx(t, 1, p1)
     capi.store_mpx(ref, 1, p2)
     assert p1.read_bytes() == p2.read_bytes() == oracle_bytes(B)
+
+
+def test_mps_decomposition_files():
+    """mps_decomposition_tensors turns an SVD result in SVDResult.copy's
+    layout (CSC of U rows (sigma1, a0) and of V^dagger cols (sigma2, a2), new
+    bond charges, values) into the LeftMatrix, RightMatrix and Lambda files
+    MPSDecomposition::store writes: the same bytes as the oracle's block SVD
+    factors and its diagonal Lambda."""
+    import os
+    import tempfile
+    from oracle.mpx import diag_mpx
+    capi = lib()
+    H = ZOO["xxz"]
+    sb = od.SuperBlock(H, tol=1e-12)
+    for _ in range(5):
+        sb.grow(10, 1e-16)
+    dec = sb.dec
+    _, _, ucp, uri, uv = to_csc(dec.U)
+    _, _, vcp, vri, vv = to_csc(dec.Vd)
+    copy = dict(values=dec.values, charges=dec.U.indices[2].charges, u=(ucp, uri, uv), vd=(vcp, vri, vv))
+    basis = basis_of(H)
+    U, Vd, Lam = capi.mps_decomposition_tensors(copy, basis, dec.U.indices[1].charges, dec.Vd.indices[2].charges)
+    lam_ref = diag_mpx(H.rules, dec.U.indices[2], dec.values)
+    with tempfile.TemporaryDirectory() as tmp:
+        for t, ref in ((U, dec.U), (Vd, dec.Vd), (Lam, lam_ref)):
+            p = os.path.join(tmp, "x.MPS_matrix")
+            capi.store_mpx(t, len(H.rules), p)
+            assert open(p, "rb").read() == oracle_bytes(ref)
