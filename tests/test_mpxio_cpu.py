@@ -192,3 +192,21 @@ def test_mps_decomposition_files():
             p = os.path.join(tmp, "x.MPS_matrix")
             capi.store_mpx(t, len(H.rules), p)
             assert open(p, "rb").read() == oracle_bytes(ref)
+
+
+def test_reader_takes_a_file_with_nzmax_zero(tmp_path):
+    """load_SparseMatrix_binary's nzmax == 0 branch (sparse_interface.cpp:
+    820-830): only the column pointers follow the header; the matrix is
+    empty."""
+    capi = lib()
+    A, basis = SAMPLES["empty"]
+    rows, cols, cp, ri, vals = to_csc(A)
+    data = oracle_bytes(A)
+    head = len(data) - (8 * 4 + 8 * (cols + 1) + 8 + 16)
+    buf = bytearray(data[:head + 8 * 4 + 8 * (cols + 1)])     # no placeholder entry
+    buf[head:head + 8] = np.int64(0).tobytes()                # nzmax = 0
+    p = tmp_path / "nzmax0.MPX_matrix"
+    p.write_bytes(bytes(buf))
+    t = capi.load_mpx(p, len(A.rules), basis)
+    assert (t.rows, t.cols) == (rows, cols)
+    assert t.colptr[-1] == 0 and t.rowind.size == 0 and t.values.size == 0
