@@ -1,6 +1,6 @@
 """Benchmark of the ChainAMPS DMRG hot path on B200.
 
-Workload (BASELINE configs[1]): iDMRG on four coupled spin-1/2 Heisenberg
+Workload: iDMRG on four coupled spin-1/2 Heisenberg
 chains treated as one vertex (local dimension 16, intrachain J = 1, rung
 J_perp = 0.5, total-Sz charge, reference-padded MPO of bond dimension 110),
 complex double, bond dimension chi = 512.  One step = one H_eff matvec

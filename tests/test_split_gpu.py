@@ -10,7 +10,7 @@ product keeps ~22 mantissa bits, but sums are accumulated in FP32 over K of
 up to ~4e4 terms, so the error grows with K.
 Ground-state energies, which the solver takes from an FP64 Rayleigh
 quotient of the split-precision eigenvector, agree with the FP64 solver to
-1e-9 relative (the BASELINE accuracy target)."""
+1e-9 relative, the accuracy the mixed-precision form is held to."""
 import numpy as np
 import pytest
 
