@@ -22,7 +22,6 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from dataclasses import dataclass
 
 import numpy as np
 
@@ -150,43 +149,8 @@ def _p(a, t):
 
 
 # ---------------------------------------------------------------------------
-@dataclass
-class MPXIndexSpec:
-    inward: bool
-    physical: bool
-    charges: np.ndarray  # (size, nq) int
-
-
-@dataclass
-class MPXTensor:
-    """MPX_matrix storage (MPX_matrix.hpp:61-66): indices, number of row
-    indices, CSC matrix (rows, cols, colptr, rowind, complex values)."""
-    indices: list
-    nrow: int
-    rows: int
-    cols: int
-    colptr: np.ndarray
-    rowind: np.ndarray
-    values: np.ndarray
-
-    def _desc(self):
-        keep = []
-        inward = np.array([1 if i.inward else 0 for i in self.indices], np.uint8)
-        phys = np.array([1 if i.physical else 0 for i in self.indices], np.uint8)
-        sizes = np.array([i.charges.shape[0] for i in self.indices], np.int64)
-        charges = np.ascontiguousarray(np.concatenate([np.asarray(i.charges, np.int16).reshape(i.charges.shape[0], -1)
-                                                       for i in self.indices], axis=0))
-        colptr = np.ascontiguousarray(self.colptr, np.int64)
-        rowind = np.ascontiguousarray(self.rowind, np.int64)
-        vals = np.ascontiguousarray(np.asarray(self.values, np.complex128)).view(np.float64)
-        if rowind.size == 0:
-            rowind = np.zeros(1, np.int64)
-            vals = np.zeros(2, np.float64)
-        keep += [inward, phys, sizes, charges, colptr, rowind, vals]
-        d = MpxDesc(len(self.indices), self.nrow, _p(inward, C.c_uint8), _p(phys, C.c_uint8), _p(sizes, C.c_int64),
-                    _p(charges, C.c_int16), self.rows, self.cols, _p(colptr, C.c_int64), _p(rowind, C.c_int64),
-                    _p(vals, C.c_double))
-        return d, keep
+# the tensor containers are numpy-only (chainamps_b200.tensors); re-exported here
+from .tensors import MPXIndexSpec, MPXTensor  # noqa: E402,F401
 
 
 def _rules(rules):

@@ -8,7 +8,9 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <set>
 #include <string>
+#include <utility>
 
 #include "heff.h"
 
@@ -60,6 +62,19 @@ cudaError_t dfree(void* p) {
   cudaError_t e = cudaDeviceSynchronize();
   cudaError_t f = cudaFreeAsync(p, cudaStreamLegacy);
   return e != cudaSuccess ? e : f;
+}
+
+static std::mutex g_optin_mu;
+static std::set<std::pair<const void*, int>> g_optin_done;  // (kernel, device)
+
+int ensure_smem_optin(const void* func, int bytes) {
+  int dev = 0;
+  CMPS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_optin_mu);
+  if (g_optin_done.count({func, dev})) return CMPS_OK;
+  CMPS_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  g_optin_done.insert({func, dev});
+  return CMPS_OK;
 }
 
 int zero_wait(void* dst, size_t bytes, cudaStream_t st) {

@@ -51,6 +51,12 @@ int zero_wait(void* dst, size_t bytes, cudaStream_t st);
 // usable from any stream, dfree waits for the device before releasing.
 cudaError_t dmalloc(void** p, size_t bytes);
 cudaError_t dfree(void* p);
+
+// Dynamic shared memory opt-in of a kernel above 48 KB.  cudaFuncSetAttribute
+// applies to the current device only, so the opt-in is made once per (kernel,
+// device ordinal), under a lock: a process may drive several GPUs, and the
+// SVD's worker threads launch the same kernels concurrently.
+int ensure_smem_optin(const void* func, int bytes);
 template <class T>
 inline cudaError_t dmalloc(T** p, size_t bytes) {
   return dmalloc(reinterpret_cast<void**>(p), bytes);

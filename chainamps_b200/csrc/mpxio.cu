@@ -23,6 +23,7 @@
 // it keeps the first colptr[cols].
 #include <cstdint>
 #include <cstdio>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -42,6 +43,23 @@ struct File {
 bool put(std::FILE* f, const void* p, size_t bytes) { return bytes == 0 || std::fwrite(p, 1, bytes, f) == bytes; }
 bool get(std::FILE* f, void* p, size_t bytes) { return bytes == 0 || std::fread(p, 1, bytes, f) == bytes; }
 
+// Bytes left between the read position and the end of the file: every count
+// read from a file is checked against it before anything of that size is
+// allocated, so a corrupt or truncated file is refused instead of exhausting
+// host memory.
+int64_t remaining(std::FILE* f) {
+  const long pos = std::ftell(f);
+  if (pos < 0 || std::fseek(f, 0, SEEK_END) != 0) return -1;
+  const long end = std::ftell(f);
+  if (end < 0 || std::fseek(f, pos, SEEK_SET) != 0) return -1;
+  return (int64_t)end - (int64_t)pos;
+}
+// true if `count` items of `size` bytes fit in what is left of the file
+bool fits(std::FILE* f, uint64_t count, uint64_t size) {
+  const int64_t left = remaining(f);
+  return left >= 0 && (size == 0 || count <= (uint64_t)left / size);
+}
+
 // Checked description of one stored MPX (sizes only).
 struct Header {
   int64_t num_indices = 0, num_row_indices = 0;
@@ -49,6 +67,10 @@ struct Header {
   std::vector<int64_t> sizes;
   int64_t total = 0;  // sum of sizes
   int64_t nzmax = 0, rows = 0, cols = 0, nnz = 0;
+  // stored charges of the non-physical indices: run i starts at charges[charge_at[i]]
+  // and belongs at element offset charge_pos[i]
+  std::vector<int16_t> charges;
+  std::vector<int64_t> charge_at, charge_pos;
 };
 
 // Reads the index section and the CSC header and column pointers; leaves the
@@ -75,10 +97,13 @@ int read_header(std::FILE* f, int32_t nq, Header& h, std::vector<int64_t>& colpt
     h.physical[i] = ph;
     h.sizes[i] = (int64_t)sz;
     if (!ph && sz > 0) {
+      if (!fits(f, sz * (uint64_t)nq, sizeof(int16_t))) return fail(CMPS_ERR_ARG, "MPX file: truncated charges");
       buf.resize((size_t)sz * nq);
       if (!get(f, buf.data(), sizeof(int16_t) * buf.size())) return fail(CMPS_ERR_ARG, "MPX file: truncated charges");
-      if (charges)
-        for (size_t e = 0; e < buf.size(); ++e) charges[(size_t)h.total * nq + e] = buf[e];
+      // kept here until the whole header has been checked
+      h.charge_at.push_back((int64_t)h.charges.size());
+      h.charge_pos.push_back(h.total);
+      h.charges.insert(h.charges.end(), buf.begin(), buf.end());
     }
     h.total += (int64_t)sz;
   }
@@ -90,6 +115,7 @@ int read_header(std::FILE* f, int32_t nq, Header& h, std::vector<int64_t>& colpt
   h.cols = params[3];
   if (h.nzmax < 0 || h.rows < 0 || h.cols < 0 || h.cols > ((int64_t)1 << 40))
     return fail(CMPS_ERR_ARG, "MPX file: bad matrix shape");
+  if (!fits(f, (uint64_t)h.cols + 1, sizeof(int64_t))) return fail(CMPS_ERR_ARG, "MPX file: truncated colptr");
   colptr.assign((size_t)h.cols + 1, 0);
   if (!get(f, colptr.data(), sizeof(int64_t) * colptr.size())) return fail(CMPS_ERR_ARG, "MPX file: truncated colptr");
   if (colptr[0] != 0) return fail(CMPS_ERR_ARG, "MPX file: colptr[0] != 0");
@@ -103,6 +129,16 @@ int read_header(std::FILE* f, int32_t nq, Header& h, std::vector<int64_t>& colpt
     for (int64_t i = 0; i < h.num_indices; ++i) (i < h.num_row_indices ? r : c) *= h.sizes[i];
     if (r != h.rows || c != h.cols) return fail(CMPS_ERR_ARG, "MPX file: matrix shape differs from the index sizes");
   }
+  // row indices and values of nzmax entries follow
+  if (!fits(f, (uint64_t)h.nzmax, sizeof(int64_t) + 2 * sizeof(double)))
+    return fail(CMPS_ERR_ARG, "MPX file: truncated entries");
+  // the header is whole: only now does the caller's charges buffer get written
+  if (charges)
+    for (size_t i = 0; i < h.charge_at.size(); ++i) {
+      const size_t from = (size_t)h.charge_at[i];
+      const size_t to = i + 1 < h.charge_at.size() ? (size_t)h.charge_at[i + 1] : h.charges.size();
+      for (size_t e = from; e < to; ++e) charges[(size_t)h.charge_pos[i] * nq + (e - from)] = h.charges[e];
+    }
   return CMPS_OK;
 }
 
@@ -218,8 +254,16 @@ int cmps_mpx_load(const char* path, int32_t nq, const int16_t* basis_charges, in
   }
   for (size_t j = 0; j < cp.size(); ++j) colptr[j] = cp[j];
   if (h.nzmax > 0 && h.nnz > 0) {
-    std::vector<int64_t> ri((size_t)h.nzmax);
-    std::vector<double> x(2 * (size_t)h.nzmax);
+    // nzmax is bounded by the file size (read_header), so these fit in memory
+    // unless the host itself is out of it
+    std::vector<int64_t> ri;
+    std::vector<double> x;
+    try {
+      ri.resize((size_t)h.nzmax);
+      x.resize(2 * (size_t)h.nzmax);
+    } catch (const std::bad_alloc&) {
+      return fail(CMPS_ERR_NOMEM, "MPX file: host allocation of " + std::to_string(h.nzmax) + " entries failed");
+    }
     if (!get(f.f, ri.data(), sizeof(int64_t) * ri.size()) || !get(f.f, x.data(), sizeof(double) * x.size()))
       return fail(CMPS_ERR_ARG, "MPX file: truncated entries");
     for (int64_t p = 0; p < h.nnz; ++p) {

@@ -68,6 +68,7 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
                                   " bytes of scratch, above the static maximum of " +
                                   std::to_string(kNoAllocScratchDoubles * 8) + " bytes");
   CMPS_CUDA(cudaSetDevice(H.device));
+  cudaGetLastError();  // drop a stale non-sticky error of an unrelated earlier call
   double* base = nullptr;
   CMPS_TRY(scratch_address(H.device, &base));
   cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;

@@ -487,21 +487,13 @@ int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double*
   const int ntiles = (int)p.tiles.size();
   const unsigned grid = (unsigned)std::min(ntiles, sms);
   if (mode == 1) {
-    static bool cfg1 = false;
-    if (!cfg1) {
-      CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-      cfg1 = true;
-    }
+    CMPS_TRY(ensure_smem_optin((const void*)tc_split_gemm<1>, kSmemBytes));
     tc_split_gemm<1><<<grid, threads_of<1>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
                                                                  p.d_bmaps, nullptr, nullptr, 0, out32, out32_plane,
                                                                  out64, out64_plane, d_err);
   } else {
     if (!ain || !p.d_adescs) return fail(CMPS_ERR_STATE, "tcgen05 mode 2: no A operand");
-    static bool cfg2 = false;
-    if (!cfg2) {
-      CMPS_CUDA(cudaFuncSetAttribute(tc_split_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-      cfg2 = true;
-    }
+    CMPS_TRY(ensure_smem_optin((const void*)tc_split_gemm<2>, kSmemBytes));
     tc_split_gemm<2><<<grid, threads_of<2>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, nullptr,
                                                                  p.d_bmaps, p.d_adescs, ain, a_plane, out32,
                                                                  out32_plane, out64, out64_plane, d_err);

@@ -191,12 +191,7 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
 
 template <bool AH, bool BH>
 int launch_variant(const GemmPlan& p, const Planar& A, const Planar& B, Planar& C, cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    CMPS_CUDA(cudaFuncSetAttribute(zgemm_grouped_fp64<AH, BH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)SMEM_BYTES));
-    configured = true;
-  }
+  CMPS_TRY(ensure_smem_optin((const void*)zgemm_grouped_fp64<AH, BH>, (int)SMEM_BYTES));
   if (p.tiles.empty()) return CMPS_OK;
   const int64_t ntiles = (int64_t)p.tiles.size();
   if (ntiles > 0x7fffffff) return fail(CMPS_ERR_ARG, "too many GEMM tiles");

@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .capi import MPXTensor, MPXIndexSpec
+from .tensors import MPXTensor, MPXIndexSpec
 
 
 def _charge_add(a, b, rules):
@@ -290,3 +290,21 @@ def random_environment(rng, rules, bond, bq, used_b, right):
     idx = [MPXIndexSpec(False, False, bond), MPXIndexSpec(True, False, z), MPXIndexSpec(True, False, bq),
            MPXIndexSpec(False, False, z), MPXIndexSpec(True, False, bond), MPXIndexSpec(False, False, z)]
     return dense_to_tensor(idx, 2, vals.reshape(chi, 1, D, 1, chi, 1))
+
+
+def ladder_workload(chi, seed=20261203, width=3.5, legs=4, j=1.0, j_perp=0.5):
+    """The synthetic H_eff workload of the ladder benchmark: the ``legs``-leg
+    Heisenberg ladder vertex (reference-padded MPO) between seeded random
+    left and right environments on a Gaussian total-Sz bond of ``chi``
+    elements (charges 2k, sector profile width ``width``), entries only on
+    the MPO slots the MPO uses.  Returns the model arrays and the three
+    tensors (L, Wt, R) as the reference would hand them over."""
+    rules, ch, W, bq = ladder_model(legs, j, j_perp)
+    used_l = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 2, 3)))[0]})
+    used_r = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 1, 2)))[0]})
+    bond = gaussian_bond(chi, step=2, width=width)
+    rng = np.random.default_rng(seed)
+    L = random_environment(rng, rules, bond, bq, used_l, right=False)
+    R = random_environment(rng, rules, bond, bq, used_r, right=True)
+    Wt = mpo_tensor(ch, W, bq)
+    return dict(rules=rules, ch=ch, W=W, bq=bq, bond=bond, L=L, R=R, Wt=Wt)

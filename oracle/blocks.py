@@ -221,3 +221,69 @@ def from_mpx(H, L, R):
     Rm = [Rt[:, b, :] if np.any(Rt[:, b, :]) else None for b in range(D)]
     return BlockHeff(H.rules, H.indices[0].charges, L.indices[5].charges, R.indices[4].charges,
                      H.indices[1].charges, H.data, Lm, Rm)
+
+
+def env_matrices(rows, D, colptr, rowind, values):
+    """Per-MPO-index dense [a', a] matrices of an environment block stored
+    as the reference's CSC matrix (MPX_matrix storage, first index fastest):
+    a left block (MakeLeftBlock layout: rows a'_dummy, a', b_dummy; columns
+    b, a_dummy, a) or a right block (MakeRightBlock layout: rows a', a'_dummy;
+    columns b, b_dummy, a, a_dummy) both have `rows` = dim a' row elements
+    and column b + D * a.  Slots without entries give None."""
+    colptr = np.asarray(colptr, np.int64)
+    ncols = colptr.size - 1
+    M = np.zeros((rows, ncols), np.complex128)
+    cols = np.repeat(np.arange(ncols), np.diff(colptr))
+    M[np.asarray(rowind, np.int64), cols] = np.asarray(values, np.complex128)
+    T = M.reshape(rows, D, ncols // D, order="F")
+    return [T[:, b, :].copy() if np.any(T[:, b, :]) else None for b in range(D)]
+
+
+class BlockTwoVertex:
+    """``TwoVertexComponents`` (DMRG_routines.cpp:779-896) with the matvec of
+    the block port: the same allowed indices, vector indices, dense small-n
+    branch and HED post-processing as ``dmrg.TwoVertexComponents``, for
+    vertices whose dense LeftPart the dense restatement cannot hold (a
+    64-state chain vertex at chi = 32 would need 1.7 GB for it)."""
+
+    def __init__(self, L, H, R):
+        self.rules = H.rules
+        self.bh = from_mpx(H, L, R)
+        sig = H.indices[2]
+        self.indices = [sig.with_dir(True), L.indices[5].with_dir(True), sig.with_dir(True),
+                        R.indices[4].with_dir(False)]
+        s1, a0, s2, a2 = self.indices
+        self.vrows = s1.size * a0.size
+        self.vcols = s2.size * a2.size
+        self.allowed = self.bh.allowed
+
+    @property
+    def length(self):
+        return self.vrows * self.vcols
+
+    def matvec(self, x):
+        return self.bh.matvec(x)
+
+    def hed(self, guess_full=None, tol=1e-14):
+        from .dmrg import SPARSE_THRESHOLD, EPS, phase_fix, lanczos_ground, eigvec_postprocess
+        n = self.allowed.size
+        if n <= SPARSE_THRESHOLD:
+            Hd = np.zeros((n, n), np.complex128)
+            for j in range(n):
+                e = np.zeros(n, np.complex128)
+                e[j] = 1.0
+                Hd[:, j] = self.matvec(e)
+            Hd = 0.5 * (Hd + Hd.conj().T)
+            w, V = np.linalg.eigh(Hd)
+            e = float(w[0])
+            vec = V[:, 0]
+            small = np.abs(vec) < EPS
+            vec = phase_fix(vec)
+            vec[small] = 0.0
+        else:
+            e, vec = lanczos_ground(self.matvec, n,
+                                    None if guess_full is None else guess_full[self.allowed], tol=tol)
+            vec = eigvec_postprocess(vec)
+        full = np.zeros(self.length, np.complex128)
+        full[self.allowed] = vec
+        return e, full

@@ -385,7 +385,13 @@ def left_shape(A: MPX) -> MPX:
 class SuperBlock:
     """SuperBlock (DMRG_routines.cpp:188-444) with in-memory environments."""
 
-    def __init__(self, H: MPX, target=None, tol=1e-14):
+    def __init__(self, H: MPX, target=None, tol=1e-14, heff="dense"):
+        """heff: "dense" solves with the dense restatement of
+        TwoVertexComponents, "blocks" with the block port (``blocks.BlockTwoVertex``,
+        the same operator), for vertices too large for the dense form."""
+        if heff not in ("dense", "blocks"):
+            raise ValueError(heff)
+        self.heff = heff
         self.H = H
         self.rules = H.rules
         self.target = np.zeros(H.nq, np.int64) if target is None else np.asarray(target, np.int64)
@@ -454,7 +460,11 @@ class SuperBlock:
                     truncation=self.dec.truncation, fidelity=fid, chi=len(self.dec.values))
 
     def _solve(self, L, R, guess):
-        h = TwoVertexComponents(L, self.H, R)
+        if self.heff == "blocks":
+            from .blocks import BlockTwoVertex
+            h = BlockTwoVertex(L, self.H, R)
+        else:
+            h = TwoVertexComponents(L, self.H, R)
         self.last_heff = h
         e, full = h.hed(guess_full=guess if guess is not None and guess.size == h.length else None,
                         tol=self.tol)

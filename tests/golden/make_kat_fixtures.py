@@ -86,4 +86,9 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: first argument, else $CHAINAMPS_REFERENCE
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CHAINAMPS_REFERENCE")
+    if not src:
+        sys.exit("usage: make_kat_fixtures.py <path to the ChainAMPS checkout> "
+                 "(or set CHAINAMPS_REFERENCE)")
+    main(src)

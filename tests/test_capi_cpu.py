@@ -47,5 +47,14 @@ def test_null_arguments_are_errors_not_crashes():
 def test_library_is_sm100a_only():
     """The shared object carries sm_100a code (checked from the build recipe)."""
     from chainamps_b200 import build
-    cmd = " ".join(build.nvcc_cmd())
-    assert "arch=compute_100a,code=sm_100a" in cmd
+    for src in build.sources():
+        cmd, _ = build.nvcc_compile(src)
+        assert "arch=compute_100a,code=sm_100a" in " ".join(cmd)
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.nvcc_link(["x.o"]))
+
+
+def test_library_matches_its_sources():
+    """The built library's stamp is the digest of the current sources and
+    flags: a library built from other sources is not reused."""
+    from chainamps_b200 import build
+    assert build.up_to_date(), "libchainamps_b200.so is stale: run python -m chainamps_b200.build"

@@ -107,3 +107,29 @@ def test_coupled_ising_mpo_matches_oracle():
     np.testing.assert_array_equal(W, Ho.data)
     np.testing.assert_array_equal(bq, Ho.indices[1].charges)
     assert pm.coupled_ising_model(12, 1.2, 64, 0.05)[2].shape == (64, 26, 64, 26)
+
+
+def test_benchmark_workload_through_the_oracle_block_port():
+    """The benchmark's synthetic ladder workload, read by the oracle's block
+    port from the CSC storage (``env_matrices``, as the CPU baseline and the
+    GPU parity test at chi = 512 read it), gives the dense oracle's matvec
+    (``TwoVertexComponents`` on the same tensors) at a size the dense
+    restatement holds."""
+    from oracle import blocks as ob, dmrg as od
+    from oracle.mpx import from_csc, Index
+
+    wl = pm.ladder_workload(24, seed=11, width=1.5)
+    D = wl["bq"].shape[0]
+    chi = wl["bond"].shape[0]
+    bh = ob.BlockHeff(wl["rules"], wl["ch"], wl["bond"], wl["bond"], wl["bq"], wl["W"],
+                      ob.env_matrices(chi, D, wl["L"].colptr, wl["L"].rowind, wl["L"].values),
+                      ob.env_matrices(chi, D, wl["R"].colptr, wl["R"].rowind, wl["R"].values))
+
+    def mpx(t):
+        idx = [Index(i.inward, i.physical, np.asarray(i.charges, np.int64)) for i in t.indices]
+        return from_csc(wl["rules"], idx, t.nrow, t.rows, t.cols, t.colptr, t.rowind, t.values)
+    ref = od.TwoVertexComponents(mpx(wl["L"]), mpx(wl["Wt"]), mpx(wl["R"]))
+    np.testing.assert_array_equal(bh.allowed, ref.allowed)
+    x = np.random.default_rng(2).standard_normal(bh.n) + 1j * np.random.default_rng(3).standard_normal(bh.n)
+    a, b = bh.matvec(x), ref.matvec(x)
+    assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))

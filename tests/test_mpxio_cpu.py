@@ -128,6 +128,32 @@ def test_reader_refuses_bad_files(tmp_path):
         capi.load_mpx(tmp_path / "none.MPX_matrix", nq, basis)
 
 
+def test_reader_refuses_counts_beyond_the_file_size(tmp_path):
+    """A corrupt header whose nzmax or column count claims more data than the
+    file holds is refused with an error before anything of that size is
+    allocated (no std::bad_alloc escapes the C ABI)."""
+    capi = lib()
+    A, basis = SAMPLES["mpo_xxz"]
+    nq = len(A.rules)
+    good = oracle_bytes(A)
+    rows, cols, cp, ri, vals = to_csc(A)
+    head = len(good) - (8 * 4 + 8 * (cols + 1) + (8 + 16) * max(int(cp[-1]), 1))
+    for field, value in ((0, 1 << 60), (0, 1 << 33)):
+        bad = bytearray(good)
+        bad[head + 8 * field:head + 8 * field + 8] = np.int64(value).tobytes()
+        p = tmp_path / f"nzmax{value}.MPX_matrix"
+        p.write_bytes(bytes(bad))
+        with pytest.raises(capi.CmpsError, match="truncated"):
+            capi.load_mpx(p, nq, basis)
+    # columns: shape check or size check refuses it, never an allocation of 2^39 entries
+    bad = bytearray(good)
+    bad[head + 24:head + 32] = np.int64(1 << 39).tobytes()
+    p = tmp_path / "cols.MPX_matrix"
+    p.write_bytes(bytes(bad))
+    with pytest.raises(capi.CmpsError):
+        capi.load_mpx(p, nq, basis)
+
+
 def test_store_refuses_inconsistent_shapes(tmp_path):
     capi = lib()
     A = SAMPLES["left_block"][0]

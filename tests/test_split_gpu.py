@@ -82,26 +82,34 @@ def test_split_ground_state_energy(ctx, name, steps, chi):
     assert abs(abs(np.vdot(v64, v32)) - 1.0) <= 1e-6
 
 
-@pytest.mark.parametrize("width", [3.5, 1.2])
-def test_split_matvec_at_benchmark_scale(ctx, width):
-    """chi = 512 ladder workload; width 1.2 gives charge sectors above 128
-    states (several N tiles per task in both stages)."""
+@pytest.mark.parametrize("width,seed", [(3.5, 20261203), (1.2, 5)])
+def test_matvecs_at_benchmark_scale_against_the_oracle(ctx, width, seed):
+    """chi = 512 ladder workload, checked against the oracle's block port at
+    its own size.  (3.5, 20261203) is exactly the benchmark's workload;
+    width 1.2 gives charge sectors above 128 states (several N tiles per task
+    in both split stages).  FP64 within 1e-12 (max-norm, relative); split-TF32
+    within SCALE_RTOL (max-norm) and 1e-4 (rms)."""
     from chainamps_b200 import TwoVertexComponents, CMPS_SPLIT_TF32, CMPS_FP64, models
-    rules, ch, W, bq = models.ladder_model(4, 1.0, 0.5)
-    used_l = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 2, 3)))[0]})
-    used_r = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 1, 2)))[0]})
-    bond = models.gaussian_bond(512, step=2, width=width)
-    rng = np.random.default_rng(5)
-    L = models.random_environment(rng, rules, bond, bq, used_l, right=False)
-    R = models.random_environment(rng, rules, bond, bq, used_r, right=True)
-    Wt = models.mpo_tensor(ch, W, bq)
-    g64 = TwoVertexComponents(ctx, rules, L, Wt, R, precision=CMPS_FP64)
-    x = rng.standard_normal(g64.n) + 1j * rng.standard_normal(g64.n)
+    from oracle import blocks as ob
+    wl = models.ladder_workload(512, seed=seed, width=width)
+    chi, D = wl["bond"].shape[0], wl["bq"].shape[0]
+    bh = ob.BlockHeff(wl["rules"], wl["ch"], wl["bond"], wl["bond"], wl["bq"], wl["W"],
+                      ob.env_matrices(chi, D, wl["L"].colptr, wl["L"].rowind, wl["L"].values),
+                      ob.env_matrices(chi, D, wl["R"].colptr, wl["R"].rowind, wl["R"].values))
+    rng = np.random.default_rng(seed + 1)
+    x = rng.standard_normal(bh.n) + 1j * rng.standard_normal(bh.n)
+    want = bh.matvec(x)
+    scale = np.max(np.abs(want))
+    g64 = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=CMPS_FP64)
+    assert g64.n == bh.n
+    np.testing.assert_array_equal(g64.allowed_indices, bh.allowed)
     a = g64.multiply(x)
     del g64
-    g32 = TwoVertexComponents(ctx, rules, L, Wt, R, precision=CMPS_SPLIT_TF32)
+    assert np.max(np.abs(a - want)) <= 1e-12 * scale
+    g32 = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=CMPS_SPLIT_TF32)
     b = g32.multiply(x)
-    err = np.max(np.abs(a - b)) / np.max(np.abs(a))
+    del g32
+    err = np.max(np.abs(b - want)) / scale
     assert err <= SCALE_RTOL, err
-    rms = np.sqrt(np.mean(np.abs(a - b) ** 2)) / np.sqrt(np.mean(np.abs(a) ** 2))
+    rms = np.sqrt(np.mean(np.abs(b - want) ** 2)) / np.sqrt(np.mean(np.abs(want) ** 2))
     assert rms <= 1e-4, rms

@@ -39,9 +39,12 @@ def test_noalloc_matvec_matches_handle_scratch_matvec():
     stream = torch.cuda.Stream()
     for call in range(2):
         x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        # the copy and the NaN fill run on torch's current stream; the matvecs
+        # run on `stream`, a non-blocking stream, so order them explicitly
         dx = torch.from_numpy(x).cuda()
         want = torch.empty_like(dx)
         got = torch.full_like(dx, complex(np.nan, np.nan))
+        stream.wait_stream(torch.cuda.current_stream())
         h.multiply_device(dx.data_ptr(), want.data_ptr(), stream.cuda_stream)
         rc = lib.cmps_heff_apply_device_noalloc(h.h, C.c_void_p(dx.data_ptr()), C.c_void_p(got.data_ptr()),
                                                 C.c_void_p(stream.cuda_stream))
