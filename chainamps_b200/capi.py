@@ -30,6 +30,9 @@ LIBPATH = os.path.join(HERE, "libchainamps_b200.so")
 
 CMPS_FP64 = 0
 CMPS_SPLIT_TF32 = 1
+CMPS_ORDER_AUTO = 0
+CMPS_ORDER_FOLDED = 1
+CMPS_ORDER_CANONICAL = 2
 
 
 class CmpsError(RuntimeError):
@@ -83,6 +86,8 @@ _SIGS = {
     "cmps_heff_apply_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_time_stages": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, c_dblp]),
     "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_heff_set_order": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_heff_order": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), c_dblp, c_dblp]),
     "cmps_heff_status": (C.c_int, [C.c_void_p]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
                                  C.POINTER(C.c_int)]),
@@ -299,6 +304,19 @@ class TwoVertexComponents:
 
     def set_precision(self, p):
         _check(lib.cmps_heff_set_precision(self.h, p))
+
+    def set_order(self, order):
+        """Contraction order of the FP64 matvec: CMPS_ORDER_AUTO, _FOLDED or
+        _CANONICAL."""
+        _check(lib.cmps_heff_set_order(self.h, order))
+
+    def order(self):
+        """(order in use, executed flops folded, executed flops canonical)."""
+        a = C.c_int()
+        f = C.c_double()
+        c = C.c_double()
+        _check(lib.cmps_heff_order(self.h, C.byref(a), C.byref(f), C.byref(c)))
+        return a.value, f.value, c.value
 
     def HED(self, guess=None, tol=1e-10, max_restarts=50, krylov_dim=24, want_vector=True):
         """Lowest eigenpair; returns (energy, eigenvector in ARPACK order or

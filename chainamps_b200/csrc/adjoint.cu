@@ -141,14 +141,14 @@ int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const En
   if (rc == CMPS_OK) {
     // <theta| (LP_d theta) RP >
     std::swap(H.LP, LPd);
-    rc = H.apply_fp64_stages(H.theta, H.y, st);
+    rc = H.apply_folded_fp64(H.theta, H.y, st);
     std::swap(H.LP, LPd);
   }
   if (rc == CMPS_OK) rc = H.ops.mdot_dev(H.theta.re(), H.theta.im(), 0, 1, H.y.re(), H.y.im(), d_out, st);
   if (rc == CMPS_OK) {
     // <theta| (LP theta) RP_d >
     std::swap(H.RP, RPd);
-    rc = H.apply_fp64_stages(H.theta, H.y, st);
+    rc = H.apply_folded_fp64(H.theta, H.y, st);
     std::swap(H.RP, RPd);
   }
   if (rc == CMPS_OK) rc = H.ops.mdot_dev(H.theta.re(), H.theta.im(), 0, 1, H.y.re(), H.y.im(), d_out + 3, st);

@@ -347,8 +347,30 @@ int cmps_heff_status(cmps_heff* h) {
 
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {
   if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
-  if (canonical) *canonical = h->impl->flops_canonical;
-  if (executed) *executed = h->impl->flops_executed;
+  const Heff& H = *h->impl;
+  if (canonical) *canonical = H.flops_canonical;
+  if (executed)
+    *executed = H.precision == CMPS_FP64 && H.order == CMPS_ORDER_CANONICAL ? H.flops_canon : H.flops_executed;
+  return CMPS_OK;
+}
+
+int cmps_heff_set_order(cmps_heff* h, int order) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (order != CMPS_ORDER_AUTO && order != CMPS_ORDER_FOLDED && order != CMPS_ORDER_CANONICAL)
+    return fail(CMPS_ERR_ARG, "unknown contraction order");
+  Heff& H = *h->impl;
+  CMPS_TRY(use_device(H.ctx));
+  CMPS_CUDA(cudaStreamSynchronize(H.ctx->stream));
+  H.order_req = order;
+  return H.select_order();
+}
+
+int cmps_heff_order(const cmps_heff* h, int* active, double* executed_folded, double* executed_canonical) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  const Heff& H = *h->impl;
+  if (active) *active = H.order;
+  if (executed_folded) *executed_folded = H.flops_folded;
+  if (executed_canonical) *executed_canonical = H.flops_canon;
   return CMPS_OK;
 }
 

@@ -225,6 +225,7 @@ int build_env_from_desc(const Rules& r, const cmps_mpx_desc* d, bool right, Env&
 // ---------------------------------------------------------------------------
 Heff::~Heff() {
   release_split(this);
+  release_canonical(this);
   L.data.release();
   R.data.release();
   LP.release();
@@ -522,19 +523,40 @@ int Heff::finish() {
       th.mq.push_back(m);
     }
   const int nm = (int)th.mq.size();
+  // charge classes of the physical states; blocks list states class by class
+  cls_mem.clear();
+  cls_of.assign(d, -1);
+  cls_pos.assign(d, -1);
+  {
+    std::map<QKey, int> cfind;
+    for (int s = 0; s < d; ++s) {
+      auto it = cfind.find(sigq[s]);
+      int c = it == cfind.end() ? -1 : it->second;
+      if (c < 0) {
+        c = (int)cls_mem.size();
+        cfind[sigq[s]] = c;
+        cls_mem.emplace_back();
+      }
+      cls_of[s] = c;
+      cls_pos[s] = (int)cls_mem[c].size();
+      cls_mem[c].push_back(s);
+    }
+  }
+  std::vector<int> sig_order;
+  for (const auto& mem : cls_mem) sig_order.insert(sig_order.end(), mem.begin(), mem.end());
   th.nrows.assign(nm, 0);
   th.ncols.assign(nm, 0);
   th.base.assign(nm, 0);
   th.rowoff.assign(nm, std::vector<int64_t>(d, -1));
   th.coloff.assign(nm, std::vector<int64_t>(d, -1));
   for (int m = 0; m < nm; ++m) {
-    for (int s1 = 0; s1 < d; ++s1) {
+    for (int s1 : sig_order) {
       int s = A0.find(r.sub(th.mq[m], sigq[s1]));
       if (s < 0) continue;
       th.rowoff[m][s1] = th.nrows[m];
       th.nrows[m] += A0.sdim[s];
     }
-    for (int s2 = 0; s2 < d; ++s2) {
+    for (int s2 : sig_order) {
       int t = A2.find(r.add(th.mq[m], sigq[s2]));
       if (t < 0) continue;
       th.coloff[m][s2] = th.ncols[m];
@@ -712,7 +734,26 @@ int Heff::finish() {
   CMPS_TRY(y.alloc(th.total));
   CMPS_CUDA(dmalloc(&d_io, sizeof(double) * 2 * std::max<int64_t>(1, n_allowed)));
   CMPS_TRY(ops.init(th.total));
+  CMPS_TRY(select_order());
   CMPS_CUDA(cudaStreamSynchronize(st));
+  return CMPS_OK;
+}
+
+// The FP64 matvec's contraction order: the one requested, or with
+// CMPS_ORDER_AUTO the canonical order when it executes at most half the
+// folded order's flops (it moves three intermediates through HBM where the
+// folded order moves one, so a small flop advantage does not pay).
+int Heff::select_order() {
+  flops_folded = flops_executed;
+  CMPS_TRY(canonical_flops(*this, &flops_canon));
+  int want = order_req;
+  if (want == CMPS_ORDER_AUTO) want = flops_canon <= 0.5 * flops_folded ? CMPS_ORDER_CANONICAL : CMPS_ORDER_FOLDED;
+  if (want == CMPS_ORDER_CANONICAL) {
+    CMPS_TRY(build_canonical(*this));
+  } else {
+    release_canonical(this);
+  }
+  order = want;
   return CMPS_OK;
 }
 
@@ -845,6 +886,7 @@ int Heff::set_owned(const uint8_t* mask) {
   for (int m = 0; m < nm; ++m) owned[m] = mask[m] ? 1 : 0;
   release_split(this);
   CMPS_TRY(build_plans());
+  CMPS_TRY(select_order());
   if (precision == CMPS_SPLIT_TF32) CMPS_TRY(prepare_precision(this, CMPS_SPLIT_TF32));
   return CMPS_OK;
 }
@@ -853,8 +895,11 @@ bool Heff::all_owned() const {
   return std::all_of(owned.begin(), owned.end(), [](uint8_t o) { return o != 0; });
 }
 
+// which = 1: the first half of the matvec (folded: T = LeftPart . in;
+// canonical: stages L and W1), 2: the second half.
 int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
   if (precision == CMPS_SPLIT_TF32) return apply_split_stage(*this, which, in, out, st);
+  if (order == CMPS_ORDER_CANONICAL) return apply_canonical(*this, which, in, out, st);
   if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
   return launch_zgemm_fp64(stage2, false, false, T, RP, out, st);
 }
@@ -867,6 +912,11 @@ int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int Heff::apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st) {
+  if (order == CMPS_ORDER_CANONICAL) return apply_canonical(*this, 0, in, out, st);
+  return apply_folded_fp64(in, out, st);
+}
+
+int Heff::apply_folded_fp64(const Planar& in, Planar& out, cudaStream_t st) {
   CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
   CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
   return CMPS_OK;

@@ -23,7 +23,8 @@ namespace cmps {
 // blocks Theta_m[(sigma1, a0), (sigma2, a2)], q(sigma1)+q(a0) = m =
 // q(a2)-q(sigma2).  Rows are grouped by sigma1 (each sigma1 contributes the
 // whole a0-sector of charge m - q(sigma1)), columns by sigma2 (a2-sector of
-// charge m + q(sigma2)); blocks are row-major.
+// charge m + q(sigma2)); the states appear class by class (Heff::cls_mem),
+// and blocks are row-major.
 struct ThetaSpace {
   std::vector<QKey> mq;                     // middle charges
   std::map<QKey, int> mfind;
@@ -38,6 +39,7 @@ struct ThetaSpace {
 
 struct SvdResult;
 struct SplitState;
+struct Canon;
 
 struct Heff {
   cmps_context* ctx = nullptr;
@@ -45,6 +47,11 @@ struct Heff {
   Rules rules;
   int d = 0;
   std::vector<QKey> sigq;       // basis charges
+  // Charge classes of the physical index: the states of one charge, classes
+  // in first-seen order, states in basis order.  Theta rows and columns are
+  // grouped by class, so a class's states are equally strided in a block.
+  std::vector<std::vector<int>> cls_mem;
+  std::vector<int> cls_of, cls_pos;  // state -> class, position inside it
   Env L, R;                     // environments (device)
   std::vector<WEntry> W;        // non-zero MPO entries
   int D = 0;
@@ -123,6 +130,15 @@ struct Heff {
   int set_projectors(int np, const double* host_arpack, const double* weights);
   int add_projectors(const Planar& in, Planar& out, cudaStream_t st);
   double flops_canonical = 0.0, flops_executed = 0.0;
+  // Contraction order of the FP64 matvec: folded (LeftPart / RightPart, the
+  // two stages above) or canonical (L, W1, W2, R one index at a time,
+  // canonical.cu).  order_req is what the caller asked for (CMPS_ORDER_*),
+  // order the one in use; flops_folded / flops_canon are the executed flops
+  // of each order.
+  int order_req = CMPS_ORDER_AUTO, order = CMPS_ORDER_FOLDED;
+  double flops_folded = 0.0, flops_canon = 0.0;
+  Canon* canon = nullptr;
+  int select_order();
   int precision = CMPS_FP64;
   SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)
   // work vectors
@@ -150,7 +166,8 @@ struct Heff {
   int finish();  // sector structure, LeftPart/RightPart, GEMM plans (L, R, W set)
   int apply_theta(const Planar& in, Planar& out, cudaStream_t st);  // theta-space matvec
   int apply_theta_fp64(const Planar& in, Planar& out, cudaStream_t st);   // with the projectors
-  int apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st);  // the two GEMM stages only
+  int apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st);  // the GEMM stages only (order in use)
+  int apply_folded_fp64(const Planar& in, Planar& out, cudaStream_t st);  // the two folded stages
   int apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st);  // 1: T = LP in, 2: out = T RP
   int apply_host(const double* in, double* out);
   int apply_device(const double* din, double* dout, cudaStream_t st);
@@ -191,6 +208,13 @@ int left_update(Heff& H, const SvdResult& s, Env& out);
 int right_update(Heff& H, const SvdResult& s, Env& out);
 int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, const Env* dL, const Env* dR,
                     Env& dLn, Env& dRn);
+
+// The canonical contraction order (canonical.cu).
+int canonical_flops(const Heff& H, double* flops);
+int build_canonical(Heff& H);
+void release_canonical(Heff* h);
+// which: 1 = stages L and W1, 2 = stages W2 and R, 0 = all four
+int apply_canonical(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
 
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);

@@ -52,15 +52,16 @@ int zero_wait(void* dst, size_t bytes, cudaStream_t st);
 cudaError_t dmalloc(void** p, size_t bytes);
 cudaError_t dfree(void* p);
 
+template <class T>
+inline cudaError_t dmalloc(T** p, size_t bytes) {
+  return dmalloc(reinterpret_cast<void**>(p), bytes);
+}
+
 // Dynamic shared memory opt-in of a kernel above 48 KB.  cudaFuncSetAttribute
 // applies to the current device only, so the opt-in is made once per (kernel,
 // device ordinal), under a lock: a process may drive several GPUs, and the
 // SVD's worker threads launch the same kernels concurrently.
 int ensure_smem_optin(const void* func, int bytes);
-template <class T>
-inline cudaError_t dmalloc(T** p, size_t bytes) {
-  return dmalloc(reinterpret_cast<void**>(p), bytes);
-}
 
 // Charge arithmetic of State (states.hpp:176-206).
 struct Rules {
@@ -122,15 +123,20 @@ struct WEntry {
 };
 
 // Grouped complex GEMM work description (device arrays).
+// With n_in > 0 the N index is two-level: column n of C (and of B) lies at
+// (n / n_in) * ldc_out + n % n_in (B: * ldb_out) from the row start, i.e. N
+// runs over n / n_in blocks of n_in consecutive elements; the plan must set
+// GemmPlan::nsplit.
 struct GemmTask {
   int64_t c_off;
   int32_t m, n, ldc;
   int32_t t0, t1;  // term range
-  int32_t pad;
+  int32_t n_in;    // 0: plain N
+  int32_t ldc_out, pad;
 };
 struct GemmTerm {
   int64_t a_off, b_off;
-  int32_t k, lda, ldb, pad;
+  int32_t k, lda, ldb, ldb_out;
 };
 struct GemmTile {
   int32_t task, m0, n0, pad;
@@ -144,6 +150,7 @@ struct GemmPlan {
   GemmTerm* d_terms = nullptr;
   GemmTile* d_tiles = nullptr;
   double flops = 0.0;
+  bool nsplit = false;  // tasks use the two-level N index (n_in > 0)
   int upload(int bm, int bn, cudaStream_t st);
   // Host check, before any launch, that every operand and output range lies
   // inside its buffer (lengths in complex elements).

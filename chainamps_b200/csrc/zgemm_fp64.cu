@@ -10,6 +10,9 @@
 // Operands are staged global -> shared with 8-byte cp.async (zero-filled
 // outside the block), double buffered.  op(A) is A or A^H (A stored K x M),
 // op(B) is B or B^H (B stored N x K), all row-major with leading dimensions.
+// NSPLIT: the N index of B and C is two-level (GemmTask::n_in), so one task
+// can run over several equally strided column ranges, e.g. the rows of
+// every state of one charge class, or one column class of every row.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,10 +46,18 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// Offset of column n under the two-level N index (NSPLIT), else n.
+template <bool NSPLIT>
+__device__ __forceinline__ int64_t ncol(int n, int n_in, int ld_out) {
+  if (!NSPLIT) return n;
+  const int q = n / n_in;
+  return (int64_t)q * ld_out + (n - q * n_in);
+}
+
 // Issue the cp.async copies of one (term, k-tile) into stage buffer `buf`.
-template <bool AH, bool BH>
+template <bool AH, bool BH, bool NSPLIT>
 __device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k0, int m0, int n0, int M,
-                                           int N, const double* __restrict__ Ar,
+                                           int N, int n_in, const double* __restrict__ Ar,
                                            const double* __restrict__ Ai, const double* __restrict__ Br,
                                            const double* __restrict__ Bi) {
   double* sAr = buf;
@@ -75,13 +86,15 @@ __device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k
     else     { kk = idx % BK; nn = idx / BK; }   // B stored [n][k]: along k
     int gn = n0 + nn, gk = k0 + kk;
     bool ok = (gn < N) && (gk < K);
-    int64_t o = ok ? (BH ? t.b_off + (int64_t)gn * t.ldb + gk : t.b_off + (int64_t)gk * t.ldb + gn) : 0;
+    int64_t o = ok ? (BH ? t.b_off + (int64_t)gn * t.ldb + gk
+                         : t.b_off + (int64_t)gk * t.ldb + ncol<NSPLIT>(gn, n_in, t.ldb_out))
+                   : 0;
     cp_async8(sBr + kk * LDS + nn, Br + o, ok);
     cp_async8(sBi + kk * LDS + nn, Bi + o, ok);
   }
 }
 
-template <bool AH, bool BH>
+template <bool AH, bool BH, bool NSPLIT>
 __global__ void __launch_bounds__(NTHREADS, 2)
 zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restrict__ tasks,
                    const GemmTerm* __restrict__ terms, const double* __restrict__ Ar,
@@ -110,7 +123,7 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
   bool have = cur_t < task.t1;
   if (have) {
     GemmTerm t = terms[cur_t];
-    load_stage<AH, BH>(smem, t, 0, m0, n0, M, N, Ar, Ai, Br, Bi);
+    load_stage<AH, BH, NSPLIT>(smem, t, 0, m0, n0, M, N, task.n_in, Ar, Ai, Br, Bi);
     cp_commit();
     nxt_k = BK;
     if (nxt_k >= t.k) { nxt_t = cur_t + 1; nxt_k = 0; }
@@ -120,7 +133,7 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
     bool more = nxt_t < task.t1;
     if (more) {
       GemmTerm t = terms[nxt_t];
-      load_stage<AH, BH>(smem + (stage ^ 1) * STAGE_DOUBLES, t, nxt_k, m0, n0, M, N, Ar, Ai, Br, Bi);
+      load_stage<AH, BH, NSPLIT>(smem + (stage ^ 1) * STAGE_DOUBLES, t, nxt_k, m0, n0, M, N, task.n_in, Ar, Ai, Br, Bi);
       cp_commit();
       cp_wait1();
     } else {
@@ -182,20 +195,20 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
         int gm = m0 + wm * 32 + i * 8 + gid;
         int gn = n0 + wn * 32 + j * 8 + 2 * tig + e;
         if (gm < M && gn < N) {
-          int64_t o = task.c_off + (int64_t)gm * task.ldc + gn;
+          int64_t o = task.c_off + (int64_t)gm * task.ldc + ncol<NSPLIT>(gn, task.n_in, task.ldc_out);
           Cr[o] = accr[i][j][e];
           Ci[o] = acci[i][j][e];
         }
       }
 }
 
-template <bool AH, bool BH>
+template <bool AH, bool BH, bool NSPLIT>
 int launch_variant(const GemmPlan& p, const Planar& A, const Planar& B, Planar& C, cudaStream_t st) {
-  CMPS_TRY(ensure_smem_optin((const void*)zgemm_grouped_fp64<AH, BH>, (int)SMEM_BYTES));
+  CMPS_TRY(ensure_smem_optin((const void*)zgemm_grouped_fp64<AH, BH, NSPLIT>, (int)SMEM_BYTES));
   if (p.tiles.empty()) return CMPS_OK;
   const int64_t ntiles = (int64_t)p.tiles.size();
   if (ntiles > 0x7fffffff) return fail(CMPS_ERR_ARG, "too many GEMM tiles");
-  zgemm_grouped_fp64<AH, BH><<<(unsigned)ntiles, NTHREADS, SMEM_BYTES, st>>>(
+  zgemm_grouped_fp64<AH, BH, NSPLIT><<<(unsigned)ntiles, NTHREADS, SMEM_BYTES, st>>>(
       p.d_tiles, p.d_tasks, p.d_terms, A.re(), A.im(), B.re(), B.im(), C.re(), C.im());
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
@@ -205,10 +218,14 @@ int launch_variant(const GemmPlan& p, const Planar& A, const Planar& B, Planar& 
 
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B, Planar& C,
                       cudaStream_t st) {
-  if (!a_h && !b_h) return launch_variant<false, false>(p, A, B, C, st);
-  if (a_h && !b_h) return launch_variant<true, false>(p, A, B, C, st);
-  if (!a_h && b_h) return launch_variant<false, true>(p, A, B, C, st);
-  return launch_variant<true, true>(p, A, B, C, st);
+  if (p.nsplit) {
+    if (a_h || b_h) return fail(CMPS_ERR_STATE, "two-level N index with a conjugate-transposed operand");
+    return launch_variant<false, false, true>(p, A, B, C, st);
+  }
+  if (!a_h && !b_h) return launch_variant<false, false, false>(p, A, B, C, st);
+  if (a_h && !b_h) return launch_variant<true, false, false>(p, A, B, C, st);
+  if (!a_h && b_h) return launch_variant<false, true, false>(p, A, B, C, st);
+  return launch_variant<true, true, false>(p, A, B, C, st);
 }
 
 int GemmPlan::upload(int bm, int bn, cudaStream_t st) {
@@ -236,7 +253,11 @@ int GemmPlan::validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t
     if (t.m < 0 || t.n < 0 || t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)terms.size())
       return fail(CMPS_ERR_STATE, std::string(what) + ": malformed task");
     if (t.m == 0 || t.n == 0) continue;
-    if (t.ldc < t.n || t.c_off < 0 || t.c_off + (int64_t)(t.m - 1) * t.ldc + t.n > c_len)
+    if ((t.n_in > 0) != nsplit || (nsplit && (a_h || b_h || t.ldc_out < t.n_in)))
+      return fail(CMPS_ERR_STATE, std::string(what) + ": malformed two-level N index");
+    // extent of one row of C or B along N: the last column's offset + 1
+    const int64_t nspan = nsplit ? (int64_t)((t.n - 1) / t.n_in) * t.ldc_out + (t.n - 1) % t.n_in + 1 : t.n;
+    if (t.c_off < 0 || t.c_off + (int64_t)(t.m - 1) * t.ldc + nspan > c_len || (!nsplit && t.ldc < t.n))
       return fail(CMPS_ERR_STATE, std::string(what) + ": output range outside its buffer");
     for (int q = t.t0; q < t.t1; ++q) {
       const GemmTerm& tm = terms[q];
@@ -246,8 +267,13 @@ int GemmPlan::validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t
       int64_t brows = b_h ? t.n : tm.k, bcols = b_h ? tm.k : t.n;
       if (tm.lda < acols || tm.a_off < 0 || tm.a_off + (arows - 1) * tm.lda + acols > a_len)
         return fail(CMPS_ERR_STATE, std::string(what) + ": A operand range outside its buffer");
-      if (tm.ldb < bcols || tm.b_off < 0 || tm.b_off + (brows - 1) * tm.ldb + bcols > b_len)
+      if (nsplit) {
+        const int64_t bspan = (int64_t)((t.n - 1) / t.n_in) * tm.ldb_out + (t.n - 1) % t.n_in + 1;
+        if (tm.ldb_out < t.n_in || tm.b_off < 0 || tm.b_off + (int64_t)(tm.k - 1) * tm.ldb + bspan > b_len)
+          return fail(CMPS_ERR_STATE, std::string(what) + ": B operand range outside its buffer");
+      } else if (tm.ldb < bcols || tm.b_off < 0 || tm.b_off + (brows - 1) * tm.ldb + bcols > b_len) {
         return fail(CMPS_ERR_STATE, std::string(what) + ": B operand range outside its buffer");
+      }
     }
   }
   return CMPS_OK;

@@ -194,7 +194,10 @@ def ising_chain_vertex(sites=12, g=1.2, keep=64, g_basis=None):
     sigma^x_i in the kept basis (parity odd)}, H (keep x keep, the vertex
     Hamiltonian at g in that basis), dH_dg (keep x keep), gap at the cut).
     The basis is built per parity sector in the sigma^z product basis with bit
-    operations; each eigenvector's sign makes its largest component positive.
+    operations; each eigenvector's sign makes its first largest component
+    (to 1e-9) positive, and degenerate levels are split by a fixed diagonal
+    operator without the chain's symmetries, so the
+    basis does not depend on the LAPACK build or its thread count.
     Near-degenerate states (momentum pairs) are kept or cut together only if
     the cut falls in a gap; the gap at the cut is returned."""
     gb = g if g_basis is None else g_basis
@@ -215,17 +218,45 @@ def ising_chain_vertex(sites=12, g=1.2, keep=64, g_basis=None):
             flip = (1 << i) | (1 << ((i + 1) % sites))
             Hs[np.arange(sel.size), pos[sel ^ flip]] -= 1.0
         w, v = np.linalg.eigh(Hs)
+        # Exactly degenerate levels (momentum pairs of the periodic chain,
+        # reflection multiplets): the eigensolver returns an arbitrary basis
+        # of each such subspace, which would make the kept state at a cut
+        # inside one depend on the LAPACK build and its thread count.  Fix
+        # it: inside each cluster, rotate to the eigenvectors of a fixed
+        # diagonal operator with no symmetry of the chain (cos(0.7 s + 0.3)
+        # on product state s) restricted to the subspace, ordered by its
+        # eigenvalue.
+        tol = 1e-9 * max(1.0, float(np.max(np.abs(w))))
+        splitter = np.cos(0.7 * sel.astype(np.float64) + 0.3)
+        k = 0
+        while k < w.size:
+            e = k + 1
+            while e < w.size and w[e] - w[e - 1] <= tol:
+                e += 1
+            if e - k > 1:
+                sub = v[:, k:e]
+                a, u = np.linalg.eigh(sub.T @ (splitter[:, None] * sub))
+                v[:, k:e] = sub @ u
+                w[k:e] = np.mean(w[k:e])
+            k = e
         for k in range(w.size):
             vec = np.zeros(n)
             vec[sel] = v[:, k]
-            j = int(np.argmax(np.abs(vec)))
+            # sign: the first component within 1e-9 (relative) of the largest
+            # magnitude is positive (symmetric states have many equal ones)
+            mag = np.abs(vec)
+            j = int(np.argmax(mag >= mag.max() * (1.0 - 1e-9)))
             if vec[j] < 0:
                 vec = -vec
             evals.append(w[k])
             vecs.append(vec)
             labels.append(par)
-    order = np.argsort(np.asarray(evals), kind="stable")
-    ev = np.asarray(evals)[order]
+    # ascending energy; levels equal to 1e-9 (relative) keep parity-then-basis
+    # order, so the order never rests on the last bits of the eigenvalues
+    evals = np.asarray(evals)
+    q = np.round(evals / (1e-9 * max(1.0, float(np.max(np.abs(evals)))))).astype(np.int64)
+    order = np.lexsort((np.arange(evals.size), np.asarray(labels), q))
+    ev = evals[order]
     gap = float(ev[keep] - ev[keep - 1]) if keep < ev.size else float("inf")
     order = order[:keep]
     V = np.stack([vecs[i] for i in order], axis=1)                   # n x keep, real

@@ -39,6 +39,19 @@ enum {
   CMPS_SPLIT_TF32 = 1      /* contractions as 3-term split TF32 on tcgen05, FP32 accumulate */
 };
 
+/* Contraction order of the FP64 matvec.  Folded: the reference's
+ * (LeftPart . V) . RightPart, W folded into the environments
+ * (DMRG_routines.cpp:779, :943).  Canonical: L . theta, then W on sigma1,
+ * W on sigma2, then . R, one index at a time -- the same operator, far fewer
+ * flops for a vertex with many states per charge and dense operators.
+ * Auto (the default) takes the canonical order when it executes at most half
+ * the folded order's flops. */
+enum {
+  CMPS_ORDER_AUTO = 0,
+  CMPS_ORDER_FOLDED = 1,
+  CMPS_ORDER_CANONICAL = 2
+};
+
 typedef struct cmps_context cmps_context;
 typedef struct cmps_heff cmps_heff;
 typedef struct cmps_svd cmps_svd;
@@ -110,9 +123,15 @@ int cmps_heff_apply(cmps_heff* h, const double* in, double* out);
 /* Same on DEVICE arrays, stream-ordered on `stream` (cudaStream_t or NULL). */
 int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void* stream);
 /* Algorithmic flops of one apply: canonical = L.theta, W1, W2, .R stages
- * over non-zero MPO entries (8 per complex MAC); executed = what the two
- * grouped GEMM launches actually issue. */
+ * over non-zero MPO entries (8 per complex MAC); executed = what the grouped
+ * GEMM launches of the handle's precision and contraction order issue. */
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
+/* Chooses the contraction order of the FP64 matvec (CMPS_ORDER_*); no
+ * counterpart in the reference, whose only order is the folded one. */
+int cmps_heff_set_order(cmps_heff* h, int order);
+/* The order in use (CMPS_ORDER_FOLDED or _CANONICAL) and the flops each
+ * order executes per FP64 matvec; any output may be NULL. */
+int cmps_heff_order(const cmps_heff* h, int* active, double* executed_folded, double* executed_canonical);
 /* H_eff matvec that allocates nothing (no counterpart in the reference).
  * For callers that cannot call cudaMalloc when they apply H_eff: an
  * eigensolver callback (ARPACK's MV, called hundreds of times per step)

@@ -246,9 +246,17 @@ class BlockTwoVertex:
     vertices whose dense LeftPart the dense restatement cannot hold (a
     64-state chain vertex at chi = 32 would need 1.7 GB for it)."""
 
-    def __init__(self, L, H, R):
+    def __init__(self, L, H, R, order="folded"):
+        """order: "folded" (LeftPart / RightPart blocks, ``BlockHeff``) or
+        "canonical" (L, W1, W2, R one index at a time, ``canonical.CanonicalHeff``)."""
         self.rules = H.rules
-        self.bh = from_mpx(H, L, R)
+        if order == "canonical":
+            from . import canonical
+            self.bh = canonical.from_mpx(H, L, R)
+        elif order == "folded":
+            self.bh = from_mpx(H, L, R)
+        else:
+            raise ValueError(order)
         sig = H.indices[2]
         self.indices = [sig.with_dir(True), L.indices[5].with_dir(True), sig.with_dir(True),
                         R.indices[4].with_dir(False)]

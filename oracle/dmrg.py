@@ -387,9 +387,11 @@ class SuperBlock:
 
     def __init__(self, H: MPX, target=None, tol=1e-14, heff="dense"):
         """heff: "dense" solves with the dense restatement of
-        TwoVertexComponents, "blocks" with the block port (``blocks.BlockTwoVertex``,
-        the same operator), for vertices too large for the dense form."""
-        if heff not in ("dense", "blocks"):
+        TwoVertexComponents; "blocks" with the folded block port and
+        "canonical" with the canonical-order block port
+        (``blocks.BlockTwoVertex``, the same operator), for vertices too large
+        for the dense form."""
+        if heff not in ("dense", "blocks", "canonical"):
             raise ValueError(heff)
         self.heff = heff
         self.H = H
@@ -460,9 +462,9 @@ class SuperBlock:
                     truncation=self.dec.truncation, fidelity=fid, chi=len(self.dec.values))
 
     def _solve(self, L, R, guess):
-        if self.heff == "blocks":
+        if self.heff in ("blocks", "canonical"):
             from .blocks import BlockTwoVertex
-            h = BlockTwoVertex(L, self.H, R)
+            h = BlockTwoVertex(L, self.H, R, order="folded" if self.heff == "blocks" else "canonical")
         else:
             h = TwoVertexComponents(L, self.H, R)
         self.last_heff = h

@@ -142,3 +142,13 @@ def charge_pool_for(H):
     pool |= {tuple(int(x) for x in s) for s in sig}
     pool.add(tuple([0] * len(rules)))
     return sorted(pool)
+
+
+def ising_mpo(sites=4, keep=8, g=1.2, j_perp=0.05):
+    """Oracle MPO of coupled transverse-field Ising chains: each vertex a
+    periodic chain of `sites` sites cut to its `keep` lowest states (Z2
+    parity), J_perp sum_i X_i X_i between vertices (MakeGeneralHMPO layout)."""
+    from chainamps_b200 import models
+    ch, ops, Hv, _, _ = models.ising_chain_vertex(sites, g, keep)
+    return om.make_general_hmpo(om.Vertex((2,), ch, ops, Hv),
+                                [om.Coupling(f"J{i}", f"X{i}", f"X{i}", j_perp) for i in range(sites)])
