@@ -553,10 +553,12 @@ class iDMRG:
         eigensolver's matvec counts and times; host wall times per phase."""
         keys = ("env_ms", "build_ms", "eig_ms", "svd_ms", "total_ms", "split_matvecs", "fp64_matvecs", "cycles",
                 "split_mv_ms", "fp64_mv_ms", "host_env_ms", "host_build_ms", "host_split_ms", "host_predict_ms",
-                "host_release_ms", "host_svd_ms", "host_total_ms")
+                "host_release_ms", "host_svd_ms", "host_total_ms", "svd_exact", "svd_gram", "svd_randomized",
+                "order")
+        ints = ("split_matvecs", "fp64_matvecs", "cycles", "svd_exact", "svd_gram", "svd_randomized", "order")
         v = np.zeros(len(keys), np.float64)
         _check(lib.cmps_dmrg_profile(self.h, _p(v, C.c_double), len(keys)))
-        return {k: (int(x) if k in ("split_matvecs", "fp64_matvecs", "cycles") else float(x)) for k, x in zip(keys, v)}
+        return {k: (int(x) if k in ints else float(x)) for k, x in zip(keys, v)}
 
     def values(self):
         v = np.zeros(self.last["chi"], np.float64)

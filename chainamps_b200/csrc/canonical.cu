@@ -45,9 +45,6 @@
 
 namespace cmps {
 
-int gemm_tile_m();
-int gemm_tile_n();
-
 struct Canon {
   Planar ops;    // MPO class blocks
   Planar xz, y;  // intermediates (X then Z; Y)

@@ -83,7 +83,7 @@ struct Dmrg {
   Env dL, dR;
   bool have_dlr = false;
   double last_grad = std::nan("");
-  static constexpr int kProfile = 17;
+  static constexpr int kProfile = 21;
   double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
 
   ~Dmrg() {
@@ -491,6 +491,17 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   svd.reset();
   heff = std::move(next);
   const auto h_rel = clock::now();
+  // a sweep step's fidelity compares the new state with the prediction the
+  // eigensolve starts from, so keep a copy of it
+  Planar guess;
+  struct PlanarGuard {
+    Planar* p;
+    ~PlanarGuard() { p->release(); }
+  } guess_guard{&guess};
+  if (dir != 0 && want_fidelity && have_guess) {
+    CMPS_TRY(guess.alloc(heff->th.total));
+    CMPS_CUDA(cudaMemcpyAsync(guess.d, heff->x.d, sizeof(double) * 2 * heff->th.total, cudaMemcpyDeviceToDevice, st));
+  }
   cudaEventRecord(ev[1], st);
   double e = 0.0;
   int nmv = 0;
@@ -520,6 +531,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   // growth steps report CheckConvergence, timed with the SVD phase
   double fid = std::nan("");
   if (dir == 0 && want_fidelity) CMPS_TRY(growth_fidelity(*heff, *svd, lambda, prev_lambda, &fid));
+  if (dir != 0 && want_fidelity && guess.d) CMPS_TRY(sweep_fidelity(*heff, *svd, lambda, guess, &fid));
   cudaEventRecord(ev[3], st);
   cudaEventSynchronize(ev[3]);
   const auto h_svd = clock::now();
@@ -549,7 +561,11 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
                                  ms_since(h_split, h_pred),
                                  ms_since(h_pred, h_rel),
                                  ms_since(h_eig, h_svd),
-                                 ms_since(h0, h_svd)};
+                                 ms_since(h0, h_svd),
+                                 (double)svd->routes[0],
+                                 (double)svd->routes[1],
+                                 (double)svd->routes[2],
+                                 (double)heff->order};
   for (int i = 0; i < kProfile; ++i) last_profile[i] = prof[i];
   if (dir == 0) size += 2;
   out[0] = e;
@@ -706,7 +722,7 @@ int cmps_dmrg_gradient(const cmps_dmrg* d, double* grad) {
 int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n) {
   if (!d || !d->impl || !out || n < 0) return fail(CMPS_ERR_ARG, "null argument");
   for (int i = 0; i < n && i < Dmrg::kProfile; ++i) out[i] = d->impl->last_profile[i];
-  return std::min(n, Dmrg::kProfile) == n ? CMPS_OK : fail(CMPS_ERR_ARG, "profile has 17 entries");
+  return std::min(n, Dmrg::kProfile) == n ? CMPS_OK : fail(CMPS_ERR_ARG, "profile has 21 entries");
 }
 
 int cmps_dmrg_unit_cell(cmps_dmrg* d, double tol, int krylov_dim, double* out6) {

@@ -23,9 +23,6 @@
 
 namespace cmps {
 
-int gemm_tile_m();
-int gemm_tile_n();
-
 // ---------------------------------------------------------------------------
 QKey Rules::add(const QKey& a, const QKey& b) const {
   QKey o = zero();

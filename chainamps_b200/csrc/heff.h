@@ -204,6 +204,7 @@ int derivative_parts(Heff& H, const std::vector<WEntry>& dW, const Env* dL, cons
 int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad);
 int growth_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, const std::vector<double>& prev,
                     double* out);
+int sweep_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, const Planar& guess, double* out);
 int left_update(Heff& H, const SvdResult& s, Env& out);
 int right_update(Heff& H, const SvdResult& s, Env& out);
 int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, const Env* dL, const Env* dR,

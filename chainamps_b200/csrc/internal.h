@@ -169,6 +169,9 @@ struct AxpyTerm {
 };
 
 // ---- kernels (launchers) ---------------------------------------------------
+// output tile of zgemm_grouped_fp64 (GemmPlan::upload splits tasks by it)
+int gemm_tile_m();
+int gemm_tile_n();
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
                       Planar& C, cudaStream_t st);
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,

@@ -15,6 +15,9 @@
 //   L'^{b1} = U^H (LeftPart^{b1} U),   R'^{b1} = (V^dag RightPart^{b1}) V^dag^H
 // as grouped GEMMs; the blocks stay on the device.
 #include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
@@ -306,6 +309,21 @@ __global__ void k_sum_final(const double* __restrict__ part, int n, double* __re
 }
 
 // G[:, j] /= s[j]  (column-major, rows x cols); zero columns where s[j] == 0
+// G (b x b, column-major) = R^H for the upper triangle R of a Householder QR
+// held in Z (column-major, leading dimension ld).
+__global__ void k_upper_adjoint(const double2* __restrict__ Z, int64_t ld, int64_t b, double2* __restrict__ G) {
+  const int64_t n = b * b;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e % b, j = e / b;
+    double2 v = make_double2(0.0, 0.0);
+    if (j <= i) {
+      const double2 r = Z[j + i * ld];  // R(j, i)
+      v = make_double2(r.x, -r.y);
+    }
+    G[e] = v;
+  }
+}
+
 __global__ void k_scale_cols_inv(double2* __restrict__ G, int64_t rows, int64_t cols, const double* __restrict__ s) {
   const int64_t n = rows * cols;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -380,6 +398,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     bool rnd = false;
     double tail = 0.0;
     std::vector<double> resid;
+    int64_t bb = 0;  // triplets the randomized route computed
     double2* dU = nullptr;
     double2* dV = nullptr;
     int64_t* drows = nullptr;
@@ -492,9 +511,12 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     // bb = chi + kRandPad triplets suffice whenever the checks of the global
     // selection pass.  Range of M (the sector, or its adjoint when it is
     // tall) by kRandIters subspace iterations with Cholesky QR
-    // re-orthonormalisation from a random start; then the eigenpairs of the
-    // bb x bb matrix B B^H with B = Q^H M.  Besides the triplets it records
-    // every triplet's residual and the weight outside the range found.
+    // re-orthonormalisation from a random start; then the SVD of the small
+    // matrix B = Q^H M itself: a Householder QR B^H = Q_B R and a one-sided
+    // Jacobi SVD of the bb x bb matrix R^H, so small singular values keep an
+    // absolute error of ~eps s_0 (the eigenvalues of B B^H would square it).
+    // Besides the triplets it records every triplet's residual and the
+    // weight outside the range found.
     const int64_t kRandPad = 32;
     const int kRandIters = 2;
     auto rand_b = [&](int64_t mn) -> int64_t {
@@ -504,17 +526,19 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     };
     auto rand_scratch = [&](int64_t nr, int64_t nc, int64_t bb) -> size_t {
       const int64_t pp = std::min(nr, nc), ll = std::max(nr, nc);
-      return (size_t)(2 * pp * bb + ll * bb + bb * bb + bb + kSumBlocks / 2 + 2);
+      return (size_t)(2 * pp * bb + 2 * ll * bb + 2 * bb * bb + 2 * bb + kSumBlocks / 2 + 2);
     };
-    auto rand_lwork = [&](cusolverDnHandle_t sol, int64_t bb, int* lw) -> int {
-      const int b32 = (int)bb;
-      int a = 0, g = 0;
+    auto rand_lwork = [&](cusolverDnHandle_t sol, gesvdjInfo_t prm, int64_t ll, int64_t bb, int* lw) -> int {
+      const int b32 = (int)bb, l32 = (int)ll;
+      int a = 0, q = 0, u = 0, g = 0;
       cuDoubleComplex* any = (cuDoubleComplex*)dA;
       if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
-          cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, b32, any, b32, dS, &g) !=
-              CUSOLVER_STATUS_SUCCESS)
+          cusolverDnZgeqrf_bufferSize(sol, l32, b32, any, l32, &q) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZungqr_bufferSize(sol, l32, b32, b32, any, l32, any, &u) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, b32, b32, any, b32, dS, any, b32, any, b32, &g,
+                                       prm) != CUSOLVER_STATUS_SUCCESS)
         return fail(CMPS_ERR_SOLVER, "randomized SVD buffer query failed");
-      *lw = std::max(std::max(a, g), 1);
+      *lw = std::max(std::max(std::max(a, q), std::max(u, g)), 1);
       return CMPS_OK;
     };
     auto factor_rand = [&](int m, int64_t bb, FW& fw) -> int {
@@ -535,16 +559,19 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (ownX && dmalloc(&X, sizeof(double2) * need) != cudaSuccess)
         return fail(CMPS_ERR_NOMEM, "randomized SVD scratch allocation failed");
       int lwork = 0;
-      int rc = rand_lwork(sol, bb, &lwork);
+      int rc = rand_lwork(sol, fw.params, ll, bb, &lwork);
       cuDoubleComplex* work = fw.work;
       const bool ownW = rc == CMPS_OK && (size_t)lwork > fw.workcap;
       if (ownW && dmalloc(&work, sizeof(cuDoubleComplex) * (size_t)lwork) != cudaSuccess)
         rc = fail(CMPS_ERR_NOMEM, "randomized SVD work allocation failed");
       double2* const Y = X;              // pp x bb: range basis Q
-      double2* const Z = Y + pp * bb;    // ll x bb: test matrix, then M^H Q
-      double2* const R = Z + ll * bb;    // pp x bb: reversed eigenvectors, then M O
-      double2* const Gb = R + pp * bb;   // bb x bb
-      double* const W = (double*)(Gb + bb * bb);
+      double2* const Z = Y + pp * bb;    // ll x bb: test matrix, then M^H Q = B^H, then Q_B
+      double2* const Z2 = Z + ll * bb;   // ll x bb: B^H kept for the tail
+      double2* const R = Z2 + ll * bb;   // pp x bb: left vectors of R^H, then M O
+      double2* const Gb = R + pp * bb;   // bb x bb: Gram matrices of the QR, then R^H
+      double2* const Vb = Gb + bb * bb;  // bb x bb: right vectors of R^H
+      double2* const tau = Vb + bb * bb; // bb: Householder scalars
+      double* const W = (double*)(tau + bb);
       double* const rs = W + bb;
       double* const part = rs + bb;
       double* const tailp = part + kSumBlocks;
@@ -595,36 +622,41 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         qr(Y, pp);
       }
       zg(opMH, CUBLAS_OP_N, ll, bb, pp, &one, dA, nr, Y, pp, &zero, Z, ll);    // Z = M^H Q = B^H
-      zg(CUBLAS_OP_C, CUBLAS_OP_N, bb, bb, ll, &one, Z, ll, Z, ll, &zero, Gb, bb);  // B B^H
-      if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)bb,
-                                            (cuDoubleComplex*)Gb, (int)bb, W, work, lwork, dinfo) !=
-                               CUSOLVER_STATUS_SUCCESS)
-        rc = fail(CMPS_ERR_SOLVER, "randomized SVD zheevd failed");
-      std::vector<double> w(bb);
+      if (rc == CMPS_OK && cudaMemcpyAsync(Z2, Z, sizeof(double2) * ll * bb, cudaMemcpyDeviceToDevice, st) !=
+                               cudaSuccess)
+        rc = fail(CMPS_ERR_CUDA, "randomized SVD copy failed");
+      // B^H = Q_B R (Householder), R^H = U_r S V_r^H, so B = U_r S (Q_B V_r)^H
+      if (rc == CMPS_OK && cusolverDnZgeqrf(sol, (int)ll, (int)bb, (cuDoubleComplex*)Z, (int)ll, (cuDoubleComplex*)tau,
+                                            work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "randomized SVD QR failed");
+      if (rc == CMPS_OK) k_upper_adjoint<<<grid_of(bb * bb), 256, 0, st>>>(Z, ll, bb, Gb);
+      if (rc == CMPS_OK && cusolverDnZungqr(sol, (int)ll, (int)bb, (int)bb, (cuDoubleComplex*)Z, (int)ll,
+                                            (const cuDoubleComplex*)tau, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "randomized SVD QR basis failed");
+      if (rc == CMPS_OK && cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)bb, (int)bb, (cuDoubleComplex*)Gb,
+                                             (int)bb, dS, (cuDoubleComplex*)R, (int)bb, (cuDoubleComplex*)Vb, (int)bb,
+                                             work, lwork, dinfo, fw.params) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(CMPS_ERR_SOLVER, "randomized SVD of the reduced matrix failed");
       int info = 0;
       if (rc == CMPS_OK) {
-        cudaMemcpyAsync(w.data(), W, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
+        b.s.assign(bb, 0.0);
+        cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess || info != 0)
-          rc = fail(CMPS_ERR_SOLVER, "randomized SVD: zheevd did not converge");
+        if (cudaStreamSynchronize(st) != cudaSuccess || info < 0)
+          rc = fail(CMPS_ERR_SOLVER, "randomized SVD: reduced SVD failed");
       }
       if (rc == CMPS_OK) {
-        b.s.assign(bb, 0.0);
-        for (int64_t j = 0; j < bb; ++j) b.s[j] = std::sqrt(std::max(0.0, w[bb - 1 - j]));
-        cudaMemcpyAsync(dS, b.s.data(), sizeof(double) * bb, cudaMemcpyHostToDevice, st);
         double2* F = left ? b.dU : b.dV;   // short-side vectors (ld pp)
         double2* O = left ? b.dV : b.dU;   // long-side vectors (ld ll)
-        k_reverse_cols<<<grid_of(bb * bb), 256, 0, st>>>(Gb, bb, R);
-        zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);  // F = Q X
-        zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, R, bb, &zero, O, ll);  // O = M^H F
-        if (rc == CMPS_OK) k_scale_cols_inv<<<grid_of(ll * bb), 256, 0, st>>>(O, ll, bb, dS);
+        zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);   // F = Q U_r
+        zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, Vb, bb, &zero, O, ll);  // O = Q_B V_r
         zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, O, ll, &zero, R, pp);     // M O
         if (rc == CMPS_OK) k_col_resid<<<(unsigned)bb, 256, 0, st>>>(R, F, dS, pp, rs);
         // A <- A - Q Q^H A (left) or A - A Q Q^H (tall): the part outside the range
         if (left)
-          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Y, nr, Z, nc, &one, dA, nr);
+          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Y, nr, Z2, nc, &one, dA, nr);
         else
-          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Z, nr, Y, nc, &one, dA, nr);
+          zg(CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, bb, &mone, Z2, nr, Y, nc, &one, dA, nr);
         if (rc == CMPS_OK) {
           k_sumsq_partial<<<kSumBlocks, 256, 0, st>>>(dA, nr * nc, part);
           k_sum_final<<<1, 32, 0, st>>>(part, kSumBlocks, tailp);
@@ -651,7 +683,8 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       return rc;
     };
     // mode 0: randomized route where eligible, else by size; 1: Gram route
-    // for sectors of at least kEigMin, else exact; 2: exact
+    // for sectors of at least kEigMin, else exact; 2: exact; 3: randomized
+    // route with blk[m].bb triplets (a wider range than mode 0's)
     auto factor = [&](int m, int mode, FW& fw) -> int {
       const cudaStream_t st = fw.st;
       const cusolverDnHandle_t sol = fw.sol;
@@ -670,7 +703,11 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       b.rnd = false;
       b.tail = 0.0;
       b.resid.clear();
-      if (mode == 0 && rand_b(mn) > 0) return factor_rand(m, rand_b(mn), fw);
+      if (mode == 0 && rand_b(mn) > 0) {
+        b.bb = rand_b(mn);
+        return factor_rand(m, b.bb, fw);
+      }
+      if (mode == 3) return factor_rand(m, b.bb, fw);
       b.s.resize(mn);
       if (mode == 2 || mn < kEigMin) {
         b.eig = false;
@@ -810,7 +847,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           int lwork = 0;
           if (rand_b(mn) > 0) {
             nX[k] = std::max(nX[k], rand_scratch(nr, nc, rand_b(mn)));
-            if (rand_lwork(w.sol, rand_b(mn), &lwork) != CMPS_OK) ok = false;
+            if (rand_lwork(w.sol, fws[k].params, std::max(nr, nc), rand_b(mn), &lwork) != CMPS_OK) ok = false;
           } else if (mn < kEigMin) {
             if (cusolverDnZgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)blk[m].dU, (int)nr,
@@ -944,15 +981,18 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
         const int64_t np = (int64_t)sv.size();
         const int64_t cap = (chi > 0 && chi < n_true) ? chi : n_true;
         bool valid = cap < n_true && cap + 1 < np && sv[0] > 0.0;
+        int failed = valid ? 0 : 0x10;  // which check failed (CMPS_SVD_TRACE)
         if (valid) {
           double beyond = tail_total;
           for (int64_t i = cap - 1; i < np; ++i) beyond += sv[i] * sv[i];
           valid = beyond >= 1.01 * max_trunc;                                   // (1)
+          if (!valid) failed = 1;
         }
         int64_t len = cap;
         if (valid) {
           while (len < n_true && len < np && (sv[len - 1] - sv[len]) / sv[len - 1] < 1.0e-3) ++len;
           valid = len < np;                                                     // (2)
+          if (!valid) failed = 2;
         }
         if (valid) {
           const double next = sv[len];
@@ -960,15 +1000,35 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           for (int64_t g = 0; g < len; ++g) kept[all[g].m] = std::max(kept[all[g].m], all[g].j + 1);
           for (int m = 0; m < nm && valid; ++m) {
             if (!blk[m].rnd) continue;
-            if (!(4.0 * blk[m].tail < next * next)) valid = false;             // (3)
+            if (!(4.0 * blk[m].tail < next * next)) valid = false, failed = 3;  // (3)
             for (int64_t j = 0; j < kept[m] && valid; ++j)
               if (!(blk[m].resid[j] <= 1e-12 * sv[0] + 500.0 * kEps * sv[0] * sv[0] / blk[m].s[j]))
-                valid = false;                                                  // (4)
+                valid = false, failed = 4;                                      // (4)
           }
         }
+        if (std::getenv("CMPS_SVD_TRACE")) {
+          std::fprintf(stderr, "svd pass %d: randomized %s (check %d)", pass, valid ? "accepted" : "rejected", failed);
+          for (int m = 0; m < nm; ++m)
+            if (blk[m].rnd)
+              std::fprintf(stderr, "  [m%d b=%lld tail=%.3g]", m, (long long)blk[m].bb, blk[m].tail);
+          std::fprintf(stderr, "\n");
+        }
         if (!valid) {
-          for (int m = 0; m < nm && status == CMPS_OK; ++m)
-            if (blk[m].rnd) status = factor(m, 1, main_fw);
+          // A spectrum that decays slowly past the range leaves too much
+          // tail (check 3): widen the range (twice the triplets) while it
+          // stays well under the sector's short side, else take the Gram
+          // route.  Both cost far less than the one-sided Jacobi SVD that
+          // the Gram route falls back to for kept values below 1e-5 s_0.
+          for (int m = 0; m < nm && status == CMPS_OK; ++m) {
+            if (!blk[m].rnd) continue;
+            const int64_t mn = std::min(blk[m].rows.size(), blk[m].cols.size());
+            if (4 * (2 * blk[m].bb) <= 3 * mn) {
+              blk[m].bb *= 2;
+              status = factor(m, 3, main_fw);
+            } else {
+              status = factor(m, 1, main_fw);
+            }
+          }
           continue;
         }
         length = len;
@@ -978,7 +1038,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       const double floor2 = 1e-10 * sv[0] * sv[0];
       bool redo = false;
       for (int m = 0; m < nm; ++m) {
-        if (!blk[m].eig) continue;
+        if (!blk[m].eig || blk[m].rnd) continue;  // the randomized route resolves small values directly
         bool low = false;
         for (int64_t g = 0; g < length; ++g)
           if (all[g].m == m && all[g].v * all[g].v < floor2) low = true;
@@ -1131,6 +1191,66 @@ int growth_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam,
   cusolverDnDestroyGesvdjInfo(params);
   CMPS_TRY(status);
   *out = 1.0 - total;
+  return CMPS_OK;
+}
+
+// CheckConvergence(Prediction, MPSDecomposition) (DMRG_routines.cpp:773-776),
+// the fidelity of a finite sweep step: 1 - |<G, U diag(lam) V^dagger>|, G the
+// predicted wavefunction the step's eigensolve started from (theta layout)
+// and U diag(lam) V^dagger the new rescaled decomposition.  Per block m:
+// P_m = U_m^H G_m (kept x ncols, one grouped GEMM), then the lam-weighted
+// dot of P_m with V^dagger_m, summed on the host (both are chi x d chi).
+int sweep_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, const Planar& guess, double* out) {
+  const ThetaSpace& th = s.th;
+  const int nm = (int)th.mq.size();
+  if (guess.len != th.total) return fail(CMPS_ERR_STATE, "fidelity: guess is not in this theta layout");
+  cudaStream_t st = H.ctx->stream;
+  GemmPlan p;
+  for (int m = 0; m < nm; ++m) {
+    if (!s.kept[m]) continue;
+    GemmTask t{};
+    t.c_off = s.voff[m];  // P_m shares V^dagger_m's layout
+    t.m = (int32_t)s.kept[m];
+    t.n = (int32_t)th.ncols[m];
+    t.ldc = (int32_t)th.ncols[m];
+    t.t0 = (int32_t)p.terms.size();
+    GemmTerm tm{};
+    tm.a_off = s.uoff[m];  // U_m stored nrows x kept: op(A) = U_m^H
+    tm.lda = (int32_t)s.kept[m];
+    tm.k = (int32_t)th.nrows[m];
+    tm.b_off = th.base[m];
+    tm.ldb = (int32_t)th.ncols[m];
+    p.terms.push_back(tm);
+    t.t1 = (int32_t)p.terms.size();
+    p.tasks.push_back(t);
+  }
+  double total_re = 0.0, total_im = 0.0;
+  if (!p.tasks.empty()) {
+    Planar P;
+    CMPS_TRY(P.alloc(s.Vd.len));
+    int rc = p.validate(true, false, s.U.len, guess.len, P.len, "fidelity");
+    if (rc == CMPS_OK) rc = p.upload(gemm_tile_m(), gemm_tile_n(), st);
+    if (rc == CMPS_OK) rc = launch_zgemm_fp64(p, true, false, s.U, guess, P, st);
+    std::vector<double> hp(2 * (size_t)s.Vd.len), hv(2 * (size_t)s.Vd.len);
+    if (rc == CMPS_OK) rc = copy_wait(hp.data(), P.d, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st);
+    if (rc == CMPS_OK) rc = copy_wait(hv.data(), s.Vd.d, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, st);
+    p.release();
+    P.release();
+    CMPS_TRY(rc);
+    const int64_t n = s.Vd.len;
+    for (int m = 0; m < nm; ++m)
+      for (int64_t j = 0; j < s.kept[m]; ++j) {
+        const double w = lam[s.gidx[m][j]];
+        for (int64_t k = 0; k < th.ncols[m]; ++k) {
+          const int64_t o = s.voff[m] + j * th.ncols[m] + k;
+          // conj(P) . Vd
+          const double pr = hp[o], pi = hp[n + o], vr = hv[o], vi = hv[n + o];
+          total_re += w * (pr * vr + pi * vi);
+          total_im += w * (pr * vi - pi * vr);
+        }
+      }
+  }
+  *out = 1.0 - std::hypot(total_re, total_im);
   return CMPS_OK;
 }
 

@@ -347,12 +347,13 @@ int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);
 int cmps_dmrg_set_gradient(cmps_dmrg* d, const cmps_mpx_desc* dW);
 int cmps_dmrg_gradient(const cmps_dmrg* d, double* grad);
 /* Breakdown of the last growth step (no reference counterpart;
- * diagnostics).  Writes the first n (<= 17) of: {environment update ms, H_eff
+ * diagnostics).  Writes the first n (<= 21) of: {environment update ms, H_eff
  * build + prediction ms, eigensolve ms, SVD ms, total ms (device time, CUDA
  * events); split matvecs, FP64 matvecs, restart cycles, split matvec ms,
  * FP64 matvec ms; host wall ms of environment update, H_eff build, split
  * operand preparation, prediction, release of the previous step, SVD, whole
- * step}. */
+ * step; SVD sectors factored exactly, by the Gram matrix, by the randomized
+ * route; contraction order of the FP64 matvec (CMPS_ORDER_*)}. */
 int cmps_dmrg_profile(const cmps_dmrg* d, double* out, int n);
 
 /* ---- MPX_matrix files (host only) ---------------------------------------

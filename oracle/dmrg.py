@@ -351,6 +351,17 @@ def check_convergence(aux, prev_lambda):
     return 1.0 - float(np.sum(s))
 
 
+def check_convergence_finite(guess, dec: Decomposition):
+    """CheckConvergence(Prediction, MPSDecomposition) (DMRG_routines.cpp:773-776):
+    1 - |Tr(G^dagger . U diag(s) V^dagger)|, G the prediction vector reshaped to
+    rows (sigma1, a0) (column-major, ``reshape`` of sparse_interface.cpp:966-1003),
+    U diag(s) V^dagger the new (rescaled) decomposition in the same layout."""
+    us = contract(dec.U, False, diag_mpx(dec.U.rules, dec.U.indices[2], dec.values), False, [(2, 0)])
+    M = contract(us, False, dec.Vd, False, [(2, 0)]).matrix()
+    G = np.asarray(guess, np.complex128).reshape(M.shape, order="F")
+    return 1.0 - abs(np.trace(G.conj().T @ M))
+
+
 def make_r_finite_prediction(dec: Decomposition, B: MPX):
     """MakeRFinitePrediction (DMRG_routines.cpp:713-716)."""
     lam = diag_mpx(dec.U.rules, dec.U.indices[2], dec.values)
@@ -507,7 +518,8 @@ class SuperBlock:
         self.lmps[self.nleft + 1] = left_shape(self.dec.U)
         self.rmps[nr + 1] = right_shape(self.dec.Vd)
         return dict(energy=e, energy_per=e / self.size, entropy=entropy(self.dec.values),
-                    truncation=self.dec.truncation, chi=len(self.dec.values))
+                    truncation=self.dec.truncation, chi=len(self.dec.values),
+                    fidelity=check_convergence_finite(guess, self.dec))
 
     def move_left(self, chi=0, trunc=0.0):
         """SuperBlock::move_left_two_vertex (DMRG_routines.cpp:411-444)."""
@@ -534,7 +546,8 @@ class SuperBlock:
         self.lmps[self.nleft + 1] = left_shape(self.dec.U)
         self.rmps[nr + 1] = right_shape(self.dec.Vd)
         return dict(energy=e, energy_per=e / self.size, entropy=entropy(self.dec.values),
-                    truncation=self.dec.truncation, chi=len(self.dec.values))
+                    truncation=self.dec.truncation, chi=len(self.dec.values),
+                    fidelity=check_convergence_finite(guess, self.dec))
 
 
 def two_vertex_initial_wavefunction(LeftH: MPX, RightH: MPX, target):

@@ -110,6 +110,13 @@ def test_device_fdmrg_reproduces_spin_half_example(ctx):
         assert abs(r["energy_per"] - e[2]) <= 1e-10 * abs(e[2])
         assert abs(r["entropy"] - e[3]) <= 1e-8, (r, e)
         assert abs(r["truncation"] - e[4]) <= 1e-12
+    # fidelity: growth rows as printed; sweep rows as the oracle's restatement
+    # of CheckConvergence(Prediction, MPSDecomposition), 0 to rounding for
+    # these converged sweeps (the README prints 1 there; see the oracle's KAT)
+    for r, e in zip(rows[:5], k["energies"][:5]):
+        assert abs(r["fidelity"] - e[5]) <= 1e-10, (r, e)
+    for r in rows[5:]:
+        assert 0.0 <= r["fidelity"] <= 1e-10, r
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -128,6 +135,9 @@ def test_device_fdmrg_matches_oracle_with_truncation(ctx, precision):
         assert abs(r["energy"] - e["energy"]) <= 1e-9 * abs(e["energy"]), (r, e)
         assert abs(r["entropy"] - e["entropy"]) <= 1e-7, (r, e)
         assert abs(r["truncation"] - e["truncation"]) <= 1e-11
+        # growth rows: CheckConvergence(Prediction, previous values); sweep
+        # rows: CheckConvergence(Prediction, MPSDecomposition)
+        assert abs(r["fidelity"] - e["fidelity"]) <= (1e-8 if precision == "fp64" else 1e-6), (r, e)
 
 
 def test_finite_prediction_starts_sweep_steps_close():

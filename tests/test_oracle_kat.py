@@ -33,6 +33,34 @@ def test_spin_half_fdmrg_kat():
         assert abs(r["truncation"] - e[4]) <= 1e-20                   # discarded weight
     for r, e in zip(rows[:5], ref[:5]):                               # growth-step fidelity
         assert abs(r["fidelity"] - e[5]) <= 1e-10
+    # Sweep rows: CheckConvergence(Prediction, MPSDecomposition)
+    # (DMRG_routines.cpp:773-776), 1 - |<prediction, new state>|.  The sweeps
+    # have converged, so the finite prediction is the new state itself and the
+    # restated formula gives 0 to rounding.  The README prints 1 in these rows,
+    # i.e. an overlap of exactly zero, which this formula gives only for a
+    # prediction orthogonal to the state; the oracle keeps the formula.
+    for r in rows[5:]:
+        assert 0.0 <= r["fidelity"] <= 1e-12, r
+
+
+def test_sweep_fidelity_formula():
+    """The restated CheckConvergence(Prediction, MPSDecomposition): 0 for a
+    prediction equal to the new state, 1 for one orthogonal to it."""
+    from oracle import dmrg as od
+    from oracle.mpx import contract, diag_mpx
+    k = json.load(open(GOLD))["spin_half_fdmrg"]
+    H = _model(k)
+    sb = od.SuperBlock(H, tol=1e-13)
+    for _ in range(3):
+        sb.grow(8, 0.0)
+    dec = sb.dec
+    us = contract(dec.U, False, diag_mpx(dec.U.rules, dec.U.indices[2], dec.values), False, [(2, 0)])
+    theta = contract(us, False, dec.Vd, False, [(2, 0)]).matrix().reshape(-1, order="F")
+    assert abs(od.check_convergence_finite(theta, dec)) <= 1e-13
+    assert abs(od.check_convergence_finite(-1j * theta, dec)) <= 1e-13
+    other = np.zeros_like(theta)
+    other[np.argmax(np.abs(theta) == 0)] = 1.0      # an entry where the state vanishes
+    assert abs(od.check_convergence_finite(other, dec) - 1.0) <= 1e-15
 
 
 def test_quench_fdmrg_kat():
