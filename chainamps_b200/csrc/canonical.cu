@@ -409,7 +409,7 @@ int build_canonical(Heff& H) {
   C->sW2 = std::move(P.sW2);
   C->sR = std::move(P.sR);
   for (GemmPlan* p : {&C->sL, &C->sW1, &C->sW2, &C->sR})
-    if ((rc = p->upload(gemm_tile_m(), gemm_tile_n(), st)) != CMPS_OK) return bail(rc);
+    if ((rc = p->upload(st)) != CMPS_OK) return bail(rc);
   C->flops = P.flops;
   return CMPS_OK;
 }

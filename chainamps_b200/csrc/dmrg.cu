@@ -245,7 +245,7 @@ int Dmrg::predict(Heff& next, bool* ok) {
       }
     if (!p.tasks.empty()) {
       status = p.validate(false, false, Vs.len, Us.len, tn.total, "prediction");
-      if (status == CMPS_OK) status = p.upload(64, 64, st);
+      if (status == CMPS_OK) status = p.upload(st);
       if (status == CMPS_OK) {
         cudaMemsetAsync(next.x.d, 0, sizeof(double) * 2 * tn.total, st);
         status = launch_zgemm_fp64(p, false, false, Vs, Us, next.x, st);
@@ -374,7 +374,7 @@ int Dmrg::finite_predict(Heff& next, int dir, bool* ok) {
     const Planar& A = dir > 0 ? S : O.U;
     const Planar& B = dir > 0 ? O.Vd : S;
     status = p.validate(false, false, A.len, B.len, tn.total, "finite prediction");
-    if (status == CMPS_OK) status = p.upload(64, 64, st);
+    if (status == CMPS_OK) status = p.upload(st);
     if (status == CMPS_OK) {
       cudaMemsetAsync(next.x.d, 0, sizeof(double) * 2 * tn.total, st);
       status = launch_zgemm_fp64(p, false, false, A, B, next.x, st);

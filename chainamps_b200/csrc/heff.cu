@@ -872,8 +872,8 @@ int Heff::build_plans() {
   CMPS_TRY(stage1.validate(false, false, LP.len, th.total, t_total, "stage 1"));
   CMPS_TRY(stage2.validate(false, false, t_total, RP.len, th.total, "stage 2"));
   if (all_owned()) sector_flops = fl;
-  CMPS_TRY(stage1.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
-  CMPS_TRY(stage2.upload(gemm_tile_m(), gemm_tile_n(), ctx->stream));
+  CMPS_TRY(stage1.upload(ctx->stream));
+  CMPS_TRY(stage2.upload(ctx->stream));
   return CMPS_OK;
 }
 

@@ -151,7 +151,10 @@ struct GemmPlan {
   GemmTile* d_tiles = nullptr;
   double flops = 0.0;
   bool nsplit = false;  // tasks use the two-level N index (n_in > 0)
-  int upload(int bm, int bn, cudaStream_t st);
+  int shape = -1;       // output tile shape (gemm_shape_m / _n), chosen by upload
+  // Picks the tile shape for these tasks, splits them into tiles and copies
+  // the plan to the device.
+  int upload(cudaStream_t st);
   // Host check, before any launch, that every operand and output range lies
   // inside its buffer (lengths in complex elements).
   int validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t c_len, const char* what) const;
@@ -169,9 +172,9 @@ struct AxpyTerm {
 };
 
 // ---- kernels (launchers) ---------------------------------------------------
-// output tile of zgemm_grouped_fp64 (GemmPlan::upload splits tasks by it)
-int gemm_tile_m();
-int gemm_tile_n();
+// output tile shapes of zgemm_grouped_fp64 (GemmPlan::shape)
+int gemm_shape_m(int shape);
+int gemm_shape_n(int shape);
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
                       Planar& C, cudaStream_t st);
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,

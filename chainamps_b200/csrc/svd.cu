@@ -1229,7 +1229,7 @@ int sweep_fidelity(Heff& H, const SvdResult& s, const std::vector<double>& lam, 
     Planar P;
     CMPS_TRY(P.alloc(s.Vd.len));
     int rc = p.validate(true, false, s.U.len, guess.len, P.len, "fidelity");
-    if (rc == CMPS_OK) rc = p.upload(gemm_tile_m(), gemm_tile_n(), st);
+    if (rc == CMPS_OK) rc = p.upload(st);
     if (rc == CMPS_OK) rc = launch_zgemm_fp64(p, true, false, s.U, guess, P, st);
     std::vector<double> hp(2 * (size_t)s.Vd.len), hv(2 * (size_t)s.Vd.len);
     if (rc == CMPS_OK) rc = copy_wait(hp.data(), P.d, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st);
@@ -1371,8 +1371,8 @@ int left_update(Heff& H, const SvdResult& s, Env& out) {
   do {
     if ((status = px.validate(false, false, H.LP.len, s.U.len, xt, "left update X")) != CMPS_OK) break;
     if ((status = pl.validate(true, false, s.U.len, xt, out.data.len, "left update")) != CMPS_OK) break;
-    if ((status = px.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
-    if ((status = pl.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = px.upload(H.ctx->stream)) != CMPS_OK) break;
+    if ((status = pl.upload(H.ctx->stream)) != CMPS_OK) break;
     Planar Ucopy = s.U;  // non-owning view
     if ((status = launch_zgemm_fp64(px, false, false, H.LP, Ucopy, X, H.ctx->stream)) != CMPS_OK) break;
     if ((status = launch_zgemm_fp64(pl, true, false, Ucopy, X, out.data, H.ctx->stream)) != CMPS_OK) break;
@@ -1467,8 +1467,8 @@ int right_update(Heff& H, const SvdResult& s, Env& out) {
   do {
     if ((status = py.validate(false, false, s.Vd.len, H.RP.len, yt, "right update Y")) != CMPS_OK) break;
     if ((status = pr.validate(false, true, yt, s.Vd.len, out.data.len, "right update")) != CMPS_OK) break;
-    if ((status = py.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
-    if ((status = pr.upload(64, 64, H.ctx->stream)) != CMPS_OK) break;
+    if ((status = py.upload(H.ctx->stream)) != CMPS_OK) break;
+    if ((status = pr.upload(H.ctx->stream)) != CMPS_OK) break;
     Planar Vview = s.Vd;
     if ((status = launch_zgemm_fp64(py, false, false, Vview, H.RP, Y, H.ctx->stream)) != CMPS_OK) break;
     if ((status = launch_zgemm_fp64(pr, false, true, Y, Vview, out.data, H.ctx->stream)) != CMPS_OK) break;

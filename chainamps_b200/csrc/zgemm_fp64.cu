@@ -24,12 +24,23 @@ namespace cmps {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, LDS = 68;  // LDS = BM + 4: conflict-free 8-byte fragment reads
+// Output tile BM x BN, four warps of 32 x 32 each (WN = BN / 32 across N).
+// Shapes: 64 x 64 (square blocks), 32 x 128 (tasks with M <= 32: a charge
+// class of 32 states, a small a0 sector) and 128 x 32 (tasks with N <= 32).
+// Shared-memory rows are padded to BM + 4 / BN + 4 doubles (= 4 mod 16):
+// conflict-free 8-byte fragment reads.
+constexpr int BK = 16;
 constexpr int NTHREADS = 128;
 constexpr int STAGES = 2;
-constexpr int PLANE = BK * LDS;                      // doubles per plane per operand per stage
-constexpr int STAGE_DOUBLES = 4 * PLANE;             // A re, A im, B re, B im
-constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DOUBLES * sizeof(double);
+template <int BM, int BN>
+struct Tile {
+  static_assert(BM % 32 == 0 && BN % 32 == 0 && (BM / 32) * (BN / 32) == 4, "four 32 x 32 warp tiles");
+  static constexpr int WN = BN / 32;
+  static constexpr int LDA = BM + 4, LDB = BN + 4;
+  static constexpr int PLANE_A = BK * LDA, PLANE_B = BK * LDB;  // doubles per plane per stage
+  static constexpr int STAGE_DOUBLES = 2 * PLANE_A + 2 * PLANE_B;  // A re, A im, B re, B im
+  static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_DOUBLES * sizeof(double);
+};
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -55,15 +66,16 @@ __device__ __forceinline__ int64_t ncol(int n, int n_in, int ld_out) {
 }
 
 // Issue the cp.async copies of one (term, k-tile) into stage buffer `buf`.
-template <bool AH, bool BH, bool NSPLIT>
+template <int BM, int BN, bool AH, bool BH, bool NSPLIT>
 __device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k0, int m0, int n0, int M,
                                            int N, int n_in, const double* __restrict__ Ar,
                                            const double* __restrict__ Ai, const double* __restrict__ Br,
                                            const double* __restrict__ Bi) {
+  using T = Tile<BM, BN>;
   double* sAr = buf;
-  double* sAi = buf + PLANE;
-  double* sBr = buf + 2 * PLANE;
-  double* sBi = buf + 3 * PLANE;
+  double* sAi = buf + T::PLANE_A;
+  double* sBr = buf + 2 * T::PLANE_A;
+  double* sBi = sBr + T::PLANE_B;
   const int tid = threadIdx.x;
   const int K = t.k;
 #pragma unroll
@@ -75,8 +87,8 @@ __device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k
     int gm = m0 + mm, gk = k0 + kk;
     bool ok = (gm < M) && (gk < K);
     int64_t o = ok ? (AH ? t.a_off + (int64_t)gk * t.lda + gm : t.a_off + (int64_t)gm * t.lda + gk) : 0;
-    cp_async8(sAr + kk * LDS + mm, Ar + o, ok);
-    cp_async8(sAi + kk * LDS + mm, Ai + o, ok);
+    cp_async8(sAr + kk * T::LDA + mm, Ar + o, ok);
+    cp_async8(sAi + kk * T::LDA + mm, Ai + o, ok);
   }
 #pragma unroll
   for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
@@ -89,12 +101,12 @@ __device__ __forceinline__ void load_stage(double* buf, const GemmTerm& t, int k
     int64_t o = ok ? (BH ? t.b_off + (int64_t)gn * t.ldb + gk
                          : t.b_off + (int64_t)gk * t.ldb + ncol<NSPLIT>(gn, n_in, t.ldb_out))
                    : 0;
-    cp_async8(sBr + kk * LDS + nn, Br + o, ok);
-    cp_async8(sBi + kk * LDS + nn, Bi + o, ok);
+    cp_async8(sBr + kk * T::LDB + nn, Br + o, ok);
+    cp_async8(sBi + kk * T::LDB + nn, Bi + o, ok);
   }
 }
 
-template <bool AH, bool BH, bool NSPLIT>
+template <int BM, int BN, bool AH, bool BH, bool NSPLIT>
 __global__ void __launch_bounds__(NTHREADS, 2)
 zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restrict__ tasks,
                    const GemmTerm* __restrict__ terms, const double* __restrict__ Ar,
@@ -105,7 +117,8 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
   const GemmTask task = tasks[tile.task];
   const int m0 = tile.m0, n0 = tile.n0, M = task.m, N = task.n;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
+  using T = Tile<BM, BN>;
+  const int wm = warp / T::WN, wn = warp % T::WN;
   const int gid = lane >> 2, tig = lane & 3;
 
   double accr[4][4][2], acci[4][4][2];
@@ -123,7 +136,7 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
   bool have = cur_t < task.t1;
   if (have) {
     GemmTerm t = terms[cur_t];
-    load_stage<AH, BH, NSPLIT>(smem, t, 0, m0, n0, M, N, task.n_in, Ar, Ai, Br, Bi);
+    load_stage<BM, BN, AH, BH, NSPLIT>(smem, t, 0, m0, n0, M, N, task.n_in, Ar, Ai, Br, Bi);
     cp_commit();
     nxt_k = BK;
     if (nxt_k >= t.k) { nxt_t = cur_t + 1; nxt_k = 0; }
@@ -133,33 +146,34 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
     bool more = nxt_t < task.t1;
     if (more) {
       GemmTerm t = terms[nxt_t];
-      load_stage<AH, BH, NSPLIT>(smem + (stage ^ 1) * STAGE_DOUBLES, t, nxt_k, m0, n0, M, N, task.n_in, Ar, Ai, Br, Bi);
+      load_stage<BM, BN, AH, BH, NSPLIT>(smem + (stage ^ 1) * T::STAGE_DOUBLES, t, nxt_k, m0, n0, M, N, task.n_in, Ar,
+                                         Ai, Br, Bi);
       cp_commit();
       cp_wait1();
     } else {
       cp_wait0();
     }
     __syncthreads();
-    const double* sAr = smem + stage * STAGE_DOUBLES;
-    const double* sAi = sAr + PLANE;
-    const double* sBr = sAr + 2 * PLANE;
-    const double* sBi = sAr + 3 * PLANE;
+    const double* sAr = smem + stage * T::STAGE_DOUBLES;
+    const double* sAi = sAr + T::PLANE_A;
+    const double* sBr = sAr + 2 * T::PLANE_A;
+    const double* sBi = sBr + T::PLANE_B;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       double ar[4], ai[4], nai[4], br[4], bi[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         int mm = wm * 32 + i * 8 + gid;
-        ar[i] = sAr[(kk + tig) * LDS + mm];
-        ai[i] = sAi[(kk + tig) * LDS + mm];
+        ar[i] = sAr[(kk + tig) * T::LDA + mm];
+        ai[i] = sAi[(kk + tig) * T::LDA + mm];
         if (AH) ai[i] = -ai[i];
         nai[i] = -ai[i];
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         int nn = wn * 32 + j * 8 + gid;
-        br[j] = sBr[(kk + tig) * LDS + nn];
-        bi[j] = sBi[(kk + tig) * LDS + nn];
+        br[j] = sBr[(kk + tig) * T::LDB + nn];
+        bi[j] = sBi[(kk + tig) * T::LDB + nn];
         if (BH) bi[j] = -bi[j];
       }
 #pragma unroll
@@ -202,33 +216,77 @@ zgemm_grouped_fp64(const GemmTile* __restrict__ tiles, const GemmTask* __restric
       }
 }
 
-template <bool AH, bool BH, bool NSPLIT>
+template <int BM, int BN, bool AH, bool BH, bool NSPLIT>
 int launch_variant(const GemmPlan& p, const Planar& A, const Planar& B, Planar& C, cudaStream_t st) {
-  CMPS_TRY(ensure_smem_optin((const void*)zgemm_grouped_fp64<AH, BH, NSPLIT>, (int)SMEM_BYTES));
+  using T = Tile<BM, BN>;
+  CMPS_TRY(ensure_smem_optin((const void*)zgemm_grouped_fp64<BM, BN, AH, BH, NSPLIT>, (int)T::SMEM_BYTES));
   if (p.tiles.empty()) return CMPS_OK;
   const int64_t ntiles = (int64_t)p.tiles.size();
   if (ntiles > 0x7fffffff) return fail(CMPS_ERR_ARG, "too many GEMM tiles");
-  zgemm_grouped_fp64<AH, BH, NSPLIT><<<(unsigned)ntiles, NTHREADS, SMEM_BYTES, st>>>(
+  zgemm_grouped_fp64<BM, BN, AH, BH, NSPLIT><<<(unsigned)ntiles, NTHREADS, T::SMEM_BYTES, st>>>(
       p.d_tiles, p.d_tasks, p.d_terms, A.re(), A.im(), B.re(), B.im(), C.re(), C.im());
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }
 
+template <int BM, int BN>
+int launch_shape(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B, Planar& C,
+                 cudaStream_t st) {
+  if (p.nsplit) {
+    if (a_h || b_h) return fail(CMPS_ERR_STATE, "two-level N index with a conjugate-transposed operand");
+    return launch_variant<BM, BN, false, false, true>(p, A, B, C, st);
+  }
+  if (!a_h && !b_h) return launch_variant<BM, BN, false, false, false>(p, A, B, C, st);
+  if (a_h && !b_h) return launch_variant<BM, BN, true, false, false>(p, A, B, C, st);
+  if (!a_h && b_h) return launch_variant<BM, BN, false, true, false>(p, A, B, C, st);
+  return launch_variant<BM, BN, true, true, false>(p, A, B, C, st);
+}
+
+constexpr int kShapes[3][2] = {{64, 64}, {32, 128}, {128, 32}};
+
 }  // namespace
+
+int gemm_shape_m(int shape) { return kShapes[shape][0]; }
+int gemm_shape_n(int shape) { return kShapes[shape][1]; }
 
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B, Planar& C,
                       cudaStream_t st) {
-  if (p.nsplit) {
-    if (a_h || b_h) return fail(CMPS_ERR_STATE, "two-level N index with a conjugate-transposed operand");
-    return launch_variant<false, false, true>(p, A, B, C, st);
+  switch (p.shape) {
+    case 0: return launch_shape<64, 64>(p, a_h, b_h, A, B, C, st);
+    case 1: return launch_shape<32, 128>(p, a_h, b_h, A, B, C, st);
+    case 2: return launch_shape<128, 32>(p, a_h, b_h, A, B, C, st);
+    default: return fail(CMPS_ERR_STATE, "GEMM plan not uploaded (no tile shape)");
   }
-  if (!a_h && !b_h) return launch_variant<false, false, false>(p, A, B, C, st);
-  if (a_h && !b_h) return launch_variant<true, false, false>(p, A, B, C, st);
-  if (!a_h && b_h) return launch_variant<false, true, false>(p, A, B, C, st);
-  return launch_variant<true, true, false>(p, A, B, C, st);
 }
 
-int GemmPlan::upload(int bm, int bn, cudaStream_t st) {
+// Tile shape of a plan, chosen from its own tasks: the shape whose padded
+// work (every task rounded up to whole tiles, times its K) plus a fixed cost
+// per tile (prologue, epilogue, scheduling: the work of 16 k-steps of a
+// 32 x 32 quarter tile) is least.  Ties keep 64 x 64.
+static int pick_shape(const GemmPlan& p) {
+  double best = 0.0;
+  int shape = 0;
+  for (int s = 0; s < 3; ++s) {
+    const int bm = kShapes[s][0], bn = kShapes[s][1];
+    double cost = 0.0;
+    for (const GemmTask& t : p.tasks) {
+      if (t.m <= 0 || t.n <= 0) continue;
+      int64_t k = 0;
+      for (int q = t.t0; q < t.t1; ++q) k += p.terms[q].k;
+      const double tm = (double)((t.m + bm - 1) / bm), tn = (double)((t.n + bn - 1) / bn);
+      cost += tm * tn * ((double)bm * bn * (double)std::max<int64_t>(k, BK) + 16.0 * 32 * 32 * BK);
+    }
+    if (s == 0 || cost < 0.97 * best) {
+      best = cost;
+      shape = s;
+    }
+  }
+  return shape;
+}
+
+int GemmPlan::upload(cudaStream_t st) {
+  shape = pick_shape(*this);
+  const int bm = kShapes[shape][0], bn = kShapes[shape][1];
   tiles.clear();
   for (size_t i = 0; i < tasks.size(); ++i) {
     const GemmTask& t = tasks[i];
@@ -288,7 +346,5 @@ void GemmPlan::release() {
   d_tiles = nullptr;
 }
 
-int gemm_tile_m() { return BM; }
-int gemm_tile_n() { return BN; }
 
 }  // namespace cmps
