@@ -65,8 +65,10 @@ def parse():
     p.add_argument("--precision", default="both", choices=["both", "fp64", "split_tf32"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--idmrg-steps", type=int, default=4, help="timed iDMRG steps at full chi (0: skip)")
-    p.add_argument("--ising-steps", type=int, default=3, help="timed coupled-Ising iDMRG steps (0: skip)")
-    p.add_argument("--ising-chi", type=int, default=64)
+    p.add_argument("--ising-steps", type=int, default=2, help="timed coupled-Ising iDMRG steps (0: skip)")
+    p.add_argument("--ising-chi", default="64,128", help="bond dimensions of the coupled-Ising steps")
+    p.add_argument("--ising-folded-chi", type=int, default=64,
+                   help="bond dimension at which the folded-order FP64 step is also timed (0: skip)")
     return p.parse_args()
 
 
@@ -445,12 +447,22 @@ def main():
     if a.idmrg_steps > 0:
         line["idmrg"] = idmrg_bench(ctx, wl, a.chi, a.idmrg_steps, dist)
     if a.ising_steps > 0:
-        from chainamps_b200 import models
+        from chainamps_b200 import models, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_ORDER_AUTO, CMPS_ORDER_FOLDED
         rules, ch, W, bq = models.coupled_ising_model(12, 1.2, 64, 0.05)
         iw = dict(rules=rules, Wt=models.mpo_tensor(ch, W, bq))
-        line["idmrg_coupled_ising"] = idmrg_bench(ctx, iw, a.ising_chi, a.ising_steps, dist, warm=2)
-        line["idmrg_coupled_ising"]["model"] = ("coupled TFIM chains: 12-site periodic chain vertex, g=1.2, 64 "
-                                                "lowest states (Z2), J_perp=0.05 sum X_i X_i, MPO D=26")
+        ising = {"model": "coupled TFIM chains: 12-site periodic chain vertex, g=1.2, 64 lowest states (Z2), "
+                          "J_perp=0.05 sum X_i X_i, MPO D=26",
+                 "forms": {"fp64": "FP64, contraction order chosen by flops (canonical for this vertex)",
+                           "mixed": "split precision (the canonical order in FP32 for this vertex), FP64 Krylov, "
+                                    "Rayleigh quotients and SVD",
+                           "fp64_folded": "FP64 in the reference's folded order (LeftPart . V . RightPart)"}}
+        for chi in [int(c) for c in str(a.ising_chi).split(",") if c.strip()]:
+            forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO)]
+            if chi == a.ising_folded_chi:
+                forms.append(("fp64_folded", CMPS_FP64, CMPS_ORDER_FOLDED))
+            ising[f"chi_{chi}"] = idmrg_bench(ctx, iw, chi, a.ising_steps, dist, warm=2, forms=forms,
+                                              unit_cell=False)
+        line["idmrg_coupled_ising"] = ising
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t, setup, cores, _ = cpu_port(wl, 1)
         line["cpu_baseline"] = {"value": canonical / t / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
@@ -464,7 +476,7 @@ def main():
     return 0
 
 
-def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True):
+def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True, forms=None):
     """iDMRG growth on the ladder MPO in FP64 and in mixed precision: `warm`
     untimed steps bring the bond dimension to chi, then `steps` timed ones.
     Step time is the library's device time of the whole step (environment
@@ -472,11 +484,13 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True):
     median over the timed steps, max over ranks.  unit_cell: after the FP64 run, the unit cell of its last step
     (energy per vertex, entropy, time)."""
     import torch
-    from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32
+    from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_ORDER_AUTO
     out = {"chi": chi, "warmup_steps": warm, "timed_steps": steps, "arnoldi_tol": tol, "krylov_dim": 24}
     energies = {}
-    for name, prec in (("fp64", CMPS_FP64), ("mixed", CMPS_SPLIT_TF32)):
-        run = iDMRG(ctx, wl["rules"], wl["Wt"], precision=prec, tol=tol, krylov_dim=24)
+    if forms is None:
+        forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO)]
+    for name, prec, order in forms:
+        run = iDMRG(ctx, wl["rules"], wl["Wt"], precision=prec, tol=tol, krylov_dim=24, order=order)
         e, prof, wall = [], [], []
         for i in range(warm + steps):
             t0 = time.perf_counter()
@@ -510,6 +524,11 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True):
     rel = np.abs(energies["mixed"] - energies["fp64"]) / np.abs(energies["fp64"])
     out["max_rel_dE_mixed_vs_fp64"] = float(rel.max())
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    if "fp64_folded" in out:
+        rel = np.abs(energies["fp64_folded"] - energies["fp64"]) / np.abs(energies["fp64"])
+        out["max_rel_dE_folded_vs_fp64"] = float(rel.max())
+        out["speedup_mixed_vs_fp64_folded"] = out["fp64_folded"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+        out["speedup_fp64_vs_fp64_folded"] = out["fp64_folded"]["ms_per_step"] / out["fp64"]["ms_per_step"]
     return out
 
 

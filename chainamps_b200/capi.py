@@ -114,6 +114,7 @@ _SIGS = {
     "cmps_dmrg_profile": (C.c_int, [C.c_void_p, c_dblp, C.c_int]),
     "cmps_dmrg_keep_blocks": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_dmrg_set_fidelity": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_dmrg_set_order": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_dmrg_move": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int),
                                  c_dblp]),
     "cmps_dmrg_position": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),
@@ -510,9 +511,10 @@ class iDMRG:
     DMRG_routines.cpp:346-374; iDMRG::run, iDMRG_routines.cpp:19-33)."""
 
     def __init__(self, ctx: Context, rules, W: MPXTensor, target=None, precision=CMPS_FP64, tol=1e-10,
-                 max_restarts=50, krylov_dim=24, gradient=None):
+                 max_restarts=50, krylov_dim=24, gradient=None, order=CMPS_ORDER_AUTO):
         """gradient: optional dW (MPXTensor, the MPO's derivative with respect
-        to one coupling); each grow() then also returns dE/dlambda."""
+        to one coupling); each grow() then also returns dE/dlambda.  order:
+        contraction order of each step's H_eff (CMPS_ORDER_*)."""
         self.ctx = ctx
         cr, self._r = _rules(rules)
         dw, kw = W._desc()
@@ -524,6 +526,7 @@ class iDMRG:
         _check(lib.cmps_dmrg_create(ctx.h, C.byref(cr), C.byref(dw), t, precision, C.byref(h)))
         self.h = h
         _check(lib.cmps_dmrg_set_solver(h, tol, max_restarts, krylov_dim))
+        _check(lib.cmps_dmrg_set_order(h, order))
         self._grad = gradient is not None
         if self._grad:
             gd, gk = gradient._desc()

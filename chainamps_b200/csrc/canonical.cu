@@ -50,6 +50,11 @@ struct Canon {
   Planar xz, y;  // intermediates (X then Z; Y)
   GemmPlan sL, sW1, sW2, sR;
   double flops = 0.0;
+  // The low-precision form (FP32 planes, the same plans): FP32 copies of the
+  // MPO blocks and the environments, theta in and out, and the intermediates
+  // as views into the FP64 ones (the two forms never run at once).
+  bool have32 = false;
+  Planar32 ops32, L32, R32, x32, o32, xz32, y32;
   ~Canon() {
     ops.release();
     xz.release();
@@ -58,6 +63,11 @@ struct Canon {
     sW1.release();
     sW2.release();
     sR.release();
+    ops32.release();
+    L32.release();
+    R32.release();
+    x32.release();
+    o32.release();
   }
 };
 
@@ -411,6 +421,59 @@ int build_canonical(Heff& H) {
   for (GemmPlan* p : {&C->sL, &C->sW1, &C->sW2, &C->sR})
     if ((rc = p->upload(st)) != CMPS_OK) return bail(rc);
   C->flops = P.flops;
+  return CMPS_OK;
+}
+
+int build_canonical32(Heff& H) {
+  Canon* C = H.canon;
+  if (!C) return fail(CMPS_ERR_STATE, "canonical-order plans not built");
+  if (C->have32) return CMPS_OK;
+  cudaStream_t st = H.ctx->stream;
+  CMPS_TRY(C->ops32.alloc(C->ops.len));
+  CMPS_TRY(C->L32.alloc(H.L.data.len));
+  CMPS_TRY(C->R32.alloc(H.R.data.len));
+  CMPS_TRY(C->x32.alloc(H.th.total));
+  CMPS_TRY(C->o32.alloc(H.th.total));
+  CMPS_TRY(to_fp32(C->ops.re(), C->ops.im(), C->ops.len, C->ops32, st));
+  CMPS_TRY(to_fp32(H.L.data.re(), H.L.data.im(), H.L.data.len, C->L32, st));
+  CMPS_TRY(to_fp32(H.R.data.re(), H.R.data.im(), H.R.data.len, C->R32, st));
+  C->xz32.d = (float*)C->xz.d;  // 2 len floats inside 2 len doubles
+  C->xz32.len = C->xz.len;
+  C->y32.d = (float*)C->y.d;
+  C->y32.len = C->y.len;
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  C->have32 = true;
+  return CMPS_OK;
+}
+
+// The low-precision canonical matvec: theta (FP64) -> FP32, the four stages
+// on FP32 planes with FP32 accumulation, the owned output sectors -> FP64.
+int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st) {
+  Canon* C = H.canon;
+  if (!C || !C->have32) return fail(CMPS_ERR_STATE, "canonical-order FP32 operands not prepared");
+  if (which != 2) {
+    CMPS_TRY(to_fp32(in.re(), in.im(), H.th.total, C->x32, st));
+    CMPS_TRY(launch_cgemm_fp32(C->sL, C->L32, C->x32, C->xz32, st));
+    CMPS_TRY(launch_cgemm_fp32(C->sW1, C->ops32, C->xz32, C->y32, st));
+  }
+  if (which != 1) {
+    CMPS_TRY(launch_cgemm_fp32(C->sW2, C->ops32, C->y32, C->xz32, st));
+    CMPS_TRY(launch_cgemm_fp32(C->sR, C->xz32, C->R32, C->o32, st));
+    if (H.all_owned()) {
+      CMPS_TRY(to_fp64(C->o32, H.th.total, out.re(), out.im(), st));
+    } else {
+      // sharded: only the owned sectors were computed; the others stay unwritten
+      Planar32 v;
+      for (size_t m = 0; m < H.th.mq.size(); ++m) {
+        if (!H.owned[m]) continue;
+        const int64_t off = H.th.base[m], n = H.th.nrows[m] * H.th.ncols[m];
+        v.d = C->o32.d + off;
+        v.len = C->o32.len;  // plane stride of o32
+        CMPS_TRY(to_fp64(v, n, out.re() + off, out.im() + off, st));
+      }
+      v.d = nullptr;
+    }
+  }
   return CMPS_OK;
 }
 

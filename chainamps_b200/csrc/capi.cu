@@ -349,8 +349,10 @@ int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {
   if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
   const Heff& H = *h->impl;
   if (canonical) *canonical = H.flops_canonical;
-  if (executed)
-    *executed = H.precision == CMPS_FP64 && H.order == CMPS_ORDER_CANONICAL ? H.flops_canon : H.flops_executed;
+  if (executed) {
+    const bool canonical = H.precision == CMPS_FP64 ? H.order == CMPS_ORDER_CANONICAL : H.low_canonical;
+    *executed = canonical ? H.flops_canon : H.flops_executed;
+  }
   return CMPS_OK;
 }
 

@@ -96,6 +96,7 @@ struct Dmrg {
   // before growth; key = number of vertices the block covers
   bool keep_blocks = false;
   bool want_fidelity = true;  // CheckConvergence on growth steps
+  int order_req = CMPS_ORDER_AUTO;  // contraction order of each step's H_eff
   std::map<int64_t, Env> lblocks, rblocks;
   // the factors each kept block was built with: lsvd[k]'s U made lblocks[k]
   // (the left MPS tensor of vertex k), rsvd[k]'s V^dagger made rblocks[k]
@@ -474,6 +475,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   next->ctx = ctx;
   next->device = ctx->device;
   next->rules = rules;
+  next->order_req = order_req;
   CMPS_TRY(next->parse_mpo(&W));
   if (grad_on) extend_pattern(next->W, dW);
   next->L = L;   // ownership of the device blocks moves to `next`
@@ -671,6 +673,14 @@ int cmps_dmrg_grow(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, in
 int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on) {
   if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
   d->impl->want_fidelity = on != 0;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_set_order(cmps_dmrg* d, int order) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (order != CMPS_ORDER_AUTO && order != CMPS_ORDER_FOLDED && order != CMPS_ORDER_CANONICAL)
+    return fail(CMPS_ERR_ARG, "unknown contraction order");
+  d->impl->order_req = order;
   return CMPS_OK;
 }
 

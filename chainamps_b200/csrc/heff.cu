@@ -14,6 +14,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -501,7 +504,20 @@ int Heff::unpack(const Planar& in, double* out, cudaStream_t st) const {
   return CMPS_OK;
 }
 
+// Phase timer of Heff::finish for CMPS_BUILD_TRACE (host wall ms to stderr).
+struct BuildTrace {
+  bool on = std::getenv("CMPS_BUILD_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "build %-22s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
 int Heff::finish() {
+  BuildTrace bt;
   const Rules& r = rules;
   const Bond& A0 = L.a;
   const Bond& A2 = R.a;
@@ -562,6 +578,7 @@ int Heff::finish() {
     th.base[m] = th.total;
     th.total += th.nrows[m] * th.ncols[m];
   }
+  bt.mark("theta space");
   // ---- allowed indices, ARPACK order (DMRG_routines.cpp:808-824) ----
   // ARPACK order = ascending s1 + d a0 + d chiL (s2 + d a2).  Every entry of
   // sector block m is allowed, so a column (s2, a2) holds exactly the rows of
@@ -598,6 +615,7 @@ int Heff::finish() {
   }
   if (n_allowed != th.total) return fail(CMPS_ERR_STATE, "internal: allowed count differs from sector total");
 
+  bt.mark("ARPACK maps");
   // ---- LeftPart blocks: key (b1, s1', s1, a0-sector s) ----
   lp_off.clear();
   lp_blocks.clear();
@@ -654,6 +672,7 @@ int Heff::finish() {
     for (auto& tt : kv2.second) rp_terms.push_back(tt);
     rp_total += len;
   }
+  bt.mark("LP/RP block lists");
   CMPS_TRY(LP.alloc(lp_total));
   CMPS_TRY(RP.alloc(rp_total));
   CMPS_TRY(upload_vec(lp_blocks, &d_lp_blocks, ctx->stream));
@@ -661,6 +680,7 @@ int Heff::finish() {
   CMPS_TRY(upload_vec(rp_blocks, &d_rp_blocks, ctx->stream));
   CMPS_TRY(upload_vec(rp_terms, &d_rp_terms, ctx->stream));
 
+  bt.mark("LP/RP alloc+upload");
   owned.assign(nm, 1);
   CMPS_TRY(build_plans());
   for (const AxpyBlock& b : lp_blocks)
@@ -680,11 +700,13 @@ int Heff::finish() {
       const int64_t rt = map_rowth[map_secs[m].rowstart + i];
       if (rt < 0 || rt >= th.nrows[m]) return fail(CMPS_ERR_STATE, "pack map row outside the sector blocks");
     }
+  bt.mark("folded plans");
   CMPS_TRY(build_pack(ctx->stream));
   cudaStream_t st = ctx->stream;
   CMPS_TRY(launch_block_axpy(d_lp_blocks, (int)lp_blocks.size(), d_lp_terms, L.data, LP, st));
   CMPS_TRY(launch_block_axpy(d_rp_blocks, (int)rp_blocks.size(), d_rp_terms, R.data, RP, st));
 
+  bt.mark("pack + LP/RP formation");
   // ---- canonical four-stage flop count ----
   {
     double f = 0.0;
@@ -727,12 +749,15 @@ int Heff::finish() {
       }
     flops_canonical = f;
   }
+  bt.mark("flop count");
   CMPS_TRY(x.alloc(th.total));
   CMPS_TRY(y.alloc(th.total));
   CMPS_CUDA(dmalloc(&d_io, sizeof(double) * 2 * std::max<int64_t>(1, n_allowed)));
   CMPS_TRY(ops.init(th.total));
+  bt.mark("work vectors");
   CMPS_TRY(select_order());
   CMPS_CUDA(cudaStreamSynchronize(st));
+  bt.mark("contraction order");
   return CMPS_OK;
 }
 
@@ -745,12 +770,17 @@ int Heff::select_order() {
   CMPS_TRY(canonical_flops(*this, &flops_canon));
   int want = order_req;
   if (want == CMPS_ORDER_AUTO) want = flops_canon <= 0.5 * flops_folded ? CMPS_ORDER_CANONICAL : CMPS_ORDER_FOLDED;
+  // the canonical plans are rebuilt (or dropped): an FP32 canonical
+  // split-precision operator built on them goes too, and is prepared again
+  const bool low = low_canonical;
+  low_canonical = false;
   if (want == CMPS_ORDER_CANONICAL) {
     CMPS_TRY(build_canonical(*this));
   } else {
     release_canonical(this);
   }
   order = want;
+  if (low || (precision == CMPS_SPLIT_TF32 && !split)) CMPS_TRY(prepare_precision(this, precision));
   return CMPS_OK;
 }
 
@@ -830,7 +860,7 @@ int Heff::build_plans() {
       }
     }
   }
-  CMPS_TRY(T.alloc(t_total));
+  t_len = t_total;  // T itself is allocated by the first folded FP64 matvec
   // ---- stage 2: Theta'_m' = sum_b1 T^{b1}_{m'-q(b1)} . RightPart^{b1} ----
   stage2 = GemmPlan();
   for (int mp = 0; mp < nm; ++mp) {
@@ -892,11 +922,20 @@ bool Heff::all_owned() const {
   return std::all_of(owned.begin(), owned.end(), [](uint8_t o) { return o != 0; });
 }
 
+// The folded order's intermediate T: a canonical-order or split-precision
+// handle never runs the folded FP64 stages, so T (about D x the wavefunction)
+// is only allocated when they first run.
+int Heff::ensure_T() {
+  if (T.d && T.len == t_len) return CMPS_OK;
+  return T.alloc(t_len);
+}
+
 // which = 1: the first half of the matvec (folded: T = LeftPart . in;
 // canonical: stages L and W1), 2: the second half.
 int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
   if (precision == CMPS_SPLIT_TF32) return apply_split_stage(*this, which, in, out, st);
   if (order == CMPS_ORDER_CANONICAL) return apply_canonical(*this, which, in, out, st);
+  CMPS_TRY(ensure_T());
   if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
   return launch_zgemm_fp64(stage2, false, false, T, RP, out, st);
 }
@@ -914,6 +953,7 @@ int Heff::apply_fp64_stages(const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int Heff::apply_folded_fp64(const Planar& in, Planar& out, cudaStream_t st) {
+  CMPS_TRY(ensure_T());
   CMPS_TRY(launch_zgemm_fp64(stage1, false, false, LP, in, T, st));
   CMPS_TRY(launch_zgemm_fp64(stage2, false, false, T, RP, out, st));
   return CMPS_OK;

@@ -106,7 +106,9 @@ struct Heff {
   AxpyTerm* d_rp_terms = nullptr;
   std::map<std::array<int, 4>, int64_t> lp_off, rp_off;  // (b1, sigma', sigma, sector) -> offset
   std::vector<int64_t> t_base;   // [b1 * nm + m] -> offset into T, -1 if absent
-  Planar T;                      // stage-1 intermediate
+  Planar T;                      // stage-1 intermediate, allocated on first use (ensure_T)
+  int64_t t_len = 0;             // its length in complex elements
+  int ensure_T();
   GemmPlan stage1, stage2;
   // Output sectors this matvec computes (1 = owned).  All of them, unless the
   // matvec is sharded across GPUs by output sector; then the output blocks
@@ -139,6 +141,9 @@ struct Heff {
   double flops_folded = 0.0, flops_canon = 0.0;
   Canon* canon = nullptr;
   int select_order();
+  // The split-precision operator runs the canonical order in FP32
+  // (canonical.cu) instead of the folded order on tcgen05 (split_tf32.cu).
+  bool low_canonical = false;
   int precision = CMPS_FP64;
   SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)
   // work vectors
@@ -216,6 +221,9 @@ int build_canonical(Heff& H);
 void release_canonical(Heff* h);
 // which: 1 = stages L and W1, 2 = stages W2 and R, 0 = all four
 int apply_canonical(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
+// the same in FP32 (FP32 copies of the operands built by build_canonical32)
+int build_canonical32(Heff& H);
+int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
 
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);

@@ -101,6 +101,18 @@ struct Planar {
   void release();
 };
 
+// Single-precision counterpart of Planar (re plane, then im plane).  A view
+// into another allocation (owned = false) is not freed by release().
+struct Planar32 {
+  float* d = nullptr;
+  int64_t len = 0;
+  bool owned = false;
+  float* re() const { return d; }
+  float* im() const { return d + len; }
+  int alloc(int64_t n);
+  void release();
+};
+
 // An environment (left or right block) on the device.  Block (b, s) of a
 // left block is the dense [a', a] matrix L^b restricted to a-sector s and
 // a'-sector s' = sector(q_s + q_b), row-major (dim s') x (dim s).  A right
@@ -177,6 +189,11 @@ int gemm_shape_m(int shape);
 int gemm_shape_n(int shape);
 int launch_zgemm_fp64(const GemmPlan& p, bool a_h, bool b_h, const Planar& A, const Planar& B,
                       Planar& C, cudaStream_t st);
+// FP32 grouped complex GEMM (cgemm_fp32.cu): the same plans as
+// launch_zgemm_fp64 without conjugated operands.
+int launch_cgemm_fp32(const GemmPlan& p, const Planar32& A, const Planar32& B, Planar32& C, cudaStream_t st);
+int to_fp32(const double* re, const double* im, int64_t n, Planar32& out, cudaStream_t st);
+int to_fp64(const Planar32& in, int64_t n, double* re, double* im, cudaStream_t st);
 int launch_block_axpy(const AxpyBlock* d_blocks, int nblocks, const AxpyTerm* d_terms,
                       const Planar& src, Planar& dst, cudaStream_t st, bool accumulate = false);
 

@@ -62,7 +62,7 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
     return fail(CMPS_ERR_ARG, "the no-allocation matvec runs the FP64 path only; set CMPS_FP64 on the handle");
   if (H.proj_np || !H.all_owned())
     return fail(CMPS_ERR_ARG, "the no-allocation matvec runs the plain unsharded operator (no projectors)");
-  const int64_t need = 4 * H.th.total + 2 * H.T.len;
+  const int64_t need = 4 * H.th.total + 2 * H.t_len;
   if (need > kNoAllocScratchDoubles)
     return fail(CMPS_ERR_ARG, "no-allocation matvec: this H_eff needs " + std::to_string(need * 8) +
                                   " bytes of scratch, above the static maximum of " +
@@ -77,8 +77,8 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
   x.d = base;
   x.len = H.th.total;
   t.d = base + 2 * H.th.total;
-  t.len = H.T.len;
-  y.d = t.d + 2 * H.T.len;
+  t.len = H.t_len;
+  y.d = t.d + 2 * H.t_len;
   y.len = H.th.total;
   CMPS_TRY(H.pack(d_in, x, st));
   CMPS_TRY(launch_zgemm_fp64(H.stage1, false, false, H.LP, x, t, st));

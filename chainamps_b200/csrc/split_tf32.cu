@@ -203,6 +203,7 @@ void TcPlan::release() {
 }  // namespace tc
 
 void release_split(Heff* h) {
+  if (h) h->low_canonical = false;  // the FP32 canonical operands go with the canonical plans
   if (!h || !h->split) return;
   SplitState* s = h->split;
   s->p1.release();
@@ -656,10 +657,22 @@ static int build_split(Heff& H) {
   return CMPS_OK;
 }
 
+// The split-precision operator of a handle: the folded order on tcgen05
+// (split-TF32, this file), or -- when the canonical order executes at most a
+// quarter of the folded order's flops -- the canonical order in FP32
+// (canonical.cu).  The quarter weighs the folded form's tensor-core rate
+// against the FP32 form's FFMA rate on the short-K canonical stages.
+constexpr double kLowCanonicalRatio = 0.25;
+
 int prepare_precision(Heff* h, int precision) {
   if (precision == CMPS_FP64) return CMPS_OK;
   if (precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
-  if (h->split) return CMPS_OK;
+  if (h->split || h->low_canonical) return CMPS_OK;
+  if (h->canon && h->flops_canon <= kLowCanonicalRatio * h->flops_folded) {
+    CMPS_TRY(build_canonical32(*h));
+    h->low_canonical = true;
+    return CMPS_OK;
+  }
   int st = build_split(*h);
   if (st != CMPS_OK) release_split(h);
   return st;
@@ -675,6 +688,7 @@ static int split_theta(const SplitState& S, const Planar& in, cudaStream_t st) {
 }
 
 int split_reset_error(Heff& H, cudaStream_t st) {
+  if (H.low_canonical) return CMPS_OK;  // no pipeline waits, no error word
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
@@ -682,6 +696,10 @@ int split_reset_error(Heff& H, cudaStream_t st) {
 }
 
 int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
+  if (H.low_canonical) {
+    CMPS_TRY(apply_canonical32(H, 0, in, out, st));
+    return H.add_projectors(in, out, st);
+  }
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   const int64_t n = H.th.total;
@@ -694,6 +712,7 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
 
 // theta-space matvec in split precision: FP64 planar in -> FP64 planar out.
 int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
+  if (H.low_canonical) return apply_split_async(H, in, out, st);
   CMPS_TRY(split_reset_error(H, st));
   CMPS_TRY(apply_split_async(H, in, out, st));
   SplitState* S = H.split;
@@ -704,6 +723,7 @@ int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st) {
+  if (H.low_canonical) return apply_canonical32(H, which, in, out, st);
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   const int64_t n = H.th.total;
@@ -716,6 +736,7 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
 }
 
 int split_error(Heff& H) {
+  if (H.low_canonical) return CMPS_OK;
   SplitState* S = H.split;
   if (!S) return CMPS_OK;
   int e = 0;

@@ -334,6 +334,9 @@ int cmps_dmrg_unit_cell(cmps_dmrg* d, double tol, int krylov_dim, double* out6);
  * returns the number of vertices left of the window and the chain length. */
 int cmps_dmrg_keep_blocks(cmps_dmrg* d, int keep);
 int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on);
+/* Contraction order of every later step's H_eff (CMPS_ORDER_*, default
+ * AUTO; see cmps_heff_set_order).  No counterpart in the reference. */
+int cmps_dmrg_set_order(cmps_dmrg* d, int order);
 int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, double* row5,
                    int64_t* bond_dim, int* matvecs, double* ms4);
 int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);

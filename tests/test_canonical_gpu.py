@@ -138,3 +138,77 @@ def test_canonical_sharded_halves(ctx):
             got[:, off[s]:off[s + 1]] = y[:, off[s]:off[s + 1]]
         del h
     assert torch.equal(got, want)
+
+
+def test_split_precision_runs_the_canonical_order_in_fp32(ctx):
+    """For the 64-state chain vertex the split-precision operator is the
+    canonical order in FP32 (its flops are a small fraction of the folded
+    order's), accurate to FP32 accumulation: within 2e-5 of the oracle
+    (max-norm, relative).  The ladder keeps the folded order on tcgen05."""
+    from chainamps_b200 import TwoVertexComponents, CMPS_SPLIT_TF32, models
+    H = ising_mpo(12, 64)
+    L, R = make_envs(H, 5, 30, 28)
+    g = TwoVertexComponents(ctx, H.rules, to_tensor(L), to_tensor(H), to_tensor(R), precision=CMPS_SPLIT_TF32)
+    _, f_fold, f_can = g.order()
+    assert g.flops()[1] == f_can and f_can <= 0.25 * f_fold
+    ref = oc.from_mpx(H, L, R)
+    rng = np.random.default_rng(4)
+    for _ in range(2):
+        x = rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n)
+        want = ref.matvec(x)
+        err = np.max(np.abs(g.multiply(x) - want)) / np.max(np.abs(want))
+        assert err <= 2e-5, err
+    del g
+    wl = models.ladder_workload(48, seed=3)
+    h = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=CMPS_SPLIT_TF32)
+    _, f_fold, f_can = h.order()
+    assert h.flops()[1] == f_fold
+
+
+def test_mixed_ground_state_on_the_fp32_canonical_operator(ctx):
+    """The mixed-precision eigensolver (FP32 canonical matvecs, FP64 Rayleigh
+    quotients) reaches the FP64 solver's energy within 1e-9 on a grown
+    coupled-Ising window."""
+    from chainamps_b200 import TwoVertexComponents, CMPS_SPLIT_TF32, CMPS_FP64
+    H = ising_mpo(4, 8)
+    sb = od.SuperBlock(H, tol=1e-13)
+    for _ in range(4):
+        sb.grow(16, 1e-16)
+    L = od.make_left_block(sb.left_blocks[sb.nleft], H, sb.dec.U)
+    R = od.make_right_block(sb.right_blocks[sb.nleft], H, sb.dec.Vd)
+    e = {}
+    for name, prec in (("fp64", CMPS_FP64), ("mixed", CMPS_SPLIT_TF32)):
+        g = TwoVertexComponents(ctx, H.rules, to_tensor(L), to_tensor(H), to_tensor(R), precision=prec)
+        e[name], v, _ = g.HED(tol=1e-12, krylov_dim=32)
+        del g
+    assert abs(e["mixed"] - e["fp64"]) <= 1e-9 * abs(e["fp64"]), e
+
+
+def test_fp32_canonical_sharded_halves(ctx):
+    """Two split-precision handles owning complementary output sectors
+    reassemble the whole FP32 canonical matvec bit for bit."""
+    import torch
+    from chainamps_b200 import TwoVertexComponents, CMPS_SPLIT_TF32
+    H = ising_mpo(12, 64)
+    L, R = make_envs(H, 12, 30, 28)
+    full = TwoVertexComponents(ctx, H.rules, to_tensor(L), to_tensor(H), to_tensor(R), precision=CMPS_SPLIT_TF32)
+    assert full.flops()[1] == full.order()[2]  # the FP32 canonical operator
+    off, fl = full.sector_table()
+    nsec = len(fl)
+    assert nsec >= 2
+    n = int(off[-1])
+    x = torch.randn(2, n, dtype=torch.float64, device="cuda")
+    want = torch.empty_like(x)
+    full.multiply_theta_device(x.data_ptr(), want.data_ptr(), None)
+    torch.cuda.synchronize()
+    got = torch.zeros_like(x)
+    for part in (np.arange(nsec) < nsec // 2, np.arange(nsec) >= nsec // 2):
+        h = TwoVertexComponents(ctx, H.rules, to_tensor(L), to_tensor(H), to_tensor(R), precision=CMPS_SPLIT_TF32)
+        h.set_owned(part.astype(np.uint8))
+        y = torch.full_like(x, float("nan"))
+        h.multiply_theta_device(x.data_ptr(), y.data_ptr(), None)
+        torch.cuda.synchronize()
+        for s in np.nonzero(part)[0]:
+            got[:, off[s]:off[s + 1]] = y[:, off[s]:off[s + 1]]
+        del h
+    assert torch.equal(got, want)
