@@ -414,7 +414,9 @@ def main():
                                "live cuBLAS TF32 8192^3 GEMM",
             "frac_of_pipe_ceiling": ach / pipe_ceiling,
             "traffic_is": "DRAM bytes (read + write) of both stages per matvec from the committed ncu summary "
-                          "profiles/heff_matvec_split_tf32_ladder4_chi512.md" if traffic else None}
+                          "profiles/heff_matvec_split_tf32_ladder4_chi512.md: a chi=384 capture scaled to chi=512 by "
+                          "the vector length (T and the environments grow with it)" if traffic else None,
+            "algorithmic_bytes": 32.0 * n}
     if head == "split_tf32":
         roof["tf32_issued_tflops"] = 3.0 * executed / (gemm_ms * 1e-3) / 1e12
     if world > 1:
