@@ -118,6 +118,11 @@ _SIGS = {
     "cmps_dmrg_move": (C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int),
                                  c_dblp]),
     "cmps_dmrg_position": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),
+    "cmps_dmrg_project_state": (C.c_int, [C.c_void_p, C.c_double]),
+    "cmps_dmrg_projected_states": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "cmps_dmrg_solve": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, c_dblp, c_i64p, C.POINTER(C.c_int), c_dblp]),
+    "cmps_dmrg_projector": (C.c_int, [C.c_void_p, C.c_int, c_dblp]),
+    "cmps_dmrg_window_length": (C.c_int, [C.c_void_p, c_i64p, c_i64p]),
     "cmps_heff_adjoint": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc), C.c_void_p, C.c_void_p, c_dblp]),
     "cmps_dmrg_set_gradient": (C.c_int, [C.c_void_p, C.POINTER(MpxDesc)]),
     "cmps_dmrg_gradient": (C.c_int, [C.c_void_p, c_dblp]),
@@ -590,6 +595,26 @@ class iDMRG:
             pass
 
 
+# the reference's default projector weight (command_line_input.hpp:470)
+DEFAULT_PROJECTOR_WEIGHT = 100.0
+
+
+def run_excited_fdmrg(ctx, rules, W, nvertices, sweeps, chi, max_trunc=1e-16, nstates=1,
+                      weight=DEFAULT_PROJECTOR_WEIGHT, target=None, precision=CMPS_FP64, tol=1e-10, max_restarts=50,
+                      krylov_dim=24):
+    """fDMRG_DRV -X nstates (fDMRG_DRV.cpp:60-72) on the device: the ground
+    state by finite DMRG, then each excited state by the same sweeps with
+    every earlier state projected out.  Returns (ground-state rows, [rows of
+    excited state 1, ...]) and the driver."""
+    run = fDMRG(ctx, rules, W, nvertices, target, precision, tol, max_restarts, krylov_dim)
+    gs = run.run(sweeps, chi, max_trunc)
+    out = []
+    for _ in range(nstates):
+        run.project_state(weight)
+        out.append(run.run_excited(sweeps, chi, max_trunc))
+    return gs, out, run
+
+
 class fDMRG(iDMRG):
     """Finite DMRG on the device: fDMRG_DRV's growth to `nvertices`, then
     FiniteDMRG::run's sweeps (fDMRG_routines.cpp:19-66) with every block kept
@@ -619,13 +644,46 @@ class fDMRG(iDMRG):
                          chi=bd.value, matvecs=mv.value, ms=ms)
         return self.last
 
-    def run(self, sweeps, chi, max_trunc=1e-16):
-        """Growth rows, then the rows written when the window passes the
-        middle of the chain (twice per sweep): the rows of the energies file."""
-        rows = [self.grow(chi, max_trunc) for _ in range(self.nvertices // 2)]
-        nl, n = self.position()
-        if n <= 2:
-            return rows
+    def _row(self, row, bd, mv, ms):
+        self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
+                         chi=bd.value, matvecs=mv.value, ms=ms)
+        return self.last
+
+    def solve(self, chi=0, max_trunc=0.0):
+        """Solve the current window again with its environments, without
+        moving (ExcitedStateFiniteDMRG::init, fDMRG_routines.cpp:68-91)."""
+        row = np.zeros(5, np.float64)
+        bd = C.c_int64()
+        mv = C.c_int()
+        ms = np.zeros(4, np.float64)
+        _check(lib.cmps_dmrg_solve(self.h, chi, max_trunc, _p(row, C.c_double), C.byref(bd), C.byref(mv),
+                                   _p(ms, C.c_double)))
+        return self._row(row, bd, mv, ms)
+
+    def project_state(self, weight=DEFAULT_PROJECTOR_WEIGHT):
+        """Store the current state as a state to project out of every later
+        solve, with weight `weight` (next_state, fDMRG_routines.hpp:39-44)."""
+        _check(lib.cmps_dmrg_project_state(self.h, float(weight)))
+
+    def projected_states(self):
+        n = C.c_int()
+        _check(lib.cmps_dmrg_projected_states(self.h, C.byref(n)))
+        return n.value
+
+    def window_length(self):
+        """(allowed entries, full length) of the current window."""
+        n, full = C.c_int64(), C.c_int64()
+        _check(lib.cmps_dmrg_window_length(self.h, C.byref(n), C.byref(full)))
+        return n.value, full.value
+
+    def projector(self, index):
+        """The current window's projector tensor P of stored state `index`
+        (ARPACK order)."""
+        out = np.zeros(2 * self.window_length()[0], np.float64)
+        _check(lib.cmps_dmrg_projector(self.h, int(index), _p(out, C.c_double)))
+        return out[0::2] + 1j * out[1::2]
+
+    def _sweeps(self, sweeps, chi, max_trunc, rows):
         for _ in range(sweeps):
             nl, n = self.position()
             for _ in range(n - nl - 2):
@@ -645,6 +703,21 @@ class fDMRG(iDMRG):
                 if nl == n - nl - 2:
                     rows.append(r)
         return rows
+
+    def run(self, sweeps, chi, max_trunc=1e-16):
+        """Growth rows, then the rows written when the window passes the
+        middle of the chain (twice per sweep): the rows of the energies file."""
+        rows = [self.grow(chi, max_trunc) for _ in range(self.nvertices // 2)]
+        nl, n = self.position()
+        if n <= 2:
+            return rows
+        return self._sweeps(sweeps, chi, max_trunc, rows)
+
+    def run_excited(self, sweeps, chi, max_trunc=1e-16):
+        """ExcitedStateFiniteDMRG::run (fDMRG_routines.cpp:198-242) for the
+        states stored so far: the init row (a solve at the current window),
+        then the rows at the centre of every sweep."""
+        return self._sweeps(sweeps, chi, max_trunc, [self.solve(chi, max_trunc)])
 
 
 def upload_block(ctx: Context, rules, block: MPXTensor, W: MPXTensor, right: bool):

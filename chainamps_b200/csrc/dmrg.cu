@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -66,11 +67,14 @@ struct Dmrg {
   std::unique_ptr<Heff> heff;
   std::shared_ptr<SvdResult> svd;  // factors of the current window (shared with lsvd / rsvd)
   static std::shared_ptr<SvdResult> new_svd() {
-    return std::shared_ptr<SvdResult>(new SvdResult(), [](SvdResult* s) {
+    static std::atomic<uint64_t> serials{0};
+    auto p = std::shared_ptr<SvdResult>(new SvdResult(), [](SvdResult* s) {
       s->U.release();
       s->Vd.release();
       delete s;
     });
+    p->serial = ++serials;
+    return p;
   }
   std::vector<double> lambda, prev_lambda;
   double tol = 1e-10;
@@ -86,7 +90,11 @@ struct Dmrg {
   static constexpr int kProfile = 21;
   double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
 
+  // excited states: the states projected out of every solve (next_state,
+  // fDMRG_routines.hpp:39-44), with their weights
+  std::vector<ProjectedState*> pstates;
   ~Dmrg() {
+    for (ProjectedState* p : pstates) projected_state_destroy(p);
     dL.data.release();
     dR.data.release();
     for (auto& kv : lblocks) kv.second.data.release();
@@ -108,8 +116,17 @@ struct Dmrg {
   int predict(Heff& next, bool* ok);
   int finite_predict(Heff& next, int dir, bool* ok);
   // dir 0: iDMRG growth step (grow_two_vertex); +1 / -1: finite sweep step
-  // to the right / left (move_{right,left}_two_vertex)
+  // to the right / left (move_{right,left}_two_vertex); 2: a new solve of the
+  // current window with its environments (ExcitedStateFiniteDMRG::init,
+  // fDMRG_routines.cpp:68-91)
   int step(int dir, int64_t chi, double trunc, double* out);
+  int project_state(double weight) {
+    if (!keep_blocks || !svd || size < 2) return fail(CMPS_ERR_STATE, "projected state: run a finite chain first");
+    ProjectedState* p = nullptr;
+    CMPS_TRY(projected_state_create(ctx, lsvd, rsvd, *svd, lambda, nleft, size, weight, &p));
+    pstates.push_back(p);
+    return CMPS_OK;
+  }
   int grow(int64_t chi, double trunc, double* out) { return step(0, chi, trunc, out); }
   static int store(std::map<int64_t, Env>& m, int64_t k, const Env& e, cudaStream_t st) {
     auto it = m.find(k);
@@ -391,12 +408,13 @@ int Dmrg::finite_predict(Heff& next, int dir, bool* ok) {
 
 int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   cudaStream_t st = ctx->stream;
+  if (dir == 0 && !pstates.empty()) return fail(CMPS_ERR_STATE, "growth with projected states: the chain is finite");
   if (dir != 0) {
     if (!keep_blocks || !heff || !svd) return fail(CMPS_ERR_STATE, "finite sweep: grow with kept blocks first");
     if (grad_on) return fail(CMPS_ERR_STATE, "the coupling gradient is carried through growth steps only");
     const int64_t nright = size - nleft - 2;
-    if (dir > 0 && nright < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the right end");
-    if (dir < 0 && nleft < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the left end");
+    if (dir == 1 && nright < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the right end");
+    if (dir == -1 && nleft < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the left end");
   }
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   struct EvGuard {
@@ -414,7 +432,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   const auto h0 = clock::now();
   cudaEventRecord(ev[0], st);
   Env L, R;
-  if (dir > 0) {
+  if (dir == 1) {
     // MakeLeftBlock with A = U of this window; the right block of the new
     // window was stored by the growth or the previous sweep
     Env nl;
@@ -440,6 +458,12 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (il == lblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: left block missing");
     CMPS_TRY(copy_env(il->second, L, st));
     CMPS_TRY(copy_env(rblocks[size - nleft - 2], R, st));
+  } else if (dir == 2) {
+    auto il = lblocks.find(nleft);
+    auto ir = rblocks.find(size - nleft - 2);
+    if (il == lblocks.end() || ir == rblocks.end()) return fail(CMPS_ERR_STATE, "window solve: a block is missing");
+    CMPS_TRY(copy_env(il->second, L, st));
+    CMPS_TRY(copy_env(ir->second, R, st));
   } else if (size == 0) {
     CMPS_TRY(dummy_blocks(L, R));
   } else {
@@ -486,8 +510,10 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   next->precision = precision;
   const auto h_split = clock::now();
   bool have_guess = false;
-  if (dir == 0) CMPS_TRY(predict(*next, &have_guess));
-  else CMPS_TRY(finite_predict(*next, dir, &have_guess));
+  if (!pstates.empty())  // no prediction on excited-state steps (fDMRG_routines.cpp:118-121)
+    CMPS_TRY(install_projectors(ctx, pstates, lsvd, rsvd, nleft, size, *next));
+  else if (dir == 0) CMPS_TRY(predict(*next, &have_guess));
+  else if (dir != 2) CMPS_TRY(finite_predict(*next, dir, &have_guess));
   const auto h_pred = clock::now();
   // the previous step's factors are released here unless a kept block needs them
   svd.reset();
@@ -519,7 +545,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   // sweep steps next to an end keep every state up to chi (no weight cut),
   // as move_{right,left}_two_vertex do
   const int64_t nright_now = (dir == 0 ? size + 2 : size) - nleft - 2;
-  const double cut = (dir > 0 && nright_now <= 1) || (dir < 0 && nleft <= 1) ? -0.0 : trunc;
+  const double cut = (dir == 1 && nright_now <= 1) || (dir == -1 && nleft <= 1) ? -0.0 : trunc;
   CMPS_TRY(theta_svd(*heff, chi, cut, *svd));
   // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
   std::vector<double> v = svd->values;
@@ -695,6 +721,56 @@ int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, d
                    int* matvecs, double* ms4) {
   if (direction != 1 && direction != -1) return fail(CMPS_ERR_ARG, "direction must be +1 (right) or -1 (left)");
   return dmrg_step(d, direction, chi, max_trunc, row5, bond_dim, matvecs, ms4);
+}
+
+int cmps_dmrg_solve(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
+                    double* ms4) {
+  return dmrg_step(d, 2, chi, max_trunc, row5, bond_dim, matvecs, ms4);
+}
+
+int cmps_dmrg_project_state(cmps_dmrg* d, double weight) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  if (!(weight >= 0.0)) return fail(CMPS_ERR_ARG, "projected state: weight must be non-negative");
+  Dmrg& D = *d->impl;
+  if (D.pstates.size() >= 64) return fail(CMPS_ERR_ARG, "projected state: at most 64 of them");
+  CMPS_CUDA(cudaSetDevice(D.device));
+  return D.project_state(weight);
+}
+
+int cmps_dmrg_projected_states(const cmps_dmrg* d, int* count) {
+  if (!d || !d->impl || !count) return fail(CMPS_ERR_ARG, "null argument");
+  *count = (int)d->impl->pstates.size();
+  return CMPS_OK;
+}
+
+int cmps_dmrg_window_length(const cmps_dmrg* d, int64_t* n_allowed, int64_t* full_length) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  const Dmrg& D = *d->impl;
+  if (!D.heff) return fail(CMPS_ERR_STATE, "no window");
+  if (n_allowed) *n_allowed = D.heff->n_allowed;
+  if (full_length) *full_length = D.heff->full_length;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_projector(const cmps_dmrg* d, int index, double* arpack_out) {
+  if (!d || !d->impl || !arpack_out) return fail(CMPS_ERR_ARG, "null argument");
+  const Dmrg& D = *d->impl;
+  if (!D.heff) return fail(CMPS_ERR_STATE, "no window");
+  Heff& H = *D.heff;
+  if (index < 0 || index >= H.proj_np) return fail(CMPS_ERR_ARG, "projector index out of range");
+  CMPS_CUDA(cudaSetDevice(D.device));
+  cudaStream_t st = H.ctx->stream;
+  Planar v;
+  v.d = H.proj.d + 2 * H.th.total * index;
+  v.len = H.th.total;
+  const int rc = H.unpack(v, H.d_io, st);
+  v.d = nullptr;
+  CMPS_TRY(rc);
+  const size_t n = (size_t)H.n_allowed;
+  CMPS_CUDA(cudaMemcpyAsync(arpack_out, H.d_io, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < n; ++i) arpack_out[2 * i + 1] = -arpack_out[2 * i + 1];  // P = conj(phi)
+  return CMPS_OK;
 }
 
 int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size) {

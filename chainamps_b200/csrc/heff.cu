@@ -1012,6 +1012,35 @@ int Heff::set_projectors(int np, const double* host_arpack, const double* weight
   return CMPS_OK;
 }
 
+int Heff::set_projectors_device(int np, const double* d_phi_arpack, const double* weights) {
+  CMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  proj.release();
+  if (d_proj) dfree(d_proj);
+  d_proj = nullptr;
+  proj_np = 0;
+  proj_w.clear();
+  if (np == 0) return CMPS_OK;
+  if (np < 0 || np > 64) return fail(CMPS_ERR_ARG, "projectors: between 0 and 64 of them");
+  if (!d_phi_arpack || !weights) return fail(CMPS_ERR_ARG, "projectors: null argument");
+  const int64_t n = th.total;
+  CMPS_TRY(proj.alloc((int64_t)np * n));
+  CMPS_CUDA(dmalloc(&d_proj, sizeof(double) * (3 * (size_t)np + 4)));
+  cudaStream_t st = ctx->stream;
+  for (int p = 0; p < np; ++p) {
+    Planar v;
+    v.d = proj.d + 2 * n * p;
+    v.len = n;
+    const int rc = pack(d_phi_arpack + 2 * (size_t)n_allowed * p, v, st);
+    v.d = nullptr;
+    CMPS_TRY(rc);
+  }
+  proj_w.assign(weights, weights + np);
+  CMPS_TRY(copy_wait(d_proj, proj_w.data(), sizeof(double) * np, cudaMemcpyHostToDevice, st));
+  CMPS_CUDA(cudaStreamSynchronize(st));
+  proj_np = np;
+  return CMPS_OK;
+}
+
 int Heff::add_projectors(const Planar& in, Planar& out, cudaStream_t st) {
   if (!proj_np) return CMPS_OK;
   const int64_t n = th.total;

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -130,6 +131,8 @@ struct Heff {
   double* d_proj = nullptr;  // weights [np], coefficients [2 np + 4]
   std::vector<double> proj_w;
   int set_projectors(int np, const double* host_arpack, const double* weights);
+  // the same from device vectors phi_p = conj(P_p), ARPACK order, interleaved
+  int set_projectors_device(int np, const double* d_phi_arpack, const double* weights);
   int add_projectors(const Planar& in, Planar& out, cudaStream_t st);
   double flops_canonical = 0.0, flops_executed = 0.0;
   // Contraction order of the FP64 matvec: folded (LeftPart / RightPart, the
@@ -183,6 +186,7 @@ struct Heff {
 
 // Result of the charge-block SVD of theta (svd.cu).
 struct SvdResult {
+  uint64_t serial = 0;  // unique per factorisation of a DMRG run (cache keys)
   Rules rules;
   int d = 0;
   std::vector<QKey> sigq;
@@ -260,6 +264,23 @@ int copy_env(const Env& src, Env& dst, cudaStream_t st);
 int build_env_from_desc(const Rules& r, const cmps_mpx_desc* desc, bool right, Env& env, int D,
                         const std::vector<QKey>& bq, cudaStream_t st);
 int parse_index_charges(const Rules& r, const cmps_mpx_desc* desc, int idx, std::vector<QKey>& out);
+
+// Excited-state projectors from stored states (projector.cu; ProjectorBlocks,
+// DMRG_routines.cpp:446-581).  A stored state is a snapshot of a finite
+// chain's state: its left tensors lsvd[1..nleft], the window's factors with
+// its values and its right tensors rsvd[1..length - nleft - 2].
+struct ProjectedState;
+int projected_state_create(cmps_context* ctx, const std::map<int64_t, std::shared_ptr<SvdResult>>& lsvd,
+                           const std::map<int64_t, std::shared_ptr<SvdResult>>& rsvd, const SvdResult& window,
+                           const std::vector<double>& lambda, int64_t nleft, int64_t length, double weight,
+                           ProjectedState** out);
+void projected_state_destroy(ProjectedState* p);
+// The projector tensor of every stored state for H's window (the current
+// state's tensors lsvd / rsvd), installed as H's projectors.
+int install_projectors(cmps_context* ctx, std::vector<ProjectedState*>& states,
+                       const std::map<int64_t, std::shared_ptr<SvdResult>>& lsvd,
+                       const std::map<int64_t, std::shared_ptr<SvdResult>>& rsvd, int64_t nleft, int64_t length,
+                       Heff& H);
 
 }  // namespace cmps
 

@@ -341,6 +341,31 @@ int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, d
                    int64_t* bond_dim, int* matvecs, double* ms4);
 int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);
 
+/* ---- excited states (fDMRG_DRV -X, ExcitedStateFiniteDMRG,
+ * fDMRG_routines.cpp:68-244; ProjectorBlocks, DMRG_routines.cpp:446-581) ----
+ * cmps_dmrg_project_state(d, w) stores the current state of a finite chain
+ * (its left tensors, the window's U diag(lambda) and V^dagger, its right
+ * tensors; on the device) as a state to project out with weight w
+ * (next_state, fDMRG_routines.hpp:39-44; the reference's default weight is
+ * 100).  Every later step builds, on the device, the overlaps of each stored
+ * state with the current left and right bases and its projector tensor P on
+ * the new window, and solves H_eff + sum_p w_p |P_p*><P_p*| (the projector
+ * term of TwoVertexMPOMPSMultiply, DMRG_routines.cpp:947-973) with no
+ * prediction vector, as the reference's excited sweeps do.  Growth steps are
+ * refused while states are stored.  cmps_dmrg_solve solves the current window
+ * again with its environments, without moving (ExcitedStateFiniteDMRG::init),
+ * and returns the same row as cmps_dmrg_move.  cmps_dmrg_projector copies the
+ * current window's P of stored state `index` in ARPACK order (n_allowed
+ * interleaved complex values). */
+int cmps_dmrg_project_state(cmps_dmrg* d, double weight);
+int cmps_dmrg_projected_states(const cmps_dmrg* d, int* count);
+int cmps_dmrg_solve(cmps_dmrg* d, int64_t chi, double max_trunc, double* row5, int64_t* bond_dim, int* matvecs,
+                    double* ms4);
+int cmps_dmrg_projector(const cmps_dmrg* d, int index, double* arpack_out);
+/* Allowed entries and full length of the current window (the length of a
+ * vector in ARPACK order, TwoVertexComponents::length()). */
+int cmps_dmrg_window_length(const cmps_dmrg* d, int64_t* n_allowed, int64_t* full_length);
+
 /* Coupling gradient along the growth (no reference counterpart).  Set before
  * the first growth step: dW as for cmps_heff_adjoint (NULL turns it off).
  * Each step then carries the derivative environments dL, dR (the environment
