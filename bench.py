@@ -492,6 +492,11 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True, fo
     if forms is None:
         forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO)]
     for name, prec, order in forms:
+        # map most of the free device memory into the library's pool before
+        # the run (setup, untimed), so that steps whose buffers outgrow the
+        # previous ones do not pay for mapping memory; returned after the run
+        torch.cuda.empty_cache()
+        ctx.reserve(int(0.6 * torch.cuda.mem_get_info()[0]))
         run = iDMRG(ctx, wl["rules"], wl["Wt"], precision=prec, tol=tol, krylov_dim=24, order=order)
         e, prof, wall = [], [], []
         for i in range(warm + steps):
@@ -509,6 +514,7 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True, fo
             uc = run.unit_cell(tol=1e-12, krylov_dim=30)
             out["unit_cell"] = dict(uc, ms=1e3 * (time.perf_counter() - t0))
         run.close()
+        ctx.reserve(0)
         torch.cuda.empty_cache()
         # median over the timed steps: a host-side stall in one step (allocator
         # growth, a busy host) would otherwise dominate a mean over few steps

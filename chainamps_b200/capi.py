@@ -69,6 +69,7 @@ class MpxDesc(C.Structure):
 _SIGS = {
     "cmps_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "cmps_context_destroy": (C.c_int, [C.c_void_p]),
+    "cmps_context_reserve": (C.c_int, [C.c_void_p, C.c_uint64]),
     "cmps_last_error": (C.c_char_p, []),
     "cmps_version": (C.c_char_p, []),
     "cmps_heff_create": (C.c_int, [C.c_void_p, C.POINTER(ChargeRules), C.POINTER(MpxDesc), C.POINTER(MpxDesc),
@@ -174,6 +175,11 @@ class Context:
         h = C.c_void_p()
         _check(lib.cmps_context_create(device, C.byref(h)))
         self.h = h
+
+    def reserve(self, nbytes):
+        """Map `nbytes` of device memory into the library's pool up front
+        (0: return the pool's unused memory); see cmps_context_reserve."""
+        _check(lib.cmps_context_reserve(self.h, int(nbytes)))
 
     def close(self):
         if self.h:

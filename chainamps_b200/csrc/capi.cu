@@ -130,6 +130,30 @@ int cmps_context_create(int device, cmps_context** out) {
   return CMPS_OK;
 }
 
+int cmps_context_reserve(cmps_context* ctx, uint64_t bytes) {
+  if (!ctx) return fail(CMPS_ERR_ARG, "null context");
+  CMPS_CUDA(cudaSetDevice(ctx->device));
+  CMPS_CUDA(pool_setup(ctx->device));
+  cudaMemPool_t pool;
+  CMPS_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+  CMPS_CUDA(cudaDeviceSynchronize());
+  if (bytes == 0) {
+    CMPS_CUDA(cudaMemPoolTrimTo(pool, 0));
+    return CMPS_OK;
+  }
+  // one allocation of the whole size maps it into the pool; freed, it stays
+  // there (release threshold: keep everything) for later allocations
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, (size_t)bytes, cudaStreamLegacy);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CMPS_ERR_NOMEM, std::string("pool reservation failed: ") + cudaGetErrorString(e));
+  }
+  CMPS_CUDA(cudaFreeAsync(p, cudaStreamLegacy));
+  CMPS_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+  return CMPS_OK;
+}
+
 int cmps_context_destroy(cmps_context* ctx) {
   if (!ctx) return CMPS_OK;
   cudaSetDevice(ctx->device);

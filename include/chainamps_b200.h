@@ -83,6 +83,12 @@ typedef struct {
 /* ---- context ---------------------------------------------------------- */
 int cmps_context_create(int device, cmps_context** out);
 int cmps_context_destroy(cmps_context* ctx);
+/* Device memory of the library comes from the device's stream-ordered pool,
+ * which keeps what is freed.  cmps_context_reserve(ctx, bytes) maps `bytes`
+ * into the pool at once, so that the first steps of a run, whose buffers grow
+ * with the bond dimension, do not pay for mapping new memory one allocation
+ * at a time; bytes = 0 returns the pool's unused memory to the device. */
+int cmps_context_reserve(cmps_context* ctx, uint64_t bytes);
 const char* cmps_last_error(void);
 /* Library build string (architecture, kernels compiled in). */
 const char* cmps_version(void);
