@@ -33,8 +33,8 @@ flush is needed between steps.
 
 Multi-GPU (N > 1): one matvec per step split across the ranks by output
 charge sector (``chainamps_b200.sharded``): every rank holds the
-environments and the MPO, all-gathers the input slices and computes the
-output sectors it owns, balanced by their flops; `value` is the whole
+environments and the MPO, receives the input sectors its outputs read by one
+all-to-all and computes the output sectors it owns, balanced by their flops; `value` is the whole
 matvec's canonical TFLOP/s over the max-over-ranks step time ("strong"
 scaling: the work per step is the same for every N).  The iDMRG step
 figures run on every rank as replicas.
@@ -259,18 +259,13 @@ def main():
 
     def measure_sharded(h, steps, warm):
         """N > 1: one matvec split over the ranks by output sector (each rank
-        computes its owned sectors after an all-gather of the input slices);
-        returns (ms per step, [all-gather ms, owned-sector matvec ms, 0, 0],
-        clocks, owned executed flops, layout)."""
-        from chainamps_b200.sharded import ShardLayout, ShardedOperator
+        receives the input sectors its owned outputs read by an all-to-all,
+        then computes its owned sectors); returns (ms per step, [exchange ms,
+        owned-sector matvec ms, 0, 0], clocks, owned executed flops, operator)."""
+        from chainamps_b200.sharded import ShardedTwoVertex
         off, fl = h.sector_table()
-        lay = ShardLayout(off, fl, world, rank)
-        h.set_owned(lay.owned)
-
-        def apply_full(xin, yout):
-            h.multiply_theta_device(xin.data_ptr(), yout.data_ptr(), stream.cuda_stream)
-
-        op = ShardedOperator(lay, apply_full, "cuda")
+        sh = ShardedTwoVertex(h)
+        op, lay = sh.op, sh.layout
         x = torch.randn(2, lay.n_local, dtype=torch.float64, device="cuda")
         for _ in range(max(3, warm)):
             op(x)
@@ -296,7 +291,7 @@ def main():
         h.status()
         # the two parts alone, on this rank
         parts = []
-        for f in (lambda: op.gather(x), lambda: apply_full(op.xfull, op.yfull)):
+        for f in (lambda: op.exchange(x), lambda: op.apply_window(op.xwin, op.yloc)):
             g0 = torch.cuda.Event(enable_timing=True)
             g1 = torch.cuda.Event(enable_timing=True)
             g0.record(stream)
@@ -307,18 +302,13 @@ def main():
             parts.append(g0.elapsed_time(g1) / 3)
         ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        return float(ms_t.item()), [parts[0], parts[1], 0.0, 0.0], summarize_clocks(clk), float(fl[lay.owned].sum()), lay
+        return float(ms_t.item()), [parts[0], parts[1], 0.0, 0.0], summarize_clocks(clk), float(fl[lay.owned].sum()), op
 
-    def e2e_sharded(h, lay, steps):
+    def e2e_sharded(op, steps):
         """N > 1, end to end: each step copies this rank's input slice from
         pinned host memory, runs the sharded matvec and copies its output
         slice back."""
-        from chainamps_b200.sharded import ShardedOperator
-
-        def apply_full(xin, yout):
-            h.multiply_theta_device(xin.data_ptr(), yout.data_ptr(), stream.cuda_stream)
-
-        op = ShardedOperator(lay, apply_full, "cuda")
+        lay = op.layout
         xh = torch.randn(2, lay.n_local, dtype=torch.float64).pin_memory()
         yh = torch.empty(2, lay.n_local, dtype=torch.float64).pin_memory()
         op(xh.to("cuda", non_blocking=True))
@@ -372,9 +362,11 @@ def main():
             e2e_s = e2e(h, max(3, a.steps // 2))
             res[p] = dict(ms=ms, st=st, clk=clk, e2e_s=e2e_s, owned=executed, n_io=n)
         else:
-            ms, st, clk, owned, lay = measure_sharded(h, a.steps, a.warmup)
-            e2e_s = e2e_sharded(h, lay, max(3, a.steps // 2))
-            res[p] = dict(ms=ms, st=st, clk=clk, e2e_s=e2e_s, owned=owned, n_io=lay.n_local)
+            ms, st, clk, owned, op = measure_sharded(h, a.steps, a.warmup)
+            e2e_s = e2e_sharded(op, max(3, a.steps // 2))
+            res[p] = dict(ms=ms, st=st, clk=clk, e2e_s=e2e_s, owned=owned, n_io=op.layout.n_local,
+                          window=op.layout.in_len)
+            del op
         del h
         torch.cuda.empty_cache()
     zgemm = gemm_peak(torch.complex128, 4096)
@@ -420,7 +412,7 @@ def main():
     if head == "split_tf32":
         roof["tf32_issued_tflops"] = 3.0 * executed / (gemm_ms * 1e-3) / 1e12
     if world > 1:
-        roof["stage_ms"] = {"allgather": r["st"][0], "owned_matvec": r["st"][1]}
+        roof["stage_ms"] = {"exchange": r["st"][0], "owned_matvec": r["st"][1]}
     else:
         roof["stage_ms"] = {"gather": r["st"][0], "stage1": r["st"][1], "stage2": r["st"][2], "scatter": r["st"][3]}
     roof["flops_canonical"] = canonical

@@ -131,6 +131,8 @@ _SIGS = {
     "cmps_heff_set_projectors": (C.c_int, [C.c_void_p, C.c_int, c_dblp, c_dblp]),
     "cmps_heff_sector_table": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_dblp]),
     "cmps_heff_set_owned": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cmps_heff_input_sectors": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cmps_heff_set_windows": (C.c_int, [C.c_void_p, c_i64p, C.c_int64, c_i64p, C.c_int64]),
     "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_theta_from_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_theta_to_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -284,8 +286,22 @@ class TwoVertexComponents:
         mask = np.ascontiguousarray(np.asarray(owned, bool).astype(np.uint8))
         _check(lib.cmps_heff_set_owned(self.h, _p(mask, C.c_uint8)))
 
+    def input_sectors(self):
+        """Mask of the input sectors the owned output sectors read."""
+        n = len(self.sector_table()[1])
+        out = np.zeros(max(n, 1), np.uint8)
+        _check(lib.cmps_heff_input_sectors(self.h, _p(out, C.c_uint8)))
+        return out[:n].astype(bool)
+
+    def set_windows(self, in_base, in_len, out_base, out_len):
+        """Vector windows of the theta-layout matvec (see cmps_heff_set_windows)."""
+        ib = np.ascontiguousarray(np.asarray(in_base, np.int64))
+        ob = np.ascontiguousarray(np.asarray(out_base, np.int64))
+        _check(lib.cmps_heff_set_windows(self.h, _p(ib, C.c_int64), int(in_len), _p(ob, C.c_int64), int(out_len)))
+
     def multiply_theta_device(self, d_in, d_out, stream=None):
-        """theta-layout matvec on device pointers (2 * total doubles, planar)."""
+        """theta-layout matvec on device pointers (planar; the windows' lengths
+        when set, else 2 * total doubles each)."""
         _check(lib.cmps_heff_apply_theta_device(self.h, C.c_void_p(d_in), C.c_void_p(d_out),
                                                 C.c_void_p(stream) if stream else None))
 

@@ -132,7 +132,7 @@ void extend_pattern(std::vector<WEntry>& W, const std::vector<WEntry>& dW) {
 
 int heff_adjoint(Heff& H, const std::vector<WEntry>& dW, const Env* dL, const Env* dR, double* grad) {
   if (!H.have_theta) return fail(CMPS_ERR_STATE, "adjoint: no wavefunction (call cmps_heff_eigs or cmps_heff_set_theta)");
-  if (!H.all_owned()) return fail(CMPS_ERR_STATE, "adjoint: the matvec is sharded");
+  if (!H.whole()) return fail(CMPS_ERR_STATE, "adjoint: the matvec is sharded");
   cudaStream_t st = H.ctx->stream;
   Planar LPd, RPd;
   int rc = derivative_parts(H, dW, dL, dR, LPd, RPd);

@@ -92,6 +92,9 @@ struct Plan {
   int64_t x_len = 0, y_len = 0, z_len = 0;
   GemmPlan sL, sW1, sW2, sR;
   double flops = 0.0;
+  // theta sectors stage L reads; missing: one of them is outside the input window
+  std::vector<uint8_t> need;
+  bool missing = false;
 };
 
 double term_flops(const GemmTask& t, const GemmTerm& tm) { return 8.0 * t.m * (double)t.n * tm.k; }
@@ -252,7 +255,10 @@ static int plan_canonical(const Heff& H, Plan& P) {
       tm.a_off = H.L.off[(size_t)b0 * ns0 + s];
       tm.lda = (int32_t)A0.sdim[s];
       tm.k = (int32_t)A0.sdim[s];
-      tm.b_off = th.base[m] + rcoff[m][c] * nc;
+      if ((int)P.need.size() != nm) P.need.assign(nm, 0);
+      P.need[m] = 1;
+      if (H.in_base[m] < 0) P.missing = true;
+      tm.b_off = std::max<int64_t>(0, H.in_base[m]) + rcoff[m][c] * nc;
       tm.ldb = (int32_t)nc;
       tm.ldb_out = (int32_t)(rcdim[m][c] * nc);
       P.sL.terms.push_back(tm);
@@ -347,7 +353,8 @@ static int plan_canonical(const Heff& H, Plan& P) {
       const int tp = A2.find(r.add(th.mq[mpp], H.sigq[H.cls_mem[c][0]]));  // a2' sector
       for (size_t i = 0; i < H.cls_mem[c].size(); ++i) {
         GemmTask t{};
-        t.c_off = th.base[mpp] + ccoff[mpp][c] + (int64_t)i * ccdim[mpp][c];
+        if (H.out_base[mpp] < 0) return fail(CMPS_ERR_ARG, "output window lacks an owned sector");
+        t.c_off = H.out_base[mpp] + ccoff[mpp][c] + (int64_t)i * ccdim[mpp][c];
         t.m = (int32_t)th.nrows[mpp];
         t.n = (int32_t)A2.sdim[tp];
         t.ldc = (int32_t)th.ncols[mpp];
@@ -378,10 +385,14 @@ static int plan_canonical(const Heff& H, Plan& P) {
   return CMPS_OK;
 }
 
-int canonical_flops(const Heff& H, double* flops) {
+int canonical_flops(const Heff& H, double* flops, std::vector<uint8_t>* need) {
   Plan P;
   CMPS_TRY(plan_canonical(H, P));
   *flops = P.flops;
+  if (need) {
+    *need = P.need;
+    need->resize(H.th.mq.size(), 0);
+  }
   return CMPS_OK;
 }
 
@@ -389,6 +400,7 @@ int build_canonical(Heff& H) {
   release_canonical(&H);
   Plan P;
   CMPS_TRY(plan_canonical(H, P));
+  if (P.missing) return fail(CMPS_ERR_ARG, "input window lacks a sector the owned outputs read");
   auto* C = new (std::nothrow) Canon();
   if (!C) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   H.canon = C;
@@ -409,10 +421,10 @@ int build_canonical(Heff& H) {
   if ((rc = C->xz.alloc(xz)) != CMPS_OK) return bail(rc);
   if ((rc = C->y.alloc(std::max<int64_t>(P.y_len, 1))) != CMPS_OK) return bail(rc);
   // every operand and output range inside its buffer, before any launch
-  if ((rc = P.sL.validate(false, false, H.L.data.len, H.th.total, xz, "canonical stage L")) != CMPS_OK ||
+  if ((rc = P.sL.validate(false, false, H.L.data.len, H.in_len, xz, "canonical stage L")) != CMPS_OK ||
       (rc = P.sW1.validate(false, false, C->ops.len, xz, C->y.len, "canonical stage W1")) != CMPS_OK ||
       (rc = P.sW2.validate(false, false, C->ops.len, C->y.len, xz, "canonical stage W2")) != CMPS_OK ||
-      (rc = P.sR.validate(false, false, xz, H.R.data.len, H.th.total, "canonical stage R")) != CMPS_OK)
+      (rc = P.sR.validate(false, false, xz, H.R.data.len, H.out_len, "canonical stage R")) != CMPS_OK)
     return bail(rc);
   C->sL = std::move(P.sL);
   C->sW1 = std::move(P.sW1);
@@ -432,8 +444,8 @@ int build_canonical32(Heff& H) {
   CMPS_TRY(C->ops32.alloc(C->ops.len));
   CMPS_TRY(C->L32.alloc(H.L.data.len));
   CMPS_TRY(C->R32.alloc(H.R.data.len));
-  CMPS_TRY(C->x32.alloc(H.th.total));
-  CMPS_TRY(C->o32.alloc(H.th.total));
+  CMPS_TRY(C->x32.alloc(std::max<int64_t>(1, H.in_len)));
+  CMPS_TRY(C->o32.alloc(std::max<int64_t>(1, H.out_len)));
   CMPS_TRY(to_fp32(C->ops.re(), C->ops.im(), C->ops.len, C->ops32, st));
   CMPS_TRY(to_fp32(H.L.data.re(), H.L.data.im(), H.L.data.len, C->L32, st));
   CMPS_TRY(to_fp32(H.R.data.re(), H.R.data.im(), H.R.data.len, C->R32, st));
@@ -452,7 +464,7 @@ int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   Canon* C = H.canon;
   if (!C || !C->have32) return fail(CMPS_ERR_STATE, "canonical-order FP32 operands not prepared");
   if (which != 2) {
-    CMPS_TRY(to_fp32(in.re(), in.im(), H.th.total, C->x32, st));
+    CMPS_TRY(to_fp32(in.re(), in.im(), H.in_len, C->x32, st));
     CMPS_TRY(launch_cgemm_fp32(C->sL, C->L32, C->x32, C->xz32, st));
     CMPS_TRY(launch_cgemm_fp32(C->sW1, C->ops32, C->xz32, C->y32, st));
   }
@@ -460,13 +472,13 @@ int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStr
     CMPS_TRY(launch_cgemm_fp32(C->sW2, C->ops32, C->y32, C->xz32, st));
     CMPS_TRY(launch_cgemm_fp32(C->sR, C->xz32, C->R32, C->o32, st));
     if (H.all_owned()) {
-      CMPS_TRY(to_fp64(C->o32, H.th.total, out.re(), out.im(), st));
+      CMPS_TRY(to_fp64(C->o32, H.out_len, out.re(), out.im(), st));
     } else {
       // sharded: only the owned sectors were computed; the others stay unwritten
       Planar32 v;
       for (size_t m = 0; m < H.th.mq.size(); ++m) {
         if (!H.owned[m]) continue;
-        const int64_t off = H.th.base[m], n = H.th.nrows[m] * H.th.ncols[m];
+        const int64_t off = H.out_base[m], n = H.th.nrows[m] * H.th.ncols[m];
         v.d = C->o32.d + off;
         v.len = C->o32.len;  // plane stride of o32
         CMPS_TRY(to_fp64(v, n, out.re() + off, out.im() + off, st));

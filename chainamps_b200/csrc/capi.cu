@@ -274,18 +274,33 @@ int cmps_heff_set_owned(cmps_heff* h, const uint8_t* owned) {
   return h->impl->set_owned(owned);
 }
 
+int cmps_heff_input_sectors(const cmps_heff* h, uint8_t* needed) {
+  if (!h || !h->impl || !needed) return fail(CMPS_ERR_ARG, "null argument");
+  const Heff& H = *h->impl;
+  for (size_t m = 0; m < H.in_need.size(); ++m) needed[m] = H.in_need[m];
+  return CMPS_OK;
+}
+
+int cmps_heff_set_windows(cmps_heff* h, const int64_t* in_base, int64_t in_len, const int64_t* out_base,
+                          int64_t out_len) {
+  if (!h || !h->impl || !in_base || !out_base) return fail(CMPS_ERR_ARG, "null argument");
+  CMPS_TRY(use_device(h->impl->ctx));
+  return h->impl->set_windows(in_base, in_len, out_base, out_len);
+}
+
 int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out, void* stream) {
   if (!h || !h->impl || !d_in || !d_out) return fail(CMPS_ERR_ARG, "null argument");
   if (d_in == d_out) return fail(CMPS_ERR_ARG, "theta-layout apply: in and out must be different arrays");
   Heff& H = *h->impl;
   CMPS_TRY(use_device(H.ctx));
   cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
-  // views of the caller's arrays (planar: re plane, then im plane)
+  // views of the caller's arrays (planar: re plane, then im plane), in the
+  // handle's windows (the theta layout unless cmps_heff_set_windows)
   Planar in, out;
   in.d = const_cast<double*>(d_in);
-  in.len = H.th.total;
+  in.len = H.in_len;
   out.d = d_out;
-  out.len = H.th.total;
+  out.len = H.out_len;
   int rc;
   if (H.precision == CMPS_SPLIT_TF32) {
     rc = apply_split_stage(H, 1, in, out, st);
@@ -332,7 +347,7 @@ int cmps_heff_time_stages(cmps_heff* h, const double* d_in, double* d_out, void*
   if (!h || !h->impl || !d_in || !d_out || !ms || reps < 1) return fail(CMPS_ERR_ARG, "bad argument");
   Heff& H = *h->impl;
   CMPS_TRY(use_device(H.ctx));
-  if (!H.all_owned()) return fail(CMPS_ERR_STATE, "stage timing: the matvec is sharded");
+  if (!H.whole()) return fail(CMPS_ERR_STATE, "stage timing: the matvec is sharded");
   cudaStream_t st = stream ? (cudaStream_t)stream : H.ctx->stream;
   cudaEvent_t ev[5];
   for (auto& e : ev) CMPS_CUDA(cudaEventCreate(&e));

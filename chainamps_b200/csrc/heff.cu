@@ -578,6 +578,7 @@ int Heff::finish() {
     th.base[m] = th.total;
     th.total += th.nrows[m] * th.ncols[m];
   }
+  default_windows();
   bt.mark("theta space");
   // ---- allowed indices, ARPACK order (DMRG_routines.cpp:808-824) ----
   // ARPACK order = ascending s1 + d a0 + d chiL (s2 + d a2).  Every entry of
@@ -767,7 +768,10 @@ int Heff::finish() {
 // folded order moves one, so a small flop advantage does not pay).
 int Heff::select_order() {
   flops_folded = flops_executed;
-  CMPS_TRY(canonical_flops(*this, &flops_canon));
+  std::vector<uint8_t> cneed;
+  CMPS_TRY(canonical_flops(*this, &flops_canon, &cneed));
+  // the input sectors of either order (the windows must hold both)
+  for (size_t m = 0; m < cneed.size() && m < in_need.size(); ++m) in_need[m] |= cneed[m];
   int want = order_req;
   if (want == CMPS_ORDER_AUTO) want = flops_canon <= 0.5 * flops_folded ? CMPS_ORDER_CANONICAL : CMPS_ORDER_FOLDED;
   // the canonical plans are rebuilt (or dropped): an FP32 canonical
@@ -797,6 +801,8 @@ int Heff::build_plans() {
   stage1.release();
   stage2.release();
   T.release();
+  if ((int)in_base.size() != nm || (int)out_base.size() != nm) return fail(CMPS_ERR_STATE, "window size");
+  in_need.assign(nm, 0);
   // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
   std::set<int> b1s;
   for (auto& kv2 : lp_off) b1s.insert(kv2.first[0]);
@@ -833,7 +839,8 @@ int Heff::build_plans() {
           tm.a_off = it->second;
           tm.lda = (int32_t)A0.sdim[s];
           tm.k = (int32_t)A0.sdim[s];
-          tm.b_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m];
+          if (in_base[m] < 0) return fail(CMPS_ERR_ARG, "input window lacks a sector the owned outputs read");
+          tm.b_off = in_base[m] + th.rowoff[m][s1] * th.ncols[m];
           tm.ldb = (int32_t)th.ncols[m];
           terms.push_back(tm);
         }
@@ -841,6 +848,7 @@ int Heff::build_plans() {
         tasks.push_back(task);
       }
       if (terms.empty()) continue;
+      in_need[m] = 1;
       int64_t tb = t_total;
       t_base[(size_t)b1 * nm + m] = tb;
       t_total += th.nrows[mp] * th.ncols[m];
@@ -869,7 +877,8 @@ int Heff::build_plans() {
       if (th.coloff[mp][s2p] < 0) continue;
       int tp = A2.find(r.add(th.mq[mp], sigq[s2p]));
       GemmTask task{};
-      task.c_off = th.base[mp] + th.coloff[mp][s2p];
+      if (out_base[mp] < 0) return fail(CMPS_ERR_ARG, "output window lacks an owned sector");
+      task.c_off = out_base[mp] + th.coloff[mp][s2p];
       task.m = (int32_t)th.nrows[mp];
       task.n = (int32_t)A2.sdim[tp];
       task.ldc = (int32_t)th.ncols[mp];
@@ -899,17 +908,51 @@ int Heff::build_plans() {
       stage2.tasks.push_back(task);
     }
   }
-  CMPS_TRY(stage1.validate(false, false, LP.len, th.total, t_total, "stage 1"));
-  CMPS_TRY(stage2.validate(false, false, t_total, RP.len, th.total, "stage 2"));
+  CMPS_TRY(stage1.validate(false, false, LP.len, in_len, t_total, "stage 1"));
+  CMPS_TRY(stage2.validate(false, false, t_total, RP.len, out_len, "stage 2"));
   if (all_owned()) sector_flops = fl;
   CMPS_TRY(stage1.upload(ctx->stream));
   CMPS_TRY(stage2.upload(ctx->stream));
   return CMPS_OK;
 }
 
+void Heff::default_windows() {
+  in_base = th.base;
+  out_base = th.base;
+  in_len = out_len = th.total;
+  windowed = false;
+}
+
+int Heff::set_windows(const int64_t* ib, int64_t il, const int64_t* ob, int64_t ol) {
+  const int nm = (int)th.mq.size();
+  if (proj_np) return fail(CMPS_ERR_STATE, "windows: the projector term needs whole vectors");
+  if (il < 0 || ol < 0) return fail(CMPS_ERR_ARG, "windows: negative length");
+  for (int m = 0; m < nm; ++m) {
+    const int64_t sz = th.nrows[m] * th.ncols[m];
+    if (in_need[m] && (ib[m] < 0 || ib[m] + sz > il)) return fail(CMPS_ERR_ARG, "input window: a read sector is outside it");
+    if (owned[m] && (ob[m] < 0 || ob[m] + sz > ol)) return fail(CMPS_ERR_ARG, "output window: an owned sector is outside it");
+  }
+  CMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  in_base.assign(ib, ib + nm);
+  out_base.assign(ob, ob + nm);
+  for (int m = 0; m < nm; ++m) {
+    if (!in_need[m]) in_base[m] = -1;
+    if (!owned[m]) out_base[m] = -1;
+  }
+  in_len = il;
+  out_len = ol;
+  windowed = true;
+  release_split(this);
+  CMPS_TRY(build_plans());
+  CMPS_TRY(select_order());
+  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(prepare_precision(this, CMPS_SPLIT_TF32));
+  return CMPS_OK;
+}
+
 int Heff::set_owned(const uint8_t* mask) {
   const int nm = (int)th.mq.size();
   CMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  default_windows();
   for (int m = 0; m < nm; ++m) owned[m] = mask[m] ? 1 : 0;
   release_split(this);
   CMPS_TRY(build_plans());
@@ -986,6 +1029,7 @@ int Heff::set_projectors(int np, const double* host_arpack, const double* weight
   if (np == 0) return CMPS_OK;
   if (np < 0 || np > 64) return fail(CMPS_ERR_ARG, "projectors: between 0 and 64 of them");
   if (!host_arpack || !weights) return fail(CMPS_ERR_ARG, "projectors: null argument");
+  if (windowed) return fail(CMPS_ERR_STATE, "projectors: the matvec has vector windows (sharded)");
   const int64_t n = th.total;
   CMPS_TRY(proj.alloc((int64_t)np * n));
   CMPS_CUDA(dmalloc(&d_proj, sizeof(double) * (3 * (size_t)np + 4)));
@@ -1054,7 +1098,7 @@ int Heff::add_projectors(const Planar& in, Planar& out, cudaStream_t st) {
 }
 
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
-  if (!all_owned()) return fail(CMPS_ERR_STATE, "matvec is sharded: use the theta-layout entry point");
+  if (!whole()) return fail(CMPS_ERR_STATE, "matvec is sharded: use the theta-layout entry point");
   CMPS_TRY(pack(din, x, st));
   if (precision == CMPS_SPLIT_TF32) {
     CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
@@ -1191,7 +1235,7 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   cudaStream_t st = ctx->stream;
   const int64_t n = th.total;
   if (n == 0) return fail(CMPS_ERR_STATE, "empty effective Hamiltonian");
-  if (!all_owned()) return fail(CMPS_ERR_STATE, "matvec is sharded: the single-GPU eigensolver needs every sector");
+  if (!whole()) return fail(CMPS_ERR_STATE, "matvec is sharded: the single-GPU eigensolver needs every sector");
   if (kdim < 2) kdim = 2;
   if (kdim > 96) kdim = 96;
   if ((int64_t)kdim > n) kdim = (int)n;

@@ -120,6 +120,20 @@ struct Heff {
   int build_plans();
   int set_owned(const uint8_t* mask);
   bool all_owned() const;
+  // Windows of the theta-layout entry point, for a sharded matvec whose ranks
+  // hold only part of the vectors: input sector m is read at in_base[m] of an
+  // input of in_len entries per plane, owned output sector m' is written at
+  // out_base[m'] of an output of out_len.  By default both are the theta
+  // layout itself.  in_need: the input sectors the owned outputs read.
+  std::vector<int64_t> in_base, out_base;
+  int64_t in_len = 0, out_len = 0;
+  bool windowed = false;
+  std::vector<uint8_t> in_need;
+  int set_windows(const int64_t* in_base, int64_t in_len, const int64_t* out_base, int64_t out_len);
+  void default_windows();
+  // every sector owned and the vectors in the theta layout: the whole-vector
+  // entry points (ARPACK order, eigensolver, adjoint) apply
+  bool whole() const { return all_owned() && !windowed; }
   // Excited-state projectors (TwoVertexComponents::ProjectorTensors,
   // DMRG_routines.hpp:205): the matvec adds sum_p w_p (P_p . x) conj(P_p),
   // the bilinear product P . x taken without conjugation
@@ -220,7 +234,8 @@ int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, 
                     Env& dLn, Env& dRn);
 
 // The canonical contraction order (canonical.cu).
-int canonical_flops(const Heff& H, double* flops);
+// need (optional): the theta sectors the canonical order's first stage reads
+int canonical_flops(const Heff& H, double* flops, std::vector<uint8_t>* need = nullptr);
 int build_canonical(Heff& H);
 void release_canonical(Heff* h);
 // which: 1 = stages L and W1, 2 = stages W2 and R, 0 = all four

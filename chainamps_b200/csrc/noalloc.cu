@@ -60,7 +60,7 @@ extern "C" int cmps_heff_apply_device_noalloc(cmps_heff* h, const double* d_in, 
   Heff& H = *h->impl;
   if (H.precision != CMPS_FP64)
     return fail(CMPS_ERR_ARG, "the no-allocation matvec runs the FP64 path only; set CMPS_FP64 on the handle");
-  if (H.proj_np || !H.all_owned())
+  if (H.proj_np || !H.whole())
     return fail(CMPS_ERR_ARG, "the no-allocation matvec runs the plain unsharded operator (no projectors)");
   const int64_t need = 4 * H.th.total + 2 * H.t_len;
   if (need > kNoAllocScratchDoubles)

@@ -362,7 +362,8 @@ static int build_split(Heff& H) {
         const int tp = A2.find(r.add(th.mq[mp], H.sigq[s2p]));
         Fused shape;
         shape.m = mp;
-        Seg sg{th.base[mp] + th.coloff[mp][s2p], (int32_t)A2.sdim[tp], {}};
+        if (H.out_base[mp] < 0) return fail(CMPS_ERR_ARG, "output window lacks an owned sector");
+        Seg sg{H.out_base[mp] + th.coloff[mp][s2p], (int32_t)A2.sdim[tp], {}};
         std::vector<int64_t> sig{(int64_t)mp};
         for (int b1 = 0; b1 < H.D; ++b1) {
           const int m = th.find(r.sub(th.mq[mp], H.bq[b1]));
@@ -460,21 +461,22 @@ static int build_split(Heff& H) {
     std::vector<ThetaTile> tiles;
     for (int m = 0; m < nm; ++m)
       for (int s1 = 0; s1 < d; ++s1) {
-        if (th.rowoff[m][s1] < 0) continue;
+        if (th.rowoff[m][s1] < 0 || !H.in_need[m]) continue;  // only the sectors the owned outputs read
+        if (H.in_base[m] < 0) return fail(CMPS_ERR_ARG, "input window lacks a sector the owned outputs read");
         int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
         const int64_t ch = s1a_chunk[{m, s1}];
         for (int s2 = 0; s2 < d; ++s2) {
           if (th.coloff[m][s2] < 0) continue;
           int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
           ThetaChunk c{};
-          c.src_off = th.base[m] + th.rowoff[m][s1] * th.ncols[m] + th.coloff[m][s2];
+          c.src_off = H.in_base[m] + th.rowoff[m][s1] * th.ncols[m] + th.coloff[m][s2];
           c.src_ld = th.ncols[m];
           c.dst_off = ch + S->coloff_pad[m][s2] * S->ldS[s];
           c.dst_ld = S->ldS[s];
           c.rows = (int32_t)A0.sdim[s];
           c.cols = (int32_t)A2.sdim[t];
           // both images inside their buffers
-          if (c.src_off + (int64_t)(c.rows - 1) * c.src_ld + c.cols > th.total ||
+          if (c.src_off + (int64_t)(c.rows - 1) * c.src_ld + c.cols > H.in_len ||
               c.dst_off + (int64_t)(c.cols - 1) * c.dst_ld + c.rows > S->s1a_len || c.dst_ld < c.rows)
             return fail(CMPS_ERR_STATE, "theta split chunk outside its buffer");
           for (int32_t r0 = 0; r0 < c.rows; r0 += 32)
@@ -583,7 +585,7 @@ static int build_split(Heff& H) {
     task.t1 = (int32_t)p2.terms.size();
     for (const Seg& sg : f.segs)
       if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
-                                th.total)
+                                H.out_len)
         return fail(CMPS_ERR_STATE, "stage-2 output outside theta");
     add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
     p2.tasks.push_back(task);
@@ -702,11 +704,9 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   }
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
-  const int64_t n = H.th.total;
-  (void)n;
   CMPS_TRY(split_theta(*S, in, st));
   CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st));
-  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->buf + S->ts_off, S->ts_len, S->d_err, st));
+  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), out.len, S->buf + S->ts_off, S->ts_len, S->d_err, st));
   return H.add_projectors(in, out, st);
 }
 
@@ -726,13 +726,12 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   if (H.low_canonical) return apply_canonical32(H, which, in, out, st);
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
-  const int64_t n = H.th.total;
   if (which == 1) {
     CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
     CMPS_TRY(split_theta(*S, in, st));
     return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st);
   }
-  return tc::launch(2, S->p2, nullptr, 0, out.re(), n, S->buf + S->ts_off, S->ts_len, S->d_err, st);
+  return tc::launch(2, S->p2, nullptr, 0, out.re(), out.len, S->buf + S->ts_off, S->ts_len, S->d_err, st);
 }
 
 int split_error(Heff& H) {

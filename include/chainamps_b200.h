@@ -170,8 +170,8 @@ int cmps_heff_set_projectors(cmps_heff* h, int count, const double* tensors, con
  * sector m of H_eff occupies elements [offsets[m], offsets[m+1]) of each
  * plane.  Each GPU of a sharded run holds the same handle (the environments
  * and the MPO are replicated), computes the output sectors it owns from the
- * whole input vector, and exchanges its slice with the others (an
- * all-gather per matvec, done by the caller).
+ * input sectors it reads, and receives those from the ranks that own them
+ * (an exchange per matvec, done by the caller).
  *
  * cmps_heff_sector_table: call with offsets = flops = NULL to read the
  * sector count into *n_sectors, then with arrays of *n_sectors + 1 offsets
@@ -183,11 +183,24 @@ int cmps_heff_sector_table(const cmps_heff* h, int64_t* n_sectors, int64_t* offs
  * other output blocks are left unwritten.  A handle that does not own every
  * sector accepts only cmps_heff_apply_theta_device (the ARPACK-order apply,
  * the eigensolver, the adjoint and the stage timing return CMPS_ERR_STATE);
- * owning every sector again restores them. */
+ * owning every sector again restores them.  It also returns the vector
+ * windows to the theta layout. */
 int cmps_heff_set_owned(cmps_heff* h, const uint8_t* owned);
-/* theta-layout matvec on DEVICE arrays, stream-ordered: d_in holds the whole
- * input vector (2 * total doubles, planar), d_out receives the owned output
- * sectors (same layout; d_out != d_in). */
+/* The input sectors the owned output sectors read (n_sectors bytes, 1 =
+ * read), for the current owned set and contraction order. */
+int cmps_heff_input_sectors(const cmps_heff* h, uint8_t* needed);
+/* Vector windows, so that a rank holds only what it reads and writes: input
+ * sector m (each sector the owned outputs read) is at in_base[m] of an input
+ * of in_len entries per plane, owned output sector m at out_base[m] of an
+ * output of out_len entries per plane (n_sectors entries each; other entries
+ * are ignored).  Every such sector must lie inside its window.  The plans are
+ * rebuilt; refused while projectors are set. */
+int cmps_heff_set_windows(cmps_heff* h, const int64_t* in_base, int64_t in_len, const int64_t* out_base,
+                          int64_t out_len);
+/* theta-layout matvec on DEVICE arrays, stream-ordered: d_in holds the input
+ * (2 * in_len doubles, planar; the whole vector, 2 * total, unless windows
+ * are set), d_out receives the owned output sectors (2 * out_len doubles;
+ * d_out != d_in). */
 int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out, void* stream);
 /* ARPACK order (n_allowed interleaved complex) <-> theta layout, on DEVICE
  * arrays.  theta_to_arpack reads every sector of its input. */

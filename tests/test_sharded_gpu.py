@@ -6,6 +6,10 @@
   their owned outputs equal the unsharded theta-layout matvec: bit for bit
   in FP64 and in split-TF32 (each output element is produced by the same
   tiles either way).
+* The same with vector windows: each handle reads a packed window of only
+  the input sectors its owned outputs read and writes only its owned slice,
+  both shorter than the vector; FP64, split-TF32 and the canonical order
+  (coupled Ising vertex) reassemble the unsharded matvec bit for bit.
 * A handle that owns only part of the sectors refuses the ARPACK-order
   apply and the eigensolver, and owns everything again after
   set_owned(all): its ARPACK-order apply is unchanged.
@@ -67,6 +71,77 @@ def test_two_shards_reassemble_the_matvec(ctx, precision):
     assert torch.equal(got, want)
 
 
+def _windowed_halves(ctx, rules, L, W, R, prec, order=None):
+    from chainamps_b200 import TwoVertexComponents
+    from chainamps_b200.sharded import ShardLayout, torch_stream_handle
+    full = TwoVertexComponents(ctx, rules, L, W, R, precision=prec)
+    if order is not None:
+        full.set_order(order)
+    off, fl = full.sector_table()
+    total = int(off[-1])
+    x = torch.randn(2, total, dtype=torch.float64, device="cuda")
+    want = torch.zeros_like(x)
+    full.multiply_theta_device(x.data_ptr(), want.data_ptr(), torch_stream_handle())
+    torch.cuda.synchronize()
+    lays = [ShardLayout(off, fl, 2, r) for r in range(2)]
+    hs = []
+    for lay in lays:
+        h = TwoVertexComponents(ctx, rules, L, W, R, precision=prec)
+        if order is not None:
+            h.set_order(order)
+        h.set_owned(lay.owned)
+        hs.append(h)
+    needs = np.stack([h.input_sectors() for h in hs])
+    got = torch.full_like(x, float("nan"))
+    for lay, h in zip(lays, hs):
+        lay.set_needs(needs)
+        assert lay.out_len < total
+        h.set_windows(lay.in_base, lay.in_len, lay.out_base, lay.out_len)
+        idx = np.concatenate([np.arange(off[m], off[m + 1]) for m in range(off.size - 1) if lay.in_base[m] >= 0])
+        xw = x[:, torch.as_tensor(idx, device="cuda")].contiguous()
+        assert xw.shape[1] == lay.in_len
+        y = torch.full((2, lay.out_len), float("nan"), dtype=torch.float64, device="cuda")
+        h.multiply_theta_device(xw.data_ptr(), y.data_ptr(), torch_stream_handle())
+        torch.cuda.synchronize()
+        h.status()
+        got[:, lay.lo:lay.hi] = y
+        h.close()
+    assert not torch.isnan(got).any()
+    return got, want, lays, total
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_windowed_shards_reassemble_the_matvec(ctx, precision):
+    from chainamps_b200 import CMPS_FP64, CMPS_SPLIT_TF32
+    rules, L, W, R = ladder(96)
+    got, want, lays, total = _windowed_halves(ctx, rules, L, W, R,
+                                              CMPS_FP64 if precision == "fp64" else CMPS_SPLIT_TF32)
+    assert torch.equal(got, want)
+    # total-Sz sectors couple to their neighbours only: each input window
+    # leaves out the far sectors
+    assert all(lay.in_len < total for lay in lays)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_windowed_shards_canonical_order(ctx, precision):
+    """The coupled-Ising vertex (canonical order; in split precision the FP32
+    canonical operator) with windows."""
+    from chainamps_b200 import CMPS_FP64, CMPS_SPLIT_TF32
+    from tests.helpers import ising_mpo, to_tensor, charge_pool_for, random_bond, random_left_block, \
+        random_right_block
+    H = ising_mpo(8, 16)
+    rng = np.random.default_rng(4)
+    pool = charge_pool_for(H)
+    bq = H.indices[1].charges
+    Lb = random_left_block(rng, H.rules, random_bond(rng, 20, pool), bq)
+    Rb = random_right_block(rng, H.rules, random_bond(rng, 18, pool), bq)
+    # (two Z2 sectors, each output reading both: the input window is the
+    # whole vector, the output window half of it)
+    got, want, _, _ = _windowed_halves(ctx, H.rules, to_tensor(Lb), to_tensor(H), to_tensor(Rb),
+                                       CMPS_FP64 if precision == "fp64" else CMPS_SPLIT_TF32)
+    assert torch.equal(got, want)
+
+
 def test_partial_handle_refuses_whole_vector_entry_points(ctx):
     from chainamps_b200 import TwoVertexComponents, CmpsError
     from chainamps_b200.sharded import ShardLayout
@@ -104,3 +179,15 @@ def test_sharded_lanczos_single_rank_matches_device_solver(ctx):
     e, x, mv, conv = sh.lowest(tol=1e-12, krylov_dim=32, max_restarts=80)
     assert conv, (e, mv)
     assert abs(e - e_dev) <= 1e-10 * abs(e_dev), (e, e_dev)
+    # HED's post-processing: the largest entry real positive, as the device
+    # eigensolver leaves its vector (overlap 1 within the solver tolerance)
+    e2, vec, _ = h.HED(tol=1e-12, krylov_dim=32)
+    xa = torch.empty(2 * h.n, dtype=torch.float64, device="cuda")
+    from chainamps_b200.sharded import torch_stream_handle
+    h.theta_to_arpack_device(x.contiguous().data_ptr(), xa.data_ptr(), torch_stream_handle())
+    torch.cuda.synchronize()
+    xv = xa.cpu().numpy()
+    xv = xv[0::2] + 1j * xv[1::2]
+    k = int(np.argmax(np.abs(xv)))
+    assert abs(xv[k].imag) == 0.0 and xv[k].real > 0
+    assert abs(abs(np.vdot(vec, xv)) - 1.0) <= 1e-8
