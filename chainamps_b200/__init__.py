@@ -7,7 +7,7 @@ library and fails loudly when it is not built -- there is no CPU fallback.
 """
 __all__ = ["Context", "TwoVertexComponents", "SVDResult", "Block", "MPXTensor", "MPXIndexSpec", "CmpsError",
            "upload_block", "iDMRG", "fDMRG", "run_excited_fdmrg", "DEFAULT_PROJECTOR_WEIGHT", "CMPS_FP64",
-           "CMPS_SPLIT_TF32", "CMPS_ORDER_AUTO", "CMPS_ORDER_FOLDED", "CMPS_ORDER_CANONICAL", "version"]
+           "CMPS_SPLIT_TF32", "CMPS_SPLIT_BF16", "CMPS_ORDER_AUTO", "CMPS_ORDER_FOLDED", "CMPS_ORDER_CANONICAL", "version"]
 
 
 def __getattr__(name):

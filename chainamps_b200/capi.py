@@ -30,6 +30,7 @@ LIBPATH = os.path.join(HERE, "libchainamps_b200.so")
 
 CMPS_FP64 = 0
 CMPS_SPLIT_TF32 = 1
+CMPS_SPLIT_BF16 = 2
 CMPS_ORDER_AUTO = 0
 CMPS_ORDER_FOLDED = 1
 CMPS_ORDER_CANONICAL = 2

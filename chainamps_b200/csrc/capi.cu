@@ -170,7 +170,7 @@ int cmps_heff_create(cmps_context* ctx, const cmps_charge_rules* rules, const cm
   CMPS_TRY(use_device(ctx));
   Rules r;
   CMPS_TRY(rules_from(rules, r));
-  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (precision != CMPS_FP64 && !is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
   auto h = std::unique_ptr<cmps_heff>(new (std::nothrow) cmps_heff());
   if (!h) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   h->impl.reset(new (std::nothrow) Heff());
@@ -188,7 +188,7 @@ int cmps_heff_create_from_blocks(cmps_context* ctx, const cmps_charge_rules* rul
   CMPS_TRY(use_device(ctx));
   Rules r;
   CMPS_TRY(rules_from(rules, r));
-  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (precision != CMPS_FP64 && !is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
   auto h = std::unique_ptr<cmps_heff>(new (std::nothrow) cmps_heff());
   if (!h) return fail(CMPS_ERR_NOMEM, "host allocation failed");
   h->impl.reset(new (std::nothrow) Heff());
@@ -302,7 +302,7 @@ int cmps_heff_apply_theta_device(cmps_heff* h, const double* d_in, double* d_out
   out.d = d_out;
   out.len = H.out_len;
   int rc;
-  if (H.precision == CMPS_SPLIT_TF32) {
+  if (is_split(H.precision)) {
     rc = apply_split_stage(H, 1, in, out, st);
     if (rc == CMPS_OK) rc = apply_split_stage(H, 2, in, out, st);
     if (rc == CMPS_OK) rc = H.add_projectors(in, out, st);
@@ -417,7 +417,7 @@ int cmps_heff_order(const cmps_heff* h, int* active, double* executed_folded, do
 
 int cmps_heff_set_precision(cmps_heff* h, int precision) {
   if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
-  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (precision != CMPS_FP64 && !is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
   CMPS_TRY(prepare_precision(h->impl.get(), precision));
   h->impl->precision = precision;
   return CMPS_OK;

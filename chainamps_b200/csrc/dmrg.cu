@@ -618,7 +618,7 @@ int cmps_dmrg_create(cmps_context* ctx, const cmps_charge_rules* rules, const cm
                      const int16_t* target, int precision, cmps_dmrg** out) {
   if (!ctx || !rules || !W || !out) return fail(CMPS_ERR_ARG, "null argument");
   *out = nullptr;
-  if (precision != CMPS_FP64 && precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (precision != CMPS_FP64 && !is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
   CMPS_CUDA(cudaSetDevice(ctx->device));
   auto d = std::unique_ptr<cmps_dmrg>(new cmps_dmrg());
   d->impl.reset(new Dmrg());

@@ -784,7 +784,7 @@ int Heff::select_order() {
     release_canonical(this);
   }
   order = want;
-  if (low || (precision == CMPS_SPLIT_TF32 && !split)) CMPS_TRY(prepare_precision(this, precision));
+  if (low || (is_split(precision) && !split)) CMPS_TRY(prepare_precision(this, precision));
   return CMPS_OK;
 }
 
@@ -945,7 +945,7 @@ int Heff::set_windows(const int64_t* ib, int64_t il, const int64_t* ob, int64_t 
   release_split(this);
   CMPS_TRY(build_plans());
   CMPS_TRY(select_order());
-  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(prepare_precision(this, CMPS_SPLIT_TF32));
+  if (is_split(precision)) CMPS_TRY(prepare_precision(this, precision));
   return CMPS_OK;
 }
 
@@ -957,7 +957,7 @@ int Heff::set_owned(const uint8_t* mask) {
   release_split(this);
   CMPS_TRY(build_plans());
   CMPS_TRY(select_order());
-  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(prepare_precision(this, CMPS_SPLIT_TF32));
+  if (is_split(precision)) CMPS_TRY(prepare_precision(this, precision));
   return CMPS_OK;
 }
 
@@ -976,7 +976,7 @@ int Heff::ensure_T() {
 // which = 1: the first half of the matvec (folded: T = LeftPart . in;
 // canonical: stages L and W1), 2: the second half.
 int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st) {
-  if (precision == CMPS_SPLIT_TF32) return apply_split_stage(*this, which, in, out, st);
+  if (is_split(precision)) return apply_split_stage(*this, which, in, out, st);
   if (order == CMPS_ORDER_CANONICAL) return apply_canonical(*this, which, in, out, st);
   CMPS_TRY(ensure_T());
   if (which == 1) return launch_zgemm_fp64(stage1, false, false, LP, in, T, st);
@@ -984,7 +984,7 @@ int Heff::apply_stage(int which, const Planar& in, Planar& out, cudaStream_t st)
 }
 
 int Heff::apply_theta(const Planar& in, Planar& out, cudaStream_t st) {
-  if (precision == CMPS_SPLIT_TF32) return apply_split(*this, in, out, st);
+  if (is_split(precision)) return apply_split(*this, in, out, st);
   CMPS_TRY(apply_stage(1, in, out, st));
   CMPS_TRY(apply_stage(2, in, out, st));
   return add_projectors(in, out, st);
@@ -1100,7 +1100,7 @@ int Heff::add_projectors(const Planar& in, Planar& out, cudaStream_t st) {
 int Heff::apply_device(const double* din, double* dout, cudaStream_t st) {
   if (!whole()) return fail(CMPS_ERR_STATE, "matvec is sharded: use the theta-layout entry point");
   CMPS_TRY(pack(din, x, st));
-  if (precision == CMPS_SPLIT_TF32) {
+  if (is_split(precision)) {
     CMPS_TRY(apply_split_stage(*this, 1, x, y, st));
     CMPS_TRY(apply_split_stage(*this, 2, x, y, st));
     CMPS_TRY(add_projectors(x, y, st));
@@ -1118,7 +1118,7 @@ int Heff::apply_host(const double* in, double* out) {
   CMPS_TRY(apply_device(d_io, d_io, st));
   CMPS_CUDA(cudaMemcpyAsync(out, d_io, bytes, cudaMemcpyDeviceToHost, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
-  if (precision == CMPS_SPLIT_TF32) CMPS_TRY(split_error(*this));
+  if (is_split(precision)) CMPS_TRY(split_error(*this));
   return CMPS_OK;
 }
 
@@ -1281,7 +1281,7 @@ int Heff::eigs(const double* guess, double tol, int max_restarts, int kdim, doub
   CMPS_TRY(ops.mdot_dev(nullptr, nullptr, 0, 0, x.re(), x.im(), nrm, st));
   CMPS_TRY(ops.scale_dev(x.re(), x.im(), nrm, true, x.re(), x.im(), st));
 
-  const bool mixed = precision == CMPS_SPLIT_TF32;
+  const bool mixed = is_split(precision);
   if (mixed) CMPS_TRY(split_reset_error(*this, st));
   bool all_fp64 = !mixed;
   const int max_cycles = std::max(1, max_restarts) * (mixed ? 4 : 1);

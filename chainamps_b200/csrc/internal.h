@@ -91,6 +91,9 @@ struct Bond {
   std::vector<QKey> element_charges() const;
 };
 
+// A split-precision form (the mixed eigensolver's low-precision operator).
+inline bool is_split(int precision) { return precision == CMPS_SPLIT_TF32 || precision == CMPS_SPLIT_BF16; }
+
 // Device buffer of complex values stored as two planes (re then im).
 struct Planar {
   double* d = nullptr;

@@ -1,25 +1,32 @@
-// Split-precision (3-term TF32 on tcgen05, FP32 accumulate) form of the
-// H_eff matvec: operand preparation, tensor maps and the two stage plans.
+// Split-precision (3-term TF32 or 3-term BF16 on tcgen05, FP32 accumulate)
+// form of the H_eff matvec: operand preparation, tensor maps and the two
+// stage plans.
 //
-// Layouts (FP32; S1A, LPS and RPTS as four planes re_hi, re_lo, im_hi, im_lo,
-// TS as two planes re, im):
+// Layouts (split-TF32: FP32; S1A, LPS and RPTS as four planes re_hi, re_lo,
+// im_hi, im_lo, TS as two planes re, im.  Split-BF16: 16-bit elements, every
+// buffer -- TS included -- as four planes re_hi, re_mid, im_hi, im_mid):
 //  * S1A  -- stage-1 A operand: theta transposed per (m, sigma1) chunk,
 //            [r][a0] with r running over the padded right index of m (each
 //            sigma2 chunk starts on a 4-element boundary) and ld = pad4(dim a0);
 //  * LPS  -- stage-1 B operand: for every term of a (fused) task, the
 //            LeftPart blocks [a0'][a0] of its column segments stacked along
 //            a0', ld = pad4(dim a0);
-//  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad], the
-//            FP32 accumulator; stage 2 splits it into TF32 hi / lo in shared
-//            memory, so T crosses HBM at 8 bytes per complex entry each way;
+//  * TS   -- stage-1 output = stage-2 A operand: T^{b1}_m as [l'][r_pad].
+//            Split-TF32: the FP32 accumulator; stage 2 splits it into TF32
+//            hi / lo in shared memory.  Split-BF16: the stage-1 epilogue
+//            writes the four BF16 planes and stage 2 loads them by TMA.  Either
+//            way T crosses HBM at 8 bytes per complex entry each way;
 //  * RPTS -- stage-2 B operand: RightPart blocks transposed, [a2'][a2], the
 //            blocks of a fused task's segments stacked along a2'.
-// Every block base is 128-byte aligned and every leading dimension a multiple
-// of 4 floats, as the TMA requires; the K tail of every operand is zero-filled
-// by the TMA (out-of-bounds fill), padding rows of S1A are zero.
+// Every block base is 128-byte aligned and every leading dimension and K
+// offset a multiple of 16 bytes (4 FP32, 8 BF16 elements), as the TMA
+// requires; the K tail of every operand is zero-filled by the TMA
+// (out-of-bounds fill), padding rows of S1A are zero.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
+
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstring>
@@ -31,11 +38,12 @@
 namespace cmps {
 
 struct SplitState {
+  bool bf16 = false;                            // split-BF16 (16-bit elements) or split-TF32 (FP32)
   std::vector<int64_t> ldS;                     // per a0 sector
   std::vector<int64_t> ldR;                     // per a2 sector
   std::vector<std::vector<int64_t>> coloff_pad;  // [m][sigma2]
   std::vector<int64_t> ncols_pad;               // per m
-  float* buf = nullptr;                         // one allocation for S1A, LPS, TS, RPTS
+  float* buf = nullptr;                         // one allocation for S1A, LPS, TS, RPTS (elements of 2 or 4 bytes)
   int64_t s1a_off = 0, s1a_len = 0, lps_off = 0, lps_len = 0, ts_off = 0, ts_len = 0, rpt_off = 0, rpt_len = 0;
   // theta -> S1A: one descriptor per (m, sigma1, sigma2) chunk, one per 32x32 tile
   void* d_theta_chunks = nullptr;
@@ -44,13 +52,15 @@ struct SplitState {
   int* d_err = nullptr;
   int* h_err = nullptr;  // pinned
   tc::TcPlan p1, p2;
-  float* plane_base(int64_t off) const { return buf + off; }
+  // element `off` of the buffer, as a raw pointer of the element type
+  void* at(int64_t off) const { return bf16 ? (void*)((uint16_t*)buf + off) : (void*)(buf + off); }
+  float* f32(int64_t off) const { return (float*)at(off); }
+  int64_t pad(int64_t x) const { return bf16 ? (x + 7) & ~int64_t(7) : (x + 3) & ~int64_t(3); }
+  int64_t align(int64_t x) const { return bf16 ? (x + 63) & ~int64_t(63) : (x + 31) & ~int64_t(31); }
 };
 
 namespace {
 
-inline int64_t pad4(int64_t x) { return (x + 3) & ~int64_t(3); }
-inline int64_t align32(int64_t x) { return (x + 31) & ~int64_t(31); }
 
 __device__ __forceinline__ float rna(float x) {
   uint32_t r;
@@ -64,6 +74,15 @@ __device__ __forceinline__ void split4(double re, double im, float* p0, float* p
   *p2 = hi;
   *p3 = rna((float)(im - (double)hi));
 }
+// BF16: hi = x rounded to BF16, mid = x - hi rounded to BF16 (raw bits)
+__device__ __forceinline__ void split4(double re, double im, uint16_t* p0, uint16_t* p1, uint16_t* p2,
+                                       uint16_t* p3) {
+  const __nv_bfloat16 hr = __double2bfloat16(re), hi = __double2bfloat16(im);
+  *p0 = __bfloat16_as_ushort(hr);
+  *p1 = __bfloat16_as_ushort(__double2bfloat16(re - (double)__bfloat162float(hr)));
+  *p2 = __bfloat16_as_ushort(hi);
+  *p3 = __bfloat16_as_ushort(__double2bfloat16(im - (double)__bfloat162float(hi)));
+}
 
 struct SplitBlock {
   int64_t src_off, dst_off;
@@ -71,8 +90,9 @@ struct SplitBlock {
 };
 
 // dst (4 planes) <- split(src block), optionally transposed.
+template <class E>
 __global__ void k_split_blocks(const SplitBlock* __restrict__ blocks, const double* __restrict__ sr,
-                               const double* __restrict__ si, float* __restrict__ dst, int64_t plane) {
+                               const double* __restrict__ si, E* __restrict__ dst, int64_t plane) {
   const SplitBlock b = blocks[blockIdx.x];
   const int64_t n = (int64_t)b.rows * b.cols;
   for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
@@ -93,12 +113,17 @@ struct ThetaTile {
 };
 
 // theta -> split S1A, one 32 x 32 tile per CTA, transposed through shared
-// memory so that both the FP64 reads and the FP32 plane writes coalesce.
+// memory so that both the FP64 reads and the plane writes coalesce.
+template <class E>
+struct Quad {
+  E x, y, z, w;
+};
+template <class E>
 __global__ void __launch_bounds__(256) k_split_theta_t(const ThetaTile* __restrict__ tiles,
                                                        const ThetaChunk* __restrict__ chunks,
                                                        const double* __restrict__ re, const double* __restrict__ im,
-                                                       float* __restrict__ dst, int64_t plane) {
-  __shared__ float4 t[32][33];
+                                                       E* __restrict__ dst, int64_t plane) {
+  __shared__ Quad<E> t[32][33];
   const ThetaTile tl = tiles[blockIdx.x];
   const ThetaChunk c = chunks[tl.chunk];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -107,7 +132,7 @@ __global__ void __launch_bounds__(256) k_split_theta_t(const ThetaTile* __restri
     const int r = tl.r0 + ty + 8 * k, col = tl.c0 + tx;
     if (r < c.rows && col < c.cols) {
       const int64_t o = c.src_off + (int64_t)r * c.src_ld + col;
-      float4 v;
+      Quad<E> v;
       split4(re[o], im[o], &v.x, &v.y, &v.z, &v.w);
       t[ty + 8 * k][tx] = v;
     }
@@ -117,7 +142,7 @@ __global__ void __launch_bounds__(256) k_split_theta_t(const ThetaTile* __restri
   for (int k = 0; k < 4; ++k) {
     const int col = tl.c0 + ty + 8 * k, r = tl.r0 + tx;
     if (r < c.rows && col < c.cols) {
-      const float4 v = t[tx][ty + 8 * k];
+      const Quad<E> v = t[tx][ty + 8 * k];
       const int64_t o = c.dst_off + (int64_t)col * c.dst_ld + r;
       dst[o] = v.x;
       dst[o + plane] = v.y;
@@ -139,22 +164,25 @@ int encoder() {
   return CMPS_OK;
 }
 
-// 3-D map over one operand block: (K, rows, 4 planes); box (16, box_rows, 4).
-// `base_off` is the block's element offset inside its plane of `plane`
-// elements; the block must lie inside the plane.
-int make_map(float* plane0, int64_t base_off, int64_t K, int64_t rows, int64_t ld, int64_t plane, CUtensorMap* out,
-             int box_rows = 128) {
-  float* base = plane0 + base_off;
-  if (((uintptr_t)base & 15) || (ld * 4) % 16 || (plane * 4) % 16 || K < 1 || rows < 1 || K > ld)
+// 3-D map over one operand block: (K, rows, 4 planes); box (64 bytes of K,
+// box_rows, 4).  The role's planes start at element role_off of the buffer,
+// `plane` elements apart (FP32, or BF16 for split-BF16); `base_off` is the
+// block's offset inside its plane, and the block must lie inside the plane.
+int make_map(const SplitState& S, int64_t role_off, int64_t base_off, int64_t K, int64_t rows, int64_t ld,
+             int64_t plane, CUtensorMap* out, int box_rows = 128) {
+  const int64_t es_b = S.bf16 ? 2 : 4;
+  const char* base = (const char*)S.at(role_off + base_off);
+  if (((uintptr_t)base & 15) || (ld * es_b) % 16 || (plane * es_b) % 16 || K < 1 || rows < 1 || K > ld)
     return fail(CMPS_ERR_STATE, "tensor map: misaligned operand block");
   if (base_off < 0 || base_off + (rows - 1) * ld + K > plane)
     return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
   cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, 4};
-  cuuint64_t strides[2] = {(cuuint64_t)(ld * 4), (cuuint64_t)(plane * 4)};
+  cuuint64_t strides[2] = {(cuuint64_t)(ld * es_b), (cuuint64_t)(plane * es_b)};
   if (box_rows < 16 || box_rows > 128 || (box_rows & 15)) return fail(CMPS_ERR_STATE, "tensor map: bad box height");
-  cuuint32_t box[3] = {16, (cuuint32_t)box_rows, 4};
+  cuuint32_t box[3] = {(cuuint32_t)(64 / es_b), (cuuint32_t)box_rows, 4};
   cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = g_encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+  CUresult r = g_encode(out, S.bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                        (void*)base, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(CMPS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -227,7 +255,7 @@ void release_split(Heff* h) {
 constexpr int32_t kFuseMaxSegN1 = CMPS_FUSE_MAX_SEG_N1;
 constexpr int32_t kFuseMaxSegN2 = CMPS_FUSE_MAX_SEG_N2;
 
-static int build_split(Heff& H) {
+static int build_split(Heff& H, bool bf16) {
   CMPS_TRY(encoder());
   const Rules& r = H.rules;
   const ThetaSpace& th = H.th;
@@ -236,10 +264,11 @@ static int build_split(Heff& H) {
   const int d = H.d, nm = (int)th.mq.size();
   auto* S = new SplitState();
   H.split = S;
+  S->bf16 = bf16;
   S->ldS.resize(A0.nsec());
-  for (int s = 0; s < A0.nsec(); ++s) S->ldS[s] = pad4(A0.sdim[s]);
+  for (int s = 0; s < A0.nsec(); ++s) S->ldS[s] = S->pad(A0.sdim[s]);
   S->ldR.resize(A2.nsec());
-  for (int t = 0; t < A2.nsec(); ++t) S->ldR[t] = pad4(A2.sdim[t]);
+  for (int t = 0; t < A2.nsec(); ++t) S->ldR[t] = S->pad(A2.sdim[t]);
   S->coloff_pad.assign(nm, std::vector<int64_t>(d, -1));
   S->ncols_pad.assign(nm, 0);
   for (int m = 0; m < nm; ++m) {
@@ -248,7 +277,7 @@ static int build_split(Heff& H) {
       if (th.coloff[m][s2] < 0) continue;
       int t = A2.find(r.add(th.mq[m], H.sigq[s2]));
       S->coloff_pad[m][s2] = o;
-      o += pad4(A2.sdim[t]);
+      o += S->pad(A2.sdim[t]);
     }
     S->ncols_pad[m] = o;
   }
@@ -260,7 +289,7 @@ static int build_split(Heff& H) {
       if (th.rowoff[m][s1] < 0) continue;
       int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
       s1a_chunk[{m, s1}] = s1a;
-      s1a += align32(S->ncols_pad[m] * S->ldS[s]);
+      s1a += S->align(S->ncols_pad[m] * S->ldS[s]);
     }
   std::vector<int64_t> ts_base((size_t)H.D * nm, -1);
   int64_t ts = 0;
@@ -269,7 +298,7 @@ static int build_split(Heff& H) {
       if (H.t_base[(size_t)b1 * nm + m] < 0) continue;
       int mp = th.find(r.add(th.mq[m], H.bq[b1]));
       ts_base[(size_t)b1 * nm + m] = ts;
-      ts += align32(th.nrows[mp] * S->ncols_pad[m]);
+      ts += S->align(th.nrows[mp] * S->ncols_pad[m]);
     }
   // ---- tasks, fused along N ----
   // A stage-1 task (b1, sigma1') computes rows sigma1' of T^{b1}_m; a stage-2
@@ -397,7 +426,7 @@ static int build_split(Heff& H) {
         lpsb.push_back(SplitBlock{H.lp_off.at(sg.keys[q]), lps + row * ld, sg.n, (int32_t)A0.sdim[sa], (int32_t)ld, 0});
         row += sg.n;
       }
-      lps += align32(f.ntot * ld);
+      lps += S->align(f.ntot * ld);
     }
   }
   for (size_t i = 0; i < f2.size(); ++i) {
@@ -412,22 +441,23 @@ static int build_split(Heff& H) {
         rptb.push_back(SplitBlock{H.rp_off.at(sg.keys[q]), rpt + row * ld, (int32_t)A2.sdim[t], sg.n, (int32_t)ld, 1});
         row += sg.n;
       }
-      rpt += align32(f.ntot * ld);
+      rpt += S->align(f.ntot * ld);
     }
   }
   S->s1a_off = 0;
-  S->s1a_len = align32(std::max<int64_t>(s1a, 32));
+  S->s1a_len = S->align(std::max<int64_t>(s1a, 32));
   S->lps_off = 4 * S->s1a_len;
-  S->lps_len = align32(std::max<int64_t>(lps, 32));
+  S->lps_len = S->align(std::max<int64_t>(lps, 32));
   S->ts_off = S->lps_off + 4 * S->lps_len;
-  S->ts_len = align32(std::max<int64_t>(ts, 32));
-  S->rpt_off = S->ts_off + 2 * S->ts_len;  // T: two FP32 planes (re, im)
-  S->rpt_len = align32(std::max<int64_t>(rpt, 32));
+  S->ts_len = S->align(std::max<int64_t>(ts, 32));
+  S->rpt_off = S->ts_off + (S->bf16 ? 4 : 2) * S->ts_len;  // T: two FP32 planes (re, im) or four BF16
+  S->rpt_len = S->align(std::max<int64_t>(rpt, 32));
   const int64_t total = S->rpt_off + 4 * S->rpt_len;
-  if (dmalloc(&S->buf, sizeof(float) * total) != cudaSuccess)
+  const size_t ebytes = S->bf16 ? 2 : 4;
+  if (dmalloc(&S->buf, ebytes * total) != cudaSuccess)
     return fail(CMPS_ERR_NOMEM, "split-TF32 operand allocation failed");
   // zero fill: padding rows and columns of every operand must read as zero
-  CMPS_TRY(zero_wait(S->buf, sizeof(float) * total, H.ctx->stream));
+  CMPS_TRY(zero_wait(S->buf, ebytes * total, H.ctx->stream));
   CMPS_CUDA(dmalloc(&S->d_err, sizeof(int)));
   CMPS_TRY(zero_wait(S->d_err, sizeof(int), H.ctx->stream));
   CMPS_CUDA(cudaMallocHost(&S->h_err, sizeof(int)));
@@ -447,9 +477,14 @@ static int build_split(Heff& H) {
       CMPS_CUDA(dmalloc(&d, sizeof(SplitBlock) * v.size()));
       CMPS_TRY(copy_wait(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice, H.ctx->stream));
       const Planar& src = pass == 0 ? H.LP : H.RP;
-      float* dst = S->buf + (pass == 0 ? S->lps_off : S->rpt_off);
       const int64_t plane = pass == 0 ? S->lps_len : S->rpt_len;
-      k_split_blocks<<<(unsigned)v.size(), 256, 0, H.ctx->stream>>>(d, src.re(), src.im(), dst, plane);
+      void* dst = S->at(pass == 0 ? S->lps_off : S->rpt_off);
+      if (S->bf16)
+        k_split_blocks<uint16_t><<<(unsigned)v.size(), 256, 0, H.ctx->stream>>>(d, src.re(), src.im(),
+                                                                               (uint16_t*)dst, plane);
+      else
+        k_split_blocks<float><<<(unsigned)v.size(), 256, 0, H.ctx->stream>>>(d, src.re(), src.im(), (float*)dst,
+                                                                            plane);
       CMPS_CUDA(cudaGetLastError());
       CMPS_CUDA(cudaStreamSynchronize(H.ctx->stream));
       dfree(d);
@@ -502,7 +537,7 @@ static int build_split(Heff& H) {
     int m = kv.first.first, s1 = kv.first.second;
     int s = A0.find(r.sub(th.mq[m], H.sigq[s1]));
     CUtensorMap cm;
-    CMPS_TRY(make_map(S->buf + S->s1a_off, kv.second, A0.sdim[s], S->ncols_pad[m], S->ldS[s], S->s1a_len, &cm));
+    CMPS_TRY(make_map(*S, S->s1a_off, kv.second, A0.sdim[s], S->ncols_pad[m], S->ldS[s], S->s1a_len, &cm));
     amap1[kv.first] = (int32_t)p1.amaps.size();
     p1.amaps.push_back(cm);
   }
@@ -530,14 +565,14 @@ static int build_split(Heff& H) {
     for (size_t q = 0; q < f.tk.size(); ++q) {
       const int s1 = f.tk[q][0], sa = f.tk[q][1];
       CUtensorMap cm;
-      CMPS_TRY(make_map(S->buf + S->lps_off, f1_base[i][q], A0.sdim[sa], f.ntot, S->ldS[sa], S->lps_len, &cm,
+      CMPS_TRY(make_map(*S, S->lps_off, f1_base[i][q], A0.sdim[sa], f.ntot, S->ldS[sa], S->lps_len, &cm,
                         tc::b_box_rows(f.ntot)));
       p1.terms.push_back(tc::TcTerm{amap1[{m, s1}], (int32_t)p1.bmaps.size(), 0, (int32_t)A0.sdim[sa]});
       p1.bmaps.push_back(cm);
       b1_rows.push_back(f.ntot);
     }
     task.t1 = (int32_t)p1.terms.size();
-    // output range check of every segment (two planes of TS)
+    // output range check of every segment (two FP32 or four BF16 planes of TS)
     for (const Seg& sg : f.segs)
       if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
                                 S->ts_len)
@@ -553,6 +588,14 @@ static int build_split(Heff& H) {
       const int64_t tb = ts_base[(size_t)b1 * nm + m];
       if (tb < 0) continue;
       int mp = th.find(r.add(th.mq[m], H.bq[b1]));
+      if (S->bf16) {
+        // T^{b1}_m as four BF16 planes, loaded by TMA
+        CUtensorMap cm;
+        CMPS_TRY(make_map(*S, S->ts_off, tb, S->ncols_pad[m], th.nrows[mp], S->ncols_pad[m], S->ts_len, &cm));
+        amap2[(size_t)b1 * nm + m] = (int32_t)p2.amaps.size();
+        p2.amaps.push_back(cm);
+        continue;
+      }
       // T^{b1}_m as two FP32 planes, read and split by the converter warps
       tc::TcADesc ad{tb, S->ncols_pad[m], (int32_t)th.nrows[mp], (int32_t)S->ncols_pad[m]};
       if (tb < 0 || tb % 4 || ad.ld % 4 || tb + (ad.rows - 1) * ad.ld + ad.cols > S->ts_len)
@@ -576,7 +619,7 @@ static int build_split(Heff& H) {
       if (am < 0) return fail(CMPS_ERR_STATE, "stage-2 term without its T block");
       CUtensorMap cm;
       // destination layout [a2'][a2]: rows = fused N, K = dim t
-      CMPS_TRY(make_map(S->buf + S->rpt_off, f2_base[i][q], A2.sdim[t], f.ntot, S->ldR[t], S->rpt_len, &cm,
+      CMPS_TRY(make_map(*S, S->rpt_off, f2_base[i][q], A2.sdim[t], f.ntot, S->ldR[t], S->rpt_len, &cm,
                         tc::b_box_rows(f.ntot)));
       p2.terms.push_back(tc::TcTerm{am, (int32_t)p2.bmaps.size(), (int32_t)S->coloff_pad[m][s2], (int32_t)A2.sdim[t]});
       p2.bmaps.push_back(cm);
@@ -595,7 +638,8 @@ static int build_split(Heff& H) {
     for (tc::TcTile& t : p->tiles) {
       const tc::TcTask& k = p->tasks[t.task];
       int64_t it = 0;
-      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + 15) / 16;
+      const int32_t ks = tc::kstep(S->bf16);
+      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + ks - 1) / ks;
       if (it > 0x7fffffff) return fail(CMPS_ERR_ARG, "tcgen05 plan: too many k-steps in one tile");
       t.kiters = (int32_t)it;
     }
@@ -610,12 +654,16 @@ static int build_split(Heff& H) {
   }
   // plan integrity: every term names an existing map, every tile an existing task
   for (const tc::TcPlan* p : {&p1, &p2}) {
-    const int32_t na = (int32_t)(p == &p1 ? p->amaps.size() : p->adescs.size());
+    const bool by_tma = p == &p1 || S->bf16;
+    const int32_t na = (int32_t)(by_tma ? p->amaps.size() : p->adescs.size());
+    // a TMA copy starts on a 16-byte boundary: the K offset a multiple of
+    // 4 FP32 or 8 BF16 elements
+    const int32_t amask = S->bf16 ? 7 : 3;
     for (const tc::TcTerm& tm : p->terms)
       if (tm.a_map < 0 || tm.a_map >= na || tm.b_map < 0 || tm.b_map >= (int32_t)p->bmaps.size() || tm.k < 1 ||
-          (tm.a_x0 & 3))
+          (tm.a_x0 & amask))
         return fail(CMPS_ERR_STATE, "tcgen05 plan: bad term");
-    if (p == &p2)
+    if (p == &p2 && !S->bf16)
       for (const tc::TcTerm& tm : p->terms)
         if (tm.a_x0 + tm.k > p->adescs[tm.a_map].cols) return fail(CMPS_ERR_STATE, "tcgen05 plan: term past its T block");
     for (const tc::TcTask& t : p->tasks)
@@ -650,7 +698,8 @@ static int build_split(Heff& H) {
       if (tl.nmma < 16 || tl.nmma > 128 || tl.nmma != ((std::min(128, t.n - tl.n0) + 15) & ~15) || tl.nmma > tl.b_rows)
         return fail(CMPS_ERR_STATE, "tcgen05 plan: tile N");
       int64_t it = 0;
-      for (int q = t.t0; q < t.t1; ++q) it += (p.terms[q].k + 15) / 16;
+      const int32_t ks = tc::kstep(S->bf16);
+      for (int q = t.t0; q < t.t1; ++q) it += (p.terms[q].k + ks - 1) / ks;
       if (it != tl.kiters) return fail(CMPS_ERR_STATE, "tcgen05 plan: tile k-steps");
     }
   }
@@ -668,23 +717,39 @@ constexpr double kLowCanonicalRatio = 0.25;
 
 int prepare_precision(Heff* h, int precision) {
   if (precision == CMPS_FP64) return CMPS_OK;
-  if (precision != CMPS_SPLIT_TF32) return fail(CMPS_ERR_ARG, "unknown precision");
+  if (!is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
+  // a split operator of the other format is rebuilt
+  if (h->split && h->split->bf16 != (precision == CMPS_SPLIT_BF16)) release_split(h);
   if (h->split || h->low_canonical) return CMPS_OK;
   if (h->canon && h->flops_canon <= kLowCanonicalRatio * h->flops_folded) {
     CMPS_TRY(build_canonical32(*h));
     h->low_canonical = true;
     return CMPS_OK;
   }
-  int st = build_split(*h);
+  int st = build_split(*h, precision == CMPS_SPLIT_BF16);
   if (st != CMPS_OK) release_split(h);
   return st;
 }
 
+// stage 1 (T = LeftPart . theta) or stage 2 (theta' = T . RightPart) of a
+// prepared split operator: tcgen05 modes 1 / 2 (TF32) or 3 / 4 (BF16)
+static int launch_stage(const SplitState& S, int which, Planar& out, cudaStream_t st) {
+  if (which == 1)
+    return tc::launch(S.bf16 ? 3 : 1, S.p1, S.f32(S.ts_off), S.ts_len, nullptr, 0, nullptr, 0, S.d_err, st);
+  if (S.bf16) return tc::launch(4, S.p2, nullptr, 0, out.re(), out.len, nullptr, 0, S.d_err, st);
+  return tc::launch(2, S.p2, nullptr, 0, out.re(), out.len, S.f32(S.ts_off), S.ts_len, S.d_err, st);
+}
+
 static int split_theta(const SplitState& S, const Planar& in, cudaStream_t st) {
   if (S.n_theta_tiles == 0) return CMPS_OK;
-  k_split_theta_t<<<(unsigned)S.n_theta_tiles, 256, 0, st>>>((const ThetaTile*)S.d_theta_tiles,
-                                                             (const ThetaChunk*)S.d_theta_chunks, in.re(), in.im(),
-                                                             S.buf + S.s1a_off, S.s1a_len);
+  if (S.bf16)
+    k_split_theta_t<uint16_t><<<(unsigned)S.n_theta_tiles, 256, 0, st>>>(
+        (const ThetaTile*)S.d_theta_tiles, (const ThetaChunk*)S.d_theta_chunks, in.re(), in.im(),
+        (uint16_t*)S.at(S.s1a_off), S.s1a_len);
+  else
+    k_split_theta_t<float><<<(unsigned)S.n_theta_tiles, 256, 0, st>>>(
+        (const ThetaTile*)S.d_theta_tiles, (const ThetaChunk*)S.d_theta_chunks, in.re(), in.im(),
+        S.f32(S.s1a_off), S.s1a_len);
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;
 }
@@ -705,8 +770,8 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   SplitState* S = H.split;
   if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
   CMPS_TRY(split_theta(*S, in, st));
-  CMPS_TRY(tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st));
-  CMPS_TRY(tc::launch(2, S->p2, nullptr, 0, out.re(), out.len, S->buf + S->ts_off, S->ts_len, S->d_err, st));
+  CMPS_TRY(launch_stage(*S, 1, out, st));
+  CMPS_TRY(launch_stage(*S, 2, out, st));
   return H.add_projectors(in, out, st);
 }
 
@@ -729,9 +794,9 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   if (which == 1) {
     CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
     CMPS_TRY(split_theta(*S, in, st));
-    return tc::launch(1, S->p1, S->buf + S->ts_off, S->ts_len, nullptr, 0, nullptr, 0, S->d_err, st);
+    return launch_stage(*S, 1, out, st);
   }
-  return tc::launch(2, S->p2, nullptr, 0, out.re(), out.len, S->buf + S->ts_off, S->ts_len, S->d_err, st);
+  return launch_stage(*S, 2, out, st);
 }
 
 int split_error(Heff& H) {

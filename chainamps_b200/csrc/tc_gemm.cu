@@ -16,6 +16,15 @@
 // TF32 planes into shared memory in the same swizzled layout, which halves
 // T's HBM traffic in both stages.
 //
+// The split-BF16 form (modes 3 and 4) keeps the same pipeline with BF16
+// operand planes re_hi, re_mid, im_hi, im_mid (hi = x rounded to BF16, mid =
+// x - hi rounded to BF16) and tcgen05.mma kind::f16 with BF16 inputs: 12
+// MMAs of 128 x N x 16 per 16-wide k-step, the same three products per real
+// product.  A 64-byte shared-memory row holds 32 BF16 K columns, so a stage
+// covers twice the K of the TF32 form for the same bytes, and each MMA runs
+// at twice the TF32 rate.  Stage 1 (mode 3) writes T split into four BF16
+// planes, so stage 2 (mode 4) reads it by TMA like any other operand.
+//
 // Persistent: one CTA per SM walks a list of 128 x N (N <= 128) output tiles
 // (tile i of CTA b is tiles[b + i * gridDim]; the host orders tiles by
 // decreasing work), each the K-concatenation of its task's terms.  Warp 0
@@ -31,20 +40,44 @@
 
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "tc_gemm.h"
 #include "tf32_round.cuh"
 
 namespace cmps {
 namespace tc {
 
-// warps 0 producer, 1 MMA, 2-5 epilogue; mode 2 adds warps 6-9, which load
-// the A tiles from global memory and split them into TF32 planes
+// Modes: 1 TF32, A by TMA, FP32 output (two planes); 2 TF32, A from two
+// FP32 planes through the converter warps, FP64 output; 3 BF16, A by TMA,
+// output split into four BF16 planes; 4 BF16, A by TMA, FP64 output.
+// Warps 0 producer, 1 MMA, 2-5 epilogue; mode 2 adds warps 6-9, which load
+// the A tiles from global memory and split them into TF32 planes.
+// epilogue warps per TMEM lane quadrant: mode 3 splits every accumulator
+// into four BF16 planes, so warps 6-9 join 2-5 (two per quadrant, taking
+// 16-column chunks in turn)
 template <int MODE>
-constexpr int threads_of() {
-  return MODE == 2 ? 320 : 192;
+__host__ __device__ constexpr int epi_per_quad() {
+  return MODE == 3 ? 2 : 1;
+}
+template <int MODE>
+__host__ __device__ constexpr int epilogue_warps() {
+  return 4 * epi_per_quad<MODE>();
+}
+template <int MODE>
+__host__ __device__ constexpr int threads_of() {
+  return MODE == 2 ? 320 : 32 * (2 + epilogue_warps<MODE>());
+}
+template <int MODE>
+__host__ __device__ constexpr bool bf16_mode() {
+  return MODE >= 3;
+}
+template <int MODE>
+__host__ __device__ constexpr bool tma_a() {
+  return MODE != 2;
 }
 constexpr int kStages = 3;
-constexpr int kBN = 128, kBK = 16;
+constexpr int kBN = 128, kBK = 16;  // TF32 k-step; a BF16 k-step is 2 kBK wide
 constexpr int kPlaneTileBytes = 128 * kBK * 4;          // 8 KB: 128 rows x 64 B
 constexpr int kOperandBytes = 4 * kPlaneTileBytes;      // 32 KB: four planes
 constexpr int kStageBytes = 2 * kOperandBytes;          // A + B
@@ -128,6 +161,42 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t a, uint64_t 
       " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
+// Instruction descriptor: kind::f16, D f32, A/B bf16, K-major, M = 128.
+__device__ __forceinline__ uint32_t idesc_bf16(int n, bool neg_a) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+template <int MODE>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  if (bf16_mode<MODE>())
+    umma_bf16(tmem_d, a, b, idesc, acc);
+  else
+    umma_tf32(tmem_d, a, b, idesc, acc);
+}
+
+// {bf16(hi_half), bf16(lo_half)} packed, round to nearest
+__device__ __forceinline__ uint32_t bf16x2(float hi_half, float lo_half) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi_half), "f"(lo_half));
+  return d;
+}
+
+// hi = x rounded to BF16, mid = x - hi rounded to BF16 (raw bits)
+__device__ __forceinline__ void bf16_split(float x, uint16_t* hi, uint16_t* mid) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const __nv_bfloat16 m = __float2bfloat16_rn(x - __bfloat162float(h));
+  *hi = __bfloat16_as_ushort(h);
+  *mid = __bfloat16_as_ushort(m);
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
@@ -168,7 +237,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+      mbar_init(&tempty[b], epilogue_warps<MODE>());  // one arrival per epilogue warp
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -192,9 +261,10 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         const TcTask task = tasks[tile.task];
         for (int t = task.t0; t < task.t1 && ok; ++t) {
           const TcTerm tm = terms[t];
-          if (MODE == 1) tensormap_acquire(amaps + tm.a_map);
+          if (tma_a<MODE>()) tensormap_acquire(amaps + tm.a_map);
           tensormap_acquire(bmaps + tm.b_map);
-          for (int k0 = 0; k0 < tm.k; k0 += kBK, ++it) {
+          constexpr int kStep = bf16_mode<MODE>() ? 2 * kBK : kBK;  // K columns per 64-byte row
+          for (int k0 = 0; k0 < tm.k; k0 += kStep, ++it) {
             const int s = it % kStages;
             const uint32_t ph = (uint32_t)((it / kStages) & 1);
             if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
@@ -206,8 +276,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
             // A: 128-row box (mode 1; written by the converter warps in mode 2);
             // B: the task's b_rows-row box; both four planes
             const uint32_t bbytes = 4u * 64u * (uint32_t)tile.b_rows;
-            mbar_expect_tx(&full[s], (MODE == 1 ? (uint32_t)kOperandBytes : 0u) + bbytes);
-            if (MODE == 1) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
+            mbar_expect_tx(&full[s], (tma_a<MODE>() ? (uint32_t)kOperandBytes : 0u) + bbytes);
+            if (tma_a<MODE>()) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
             tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
           }
         }
@@ -231,7 +301,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         const TcTile tile = nxt;
         if (ti + (int)gridDim.x < ntiles) nxt = tiles[ti + gridDim.x];  // in flight during this tile
         const int nmma = tile.nmma;  // multiple of 16 for M = 128
-        const uint32_t id_pos = idesc_tf32(nmma, false), id_neg = idesc_tf32(nmma, true);
+        const uint32_t id_pos = bf16_mode<MODE>() ? idesc_bf16(nmma, false) : idesc_tf32(nmma, false);
+        const uint32_t id_neg = bf16_mode<MODE>() ? idesc_bf16(nmma, true) : idesc_tf32(nmma, true);
         const int buf = tc & 1;
         const uint32_t use = (uint32_t)(tc >> 1);
         if (!mbar_wait(&tempty[buf], (use & 1u) ^ 1u, err, 4)) {
@@ -264,18 +335,19 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
               }
               const uint32_t acc = first ? 0u : 1u;
               first = false;
-              umma_tf32(d_re, A[0], B[0], id_pos, acc);
-              umma_tf32(d_re, A[0], B[1], id_pos, 1u);
-              umma_tf32(d_re, A[1], B[0], id_pos, 1u);
-              umma_tf32(d_re, A[2], B[2], id_neg, 1u);
-              umma_tf32(d_re, A[2], B[3], id_neg, 1u);
-              umma_tf32(d_re, A[3], B[2], id_neg, 1u);
-              umma_tf32(d_im, A[0], B[2], id_pos, acc);
-              umma_tf32(d_im, A[0], B[3], id_pos, 1u);
-              umma_tf32(d_im, A[1], B[2], id_pos, 1u);
-              umma_tf32(d_im, A[2], B[0], id_pos, 1u);
-              umma_tf32(d_im, A[2], B[1], id_pos, 1u);
-              umma_tf32(d_im, A[3], B[0], id_pos, 1u);
+              // planes 1 and 3 are lo (TF32) or mid (BF16)
+              umma<MODE>(d_re, A[0], B[0], id_pos, acc);
+              umma<MODE>(d_re, A[0], B[1], id_pos, 1u);
+              umma<MODE>(d_re, A[1], B[0], id_pos, 1u);
+              umma<MODE>(d_re, A[2], B[2], id_neg, 1u);
+              umma<MODE>(d_re, A[2], B[3], id_neg, 1u);
+              umma<MODE>(d_re, A[3], B[2], id_neg, 1u);
+              umma<MODE>(d_im, A[0], B[2], id_pos, acc);
+              umma<MODE>(d_im, A[0], B[3], id_pos, 1u);
+              umma<MODE>(d_im, A[1], B[2], id_pos, 1u);
+              umma<MODE>(d_im, A[2], B[0], id_pos, 1u);
+              umma<MODE>(d_im, A[2], B[1], id_pos, 1u);
+              umma<MODE>(d_im, A[3], B[0], id_pos, 1u);
             }
             umma_commit(&empty[s]);
           }
@@ -398,8 +470,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         ai[q] = bi[q];
       }
     }
-  } else if (warp >= 2 && warp < 6) {
-    // ---------------- epilogue: warps 2..5 ----------------
+  } else if ((warp >= 2 && warp < 6) || (MODE == 3 && warp >= 6)) {
+    // ---------------- epilogue: warps 2..5 (and 6..9 in mode 3) ----------------
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = quad * 32 + lane;
     int tc = 0;
@@ -429,7 +501,10 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
       const int gm = tile.m0 + row;
       const bool row_ok = gm < task.m;
       const uint32_t tbase = tmem + (uint32_t)(buf * 256) + ((uint32_t)(quad * 32) << 16);
-      for (int c = 0; c < nmma; c += 16) {
+      // mode 3: the warps of a quadrant take 16-column chunks in turn
+      const int c_first = 16 * ((warp - 2) / 4);
+      const int c_step = 16 * epi_per_quad<MODE>();
+      for (int c = c_first; c < nmma; c += c_step) {
         float vr[16], vi[16];
         if (have) {
           tmem_ld16(tbase + c, vr);
@@ -439,6 +514,38 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
           for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
         }
         if (!row_ok) continue;
+        if (MODE == 3) {
+          // Fast path: a chunk whose 16 columns lie in one segment (the
+          // usual case) stores from one base pointer; re and im are split
+          // together with packed conversions: h2 = {hi_im, hi_re}, m2 =
+          // {mid_im, mid_re}.
+          const int cnt = min(16, ntile - c);
+          const int colA = tile.n0 + c, colB = colA + cnt - 1;
+          const int qa = (colA >= task.seg_n0[1]) + (colA >= task.seg_n0[2]) + (colA >= task.seg_n0[3]);
+          const int qb = (colB >= task.seg_n0[1]) + (colB >= task.seg_n0[2]) + (colB >= task.seg_n0[3]);
+          if (cnt > 0 && qa == qb) {
+            int64_t so = task.seg_off[0];
+            int n0 = 0;
+            if (qa == 1) so = task.seg_off[1], n0 = task.seg_n0[1];
+            if (qa == 2) so = task.seg_off[2], n0 = task.seg_n0[2];
+            if (qa == 3) so = task.seg_off[3], n0 = task.seg_n0[3];
+            uint16_t* b0 = reinterpret_cast<uint16_t*>(out32) + so + (int64_t)gm * task.row_stride +
+                           (int64_t)(colA - n0) * task.col_stride;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              if (i >= cnt) break;
+              const uint32_t h2 = bf16x2(vi[i], vr[i]);
+              const float rh = __uint_as_float(h2 << 16), ih = __uint_as_float(h2 & 0xffff0000u);
+              const uint32_t m2 = bf16x2(vi[i] - ih, vr[i] - rh);
+              uint16_t* q = b0 + (int64_t)i * task.col_stride;
+              q[0] = (uint16_t)h2;
+              q[out32_plane] = (uint16_t)m2;
+              q[2 * out32_plane] = (uint16_t)(h2 >> 16);
+              q[3 * out32_plane] = (uint16_t)(m2 >> 16);
+            }
+            continue;
+          }
+        }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int j = c + i;
@@ -457,6 +564,11 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
             // stage-2 converter warps split it into TF32 hi / lo)
             out32[o] = vr[i];
             out32[o + out32_plane] = vi[i];
+          } else if (MODE == 3) {
+            // stage-1 output split into BF16 planes re_hi, re_mid, im_hi, im_mid
+            uint16_t* o16 = reinterpret_cast<uint16_t*>(out32);
+            bf16_split(vr[i], o16 + o, o16 + o + out32_plane);
+            bf16_split(vi[i], o16 + o + 2 * out32_plane, o16 + o + 3 * out32_plane);
           } else {
             out64[o] = (double)vr[i];
             out64[o + out64_plane] = (double)vi[i];
@@ -486,17 +598,21 @@ int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double*
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (int)p.tiles.size();
   const unsigned grid = (unsigned)std::min(ntiles, sms);
-  if (mode == 1) {
-    CMPS_TRY(ensure_smem_optin((const void*)tc_split_gemm<1>, kSmemBytes));
-    tc_split_gemm<1><<<grid, threads_of<1>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps,
-                                                                 p.d_bmaps, nullptr, nullptr, 0, out32, out32_plane,
-                                                                 out64, out64_plane, d_err);
-  } else {
+  if (mode == 1 || mode == 3 || mode == 4) {
+    if (!p.d_amaps) return fail(CMPS_ERR_STATE, "tcgen05: no A tensor maps");
+    auto kern = mode == 1 ? tc_split_gemm<1> : mode == 3 ? tc_split_gemm<3> : tc_split_gemm<4>;
+    CMPS_TRY(ensure_smem_optin((const void*)kern, kSmemBytes));
+    const int threads = mode == 3 ? threads_of<3>() : threads_of<1>();
+    kern<<<grid, threads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, nullptr,
+                                            nullptr, 0, out32, out32_plane, out64, out64_plane, d_err);
+  } else if (mode == 2) {
     if (!ain || !p.d_adescs) return fail(CMPS_ERR_STATE, "tcgen05 mode 2: no A operand");
     CMPS_TRY(ensure_smem_optin((const void*)tc_split_gemm<2>, kSmemBytes));
     tc_split_gemm<2><<<grid, threads_of<2>(), kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, nullptr,
                                                                  p.d_bmaps, p.d_adescs, ain, a_plane, out32,
                                                                  out32_plane, out64, out64_plane, d_err);
+  } else {
+    return fail(CMPS_ERR_ARG, "tcgen05: unknown mode");
   }
   CMPS_CUDA(cudaGetLastError());
   return CMPS_OK;

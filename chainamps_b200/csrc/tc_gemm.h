@@ -1,4 +1,4 @@
-// Split-TF32 tcgen05 grouped GEMM (internal).
+// Split-TF32 / split-BF16 tcgen05 grouped GEMM (internal).
 #pragma once
 
 #include <cuda.h>
@@ -38,7 +38,7 @@ struct TcADesc {
 };
 // b_rows: row count of the B boxes of this tile's task (its N rounded up to
 // 16, at most 128); the B tensor maps of that task are encoded with it.
-// kiters: 16-wide k-steps of the task's terms; nmma: the tile's N rounded up
+// kiters: k-steps (kstep() columns each) of the task's terms; nmma: the tile's N rounded up
 // to 16 (the MMA N) -- so the MMA warp needs no task or term lookups.
 struct TcTile {
   int32_t task, m0, n0, b_rows, kiters, nmma;
@@ -63,11 +63,17 @@ struct TcPlan {
 };
 
 int smem_bytes();
+// K columns of one k-step: a 64-byte shared-memory row of 16 TF32 or 32 BF16
+inline int32_t kstep(bool bf16) { return bf16 ? 32 : 16; }
 // mode 1: A and B by TMA (four TF32 planes each); FP32 output in two planes
 //         (re, im; plane stride out32_plane), the raw accumulator.
 // mode 2: A read from two FP32 planes (ain, plane stride a_plane; blocks
 //         described by p.adescs) and split to TF32 hi/lo in shared memory;
 //         B by TMA; FP64 planar output (re, im; plane stride out64_plane).
+// mode 3: A and B by TMA (four BF16 planes each: re_hi, re_mid, im_hi,
+//         im_mid); output split into four BF16 planes at out32 (read as
+//         16-bit elements; plane stride out32_plane elements).
+// mode 4: A and B by TMA (four BF16 planes each); FP64 planar output.
 int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double* out64, int64_t out64_plane,
            const float* ain, int64_t a_plane, int* d_err, cudaStream_t st);
 

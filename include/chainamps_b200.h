@@ -36,7 +36,11 @@ enum {
 
 enum {
   CMPS_FP64 = 0,           /* all contraction arithmetic in complex double */
-  CMPS_SPLIT_TF32 = 1      /* contractions as 3-term split TF32 on tcgen05, FP32 accumulate */
+  CMPS_SPLIT_TF32 = 1,     /* contractions as 3-term split TF32 on tcgen05, FP32 accumulate */
+  CMPS_SPLIT_BF16 = 2      /* contractions as 3-term split BF16 (hi + mid) on tcgen05, FP32
+                              accumulate: about twice the split-TF32 rate, operands held to
+                              16 significant bits (matvec error ~1e-5 relative); the mixed
+                              eigensolver refines with FP64 cycles as for split-TF32 */
 };
 
 /* Contraction order of the FP64 matvec.  Folded: the reference's
