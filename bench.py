@@ -7,26 +7,30 @@ complex double, bond dimension chi = 512.  One step = one H_eff matvec
 (``TwoVertexMPOMPSMultiply``, the operation the Arnoldi solver repeats) at
 the chi = 512 sector structure of that run: environments are seeded
 synthetic blocks with a Gaussian total-Sz sector profile, the MPO is the
-real one.  Inputs (~0.25 GB vector, ~5 GB intermediate) exceed L2, so no L2
+real one.  Inputs (~0.15 GB vector, ~3 GB intermediate) exceed L2, so no L2
 flush is needed between steps.
 
 * value: canonical algorithmic TFLOP/s of the device matvec with the vector
-  already resident in HBM (CUDA events, max over ranks);
+  already resident in HBM (CUDA events, max over ranks), for the faster of
+  the two split-precision forms (split-TF32, split-BF16; `headline_form`);
+  `split_forms` and `fp64_form` give every form;
 * e2e: the same through the C ABI with host buffers
   (``cmps_heff_apply``: H2D, matvec, D2H inside the timed region);
-* roofline: the grouped FP64 GEMM stages against a live cuBLAS complex128
-  GEMM measurement (the FP64 tensor-path ceiling for a library GEMM);
+* roofline: the two grouped GEMM stages' canonical flops over their CUDA-event
+  time against the measured dense bf16 peak (MEASURED_PEAKS.json), with the
+  DRAM traffic per matvec from the committed ncu summary;
 * idmrg: the iDMRG growth step itself on the same model (real MPO, real
   environments grown from the dummy blocks up to chi = 512; Arnoldi
   tolerance 1e-10): device time per step at full chi in FP64 and in mixed
-  precision (split-TF32 matvecs, FP64 Krylov/SVD/energies), the per-phase
-  profile, and the largest relative energy difference between the two runs;
+  precision (split-TF32 and split-BF16 matvecs, FP64 Krylov/SVD/energies),
+  the per-phase profile, and the largest relative energy difference between
+  the runs;
 * idmrg_coupled_ising: the same FP64-vs-mixed iDMRG step on the
   coupled transverse-field Ising chain config (each vertex a periodic
   12-site chain at g = 1.2 cut by exact diagonalisation to its 64 lowest
   states with Z2 parity, interchain J_perp = 0.05 sum_i X_i X_i, MPO D = 26)
-  at chi = 64, the largest bond dimension whose FP64 step fits the bench's
-  time budget (the config's chi = 2048 needs a 137 GB wavefunction);
+  at chi = 64 and 128 (the config's chi = 2048 needs a 137 GB wavefunction),
+  plus the FP64 step in the reference's folded contraction order at chi = 64;
 * cpu_baseline: the oracle's block-sparse numpy port of the same matvec on
   the host cores (one full matvec);
 * --impl reference: the CPU port timed as the reference arm.
@@ -34,10 +38,10 @@ flush is needed between steps.
 Multi-GPU (N > 1): one matvec per step split across the ranks by output
 charge sector (``chainamps_b200.sharded``): every rank holds the
 environments and the MPO, receives the input sectors its outputs read by one
-all-to-all and computes the output sectors it owns, balanced by their flops; `value` is the whole
-matvec's canonical TFLOP/s over the max-over-ranks step time ("strong"
-scaling: the work per step is the same for every N).  The iDMRG step
-figures run on every rank as replicas.
+all-to-all and computes the output sectors it owns, balanced by their flops;
+`value` is the whole matvec's canonical TFLOP/s over the max-over-ranks step
+time ("strong" scaling: the work per step is the same for every N).  The
+iDMRG step figures run on every rank as replicas.
 """
 import argparse
 import json
