@@ -644,8 +644,11 @@ class fDMRG(iDMRG):
     in device memory."""
 
     def __init__(self, ctx: Context, rules, W: MPXTensor, nvertices, target=None, precision=CMPS_FP64, tol=1e-10,
-                 max_restarts=50, krylov_dim=24):
-        super().__init__(ctx, rules, W, target, precision, tol, max_restarts, krylov_dim)
+                 max_restarts=50, krylov_dim=24, gradient=None):
+        """gradient: optional dW, as for iDMRG; the gradient is then carried
+        through the growth and every sweep step (derivative blocks kept
+        beside the blocks) and each row gets dE/dlambda."""
+        super().__init__(ctx, rules, W, target, precision, tol, max_restarts, krylov_dim, gradient=gradient)
         _check(lib.cmps_dmrg_keep_blocks(self.h, 1))
         self.nvertices = int(nvertices)
 
@@ -663,13 +666,15 @@ class fDMRG(iDMRG):
         ms = np.zeros(4, np.float64)
         _check(lib.cmps_dmrg_move(self.h, int(direction), chi, max_trunc, _p(row, C.c_double), C.byref(bd),
                                   C.byref(mv), _p(ms, C.c_double)))
-        self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
-                         chi=bd.value, matvecs=mv.value, ms=ms)
-        return self.last
+        return self._row(row, bd, mv, ms)
 
     def _row(self, row, bd, mv, ms):
         self.last = dict(energy=row[0], energy_per=row[1], entropy=row[2], truncation=row[3], fidelity=row[4],
                          chi=bd.value, matvecs=mv.value, ms=ms)
+        if self._grad:
+            g = C.c_double()
+            _check(lib.cmps_dmrg_gradient(self.h, C.byref(g)))
+            self.last["gradient"] = g.value
         return self.last
 
     def solve(self, chi=0, max_trunc=0.0):

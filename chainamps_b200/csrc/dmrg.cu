@@ -81,11 +81,39 @@ struct Dmrg {
   int restarts = 50, kdim = 24;
   int last_matvecs = 0;
   double last_ms[4] = {0, 0, 0, 0};  // env update + H_eff build + prediction, eigensolve, svd, total
-  // coupling gradient: dW and the derivative environments carried along
+  // coupling gradient: dW and the derivative environments of the current
+  // window carried along (no device data: zero, as for the dummy blocks);
+  // with kept blocks, the derivative blocks of every length beside them
   bool grad_on = false;
   std::vector<WEntry> dW;
   Env dL, dR;
   bool have_dlr = false;
+  std::map<int64_t, Env> dlblocks, drblocks;
+  const Env* dl_ptr() const { return dL.data.d ? &dL : nullptr; }
+  const Env* dr_ptr() const { return dR.data.d ? &dR : nullptr; }
+  // the current window's derivative environments from the kept ones
+  int load_derivatives(int64_t nl, int64_t nr, cudaStream_t st) {
+    dL.data.release();
+    dR.data.release();
+    dL = Env();
+    dR = Env();
+    auto il = dlblocks.find(nl);
+    auto ir = drblocks.find(nr);
+    if (il != dlblocks.end()) CMPS_TRY(copy_env(il->second, dL, st));
+    if (ir != drblocks.end()) CMPS_TRY(copy_env(ir->second, dR, st));
+    have_dlr = dL.data.d || dR.data.d;
+    return CMPS_OK;
+  }
+  // the derivative of MakeLeftBlock (right = false) or MakeRightBlock with
+  // this window's factors, stored beside the block of length k
+  int store_derivative(bool right, int64_t k, cudaStream_t st) {
+    Env nl, nr;
+    int rc = derivative_envs(*heff, *svd, dW, dl_ptr(), dr_ptr(), nl, nr);
+    if (rc == CMPS_OK) rc = store(right ? drblocks : dlblocks, k, right ? nr : nl, st);
+    nl.data.release();
+    nr.data.release();
+    return rc;
+  }
   double last_grad = std::nan("");
   static constexpr int kProfile = 21;
   double last_profile[kProfile] = {0};  // cmps_dmrg_profile layout
@@ -99,6 +127,8 @@ struct Dmrg {
     dR.data.release();
     for (auto& kv : lblocks) kv.second.data.release();
     for (auto& kv : rblocks) kv.second.data.release();
+    for (auto& kv : dlblocks) kv.second.data.release();
+    for (auto& kv : drblocks) kv.second.data.release();
   }
   // finite sweeps: the blocks of every length, kept when keep_blocks is set
   // before growth; key = number of vertices the block covers
@@ -411,7 +441,6 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   if (dir == 0 && !pstates.empty()) return fail(CMPS_ERR_STATE, "growth with projected states: the chain is finite");
   if (dir != 0) {
     if (!keep_blocks || !heff || !svd) return fail(CMPS_ERR_STATE, "finite sweep: grow with kept blocks first");
-    if (grad_on) return fail(CMPS_ERR_STATE, "the coupling gradient is carried through growth steps only");
     const int64_t nright = size - nleft - 2;
     if (dir == 1 && nright < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the right end");
     if (dir == -1 && nleft < 1) return fail(CMPS_ERR_STATE, "finite sweep: already at the left end");
@@ -435,6 +464,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   if (dir == 1) {
     // MakeLeftBlock with A = U of this window; the right block of the new
     // window was stored by the growth or the previous sweep
+    if (grad_on) CMPS_TRY(store_derivative(false, nleft + 1, st));
     Env nl;
     CMPS_TRY(left_update(*heff, *svd, nl));
     int rc = store(lblocks, nleft + 1, nl, st);
@@ -446,7 +476,9 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (ir == rblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: right block missing");
     CMPS_TRY(copy_env(lblocks[nleft], L, st));
     CMPS_TRY(copy_env(ir->second, R, st));
+    if (grad_on) CMPS_TRY(load_derivatives(nleft, size - nleft - 2, st));
   } else if (dir < 0) {
+    if (grad_on) CMPS_TRY(store_derivative(true, size - nleft - 1, st));
     Env nr;
     CMPS_TRY(right_update(*heff, *svd, nr));
     int rc = store(rblocks, size - nleft - 1, nr, st);
@@ -458,6 +490,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (il == lblocks.end()) return fail(CMPS_ERR_STATE, "finite sweep: left block missing");
     CMPS_TRY(copy_env(il->second, L, st));
     CMPS_TRY(copy_env(rblocks[size - nleft - 2], R, st));
+    if (grad_on) CMPS_TRY(load_derivatives(nleft, size - nleft - 2, st));
   } else if (dir == 2) {
     auto il = lblocks.find(nleft);
     auto ir = rblocks.find(size - nleft - 2);
@@ -472,7 +505,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (grad_on) {
       // derivative environments with the same truncation factors
       Env nl, nr;
-      int rc = derivative_envs(*heff, *svd, dW, have_dlr ? &dL : nullptr, have_dlr ? &dR : nullptr, nl, nr);
+      int rc = derivative_envs(*heff, *svd, dW, dl_ptr(), dr_ptr(), nl, nr);
       if (rc != CMPS_OK) {
         nl.data.release();
         nr.data.release();
@@ -490,6 +523,8 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
     if (keep_blocks) {
       CMPS_TRY(store(lblocks, nleft, L, st));
       CMPS_TRY(store(rblocks, nleft, R, st));
+      if (grad_on && dL.data.d) CMPS_TRY(store(dlblocks, nleft, dL, st));
+      if (grad_on && dR.data.d) CMPS_TRY(store(drblocks, nleft, dR, st));
       if (svd) lsvd[nleft] = rsvd[nleft] = svd;  // the previous window's U and V^dagger made them
     }
   }
@@ -538,7 +573,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   last_matvecs = nmv;
   last_grad = std::nan("");
   if (grad_on && rc == CMPS_OK)
-    CMPS_TRY(heff_adjoint(*heff, dW, have_dlr ? &dL : nullptr, have_dlr ? &dR : nullptr, &last_grad));
+    CMPS_TRY(heff_adjoint(*heff, dW, dl_ptr(), dr_ptr(), &last_grad));
   const auto h_eig = clock::now();
   cudaEventRecord(ev[2], st);
   svd = new_svd();
