@@ -17,6 +17,14 @@
 // sum_k RowX_k ColX_k (RowX_k = W[D-1, k], ColX_k = W[k, 0]) inside the cell
 // and the bond into the next cell against Lambda'^2.
 //
+// The dominant eigenpairs are found on charge blocks: the maps preserve the
+// charge difference of their two indices and start from the identity, so the
+// fixed points stay block diagonal in the bond's charge sectors.  Each map is
+// four grouped FP64 GEMM launches over the sector blocks of U and of
+// diag(s) V^dagger diag(1/lambda_prev), at O(sum of sector dim^3) instead of
+// O(chi^3) per application; the converged blocks are then placed in dense
+// chi0 x chi0 matrices for the rest of the measurement.
+//
 // Here the same numbers come from the fixed points directly, which the
 // regauging leaves invariant: <O> = Tr[T_O(l) r] / (eta Tr[l r]) for an
 // operator on one cell (T_O the left map with O inserted) and
@@ -35,6 +43,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <functional>
 #include <map>
 #include <vector>
 
@@ -65,6 +74,37 @@ __global__ void k_scatter_cell(const double* __restrict__ re, const double* __re
     const double f = (rscale ? rscale[r] : 1.0) * (cscale ? cscale[c] : 1.0);
     dst[sig * stride + rdst[r] + ld * cdst[c]] = make_cuDoubleComplex(re[e] * f, im[e] * f);
   }
+}
+
+// interleaved complex <-> two planes
+__global__ void k_deinterleave(const cplx* __restrict__ in, int64_t n, double* __restrict__ re,
+                               double* __restrict__ im) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    re[e] = in[e].x;
+    im[e] = in[e].y;
+  }
+}
+__global__ void k_interleave(const double* __restrict__ re, const double* __restrict__ im, int64_t n,
+                             cplx* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = make_cuDoubleComplex(re[e], im[e]);
+}
+// out[r, c] = rs[r] * in[r, c] * cs[c], one row-major block (planar)
+__global__ void k_scale_rc(const double* __restrict__ re, const double* __restrict__ im, int64_t rows, int64_t cols,
+                           const double* __restrict__ rs, const double* __restrict__ cs, double* __restrict__ ore,
+                           double* __restrict__ oim) {
+  const int64_t n = rows * cols;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const double f = rs[e / cols] * cs[e % cols];
+    ore[e] = re[e] * f;
+    oim[e] = im[e] * f;
+  }
+}
+// dense[dst[e]] = v[e]
+__global__ void k_scatter_index(const cplx* __restrict__ v, const int64_t* __restrict__ dst, int64_t n,
+                                cplx* __restrict__ dense) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    dense[dst[e]] = v[e];
 }
 
 // v <- Hermitian part of (phase * v), in place (n x n, column-major).
@@ -124,28 +164,241 @@ struct Blas {
 
 const cplx kOne = {1.0, 0.0}, kZero = {0.0, 0.0};
 
-// out = L(in) (left) or R(in) (right); w01: c0 x c1, w11: c1 x c1, w10: c1 x c0.
-void transfer(Blas& b, const Cell& c, bool left, const cplx* in, cplx* out, cplx* w01, cplx* w11, cplx* w10) {
-  const int64_t c0 = c.c0, c1 = c.c1;
-  if (left) {
-    for (int s = 0; s < c.d; ++s) {
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c0, kOne, in, c0, c.a0(s), c0, kZero, w01, c0);
-      b.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c1, c1, c0, kOne, c.a0(s), c0, w01, c0, s ? kOne : kZero, w11, c1);
+// The left and right transfer maps on block-diagonal fixed points.  A vector
+// is the concatenation of the row-major blocks l_s (dim s x dim s) over the
+// sectors s of the cell's end bond.  Left: X = l_s A0, W_m = sum A0^H X,
+// Y = W_m A1, l'_u = sum A1^H Y; right: Z = A1 r_u, V_m = sum Z A1^H,
+// P = A0 V_m, r'_s = sum P A0^H -- A0[s1] the rows of U's block m of state
+// s1 (sector s = m - q(s1)), A1[s2] the columns of the scaled V^dagger's
+// block m of state s2 (sector u = m + q(s2)).
+struct BlockMaps {
+  int64_t nb = 0;
+  std::vector<int64_t> boff, bdim;  // per bond sector
+  std::vector<int64_t> dense_of;    // vector entry -> column-major dense index
+  GemmPlan L1, L2, L3, L4, R1, R2, R3, R4;
+  Planar vin, vout, X, W, Y, Vs;
+  const Planar* U = nullptr;
+  void release() {
+    for (GemmPlan* p : {&L1, &L2, &L3, &L4, &R1, &R2, &R3, &R4}) p->release();
+    for (Planar* q : {&vin, &vout, &X, &W, &Y, &Vs}) q->release();
+  }
+};
+
+int build_block_maps(const SvdResult& S, const std::vector<double>& lam, const std::vector<double>& inv_prev,
+                     cudaStream_t st, BlockMaps& M) {
+  const ThetaSpace& th = S.th;
+  const Bond& A0 = S.a0;
+  const Bond& A2 = S.a2;
+  const int nm = (int)th.mq.size(), d = S.d, ns = A0.nsec();
+  const int64_t c0 = A0.size();
+  M.U = &S.U;
+  M.boff.assign(ns, 0);
+  M.bdim.assign(ns, 0);
+  M.dense_of.clear();
+  for (int s = 0; s < ns; ++s) {
+    M.boff[s] = M.nb;
+    M.bdim[s] = A0.sdim[s];
+    for (int64_t p = 0; p < A0.sdim[s]; ++p)
+      for (int64_t q = 0; q < A0.sdim[s]; ++q) M.dense_of.push_back(A0.selem[s][p] + c0 * A0.selem[s][q]);
+    M.nb += A0.sdim[s] * A0.sdim[s];
+  }
+  // a2 sector -> the a0 sector of the same charge (the cell's end bonds are identified)
+  auto a0_of_a2 = [&](int t) { return A0.find(A2.sq[t]); };
+  std::map<std::pair<int, int>, int64_t> xo, yo;  // (state, m) -> offset
+  std::vector<int64_t> wo(nm, -1);
+  int64_t xl = 0, wl = 0, yl = 0;
+  for (int m = 0; m < nm; ++m) {
+    const int64_t k = S.kept[m];
+    if (!k) continue;
+    wo[m] = wl;
+    wl += k * k;
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (th.rowoff[m][s1] < 0) continue;
+      const int sa = A0.find(S.rules.sub(th.mq[m], S.sigq[s1]));
+      if (sa < 0) return fail(CMPS_ERR_STATE, "unit cell: left tensor sector");
+      xo[{s1, m}] = xl;
+      xl += A0.sdim[sa] * k;
     }
-    for (int s = 0; s < c.d; ++s) {
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c1, kOne, w11, c1, c.a1(s), c1, kZero, w10, c1);
-      b.gemm(CUBLAS_OP_C, CUBLAS_OP_N, c0, c0, c1, kOne, c.a1(s), c1, w10, c1, s ? kOne : kZero, out, c0);
-    }
-  } else {
-    for (int s = 0; s < c.d; ++s) {
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c1, c0, c0, kOne, c.a1(s), c1, in, c0, kZero, w10, c1);
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c1, c1, c0, kOne, w10, c1, c.a1(s), c1, s ? kOne : kZero, w11, c1);
-    }
-    for (int s = 0; s < c.d; ++s) {
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_N, c0, c1, c1, kOne, c.a0(s), c0, w11, c1, kZero, w01, c0);
-      b.gemm(CUBLAS_OP_N, CUBLAS_OP_C, c0, c0, c1, kOne, w01, c0, c.a0(s), c0, s ? kOne : kZero, out, c0);
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      const int t = A2.find(S.rules.add(th.mq[m], S.sigq[s2]));
+      if (t < 0 || a0_of_a2(t) < 0 || A0.sdim[a0_of_a2(t)] != A2.sdim[t])
+        return fail(CMPS_ERR_STATE, "unit cell: end bonds differ");
+      yo[{s2, m}] = yl;
+      yl += k * A2.sdim[t];
     }
   }
+  CMPS_TRY(M.vin.alloc(std::max<int64_t>(1, M.nb)));
+  CMPS_TRY(M.vout.alloc(std::max<int64_t>(1, M.nb)));
+  CMPS_TRY(M.X.alloc(std::max<int64_t>(1, xl)));
+  CMPS_TRY(M.W.alloc(std::max<int64_t>(1, wl)));
+  CMPS_TRY(M.Y.alloc(std::max<int64_t>(1, yl)));
+  CMPS_TRY(M.Vs.alloc(std::max<int64_t>(1, S.Vd.len)));
+  // A1 = diag(s) V^dagger diag(1 / lambda_prev), block by block
+  for (int m = 0; m < nm; ++m) {
+    const int64_t k = S.kept[m], C = th.ncols[m];
+    if (!k) continue;
+    std::vector<double> rs(k), cs(C, 0.0);
+    for (int64_t j = 0; j < k; ++j) rs[j] = lam[S.gidx[m][j]];
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      const int t = A2.find(S.rules.add(th.mq[m], S.sigq[s2]));
+      for (int64_t p = 0; p < A2.sdim[t]; ++p) cs[th.coloff[m][s2] + p] = inv_prev[A2.selem[t][p]];
+    }
+    double *d_rs = nullptr, *d_cs = nullptr;
+    if (dmalloc(&d_rs, sizeof(double) * k) != cudaSuccess || dmalloc(&d_cs, sizeof(double) * C) != cudaSuccess) {
+      if (d_rs) dfree(d_rs);
+      return fail(CMPS_ERR_NOMEM, "unit cell: scale allocation failed");
+    }
+    int rc = copy_wait(d_rs, rs.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st);
+    if (rc == CMPS_OK) rc = copy_wait(d_cs, cs.data(), sizeof(double) * C, cudaMemcpyHostToDevice, st);
+    if (rc == CMPS_OK) {
+      k_scale_rc<<<grid_of(k * C), 256, 0, st>>>(S.Vd.re() + S.voff[m], S.Vd.im() + S.voff[m], k, C, d_rs, d_cs,
+                                                 M.Vs.re() + S.voff[m], M.Vs.im() + S.voff[m]);
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = fail(CMPS_ERR_CUDA, "unit cell: scaling failed");
+    }
+    dfree(d_rs);
+    dfree(d_cs);
+    CMPS_TRY(rc);
+  }
+  auto task = [](GemmPlan& p, int64_t c_off, int64_t m, int64_t n, int64_t ldc) {
+    GemmTask t{};
+    t.c_off = c_off;
+    t.m = (int32_t)m;
+    t.n = (int32_t)n;
+    t.ldc = (int32_t)ldc;
+    t.t0 = t.t1 = (int32_t)p.terms.size();
+    p.tasks.push_back(t);
+  };
+  auto term = [](GemmPlan& p, int64_t a_off, int64_t lda, int64_t b_off, int64_t ldb, int64_t k) {
+    GemmTerm tm{};
+    tm.a_off = a_off;
+    tm.lda = (int32_t)lda;
+    tm.b_off = b_off;
+    tm.ldb = (int32_t)ldb;
+    tm.k = (int32_t)k;
+    p.terms.push_back(tm);
+    p.tasks.back().t1 = (int32_t)p.terms.size();
+  };
+  // per (state, m): the A0 block (rows of state s1: dim sa x k, ld k) and
+  // the A1 block (columns of state s2: k x dim t, ld ncols)
+  for (int m = 0; m < nm; ++m) {
+    const int64_t k = S.kept[m], C = th.ncols[m];
+    if (!k) continue;
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (th.rowoff[m][s1] < 0) continue;
+      const int sa = A0.find(S.rules.sub(th.mq[m], S.sigq[s1]));
+      const int64_t ds = A0.sdim[sa], a0b = S.uoff[m] + th.rowoff[m][s1] * k, x = xo[{s1, m}];
+      task(M.L1, x, ds, k, k);                       // X = l_s A0
+      term(M.L1, M.boff[sa], ds, a0b, k, ds);
+      task(M.R3, x, ds, k, k);                       // P = A0 V_m
+      term(M.R3, a0b, k, wo[m], k, k);
+    }
+    task(M.L2, wo[m], k, k, k);                      // W_m = sum A0^H X
+    for (int s1 = 0; s1 < d; ++s1) {
+      if (th.rowoff[m][s1] < 0) continue;
+      const int sa = A0.find(S.rules.sub(th.mq[m], S.sigq[s1]));
+      term(M.L2, S.uoff[m] + th.rowoff[m][s1] * k, k, xo[{s1, m}], k, A0.sdim[sa]);
+    }
+    task(M.R2, wo[m], k, k, k);                      // V_m = sum Z A1^H
+    for (int s2 = 0; s2 < d; ++s2) {
+      if (th.coloff[m][s2] < 0) continue;
+      const int t = A2.find(S.rules.add(th.mq[m], S.sigq[s2]));
+      const int64_t du = A2.sdim[t], a1b = S.voff[m] + th.coloff[m][s2], y = yo[{s2, m}];
+      term(M.R2, y, du, a1b, C, du);
+      task(M.L3, y, k, du, du);                      // Y = W_m A1
+      term(M.L3, wo[m], k, a1b, C, k);
+      task(M.R1, y, k, du, du);                      // Z = A1 r_u
+      term(M.R1, a1b, C, M.boff[a0_of_a2(t)], du, du);
+    }
+  }
+  for (int sb = 0; sb < ns; ++sb) {
+    const int64_t db = A0.sdim[sb];
+    task(M.L4, M.boff[sb], db, db, db);              // l'_u = sum A1^H Y
+    task(M.R4, M.boff[sb], db, db, db);              // r'_s = sum P A0^H
+  }
+  // L4 / R4: one task per output sector, its terms from every (state, m) that reaches it
+  {
+    std::vector<std::vector<GemmTerm>> l4(ns), r4(ns);
+    for (int m = 0; m < nm; ++m) {
+      const int64_t k = S.kept[m], C = th.ncols[m];
+      if (!k) continue;
+      for (int s2 = 0; s2 < d; ++s2) {
+        if (th.coloff[m][s2] < 0) continue;
+        const int t = A2.find(S.rules.add(th.mq[m], S.sigq[s2]));
+        GemmTerm tm{};
+        tm.a_off = S.voff[m] + th.coloff[m][s2];
+        tm.lda = (int32_t)C;
+        tm.b_off = yo[{s2, m}];
+        tm.ldb = (int32_t)A2.sdim[t];
+        tm.k = (int32_t)k;
+        l4[a0_of_a2(t)].push_back(tm);
+      }
+      for (int s1 = 0; s1 < d; ++s1) {
+        if (th.rowoff[m][s1] < 0) continue;
+        const int sa = A0.find(S.rules.sub(th.mq[m], S.sigq[s1]));
+        GemmTerm tm{};
+        tm.a_off = xo[{s1, m}];
+        tm.lda = (int32_t)k;
+        tm.b_off = S.uoff[m] + th.rowoff[m][s1] * k;
+        tm.ldb = (int32_t)k;
+        tm.k = (int32_t)k;
+        r4[sa].push_back(tm);
+      }
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      GemmPlan& p = pass == 0 ? M.L4 : M.R4;
+      std::vector<std::vector<GemmTerm>>& lists = pass == 0 ? l4 : r4;
+      p.terms.clear();
+      for (int sb = 0; sb < ns; ++sb) {
+        p.tasks[sb].t0 = (int32_t)p.terms.size();
+        p.terms.insert(p.terms.end(), lists[sb].begin(), lists[sb].end());
+        p.tasks[sb].t1 = (int32_t)p.terms.size();
+      }
+    }
+  }
+  // every operand and output range inside its buffer, then upload
+  const int64_t ul = S.U.len, vl = M.Vs.len, nb = std::max<int64_t>(1, M.nb);
+  struct Check {
+    GemmPlan* p;
+    bool ah, bh;
+    int64_t a, b, c;
+    const char* what;
+  };
+  const Check checks[] = {{&M.L1, false, false, nb, ul, M.X.len, "unit cell L1"},
+                          {&M.L2, true, false, ul, M.X.len, M.W.len, "unit cell L2"},
+                          {&M.L3, false, false, M.W.len, vl, M.Y.len, "unit cell L3"},
+                          {&M.L4, true, false, vl, M.Y.len, nb, "unit cell L4"},
+                          {&M.R1, false, false, vl, nb, M.Y.len, "unit cell R1"},
+                          {&M.R2, false, true, M.Y.len, vl, M.W.len, "unit cell R2"},
+                          {&M.R3, false, false, ul, M.W.len, M.X.len, "unit cell R3"},
+                          {&M.R4, false, true, M.X.len, ul, nb, "unit cell R4"}};
+  for (const Check& c : checks) {
+    CMPS_TRY(c.p->validate(c.ah, c.bh, c.a, c.b, c.c, c.what));
+    CMPS_TRY(c.p->upload(st));
+  }
+  return CMPS_OK;
+}
+
+// out = L(in) or R(in) on block vectors (interleaved, nb entries)
+int apply_block_map(BlockMaps& M, bool left, const cplx* in, cplx* out, cudaStream_t st) {
+  const int64_t nb = M.nb;
+  k_deinterleave<<<grid_of(nb), 256, 0, st>>>(in, nb, M.vin.re(), M.vin.im());
+  CMPS_CUDA(cudaMemsetAsync(M.vout.d, 0, sizeof(double) * 2 * M.vout.len, st));
+  if (left) {
+    CMPS_TRY(launch_zgemm_fp64(M.L1, false, false, M.vin, *M.U, M.X, st));
+    CMPS_TRY(launch_zgemm_fp64(M.L2, true, false, *M.U, M.X, M.W, st));
+    CMPS_TRY(launch_zgemm_fp64(M.L3, false, false, M.W, M.Vs, M.Y, st));
+    CMPS_TRY(launch_zgemm_fp64(M.L4, true, false, M.Vs, M.Y, M.vout, st));
+  } else {
+    CMPS_TRY(launch_zgemm_fp64(M.R1, false, false, M.Vs, M.vin, M.Y, st));
+    CMPS_TRY(launch_zgemm_fp64(M.R2, false, true, M.Y, M.Vs, M.W, st));
+    CMPS_TRY(launch_zgemm_fp64(M.R3, false, false, *M.U, M.W, M.X, st));
+    CMPS_TRY(launch_zgemm_fp64(M.R4, false, true, M.X, *M.U, M.vout, st));
+  }
+  k_interleave<<<grid_of(nb), 256, 0, st>>>(M.vout.re(), M.vout.im(), nb, out);
+  CMPS_CUDA(cudaGetLastError());
+  return CMPS_OK;
 }
 
 // Dominant eigenpair of a small complex matrix H (k x k, column-major):
@@ -220,11 +473,11 @@ bool small_dominant(int k, const std::vector<zc>& H, zc* theta, std::vector<zc>&
   return std::isfinite(theta->real()) && std::isfinite(theta->imag());
 }
 
-// Dominant eigenpair of L or R by restarted Arnoldi; x (n = c0^2) holds the
-// start vector and receives the eigenvector.  V: (kdim + 1) x n workspace.
-int dominant(Blas& b, cudaStream_t st, const Cell& c, bool left, double tol, int kdim, int max_restarts, cplx* x,
-             cplx* V, cplx* hvec, cplx* w01, cplx* w11, cplx* w10, zc* eta) {
-  const int64_t n = c.c0 * c.c0;
+// Dominant eigenpair of a map (apply: out = map(in), n entries) by restarted
+// Arnoldi; x holds the start vector and receives the eigenvector.  V:
+// (kdim + 1) x n workspace.
+int dominant(Blas& b, cudaStream_t st, int64_t n, const std::function<int(const cplx*, cplx*)>& apply, double tol,
+             int kdim, int max_restarts, cplx* x, cplx* V, cplx* hvec, zc* eta) {
   kdim = std::max(2, std::min<int>(kdim, (int)std::min<int64_t>(n, 64)));
   zc theta = 0.0;
   bool converged = false;
@@ -241,7 +494,7 @@ int dominant(Blas& b, cudaStream_t st, const Cell& c, bool left, double tol, int
     for (int j = 0; j < kdim; ++j) {
       cplx* vj = V + (int64_t)j * n;
       cplx* w = V + (int64_t)(j + 1) * n;
-      transfer(b, c, left, vj, w, w01, w11, w10);
+      CMPS_TRY(apply(vj, w));
       if (b.st != CMPS_OK) return b.st;
       for (int pass = 0; pass < 2; ++pass) {
         const cplx mone = {-1.0, 0.0};
@@ -400,27 +653,49 @@ int unit_cell_measure(cmps_context* ctx, const SvdResult& S, const std::vector<d
     CMPS_CUDA(cudaGetLastError());
   }
 
-  // ---- dominant fixed points ----
+  // ---- dominant fixed points, on the charge blocks of the end bond ----
   const int64_t n = c0 * c0;
-  const int kd = std::max(2, std::min<int>(kdim, (int)std::min<int64_t>(n, 64)));
-  cplx *V, *hvec, *w01, *w11, *w10, *lft, *rgt;
-  CMPS_TRY(alloc(&V, sizeof(cplx) * (kd + 1) * n));
-  CMPS_TRY(alloc(&hvec, sizeof(cplx) * (kd + 1)));
+  cplx *w01, *w11, *w10, *lft, *rgt;
   CMPS_TRY(alloc(&w01, sizeof(cplx) * c0 * c1));
   CMPS_TRY(alloc(&w11, sizeof(cplx) * c1 * c1));
   CMPS_TRY(alloc(&w10, sizeof(cplx) * c1 * c0));
   CMPS_TRY(alloc(&lft, sizeof(cplx) * n));
   CMPS_TRY(alloc(&rgt, sizeof(cplx) * n));
+  BlockMaps bm;
+  struct BmFree {
+    BlockMaps& m;
+    ~BmFree() { m.release(); }
+  } bm_free{bm};
+  CMPS_TRY(build_block_maps(S, lam, inv_prev, st, bm));
+  const int64_t nb = bm.nb;
+  const int kd = std::max(2, std::min<int>(kdim, (int)std::min<int64_t>(nb, 64)));
+  cplx *V, *hvec, *xl, *xr;
+  int64_t* d_dense;
+  CMPS_TRY(alloc(&V, sizeof(cplx) * (kd + 1) * nb));
+  CMPS_TRY(alloc(&hvec, sizeof(cplx) * (kd + 1)));
+  CMPS_TRY(alloc(&xl, sizeof(cplx) * nb));
+  CMPS_TRY(alloc(&xr, sizeof(cplx) * nb));
+  CMPS_TRY(alloc(&d_dense, sizeof(int64_t) * nb));
+  CMPS_TRY(copy_wait(d_dense, bm.dense_of.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, st));
   {
-    // start: the identity (the fixed point of a canonical cell)
-    std::vector<cplx> id((size_t)n, kZero);
-    for (int64_t i = 0; i < c0; ++i) id[i + c0 * i] = kOne;
-    CMPS_TRY(copy_wait(lft, id.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
-    CMPS_TRY(copy_wait(rgt, id.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
+    // start: the identity (the fixed point of a canonical cell), block by block
+    std::vector<cplx> id((size_t)nb, kZero);
+    for (size_t s = 0; s < bm.boff.size(); ++s)
+      for (int64_t i = 0; i < bm.bdim[s]; ++i) id[bm.boff[s] + i * bm.bdim[s] + i] = kOne;
+    CMPS_TRY(copy_wait(xl, id.data(), sizeof(cplx) * nb, cudaMemcpyHostToDevice, st));
+    CMPS_TRY(copy_wait(xr, id.data(), sizeof(cplx) * nb, cudaMemcpyHostToDevice, st));
   }
   zc eta_l = 0.0, eta_r = 0.0;
-  CMPS_TRY(dominant(bl, st, c, true, tol, kd, 200, lft, V, hvec, w01, w11, w10, &eta_l));
-  CMPS_TRY(dominant(bl, st, c, false, tol, kd, 200, rgt, V, hvec, w01, w11, w10, &eta_r));
+  CMPS_TRY(dominant(bl, st, nb, [&](const cplx* in, cplx* out) { return apply_block_map(bm, true, in, out, st); },
+                    tol, kd, 200, xl, V, hvec, &eta_l));
+  CMPS_TRY(dominant(bl, st, nb, [&](const cplx* in, cplx* out) { return apply_block_map(bm, false, in, out, st); },
+                    tol, kd, 200, xr, V, hvec, &eta_r));
+  // the block-diagonal fixed points as dense chi0 x chi0 (column-major [bra, ket] / [ket, bra])
+  CMPS_CUDA(cudaMemsetAsync(lft, 0, sizeof(cplx) * n, st));
+  CMPS_CUDA(cudaMemsetAsync(rgt, 0, sizeof(cplx) * n, st));
+  k_scatter_index<<<grid_of(nb), 256, 0, st>>>(xl, d_dense, nb, lft);
+  k_scatter_index<<<grid_of(nb), 256, 0, st>>>(xr, d_dense, nb, rgt);
+  CMPS_CUDA(cudaGetLastError());
   for (zc e : {eta_l, eta_r})
     if (std::abs(e.imag()) >= 1e-10 * std::abs(e.real()) || !(e.real() > 0.0))
       return fail(CMPS_ERR_SOLVER, "unit cell: dominant transfer-matrix eigenvalue is not real and positive");
