@@ -133,6 +133,9 @@ _SIGS = {
     "cmps_heff_sector_table": (C.c_int, [C.c_void_p, c_i64p, c_i64p, c_dblp]),
     "cmps_heff_set_owned": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
     "cmps_heff_input_sectors": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8)]),
+    "cmps_heff_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), c_dblp, c_dblp]),
+    "cmps_dmrg_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "cmps_dmrg_autotune_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), c_dblp, c_dblp]),
     "cmps_heff_set_windows": (C.c_int, [C.c_void_p, c_i64p, C.c_int64, c_i64p, C.c_int64]),
     "cmps_heff_apply_theta_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cmps_heff_theta_from_arpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -286,6 +289,14 @@ class TwoVertexComponents:
         """Compute only the output sectors with owned[m] true (sharded matvec)."""
         mask = np.ascontiguousarray(np.asarray(owned, bool).astype(np.uint8))
         _check(lib.cmps_heff_set_owned(self.h, _p(mask, C.c_uint8)))
+
+    def autotune(self):
+        """Measured tile shapes of the matvec's grouped GEMM plans; returns
+        dict(tuned, cached, ms_heuristic, ms_best) (cmps_heff_autotune)."""
+        t, c = C.c_int(), C.c_int()
+        a, b = C.c_double(), C.c_double()
+        _check(lib.cmps_heff_autotune(self.h, C.byref(t), C.byref(c), C.byref(a), C.byref(b)))
+        return dict(tuned=t.value, cached=c.value, ms_heuristic=a.value, ms_best=b.value)
 
     def input_sectors(self):
         """Mask of the input sectors the owned output sectors read."""
@@ -539,10 +550,11 @@ class iDMRG:
     DMRG_routines.cpp:346-374; iDMRG::run, iDMRG_routines.cpp:19-33)."""
 
     def __init__(self, ctx: Context, rules, W: MPXTensor, target=None, precision=CMPS_FP64, tol=1e-10,
-                 max_restarts=50, krylov_dim=24, gradient=None, order=CMPS_ORDER_AUTO):
+                 max_restarts=50, krylov_dim=24, gradient=None, order=CMPS_ORDER_AUTO, autotune=False):
         """gradient: optional dW (MPXTensor, the MPO's derivative with respect
         to one coupling); each grow() then also returns dE/dlambda.  order:
-        contraction order of each step's H_eff (CMPS_ORDER_*)."""
+        contraction order of each step's H_eff (CMPS_ORDER_*).  autotune:
+        measured tile shapes for each step's grouped GEMM plans."""
         self.ctx = ctx
         cr, self._r = _rules(rules)
         dw, kw = W._desc()
@@ -555,6 +567,8 @@ class iDMRG:
         self.h = h
         _check(lib.cmps_dmrg_set_solver(h, tol, max_restarts, krylov_dim))
         _check(lib.cmps_dmrg_set_order(h, order))
+        if autotune:
+            _check(lib.cmps_dmrg_set_autotune(h, 1))
         self._grad = gradient is not None
         if self._grad:
             gd, gk = gradient._desc()
@@ -577,6 +591,12 @@ class iDMRG:
             _check(lib.cmps_dmrg_gradient(self.h, C.byref(g)))
             self.last["gradient"] = g.value
         return self.last
+
+    def autotune_stats(self):
+        t, c = C.c_int(), C.c_int()
+        a, b = C.c_double(), C.c_double()
+        _check(lib.cmps_dmrg_autotune_stats(self.h, C.byref(t), C.byref(c), C.byref(a), C.byref(b)))
+        return dict(tuned=t.value, cached=c.value, ms_heuristic=a.value, ms_best=b.value)
 
     def profile(self):
         """Breakdown of the last step: device times (CUDA events) of the

@@ -489,6 +489,35 @@ int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStr
   return CMPS_OK;
 }
 
+// The four canonical plans' tile shapes, measured (autotune_plan): on the FP32
+// operands when the handle runs the FP32 form, else on the FP64 ones.  The
+// input is the handle's zeroed work vector, the output its other one.
+int autotune_canonical(Heff& H, bool fp32, cudaStream_t st, TuneStats* stats) {
+  Canon* C = H.canon;
+  if (!C) return CMPS_OK;
+  Planar in, out;
+  in.d = H.x.d;
+  in.len = H.in_len;
+  out.d = H.y.d;
+  out.len = H.out_len;
+  int rc = CMPS_OK;
+  if (fp32) {
+    if (!C->have32) rc = fail(CMPS_ERR_STATE, "canonical-order FP32 operands not prepared");
+    if (rc == CMPS_OK) rc = to_fp32(in.re(), in.im(), H.in_len, C->x32, st);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sL, 20, [&] { return launch_cgemm_fp32(C->sL, C->L32, C->x32, C->xz32, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sW1, 21, [&] { return launch_cgemm_fp32(C->sW1, C->ops32, C->xz32, C->y32, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sW2, 22, [&] { return launch_cgemm_fp32(C->sW2, C->ops32, C->y32, C->xz32, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sR, 23, [&] { return launch_cgemm_fp32(C->sR, C->xz32, C->R32, C->o32, st); }, st, stats);
+  } else {
+    rc = autotune_plan(C->sL, 10, [&] { return launch_zgemm_fp64(C->sL, false, false, H.L.data, in, C->xz, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sW1, 11, [&] { return launch_zgemm_fp64(C->sW1, false, false, C->ops, C->xz, C->y, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sW2, 12, [&] { return launch_zgemm_fp64(C->sW2, false, false, C->ops, C->y, C->xz, st); }, st, stats);
+    if (rc == CMPS_OK) rc = autotune_plan(C->sR, 13, [&] { return launch_zgemm_fp64(C->sR, false, false, C->xz, H.R.data, out, st); }, st, stats);
+  }
+  in.d = out.d = nullptr;
+  return rc;
+}
+
 // which: 1 = stages L and W1, 2 = stages W2 and R, 0 = all four.
 int apply_canonical(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st) {
   Canon* C = H.canon;

@@ -274,6 +274,18 @@ int cmps_heff_set_owned(cmps_heff* h, const uint8_t* owned) {
   return h->impl->set_owned(owned);
 }
 
+int cmps_heff_autotune(cmps_heff* h, int* tuned, int* cached, double* ms_heuristic, double* ms_best) {
+  if (!h || !h->impl) return fail(CMPS_ERR_ARG, "null handle");
+  CMPS_TRY(use_device(h->impl->ctx));
+  TuneStats s;
+  CMPS_TRY(h->impl->autotune(&s));
+  if (tuned) *tuned = s.tuned;
+  if (cached) *cached = s.cached;
+  if (ms_heuristic) *ms_heuristic = s.ms_heuristic;
+  if (ms_best) *ms_best = s.ms_best;
+  return CMPS_OK;
+}
+
 int cmps_heff_input_sectors(const cmps_heff* h, uint8_t* needed) {
   if (!h || !h->impl || !needed) return fail(CMPS_ERR_ARG, "null argument");
   const Heff& H = *h->impl;

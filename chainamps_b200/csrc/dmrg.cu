@@ -135,6 +135,8 @@ struct Dmrg {
   bool keep_blocks = false;
   bool want_fidelity = true;  // CheckConvergence on growth steps
   int order_req = CMPS_ORDER_AUTO;  // contraction order of each step's H_eff
+  bool autotune = false;            // measured tile shapes for each step's grouped GEMM plans
+  TuneStats tune;                   // accumulated over the run
   std::map<int64_t, Env> lblocks, rblocks;
   // the factors each kept block was built with: lsvd[k]'s U made lblocks[k]
   // (the left MPS tensor of vertex k), rsvd[k]'s V^dagger made rblocks[k]
@@ -543,6 +545,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   const auto h_fin = clock::now();
   CMPS_TRY(prepare_precision(next.get(), precision));
   next->precision = precision;
+  if (autotune) CMPS_TRY(next->autotune(&tune));
   const auto h_split = clock::now();
   bool have_guess = false;
   if (!pstates.empty())  // no prediction on excited-state steps (fDMRG_routines.cpp:118-121)
@@ -742,6 +745,22 @@ int cmps_dmrg_set_order(cmps_dmrg* d, int order) {
   if (order != CMPS_ORDER_AUTO && order != CMPS_ORDER_FOLDED && order != CMPS_ORDER_CANONICAL)
     return fail(CMPS_ERR_ARG, "unknown contraction order");
   d->impl->order_req = order;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_set_autotune(cmps_dmrg* d, int on) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  d->impl->autotune = on != 0;
+  return CMPS_OK;
+}
+
+int cmps_dmrg_autotune_stats(const cmps_dmrg* d, int* tuned, int* cached, double* ms_heuristic, double* ms_best) {
+  if (!d || !d->impl) return fail(CMPS_ERR_ARG, "null handle");
+  const TuneStats& s = d->impl->tune;
+  if (tuned) *tuned = s.tuned;
+  if (cached) *cached = s.cached;
+  if (ms_heuristic) *ms_heuristic = s.ms_heuristic;
+  if (ms_best) *ms_best = s.ms_best;
   return CMPS_OK;
 }
 

@@ -916,6 +916,25 @@ int Heff::build_plans() {
   return CMPS_OK;
 }
 
+int Heff::autotune(TuneStats* stats) {
+  cudaStream_t st = ctx->stream;
+  if (is_split(precision) && !low_canonical) return CMPS_OK;
+  CMPS_TRY(zero_wait(x.d, sizeof(double) * 2 * x.len, st));
+  if (low_canonical) return autotune_canonical(*this, true, st, stats);
+  if (order == CMPS_ORDER_CANONICAL) return autotune_canonical(*this, false, st, stats);
+  CMPS_TRY(ensure_T());
+  Planar in, out;
+  in.d = x.d;
+  in.len = in_len;
+  out.d = y.d;
+  out.len = out_len;
+  int rc = autotune_plan(stage1, 1, [&] { return launch_zgemm_fp64(stage1, false, false, LP, in, T, st); }, st, stats);
+  if (rc == CMPS_OK)
+    rc = autotune_plan(stage2, 2, [&] { return launch_zgemm_fp64(stage2, false, false, T, RP, out, st); }, st, stats);
+  in.d = out.d = nullptr;
+  return rc;
+}
+
 void Heff::default_windows() {
   in_base = th.base;
   out_base = th.base;

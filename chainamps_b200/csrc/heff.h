@@ -144,6 +144,9 @@ struct Heff {
   int proj_np = 0;
   double* d_proj = nullptr;  // weights [np], coefficients [2 np + 4]
   std::vector<double> proj_w;
+  // Measured tile shapes of the grouped GEMM plans the handle's matvec runs
+  // (autotune_plan); the tcgen05 split stages have fixed tiles.
+  int autotune(TuneStats* stats);
   int set_projectors(int np, const double* host_arpack, const double* weights);
   // the same from device vectors phi_p = conj(P_p), ARPACK order, interleaved
   int set_projectors_device(int np, const double* d_phi_arpack, const double* weights);
@@ -236,6 +239,8 @@ int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, 
 // The canonical contraction order (canonical.cu).
 // need (optional): the theta sectors the canonical order's first stage reads
 int canonical_flops(const Heff& H, double* flops, std::vector<uint8_t>* need = nullptr);
+// measured tile shapes of the canonical plans (FP32 or FP64 launches)
+int autotune_canonical(Heff& H, bool fp32, cudaStream_t st, TuneStats* stats);
 int build_canonical(Heff& H);
 void release_canonical(Heff* h);
 // which: 1 = stages L and W1, 2 = stages W2 and R, 0 = all four

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <array>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -170,11 +171,24 @@ struct GemmPlan {
   // Picks the tile shape for these tasks, splits them into tiles and copies
   // the plan to the device.
   int upload(cudaStream_t st);
+  // The tiles again for another shape (an uploaded plan; tasks and terms unchanged).
+  int retile(int shape, cudaStream_t st);
   // Host check, before any launch, that every operand and output range lies
   // inside its buffer (lengths in complex elements).
   int validate(bool a_h, bool b_h, int64_t a_len, int64_t b_len, int64_t c_len, const char* what) const;
   void release();
 };
+
+// Empirical tile-shape choice: `run` launches the plan once; every shape is
+// timed (one warm-up, three timed launches, CUDA events on st) and the
+// fastest kept.  Results are cached per process by plan signature (role,
+// task and term counts, flops, padded-work choice), so a plan of the same
+// population is not timed again.
+struct TuneStats {
+  int tuned = 0, cached = 0;
+  double ms_heuristic = 0.0, ms_best = 0.0;  // per launch, summed over the tuned plans
+};
+int autotune_plan(GemmPlan& p, int role, const std::function<int()>& run, cudaStream_t st, TuneStats* stats);
 
 // Block AXPY lists: dst block = sum_t w_t * src_t (same shapes).
 struct AxpyBlock {

@@ -16,7 +16,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <map>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -282,6 +290,97 @@ static int pick_shape(const GemmPlan& p) {
     }
   }
   return shape;
+}
+
+int GemmPlan::retile(int s, cudaStream_t st) {
+  if (s < 0 || s > 2) return fail(CMPS_ERR_ARG, "GEMM plan: unknown tile shape");
+  if (!d_tasks && !tasks.empty()) return fail(CMPS_ERR_STATE, "GEMM plan not uploaded");
+  const int bm = kShapes[s][0], bn = kShapes[s][1];
+  std::vector<GemmTile> nt;
+  for (size_t i = 0; i < tasks.size(); ++i) {
+    const GemmTask& t = tasks[i];
+    for (int m0 = 0; m0 < t.m; m0 += bm)
+      for (int n0 = 0; n0 < t.n; n0 += bn) nt.push_back(GemmTile{(int32_t)i, m0, n0, 0});
+  }
+  GemmTile* d = nullptr;
+  if (!nt.empty()) {
+    CMPS_CUDA(dmalloc((void**)&d, nt.size() * sizeof(GemmTile)));
+    const int rc = copy_wait(d, nt.data(), nt.size() * sizeof(GemmTile), cudaMemcpyHostToDevice, st);
+    if (rc != CMPS_OK) {
+      dfree(d);
+      return rc;
+    }
+  }
+  if (d_tiles) dfree(d_tiles);
+  d_tiles = d;
+  tiles.swap(nt);
+  shape = s;
+  return CMPS_OK;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::vector<int64_t>, int> g_tune_cache;  // plan signature -> measured best shape
+}  // namespace
+
+int autotune_plan(GemmPlan& p, int role, const std::function<int()>& run, cudaStream_t st, TuneStats* stats) {
+  if (p.tasks.empty()) return CMPS_OK;
+  // signature: the role, the task and term counts, the flops to 3 digits and
+  // the padded-work choice -- plans of the same shape population share it
+  double fl = 0.0;
+  for (const GemmTask& t : p.tasks)
+    for (int q = t.t0; q < t.t1; ++q) fl += 8.0 * t.m * (double)t.n * p.terms[q].k;
+  const int64_t fq = fl > 0.0 ? (int64_t)std::llround(std::log10(fl) * 300.0) : 0;
+  const std::vector<int64_t> sig{role, (int64_t)p.tasks.size(), (int64_t)p.terms.size(), fq, p.shape};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(sig);
+    if (it != g_tune_cache.end()) {
+      if (stats) ++stats->cached;
+      return it->second == p.shape ? CMPS_OK : p.retile(it->second, st);
+    }
+  }
+  const int heuristic = p.shape;
+  float best = 0.0f, heur = 0.0f;
+  int pick = heuristic;
+  cudaEvent_t e0, e1;
+  CMPS_CUDA(cudaEventCreate(&e0));
+  CMPS_CUDA(cudaEventCreate(&e1));
+  int rc = CMPS_OK;
+  for (int s = 0; s < 3 && rc == CMPS_OK; ++s) {
+    rc = p.retile(s, st);
+    if (rc == CMPS_OK) rc = run();  // warm-up
+    if (rc != CMPS_OK) break;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3 && rc == CMPS_OK; ++r) rc = run();
+    cudaEventRecord(e1, st);
+    if (rc != CMPS_OK || cudaEventSynchronize(e1) != cudaSuccess) {
+      if (rc == CMPS_OK) rc = fail(CMPS_ERR_CUDA, "autotune: timing failed");
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (s == heuristic) heur = ms;
+    if (s == 0 || ms < best) {
+      best = ms;
+      pick = s;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CMPS_TRY(rc);
+  CMPS_TRY(p.retile(pick, st));
+  if (std::getenv("CMPS_TUNE_TRACE"))
+    std::fprintf(stderr, "autotune role %d: tasks %zu, heuristic shape %d %.3f ms, best shape %d %.3f ms\n", role,
+                 p.tasks.size(), heuristic, heur / 3, pick, best / 3);
+  if (stats) {
+    ++stats->tuned;
+    stats->ms_heuristic += heur / 3;
+    stats->ms_best += best / 3;
+  }
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_cache[sig] = pick;
+  return CMPS_OK;
 }
 
 int GemmPlan::upload(cudaStream_t st) {

@@ -136,6 +136,15 @@ int cmps_heff_apply_device(cmps_heff* h, const double* d_in, double* d_out, void
  * over non-zero MPO entries (8 per complex MAC); executed = what the grouped
  * GEMM launches of the handle's precision and contraction order issue. */
 int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed);
+/* Measured tile shapes (no counterpart in the reference): every grouped GEMM
+ * plan the handle's matvec runs (folded or canonical, FP64 or the FP32
+ * canonical form; the tcgen05 split stages have fixed tiles) is launched
+ * with each output tile shape -- 64x64, 32x128, 128x32 -- and keeps the
+ * fastest.  Choices are cached per process by plan signature; `cached`
+ * counts the plans that took a cached choice.  ms_heuristic / ms_best: the
+ * summed per-launch times of the tuned plans with the padded-work choice and
+ * with the measured one.  Outputs may be NULL. */
+int cmps_heff_autotune(cmps_heff* h, int* tuned, int* cached, double* ms_heuristic, double* ms_best);
 /* Chooses the contraction order of the FP64 matvec (CMPS_ORDER_*); no
  * counterpart in the reference, whose only order is the folded one. */
 int cmps_heff_set_order(cmps_heff* h, int order);
@@ -360,6 +369,10 @@ int cmps_dmrg_set_fidelity(cmps_dmrg* d, int on);
 /* Contraction order of every later step's H_eff (CMPS_ORDER_*, default
  * AUTO; see cmps_heff_set_order).  No counterpart in the reference. */
 int cmps_dmrg_set_order(cmps_dmrg* d, int order);
+/* Autotune (cmps_heff_autotune) every later step's H_eff; the stats are
+ * summed over the run. */
+int cmps_dmrg_set_autotune(cmps_dmrg* d, int on);
+int cmps_dmrg_autotune_stats(const cmps_dmrg* d, int* tuned, int* cached, double* ms_heuristic, double* ms_best);
 int cmps_dmrg_move(cmps_dmrg* d, int direction, int64_t chi, double max_trunc, double* row5,
                    int64_t* bond_dim, int* matvecs, double* ms4);
 int cmps_dmrg_position(const cmps_dmrg* d, int64_t* nleft, int64_t* size);
