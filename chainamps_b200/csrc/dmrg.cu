@@ -553,6 +553,10 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   else if (dir == 0) CMPS_TRY(predict(*next, &have_guess));
   else if (dir != 2) CMPS_TRY(finite_predict(*next, dir, &have_guess));
   const auto h_pred = clock::now();
+  // the previous step's kept count per charge sizes this step's randomized SVD ranges
+  std::map<QKey, int64_t> kept_hint;
+  if (svd)
+    for (size_t m = 0; m < svd->th.mq.size(); ++m) kept_hint[svd->th.mq[m]] = svd->kept[m];
   // the previous step's factors are released here unless a kept block needs them
   svd.reset();
   heff = std::move(next);
@@ -584,7 +588,7 @@ int Dmrg::step(int dir, int64_t chi, double trunc, double* out) {
   // as move_{right,left}_two_vertex do
   const int64_t nright_now = (dir == 0 ? size + 2 : size) - nleft - 2;
   const double cut = (dir == 1 && nright_now <= 1) || (dir == -1 && nleft <= 1) ? -0.0 : trunc;
-  CMPS_TRY(theta_svd(*heff, chi, cut, *svd));
+  CMPS_TRY(theta_svd(*heff, chi, cut, *svd, kept_hint.empty() ? nullptr : &kept_hint));
   // SquareRescale(1.0) (MPS_matrix.hpp:66-70)
   std::vector<double> v = svd->values;
   double sq = 0.0;

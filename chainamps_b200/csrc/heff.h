@@ -219,7 +219,10 @@ struct SvdResult {
   int routes[3] = {0, 0, 0};  // sectors factored exactly, by the Gram matrix, by the randomized route
 };
 
-int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out);
+// kept_hint (optional): per middle charge, the values a previous
+// factorisation kept; it sizes the randomized route's range.
+int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out,
+              const std::map<QKey, int64_t>* kept_hint = nullptr);
 // adjoint.cu: derivative of the contraction with respect to a vertex coupling
 int parse_derivative_mpo(const Heff& H, const cmps_mpx_desc* dW, std::vector<WEntry>& out);
 // W gains a zero-weight entry at every position where dW is non-zero and W

@@ -22,6 +22,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -375,7 +376,7 @@ static int64_t truncation_length(const std::vector<double>& sv, int64_t D, doubl
   return length;
 }
 
-int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
+int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std::map<QKey, int64_t>* kept_hint) {
   if (!H.have_theta) return fail(CMPS_ERR_STATE, "no wavefunction: call cmps_heff_eigs or cmps_heff_set_theta first");
   cudaStream_t st = H.ctx->stream;
   cusolverDnHandle_t sol;
@@ -396,6 +397,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     // tail = |A - Q Q^H A|_F^2 (the weight outside the range found),
     // resid[j] = |A v_j - s_j u_j| (or its transpose form)
     bool rnd = false;
+    bool red_exact = false;  // the reduced b x b problem by QR + Jacobi SVD (else Hermitian eigensolver)
     double tail = 0.0;
     std::vector<double> resid;
     int64_t bb = 0;  // triplets the randomized route computed
@@ -519,9 +521,17 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     // weight outside the range found.
     const int64_t kRandPad = 32;
     const int kRandIters = 2;
-    auto rand_b = [&](int64_t mn) -> int64_t {
+    // With a hint -- the values the sector of the same charge kept at the
+    // previous step -- the range is 2.5 times that plus 64 (at least 64),
+    // not the whole chi + kRandPad: the tail check (3) widens it where the
+    // spectrum needs more.
+    auto rand_b = [&](int m, int64_t mn) -> int64_t {
       if (chi <= 0 || mn < kEigMin) return 0;
-      const int64_t bb = std::min<int64_t>(mn, chi + kRandPad);
+      int64_t bb = std::min<int64_t>(mn, chi + kRandPad);
+      if (kept_hint) {
+        auto it = kept_hint->find(th.mq[m]);
+        if (it != kept_hint->end()) bb = std::min<int64_t>(bb, std::max<int64_t>(64, 5 * it->second / 2 + 64));
+      }
       return 4 * bb <= 3 * mn ? bb : 0;
     };
     auto rand_scratch = [&](int64_t nr, int64_t nc, int64_t bb) -> size_t {
@@ -530,15 +540,17 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
     };
     auto rand_lwork = [&](cusolverDnHandle_t sol, gesvdjInfo_t prm, int64_t ll, int64_t bb, int* lw) -> int {
       const int b32 = (int)bb, l32 = (int)ll;
-      int a = 0, q = 0, u = 0, g = 0;
+      int a = 0, q = 0, u = 0, g = 0, e = 0;
       cuDoubleComplex* any = (cuDoubleComplex*)dA;
-      if (cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
+      if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, b32, any, b32, dS, &e) !=
+              CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZgeqrf_bufferSize(sol, l32, b32, any, l32, &q) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZungqr_bufferSize(sol, l32, b32, b32, any, l32, any, &u) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, b32, b32, any, b32, dS, any, b32, any, b32, &g,
                                        prm) != CUSOLVER_STATUS_SUCCESS)
         return fail(CMPS_ERR_SOLVER, "randomized SVD buffer query failed");
-      *lw = std::max(std::max(std::max(a, q), std::max(u, g)), 1);
+      *lw = std::max(std::max(std::max(a, q), std::max(u, g)), std::max(e, 1));
       return CMPS_OK;
     };
     auto factor_rand = [&](int m, int64_t bb, FW& fw) -> int {
@@ -625,20 +637,52 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (rc == CMPS_OK && cudaMemcpyAsync(Z2, Z, sizeof(double2) * ll * bb, cudaMemcpyDeviceToDevice, st) !=
                                cudaSuccess)
         rc = fail(CMPS_ERR_CUDA, "randomized SVD copy failed");
+      int info = 0;
+      if (!b.red_exact) {
+        // The reduced problem by the Hermitian eigensolver: B B^H = U_r S^2 U_r^H,
+        // B = U_r S (B^H U_r S^-1)^H.  Small values carry the Gram error
+        // eps s_0^2 / s_j, which check (4) of the selection bounds; a sector
+        // that fails it is redone with the reduced SVD below.
+        zg(CUBLAS_OP_C, CUBLAS_OP_N, bb, bb, ll, &one, Z, ll, Z, ll, &zero, Gb, bb);
+        if (rc == CMPS_OK && cusolverDnZheevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)bb,
+                                              (cuDoubleComplex*)Gb, (int)bb, W, work, lwork, dinfo) !=
+                                 CUSOLVER_STATUS_SUCCESS)
+          rc = fail(CMPS_ERR_SOLVER, "randomized SVD: reduced eigensolver failed");
+        std::vector<double> w(bb);
+        if (rc == CMPS_OK) {
+          cudaMemcpyAsync(w.data(), W, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
+          if (cudaStreamSynchronize(st) != cudaSuccess || info != 0)
+            rc = fail(CMPS_ERR_SOLVER, "randomized SVD: reduced eigensolver did not converge");
+        }
+        if (rc == CMPS_OK) {
+          b.s.assign(bb, 0.0);
+          for (int64_t j = 0; j < bb; ++j) b.s[j] = std::sqrt(std::max(0.0, w[bb - 1 - j]));
+          rc = copy_wait(dS, b.s.data(), sizeof(double) * bb, cudaMemcpyHostToDevice, st);
+        }
+        if (rc == CMPS_OK) {
+          k_reverse_cols<<<grid_of(bb * bb), 256, 0, st>>>(Gb, bb, R);  // U_r, descending
+          double2* F = left ? b.dU : b.dV;   // short-side vectors (ld pp)
+          double2* O = left ? b.dV : b.dU;   // long-side vectors (ld ll)
+          zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);   // F = Q U_r
+          zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, R, bb, &zero, O, ll);   // O = B^H U_r
+          if (rc == CMPS_OK) k_scale_cols_inv<<<grid_of(ll * bb), 256, 0, st>>>(O, ll, bb, dS);  // ... S^-1
+        }
+      }
       // B^H = Q_B R (Householder), R^H = U_r S V_r^H, so B = U_r S (Q_B V_r)^H
-      if (rc == CMPS_OK && cusolverDnZgeqrf(sol, (int)ll, (int)bb, (cuDoubleComplex*)Z, (int)ll, (cuDoubleComplex*)tau,
+      if (b.red_exact && rc == CMPS_OK &&
+          cusolverDnZgeqrf(sol, (int)ll, (int)bb, (cuDoubleComplex*)Z, (int)ll, (cuDoubleComplex*)tau,
                                             work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
         rc = fail(CMPS_ERR_SOLVER, "randomized SVD QR failed");
-      if (rc == CMPS_OK) k_upper_adjoint<<<grid_of(bb * bb), 256, 0, st>>>(Z, ll, bb, Gb);
-      if (rc == CMPS_OK && cusolverDnZungqr(sol, (int)ll, (int)bb, (int)bb, (cuDoubleComplex*)Z, (int)ll,
+      if (b.red_exact && rc == CMPS_OK) k_upper_adjoint<<<grid_of(bb * bb), 256, 0, st>>>(Z, ll, bb, Gb);
+      if (b.red_exact && rc == CMPS_OK && cusolverDnZungqr(sol, (int)ll, (int)bb, (int)bb, (cuDoubleComplex*)Z, (int)ll,
                                             (const cuDoubleComplex*)tau, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS)
         rc = fail(CMPS_ERR_SOLVER, "randomized SVD QR basis failed");
-      if (rc == CMPS_OK && cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)bb, (int)bb, (cuDoubleComplex*)Gb,
+      if (b.red_exact && rc == CMPS_OK && cusolverDnZgesvdj(sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)bb, (int)bb, (cuDoubleComplex*)Gb,
                                              (int)bb, dS, (cuDoubleComplex*)R, (int)bb, (cuDoubleComplex*)Vb, (int)bb,
                                              work, lwork, dinfo, fw.params) != CUSOLVER_STATUS_SUCCESS)
         rc = fail(CMPS_ERR_SOLVER, "randomized SVD of the reduced matrix failed");
-      int info = 0;
-      if (rc == CMPS_OK) {
+      if (b.red_exact && rc == CMPS_OK) {
         b.s.assign(bb, 0.0);
         cudaMemcpyAsync(b.s.data(), dS, sizeof(double) * bb, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -648,8 +692,10 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       if (rc == CMPS_OK) {
         double2* F = left ? b.dU : b.dV;   // short-side vectors (ld pp)
         double2* O = left ? b.dV : b.dU;   // long-side vectors (ld ll)
-        zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);   // F = Q U_r
-        zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, Vb, bb, &zero, O, ll);  // O = Q_B V_r
+        if (b.red_exact) {
+          zg(CUBLAS_OP_N, CUBLAS_OP_N, pp, bb, bb, &one, Y, pp, R, bb, &zero, F, pp);   // F = Q U_r
+          zg(CUBLAS_OP_N, CUBLAS_OP_N, ll, bb, bb, &one, Z, ll, Vb, bb, &zero, O, ll);  // O = Q_B V_r
+        }
         zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, O, ll, &zero, R, pp);     // M O
         if (rc == CMPS_OK) k_col_resid<<<(unsigned)bb, 256, 0, st>>>(R, F, dS, pp, rs);
         // A <- A - Q Q^H A (left) or A - A Q Q^H (tall): the part outside the range
@@ -703,8 +749,8 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       b.rnd = false;
       b.tail = 0.0;
       b.resid.clear();
-      if (mode == 0 && rand_b(mn) > 0) {
-        b.bb = rand_b(mn);
+      if (mode == 0 && rand_b(m, mn) > 0) {
+        b.bb = rand_b(m, mn);
         return factor_rand(m, b.bb, fw);
       }
       if (mode == 3) return factor_rand(m, b.bb, fw);
@@ -820,7 +866,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
       auto cost = [&](int m) {
         const double nr = (double)blk[m].rows.size(), nc = (double)blk[m].cols.size();
         const int64_t mn = (int64_t)std::min(nr, nc);
-        if (rand_b(mn) > 0) return 10.0 + 2e-8 * nr * nc * (double)rand_b(mn);
+        if (rand_b(m, mn) > 0) return 10.0 + 2e-8 * nr * nc * (double)rand_b(m, mn);
         if (mn >= kEigMin) return 0.013 * (double)mn + 2.5e-9 * (double)mn * (double)mn * (double)mn;
         return 0.1 + 0.09 * (double)mn;
       };
@@ -845,9 +891,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           nA[k] = std::max(nA[k], (size_t)(nr * nc));
           nS[k] = std::max(nS[k], (size_t)mn);
           int lwork = 0;
-          if (rand_b(mn) > 0) {
-            nX[k] = std::max(nX[k], rand_scratch(nr, nc, rand_b(mn)));
-            if (rand_lwork(w.sol, fws[k].params, std::max(nr, nc), rand_b(mn), &lwork) != CMPS_OK) ok = false;
+          if (rand_b(m, mn) > 0) {
+            nX[k] = std::max(nX[k], rand_scratch(nr, nc, rand_b(m, mn)));
+            if (rand_lwork(w.sol, fws[k].params, std::max(nr, nc), rand_b(m, mn), &lwork) != CMPS_OK) ok = false;
           } else if (mn < kEigMin) {
             if (cusolverDnZgesvdj_bufferSize(w.sol, CUSOLVER_EIG_MODE_VECTOR, 1, (int)nr, (int)nc,
                                              (cuDoubleComplex*)dA, (int)nr, dS, (cuDoubleComplex*)blk[m].dU, (int)nr,
@@ -907,7 +953,17 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
               for (;;) {
                 const size_t i = next.fetch_add(1);
                 if (i >= order.size() || code[k] != CMPS_OK) break;
+                const auto t0 = std::chrono::steady_clock::now();
                 const int rc = factor(order[i], 0, fws[k]);
+                if (std::getenv("CMPS_SVD_TRACE")) {
+                  cudaStreamSynchronize(fws[k].st);
+                  const Blk& bk = blk[order[i]];
+                  std::fprintf(stderr, "svd sector %d (%zu x %zu) route %s b=%lld: %.2f ms (worker %d)\n", order[i],
+                               bk.rows.size(), bk.cols.size(), bk.rnd ? "rnd" : bk.eig ? "gram" : "exact",
+                               (long long)bk.bb,
+                               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(),
+                               k);
+                }
                 if (rc != CMPS_OK) {
                   code[k] = rc;
                   msg[k] = cmps_last_error();
@@ -994,6 +1050,7 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           valid = len < np;                                                     // (2)
           if (!valid) failed = 2;
         }
+        std::vector<char> bad4(nm, 0);  // sectors whose kept triplets miss check (4)
         if (valid) {
           const double next = sv[len];
           std::vector<int64_t> kept(nm, 0);
@@ -1001,10 +1058,15 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
           for (int m = 0; m < nm && valid; ++m) {
             if (!blk[m].rnd) continue;
             if (!(4.0 * blk[m].tail < next * next)) valid = false, failed = 3;  // (3)
-            for (int64_t j = 0; j < kept[m] && valid; ++j)
-              if (!(blk[m].resid[j] <= 1e-12 * sv[0] + 500.0 * kEps * sv[0] * sv[0] / blk[m].s[j]))
-                valid = false, failed = 4;                                      // (4)
           }
+          for (int m = 0; m < nm && valid; ++m) {
+            if (!blk[m].rnd) continue;
+            for (int64_t j = 0; j < kept[m] && !bad4[m]; ++j)
+              if (!(blk[m].resid[j] <= 1e-12 * sv[0] + 500.0 * kEps * sv[0] * sv[0] / blk[m].s[j]))
+                bad4[m] = 1;                                                    // (4)
+          }
+          for (int m = 0; m < nm && valid; ++m)
+            if (bad4[m]) valid = false, failed = 4;
         }
         if (std::getenv("CMPS_SVD_TRACE")) {
           std::fprintf(stderr, "svd pass %d: randomized %s (check %d)", pass, valid ? "accepted" : "rejected", failed);
@@ -1012,6 +1074,19 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out) {
             if (blk[m].rnd)
               std::fprintf(stderr, "  [m%d b=%lld tail=%.3g]", m, (long long)blk[m].bb, blk[m].tail);
           std::fprintf(stderr, "\n");
+        }
+        if (!valid && failed == 4) {
+          // kept triplets of the reduced eigensolver not accurate enough:
+          // those sectors again with the reduced SVD (QR + one-sided Jacobi),
+          // same range
+          bool retried = false;
+          for (int m = 0; m < nm && status == CMPS_OK; ++m) {
+            if (!bad4[m] || blk[m].red_exact) continue;
+            blk[m].red_exact = true;
+            status = factor(m, 3, main_fw);
+            retried = true;
+          }
+          if (retried) continue;
         }
         if (!valid) {
           // A spectrum that decays slowly past the range leaves too much
