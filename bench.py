@@ -462,17 +462,21 @@ def main():
     if a.idmrg_steps > 0:
         line["idmrg"] = idmrg_bench(ctx, wl, a.chi, a.idmrg_steps, dist)
     if a.ising_steps > 0:
-        from chainamps_b200 import models, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_ORDER_AUTO, CMPS_ORDER_FOLDED
+        from chainamps_b200 import (models, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_SPLIT_BF16, CMPS_ORDER_AUTO,
+                                    CMPS_ORDER_FOLDED)
         rules, ch, W, bq = models.coupled_ising_model(12, 1.2, 64, 0.05)
         iw = dict(rules=rules, Wt=models.mpo_tensor(ch, W, bq))
         ising = {"model": "coupled TFIM chains: 12-site periodic chain vertex, g=1.2, 64 lowest states (Z2), "
                           "J_perp=0.05 sum X_i X_i, MPO D=26",
                  "forms": {"fp64": "FP64, contraction order chosen by flops (canonical for this vertex)",
-                           "mixed": "split precision (the canonical order in FP32 for this vertex), FP64 Krylov, "
-                                    "Rayleigh quotients and SVD",
+                           "mixed": "split TF32 precision (the canonical order in FP32 FMA for this vertex), FP64 "
+                                    "Krylov, Rayleigh quotients and SVD",
+                           "mixed_bf16": "split BF16 precision (the canonical order as four tcgen05 split-BF16 "
+                                         "stages for this vertex), FP64 Krylov, Rayleigh quotients and SVD",
                            "fp64_folded": "FP64 in the reference's folded order (LeftPart . V . RightPart)"}}
         for chi in [int(c) for c in str(a.ising_chi).split(",") if c.strip()]:
-            forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO)]
+            forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO),
+                     ("mixed_bf16", CMPS_SPLIT_BF16, CMPS_ORDER_AUTO)]
             if chi == a.ising_folded_chi:
                 forms.append(("fp64_folded", CMPS_FP64, CMPS_ORDER_FOLDED))
             ising[f"chi_{chi}"] = idmrg_bench(ctx, iw, chi, a.ising_steps, dist, warm=2, forms=forms,

@@ -7,7 +7,8 @@ library and fails loudly when it is not built -- there is no CPU fallback.
 """
 __all__ = ["Context", "TwoVertexComponents", "SVDResult", "Block", "MPXTensor", "MPXIndexSpec", "CmpsError",
            "upload_block", "iDMRG", "fDMRG", "run_excited_fdmrg", "DEFAULT_PROJECTOR_WEIGHT", "CMPS_FP64",
-           "CMPS_SPLIT_TF32", "CMPS_SPLIT_BF16", "CMPS_ORDER_AUTO", "CMPS_ORDER_FOLDED", "CMPS_ORDER_CANONICAL", "version"]
+           "CMPS_SPLIT_TF32", "CMPS_SPLIT_BF16", "CMPS_ORDER_AUTO", "CMPS_ORDER_FOLDED", "CMPS_ORDER_CANONICAL", "CMPS_FORM_NONE", "CMPS_FORM_FOLDED_TC",
+           "CMPS_FORM_CANONICAL_FP32", "CMPS_FORM_CANONICAL_TC", "version"]
 
 
 def __getattr__(name):

@@ -24,7 +24,8 @@ LIB = os.path.join(HERE, "libchainamps_b200.so")
 STAMP = LIB + ".sha256"
 OBJDIR = os.path.join(ROOT, "_build", "chainamps_b200")
 SOURCES = ["capi.cu", "heff.cu", "kernels.cu", "zgemm_fp64.cu", "svd.cu", "split_tf32.cu", "tc_gemm.cu", "noalloc.cu",
-           "dmrg.cu", "adjoint.cu", "unitcell.cu", "mpxio.cu", "canonical.cu", "cgemm_fp32.cu", "projector.cu"]
+           "dmrg.cu", "adjoint.cu", "unitcell.cu", "mpxio.cu", "canonical.cu", "canonical_tc.cu", "cgemm_fp32.cu",
+           "projector.cu"]
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]

@@ -34,6 +34,10 @@ CMPS_SPLIT_BF16 = 2
 CMPS_ORDER_AUTO = 0
 CMPS_ORDER_FOLDED = 1
 CMPS_ORDER_CANONICAL = 2
+CMPS_FORM_NONE = 0
+CMPS_FORM_FOLDED_TC = 1
+CMPS_FORM_CANONICAL_FP32 = 2
+CMPS_FORM_CANONICAL_TC = 3
 
 
 class CmpsError(RuntimeError):
@@ -90,6 +94,7 @@ _SIGS = {
     "cmps_heff_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_heff_set_order": (C.c_int, [C.c_void_p, C.c_int]),
     "cmps_heff_order": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), c_dblp, c_dblp]),
+    "cmps_heff_split_form": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cmps_heff_status": (C.c_int, [C.c_void_p]),
     "cmps_heff_eigs": (C.c_int, [C.c_void_p, c_dblp, C.c_double, C.c_int, C.c_int, c_dblp, c_dblp,
                                  C.POINTER(C.c_int)]),
@@ -357,6 +362,12 @@ class TwoVertexComponents:
         c = C.c_double()
         _check(lib.cmps_heff_order(self.h, C.byref(a), C.byref(f), C.byref(c)))
         return a.value, f.value, c.value
+
+    def split_form(self):
+        """Form of the split operator the precision runs (CMPS_FORM_*)."""
+        f = C.c_int()
+        _check(lib.cmps_heff_split_form(self.h, C.byref(f)))
+        return f.value
 
     def HED(self, guess=None, tol=1e-10, max_restarts=50, krylov_dim=24, want_vector=True):
         """Lowest eigenpair; returns (energy, eigenvector in ARPACK order or

@@ -72,6 +72,7 @@ struct Canon {
 };
 
 void release_canonical(Heff* h) {
+  release_canonical_tc(h);  // it may borrow the intermediates below
   if (!h || !h->canon) return;
   delete h->canon;
   h->canon = nullptr;
@@ -382,6 +383,13 @@ static int plan_canonical(const Heff& H, Plan& P) {
       }
     }
   }
+  return CMPS_OK;
+}
+
+int canonical_scratch(const Heff& H, const Planar** xz, const Planar** y) {
+  if (!H.canon) return fail(CMPS_ERR_STATE, "canonical-order plans not built");
+  *xz = &H.canon->xz;
+  *y = &H.canon->y;
   return CMPS_OK;
 }
 

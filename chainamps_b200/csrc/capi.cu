@@ -402,7 +402,9 @@ int cmps_heff_flops(const cmps_heff* h, double* canonical, double* executed) {
   if (canonical) *canonical = H.flops_canonical;
   if (executed) {
     const bool canonical = H.precision == CMPS_FP64 ? H.order == CMPS_ORDER_CANONICAL : H.low_canonical;
-    *executed = canonical ? H.flops_canon : H.flops_executed;
+    *executed = H.precision != CMPS_FP64 && H.ctc ? canonical_tc_flops(H)
+                : canonical                        ? H.flops_canon
+                                                   : H.flops_executed;
   }
   return CMPS_OK;
 }
@@ -424,6 +426,12 @@ int cmps_heff_order(const cmps_heff* h, int* active, double* executed_folded, do
   if (active) *active = H.order;
   if (executed_folded) *executed_folded = H.flops_folded;
   if (executed_canonical) *executed_canonical = H.flops_canon;
+  return CMPS_OK;
+}
+
+int cmps_heff_split_form(const cmps_heff* h, int* form) {
+  if (!h || !h->impl || !form) return fail(CMPS_ERR_ARG, "null argument");
+  *form = split_form(*h->impl);
   return CMPS_OK;
 }
 

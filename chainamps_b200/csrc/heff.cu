@@ -774,17 +774,16 @@ int Heff::select_order() {
   for (size_t m = 0; m < cneed.size() && m < in_need.size(); ++m) in_need[m] |= cneed[m];
   int want = order_req;
   if (want == CMPS_ORDER_AUTO) want = flops_canon <= 0.5 * flops_folded ? CMPS_ORDER_CANONICAL : CMPS_ORDER_FOLDED;
-  // the canonical plans are rebuilt (or dropped): an FP32 canonical
-  // split-precision operator built on them goes too, and is prepared again
-  const bool low = low_canonical;
-  low_canonical = false;
+  // the canonical plans are rebuilt (or dropped), and the split-precision
+  // operator, whose form follows the order, is prepared again
+  release_split(this);
   if (want == CMPS_ORDER_CANONICAL) {
     CMPS_TRY(build_canonical(*this));
   } else {
     release_canonical(this);
   }
   order = want;
-  if (low || (is_split(precision) && !split)) CMPS_TRY(prepare_precision(this, precision));
+  if (is_split(precision)) CMPS_TRY(prepare_precision(this, precision));
   return CMPS_OK;
 }
 
@@ -920,6 +919,7 @@ int Heff::autotune(TuneStats* stats) {
   cudaStream_t st = ctx->stream;
   if (is_split(precision) && !low_canonical) return CMPS_OK;
   CMPS_TRY(zero_wait(x.d, sizeof(double) * 2 * x.len, st));
+  if (low_canonical && ctc) return CMPS_OK;  // tcgen05 stages: fixed tiles
   if (low_canonical) return autotune_canonical(*this, true, st, stats);
   if (order == CMPS_ORDER_CANONICAL) return autotune_canonical(*this, false, st, stats);
   CMPS_TRY(ensure_T());

@@ -41,6 +41,7 @@ struct ThetaSpace {
 struct SvdResult;
 struct SplitState;
 struct Canon;
+struct CanonTc;
 
 struct Heff {
   cmps_context* ctx = nullptr;
@@ -161,9 +162,11 @@ struct Heff {
   double flops_folded = 0.0, flops_canon = 0.0;
   Canon* canon = nullptr;
   int select_order();
-  // The split-precision operator runs the canonical order in FP32
-  // (canonical.cu) instead of the folded order on tcgen05 (split_tf32.cu).
+  // The split-precision operator runs the canonical order instead of the
+  // folded order on tcgen05 (split_tf32.cu): on tcgen05 in split BF16 when
+  // ctc is set (canonical_tc.cu), else in FP32 (canonical.cu).
   bool low_canonical = false;
+  CanonTc* ctc = nullptr;
   int precision = CMPS_FP64;
   SplitState* split = nullptr;   // split-TF32 operands and plans (split_tf32.cu)
   // work vectors
@@ -240,6 +243,8 @@ int derivative_envs(Heff& H, const SvdResult& s, const std::vector<WEntry>& dW, 
                     Env& dLn, Env& dRn);
 
 // The canonical contraction order (canonical.cu).
+// the FP64 form's intermediates (X/Z and Y), which the split forms borrow
+int canonical_scratch(const Heff& H, const Planar** xz, const Planar** y);
 // need (optional): the theta sectors the canonical order's first stage reads
 int canonical_flops(const Heff& H, double* flops, std::vector<uint8_t>* need = nullptr);
 // measured tile shapes of the canonical plans (FP32 or FP64 launches)
@@ -252,6 +257,16 @@ int apply_canonical(Heff& H, int which, const Planar& in, Planar& out, cudaStrea
 int build_canonical32(Heff& H);
 int apply_canonical32(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
 
+// The canonical order in split BF16 on tcgen05 (canonical_tc.cu): whole
+// vectors only (no windows, every sector owned).
+int build_canonical_tc(Heff& H);
+void release_canonical_tc(Heff* h);
+// which: 1 = theta in, stages R and W2; 2 = stages W1 and L; 0 = all four
+int apply_canonical_tc(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
+void canonical_tc_error_words(const Heff& H, int** d_err, int** h_err);
+// executed complex flops of one matvec, padding included
+double canonical_tc_flops(const Heff& H);
+
 // Split-precision operands for the tcgen05 path (split_tf32.cu).
 int prepare_precision(Heff* h, int precision);
 void release_split(Heff* h);
@@ -263,6 +278,8 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st);
 int split_reset_error(Heff& H, cudaStream_t st);
 int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st);
 int split_error(Heff& H);
+// The form of the handle's split operator (CMPS_FORM_*).
+int split_form(const Heff& H);
 // cuSOLVER handle owned by the context (svd.cu).
 void release_solver(cmps_context* ctx);
 // The context's cuBLAS / cuSOLVER handles, bound to its stream (svd.cu).

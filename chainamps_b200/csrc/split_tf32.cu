@@ -33,6 +33,7 @@
 #include <set>
 
 #include "heff.h"
+#include "split_common.cuh"
 #include "tc_gemm.h"
 
 namespace cmps {
@@ -60,47 +61,6 @@ struct SplitState {
 };
 
 namespace {
-
-
-__device__ __forceinline__ float rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-__device__ __forceinline__ void split4(double re, double im, float* p0, float* p1, float* p2, float* p3) {
-  const float hr = rna((float)re), hi = rna((float)im);
-  *p0 = hr;
-  *p1 = rna((float)(re - (double)hr));
-  *p2 = hi;
-  *p3 = rna((float)(im - (double)hi));
-}
-// BF16: hi = x rounded to BF16, mid = x - hi rounded to BF16 (raw bits)
-__device__ __forceinline__ void split4(double re, double im, uint16_t* p0, uint16_t* p1, uint16_t* p2,
-                                       uint16_t* p3) {
-  const __nv_bfloat16 hr = __double2bfloat16(re), hi = __double2bfloat16(im);
-  *p0 = __bfloat16_as_ushort(hr);
-  *p1 = __bfloat16_as_ushort(__double2bfloat16(re - (double)__bfloat162float(hr)));
-  *p2 = __bfloat16_as_ushort(hi);
-  *p3 = __bfloat16_as_ushort(__double2bfloat16(im - (double)__bfloat162float(hi)));
-}
-
-struct SplitBlock {
-  int64_t src_off, dst_off;
-  int32_t rows, cols, ld_dst, transpose;
-};
-
-// dst (4 planes) <- split(src block), optionally transposed.
-template <class E>
-__global__ void k_split_blocks(const SplitBlock* __restrict__ blocks, const double* __restrict__ sr,
-                               const double* __restrict__ si, E* __restrict__ dst, int64_t plane) {
-  const SplitBlock b = blocks[blockIdx.x];
-  const int64_t n = (int64_t)b.rows * b.cols;
-  for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
-    const int64_t r = e / b.cols, c = e % b.cols;
-    const int64_t o = b.transpose ? b.dst_off + c * b.ld_dst + r : b.dst_off + r * b.ld_dst + c;
-    split4(sr[b.src_off + e], si[b.src_off + e], dst + o, dst + o + plane, dst + o + 2 * plane, dst + o + 3 * plane);
-  }
-}
 
 // A (m, sigma1, sigma2) chunk of theta: rows a0 (sector dim), columns a2,
 // row-major inside its sector block; its S1A image is the transpose [a2][a0].
@@ -154,7 +114,9 @@ __global__ void __launch_bounds__(256) k_split_theta_t(const ThetaTile* __restri
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
-int encoder() {
+}  // namespace
+
+static int encoder() {
   if (g_encode) return CMPS_OK;
   cudaDriverEntryPointQueryResult q;
   void* fn = nullptr;
@@ -164,40 +126,110 @@ int encoder() {
   return CMPS_OK;
 }
 
-// 3-D map over one operand block: (K, rows, 4 planes); box (64 bytes of K,
-// box_rows, 4).  The role's planes start at element role_off of the buffer,
-// `plane` elements apart (FP32, or BF16 for split-BF16); `base_off` is the
-// block's offset inside its plane, and the block must lie inside the plane.
-int make_map(const SplitState& S, int64_t role_off, int64_t base_off, int64_t K, int64_t rows, int64_t ld,
-             int64_t plane, CUtensorMap* out, int box_rows = 128) {
-  const int64_t es_b = S.bf16 ? 2 : 4;
-  const char* base = (const char*)S.at(role_off + base_off);
+namespace tc {
+// 3-D map over one operand block of 2- or 4-byte elements: (K, rows, 4
+// planes); box (64 bytes of K, box_rows, 4).  `base` is the block's first
+// element in plane 0, the planes lie `plane` elements apart, and the block
+// (rows x ld, K used per row) must fit inside `room` elements from base.
+int encode_map(bool bf16, const void* base, int64_t K, int64_t rows, int64_t ld, int64_t plane, int64_t room,
+               int box_rows, CUtensorMap* out) {
+  CMPS_TRY(encoder());
+  const int64_t es_b = bf16 ? 2 : 4;
   if (((uintptr_t)base & 15) || (ld * es_b) % 16 || (plane * es_b) % 16 || K < 1 || rows < 1 || K > ld)
     return fail(CMPS_ERR_STATE, "tensor map: misaligned operand block");
-  if (base_off < 0 || base_off + (rows - 1) * ld + K > plane)
-    return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
+  if ((rows - 1) * ld + K > room) return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
   cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, 4};
   cuuint64_t strides[2] = {(cuuint64_t)(ld * es_b), (cuuint64_t)(plane * es_b)};
   if (box_rows < 16 || box_rows > 128 || (box_rows & 15)) return fail(CMPS_ERR_STATE, "tensor map: bad box height");
   cuuint32_t box[3] = {(cuuint32_t)(64 / es_b), (cuuint32_t)box_rows, 4};
   cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = g_encode(out, S.bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                        (void*)base, dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+  CUresult r = g_encode(out, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                        const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(CMPS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return CMPS_OK;
 }
+}  // namespace tc
 
-void add_tiles(tc::TcPlan& p, int32_t task, int32_t m, int32_t n) {
-  for (int32_t m0 = 0; m0 < m; m0 += 128)
-    for (int32_t n0 = 0; n0 < n; n0 += 128)
-      p.tiles.push_back(tc::TcTile{task, m0, n0, tc::b_box_rows(n), 0, ((std::min(128, n - n0)) + 15) & ~15});
+namespace {
+
+// A map over block `base_off` of a role of the split buffer (planes `plane`
+// elements apart from element role_off); the block must lie inside the plane.
+int make_map(const SplitState& S, int64_t role_off, int64_t base_off, int64_t K, int64_t rows, int64_t ld,
+             int64_t plane, CUtensorMap* out, int box_rows = 128) {
+  if (base_off < 0) return fail(CMPS_ERR_STATE, "tensor map: operand block outside its buffer");
+  return tc::encode_map(S.bf16, S.at(role_off + base_off), K, rows, ld, plane, plane - base_off, box_rows, out);
 }
 
 }  // namespace
 
 namespace tc {
+void add_tiles(TcPlan& p, int32_t task, int32_t m, int32_t n) {
+  for (int32_t m0 = 0; m0 < m; m0 += 128)
+    for (int32_t n0 = 0; n0 < n; n0 += 128)
+      p.tiles.push_back(TcTile{task, m0, n0, b_box_rows(n), 0, ((std::min(128, n - n0)) + 15) & ~15});
+}
+
+int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first) {
+  // k-steps per tile (the MMA warp walks them without term lookups)
+  const int32_t ks = kstep(bf16);
+  for (TcTile& t : p.tiles) {
+    if (t.task < 0 || t.task >= (int32_t)p.tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
+    const TcTask& k = p.tasks[t.task];
+    if (k.t0 < 0 || k.t1 < k.t0 || k.t1 > (int32_t)p.terms.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
+    int64_t it = 0;
+    for (int q = k.t0; q < k.t1; ++q) it += (p.terms[q].k + ks - 1) / ks;
+    if (it > 0x7fffffff) return fail(CMPS_ERR_ARG, "tcgen05 plan: too many k-steps in one tile");
+    t.kiters = (int32_t)it;
+  }
+  // heaviest tiles first: the persistent kernel deals tiles round-robin to
+  // the SMs, so this ordering balances the per-SM work
+  if (heaviest_first) {
+    auto cost = [&](const TcTile& t) {
+      return (int64_t)(t.kiters + 2) * (t.nmma / 16);  // +2: fixed per-tile cost (epilogue)
+    };
+    std::stable_sort(p.tiles.begin(), p.tiles.end(), [&](const TcTile& a, const TcTile& b) { return cost(a) > cost(b); });
+  }
+  // plan integrity: every term names an existing map, every tile an existing task
+  const int32_t na = (int32_t)(by_tma ? p.amaps.size() : p.adescs.size());
+  // a TMA copy starts on a 16-byte boundary: the K offset a multiple of
+  // 4 FP32 or 8 BF16 elements; a row offset only for A tiles loaded by TMA
+  const int32_t amask = bf16 ? 7 : 3;
+  for (const TcTerm& tm : p.terms)
+    if (tm.a_map < 0 || tm.a_map >= na || tm.b_map < 0 || tm.b_map >= (int32_t)p.bmaps.size() || tm.k < 1 ||
+        (tm.a_x0 & amask) || tm.a_y0 < 0 || (!by_tma && tm.a_y0 != 0))
+      return fail(CMPS_ERR_STATE, "tcgen05 plan: bad term");
+  for (const TcTask& t : p.tasks)
+    if (t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)p.terms.size() || t.m < 1 || t.n < 1 || t.out_off < 0)
+      return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
+  // segments: start at column 0, increase, cover N; a task wider than one
+  // 128-column tile has a single segment
+  for (const TcTask& t : p.tasks) {
+    if (t.nseg < 1 || t.nseg > 4 || t.seg_n0[0] != 0 || t.seg_off[0] != t.out_off || (t.nseg > 1 && t.n > 128))
+      return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
+    for (int q = 1; q < 4; ++q) {
+      if (q < t.nseg ? (t.seg_n0[q] <= t.seg_n0[q - 1] || t.seg_n0[q] >= t.n || t.seg_off[q] < 0)
+                     : t.seg_n0[q] != 0x7fffffff)
+        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
+    }
+  }
+  // every B map of a task has the task's N rows, so the tile's B box height
+  // (and the transaction bytes the producer expects) matches each map
+  if (b_rows.size() != p.bmaps.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map count");
+  for (const TcTask& t : p.tasks)
+    for (int q = t.t0; q < t.t1; ++q)
+      if (b_rows[p.terms[q].b_map] != t.n) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map rows differ from N");
+  for (const TcTile& tl : p.tiles) {
+    const TcTask& t = p.tasks[tl.task];
+    if (tl.m0 < 0 || tl.m0 >= t.m || tl.n0 < 0 || tl.n0 >= t.n) return fail(CMPS_ERR_STATE, "tcgen05 plan: tile origin");
+    if (tl.b_rows != b_box_rows(t.n)) return fail(CMPS_ERR_STATE, "tcgen05 plan: B box height");
+    if (tl.nmma < 16 || tl.nmma > 128 || tl.nmma != ((std::min(128, t.n - tl.n0) + 15) & ~15) || tl.nmma > tl.b_rows)
+      return fail(CMPS_ERR_STATE, "tcgen05 plan: tile N");
+  }
+  return CMPS_OK;
+}
+
 int TcPlan::upload(cudaStream_t st) {
   release();
   auto up = [st](auto& v, auto** d) -> int {
@@ -232,6 +264,7 @@ void TcPlan::release() {
 
 void release_split(Heff* h) {
   if (h) h->low_canonical = false;  // the FP32 canonical operands go with the canonical plans
+  release_canonical_tc(h);
   if (!h || !h->split) return;
   SplitState* s = h->split;
   s->p1.release();
@@ -256,7 +289,6 @@ constexpr int32_t kFuseMaxSegN1 = CMPS_FUSE_MAX_SEG_N1;
 constexpr int32_t kFuseMaxSegN2 = CMPS_FUSE_MAX_SEG_N2;
 
 static int build_split(Heff& H, bool bf16) {
-  CMPS_TRY(encoder());
   const Rules& r = H.rules;
   const ThetaSpace& th = H.th;
   const Bond& A0 = H.L.a;
@@ -577,7 +609,7 @@ static int build_split(Heff& H, bool bf16) {
       if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
                                 S->ts_len)
         return fail(CMPS_ERR_STATE, "stage-1 output outside TS");
-    add_tiles(p1, (int32_t)p1.tasks.size(), task.m, task.n);
+    tc::add_tiles(p1, (int32_t)p1.tasks.size(), task.m, task.n);
     p1.tasks.push_back(task);
   }
   // ---- stage 2 plan: C2[l', a2'] = sum TS[l', r_pad] RPTS[a2', a2] ----
@@ -630,105 +662,59 @@ static int build_split(Heff& H, bool bf16) {
       if (sg.out_off < 0 || sg.out_off + (int64_t)(task.m - 1) * task.row_stride + (int64_t)(sg.n - 1) * task.col_stride >=
                                 H.out_len)
         return fail(CMPS_ERR_STATE, "stage-2 output outside theta");
-    add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
+    tc::add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
     p2.tasks.push_back(task);
   }
-  // k-steps per tile (the MMA warp walks them without term lookups)
-  for (tc::TcPlan* p : {&p1, &p2})
-    for (tc::TcTile& t : p->tiles) {
-      const tc::TcTask& k = p->tasks[t.task];
-      int64_t it = 0;
-      const int32_t ks = tc::kstep(S->bf16);
-      for (int q = k.t0; q < k.t1; ++q) it += (p->terms[q].k + ks - 1) / ks;
-      if (it > 0x7fffffff) return fail(CMPS_ERR_ARG, "tcgen05 plan: too many k-steps in one tile");
-      t.kiters = (int32_t)it;
-    }
-  // heaviest tiles first: the persistent kernel deals tiles round-robin to
-  // the SMs, so this ordering balances the per-SM work
-  for (tc::TcPlan* p : {&p1, &p2}) {
-    auto cost = [&](const tc::TcTile& t) {
-      return (int64_t)(t.kiters + 2) * (t.nmma / 16);  // +2: fixed per-tile cost (epilogue)
-    };
-    std::stable_sort(p->tiles.begin(), p->tiles.end(),
-                     [&](const tc::TcTile& a, const tc::TcTile& b) { return cost(a) > cost(b); });
-  }
-  // plan integrity: every term names an existing map, every tile an existing task
-  for (const tc::TcPlan* p : {&p1, &p2}) {
-    const bool by_tma = p == &p1 || S->bf16;
-    const int32_t na = (int32_t)(by_tma ? p->amaps.size() : p->adescs.size());
-    // a TMA copy starts on a 16-byte boundary: the K offset a multiple of
-    // 4 FP32 or 8 BF16 elements
-    const int32_t amask = S->bf16 ? 7 : 3;
-    for (const tc::TcTerm& tm : p->terms)
-      if (tm.a_map < 0 || tm.a_map >= na || tm.b_map < 0 || tm.b_map >= (int32_t)p->bmaps.size() || tm.k < 1 ||
-          (tm.a_x0 & amask))
-        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad term");
-    if (p == &p2 && !S->bf16)
-      for (const tc::TcTerm& tm : p->terms)
-        if (tm.a_x0 + tm.k > p->adescs[tm.a_map].cols) return fail(CMPS_ERR_STATE, "tcgen05 plan: term past its T block");
-    for (const tc::TcTask& t : p->tasks)
-      if (t.t0 < 0 || t.t1 < t.t0 || t.t1 > (int32_t)p->terms.size() || t.m < 1 || t.n < 1 || t.out_off < 0)
-        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad task");
-    // segments: start at column 0, increase, cover N; a task wider than one
-    // 128-column tile has a single segment
-    for (const tc::TcTask& t : p->tasks) {
-      if (t.nseg < 1 || t.nseg > 4 || t.seg_n0[0] != 0 || t.seg_off[0] != t.out_off || (t.nseg > 1 && t.n > 128))
-        return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
-      for (int q = 1; q < 4; ++q) {
-        if (q < t.nseg ? (t.seg_n0[q] <= t.seg_n0[q - 1] || t.seg_n0[q] >= t.n || t.seg_off[q] < 0)
-                       : t.seg_n0[q] != 0x7fffffff)
-          return fail(CMPS_ERR_STATE, "tcgen05 plan: bad segments");
-      }
-    }
-    for (const tc::TcTile& tl : p->tiles)
-      if (tl.task < 0 || tl.task >= (int32_t)p->tasks.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: bad tile");
-  }
-  // every B map of a task has the task's N rows, so the tile's B box height
-  // (and the transaction bytes the producer expects) matches each map
-  for (int stage = 0; stage < 2; ++stage) {
-    const tc::TcPlan& p = stage == 0 ? p1 : p2;
-    const std::vector<int32_t>& rows = stage == 0 ? b1_rows : b2_rows;
-    if (rows.size() != p.bmaps.size()) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map count");
-    for (const tc::TcTask& t : p.tasks)
-      for (int q = t.t0; q < t.t1; ++q)
-        if (rows[p.terms[q].b_map] != t.n) return fail(CMPS_ERR_STATE, "tcgen05 plan: B map rows differ from N");
-    for (const tc::TcTile& tl : p.tiles) {
-      const tc::TcTask& t = p.tasks[tl.task];
-      if (tl.b_rows != tc::b_box_rows(t.n)) return fail(CMPS_ERR_STATE, "tcgen05 plan: B box height");
-      if (tl.nmma < 16 || tl.nmma > 128 || tl.nmma != ((std::min(128, t.n - tl.n0) + 15) & ~15) || tl.nmma > tl.b_rows)
-        return fail(CMPS_ERR_STATE, "tcgen05 plan: tile N");
-      int64_t it = 0;
-      const int32_t ks = tc::kstep(S->bf16);
-      for (int q = t.t0; q < t.t1; ++q) it += (p.terms[q].k + ks - 1) / ks;
-      if (it != tl.kiters) return fail(CMPS_ERR_STATE, "tcgen05 plan: tile k-steps");
-    }
-  }
+  CMPS_TRY(tc::finish_plan(p1, S->bf16, true, b1_rows, true));
+  CMPS_TRY(tc::finish_plan(p2, S->bf16, S->bf16, b2_rows, true));
+  if (!S->bf16)
+    for (const tc::TcTerm& tm : p2.terms)
+      if (tm.a_x0 + tm.k > p2.adescs[tm.a_map].cols) return fail(CMPS_ERR_STATE, "tcgen05 plan: term past its T block");
   CMPS_TRY(p1.upload(H.ctx->stream));
   CMPS_TRY(p2.upload(H.ctx->stream));
   return CMPS_OK;
 }
 
 // The split-precision operator of a handle: the folded order on tcgen05
-// (split-TF32, this file), or -- when the canonical order executes at most a
-// quarter of the folded order's flops -- the canonical order in FP32
-// (canonical.cu).  The quarter weighs the folded form's tensor-core rate
-// against the FP32 form's FFMA rate on the short-K canonical stages.
+// (this file), or -- when the canonical order is requested, or executes at
+// most a quarter of the folded order's flops -- the canonical order: on
+// tcgen05 in split BF16 (canonical_tc.cu), else in FP32 (canonical.cu).  The
+// quarter weighs the folded form's large-K tensor-core GEMMs against the
+// canonical form's short-K stages and three intermediates in HBM.
 constexpr double kLowCanonicalRatio = 0.25;
 
 int prepare_precision(Heff* h, int precision) {
   if (precision == CMPS_FP64) return CMPS_OK;
   if (!is_split(precision)) return fail(CMPS_ERR_ARG, "unknown precision");
+  const bool bf16 = precision == CMPS_SPLIT_BF16;
   // a split operator of the other format is rebuilt
-  if (h->split && h->split->bf16 != (precision == CMPS_SPLIT_BF16)) release_split(h);
+  if (h->split && h->split->bf16 != bf16) release_split(h);
+  if (h->low_canonical && (h->ctc != nullptr) != (bf16 && h->whole())) release_split(h);
   if (h->split || h->low_canonical) return CMPS_OK;
-  if (h->canon && h->flops_canon <= kLowCanonicalRatio * h->flops_folded) {
+  if (h->canon && (h->order_req == CMPS_ORDER_CANONICAL || h->flops_canon <= kLowCanonicalRatio * h->flops_folded)) {
+    if (bf16 && h->whole()) {
+      const int st = build_canonical_tc(*h);
+      if (st == CMPS_OK) {
+        h->low_canonical = true;
+        return CMPS_OK;
+      }
+      release_canonical_tc(h);
+      if (st != CMPS_ERR_NOMEM) return st;
+      cudaGetLastError();  // no room for the BF16 intermediates: the FP32 form
+    }
     CMPS_TRY(build_canonical32(*h));
     h->low_canonical = true;
     return CMPS_OK;
   }
-  int st = build_split(*h, precision == CMPS_SPLIT_BF16);
+  int st = build_split(*h, bf16);
   if (st != CMPS_OK) release_split(h);
   return st;
+}
+
+int split_form(const Heff& H) {
+  if (H.precision == CMPS_FP64) return CMPS_FORM_NONE;
+  if (H.low_canonical) return H.ctc ? CMPS_FORM_CANONICAL_TC : CMPS_FORM_CANONICAL_FP32;
+  return H.split ? CMPS_FORM_FOLDED_TC : CMPS_FORM_NONE;
 }
 
 // stage 1 (T = LeftPart . theta) or stage 2 (theta' = T . RightPart) of a
@@ -754,21 +740,39 @@ static int split_theta(const SplitState& S, const Planar& in, cudaStream_t st) {
   return CMPS_OK;
 }
 
+// The error word of the handle's tcgen05 pipelines (device, pinned host);
+// false for the FP32 canonical form, which has no pipeline waits.
+static bool error_words(const Heff& H, int** d_err, int** h_err) {
+  *d_err = *h_err = nullptr;
+  if (H.low_canonical) {
+    canonical_tc_error_words(H, d_err, h_err);
+  } else if (H.split) {
+    *d_err = H.split->d_err;
+    *h_err = H.split->h_err;
+  }
+  return *d_err != nullptr;
+}
+
 int split_reset_error(Heff& H, cudaStream_t st) {
-  if (H.low_canonical) return CMPS_OK;  // no pipeline waits, no error word
-  SplitState* S = H.split;
-  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
-  CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
+  int *d_err, *h_err;
+  if (!error_words(H, &d_err, &h_err)) {
+    if (H.low_canonical) return CMPS_OK;
+    return fail(CMPS_ERR_STATE, "split-precision operands not prepared");
+  }
+  CMPS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   return CMPS_OK;
 }
 
 int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
   if (H.low_canonical) {
-    CMPS_TRY(apply_canonical32(H, 0, in, out, st));
+    if (H.ctc)
+      CMPS_TRY(apply_canonical_tc(H, 0, in, out, st));
+    else
+      CMPS_TRY(apply_canonical32(H, 0, in, out, st));
     return H.add_projectors(in, out, st);
   }
   SplitState* S = H.split;
-  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
+  if (!S) return fail(CMPS_ERR_STATE, "split-precision operands not prepared");
   CMPS_TRY(split_theta(*S, in, st));
   CMPS_TRY(launch_stage(*S, 1, out, st));
   CMPS_TRY(launch_stage(*S, 2, out, st));
@@ -777,22 +781,23 @@ int apply_split_async(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
 
 // theta-space matvec in split precision: FP64 planar in -> FP64 planar out.
 int apply_split(Heff& H, const Planar& in, Planar& out, cudaStream_t st) {
-  if (H.low_canonical) return apply_split_async(H, in, out, st);
+  int *d_err, *h_err;
+  if (!error_words(H, &d_err, &h_err)) return apply_split_async(H, in, out, st);
   CMPS_TRY(split_reset_error(H, st));
   CMPS_TRY(apply_split_async(H, in, out, st));
-  SplitState* S = H.split;
-  CMPS_CUDA(cudaMemcpyAsync(S->h_err, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CMPS_CUDA(cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CMPS_CUDA(cudaStreamSynchronize(st));
-  if (*S->h_err) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(*S->h_err) + ")");
+  if (*h_err) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(*h_err) + ")");
   return CMPS_OK;
 }
 
 int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStream_t st) {
-  if (H.low_canonical) return apply_canonical32(H, which, in, out, st);
+  if (H.low_canonical && !H.ctc) return apply_canonical32(H, which, in, out, st);
+  if (which == 1) CMPS_TRY(split_reset_error(H, st));
+  if (H.ctc) return apply_canonical_tc(H, which, in, out, st);
   SplitState* S = H.split;
-  if (!S) return fail(CMPS_ERR_STATE, "split-TF32 operands not prepared");
+  if (!S) return fail(CMPS_ERR_STATE, "split-precision operands not prepared");
   if (which == 1) {
-    CMPS_CUDA(cudaMemsetAsync(S->d_err, 0, sizeof(int), st));
     CMPS_TRY(split_theta(*S, in, st));
     return launch_stage(*S, 1, out, st);
   }
@@ -800,11 +805,10 @@ int apply_split_stage(Heff& H, int which, const Planar& in, Planar& out, cudaStr
 }
 
 int split_error(Heff& H) {
-  if (H.low_canonical) return CMPS_OK;
-  SplitState* S = H.split;
-  if (!S) return CMPS_OK;
+  int *d_err, *h_err;
+  if (!error_words(H, &d_err, &h_err)) return CMPS_OK;
   int e = 0;
-  CMPS_TRY(copy_wait(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost, H.ctx->stream));
+  CMPS_TRY(copy_wait(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, H.ctx->stream));
   if (e) return fail(CMPS_ERR_CUDA, "tcgen05 pipeline wait timed out (code " + std::to_string(e) + ")");
   return CMPS_OK;
 }

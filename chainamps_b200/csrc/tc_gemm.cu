@@ -174,6 +174,25 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t 
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
+// tcgen05.ld of 16 columns without the wait: the registers are written
+// asynchronously and may be read only after tmem_wait(r) on them
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+// wait for the outstanding tcgen05.ld; the registers pass through the asm so
+// that no read of them moves above the wait
+__device__ __forceinline__ void tmem_wait(uint32_t* a, uint32_t* b) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  asm volatile("" : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]),
+               "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]), "+r"(a[12]), "+r"(a[13]), "+r"(a[14]), "+r"(a[15]));
+  asm volatile("" : "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]), "+r"(b[7]),
+               "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]), "+r"(b[14]), "+r"(b[15]));
+}
+
 template <int MODE>
 __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   if (bf16_mode<MODE>())
@@ -277,7 +296,7 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
             // B: the task's b_rows-row box; both four planes
             const uint32_t bbytes = 4u * 64u * (uint32_t)tile.b_rows;
             mbar_expect_tx(&full[s], (tma_a<MODE>() ? (uint32_t)kOperandBytes : 0u) + bbytes);
-            if (tma_a<MODE>()) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0, 0, &full[s]);
+            if (tma_a<MODE>()) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0 + tm.a_y0, 0, &full[s]);
             tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
           }
         }
@@ -504,11 +523,27 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
       // mode 3: the warps of a quadrant take 16-column chunks in turn
       const int c_first = 16 * ((warp - 2) / 4);
       const int c_step = 16 * epi_per_quad<MODE>();
+      // TMEM loads run one chunk ahead: chunk c + c_step is in flight while
+      // chunk c is stored (every lane issues and waits; tcgen05.ld is
+      // warp-collective, so the row check comes after)
+      uint32_t ra[16], ia[16];
+      if (have && c_first < nmma) {
+        tmem_ld16_issue(tbase + c_first, ra);
+        tmem_ld16_issue(tbase + 128 + c_first, ia);
+      }
       for (int c = c_first; c < nmma; c += c_step) {
         float vr[16], vi[16];
         if (have) {
-          tmem_ld16(tbase + c, vr);
-          tmem_ld16(tbase + 128 + c, vi);
+          tmem_wait(ra, ia);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            vr[i] = __uint_as_float(ra[i]);
+            vi[i] = __uint_as_float(ia[i]);
+          }
+          if (c + c_step < nmma) {
+            tmem_ld16_issue(tbase + c + c_step, ra);
+            tmem_ld16_issue(tbase + 128 + c + c_step, ia);
+          }
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;

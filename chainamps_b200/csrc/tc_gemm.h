@@ -26,9 +26,12 @@ struct TcTask {
   int32_t seg_n0[4];
   int64_t seg_off[4];
 };
-// One K-concatenated term: A tile at (a_x0 + k, row) of map a_map, B tile at (k, row) of b_map.
+// One K-concatenated term: A tile at (a_x0 + k, a_y0 + row) of map a_map, B
+// tile at (k, row) of b_map.  a_y0 (a row offset into the A map) applies to A
+// tiles loaded by TMA only.
 struct TcTerm {
   int32_t a_map, b_map, a_x0, k;
+  int32_t a_y0;
 };
 // A operand read by the converter warps (mode 2): element (i, j) of the block
 // at off + i * ld + j in each of two FP32 planes (re, im); rows x cols.
@@ -63,6 +66,19 @@ struct TcPlan {
 };
 
 int smem_bytes();
+// 3-D tensor map (K, rows, 4 planes) over one operand block of FP32 or BF16
+// elements at `base` (plane 0), planes `plane` elements apart, rows `ld`
+// elements apart; the block must fit in `room` elements from base.  Box: 64
+// bytes of K by box_rows rows by the four planes, 64-byte swizzle.
+int encode_map(bool bf16, const void* base, int64_t K, int64_t rows, int64_t ld, int64_t plane, int64_t room,
+               int box_rows, CUtensorMap* out);
+// Tiles of a task of m x n outputs, 128 x 128 each (row-major over the task).
+void add_tiles(TcPlan& p, int32_t task, int32_t m, int32_t n);
+// Completes a plan built term by term: k-steps per tile, optionally the
+// heaviest tiles first, and checks every term, task, segment list and tile.
+// by_tma: the A operands are tensor maps (else converter descriptors);
+// b_rows: the row count each B map was encoded with.
+int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first);
 // K columns of one k-step: a 64-byte shared-memory row of 16 TF32 or 32 BF16
 inline int32_t kstep(bool bf16) { return bf16 ? 32 : 16; }
 // mode 1: A and B by TMA (four TF32 planes each); FP32 output in two planes

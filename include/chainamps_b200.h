@@ -56,6 +56,18 @@ enum {
   CMPS_ORDER_CANONICAL = 2
 };
 
+/* Form of a handle's split-precision operator (cmps_heff_split_form).  The
+ * canonical order is taken when it executes at most a quarter of the folded
+ * order's flops; split BF16 runs it on tcgen05 (whole vectors only; a
+ * sharded or windowed handle, split TF32, or a device without room for the
+ * BF16 intermediates runs it in FP32). */
+enum {
+  CMPS_FORM_NONE = 0,            /* FP64 handle: no split operator */
+  CMPS_FORM_FOLDED_TC = 1,       /* folded order, two tcgen05 stages */
+  CMPS_FORM_CANONICAL_FP32 = 2,  /* canonical order, four FP32 FMA stages */
+  CMPS_FORM_CANONICAL_TC = 3     /* canonical order, four tcgen05 split-BF16 stages */
+};
+
 typedef struct cmps_context cmps_context;
 typedef struct cmps_heff cmps_heff;
 typedef struct cmps_svd cmps_svd;
@@ -151,6 +163,8 @@ int cmps_heff_set_order(cmps_heff* h, int order);
 /* The order in use (CMPS_ORDER_FOLDED or _CANONICAL) and the flops each
  * order executes per FP64 matvec; any output may be NULL. */
 int cmps_heff_order(const cmps_heff* h, int* active, double* executed_folded, double* executed_canonical);
+/* The form of the split operator the handle's precision runs (CMPS_FORM_*). */
+int cmps_heff_split_form(const cmps_heff* h, int* form);
 /* H_eff matvec that allocates nothing (no counterpart in the reference).
  * For callers that cannot call cudaMalloc when they apply H_eff: an
  * eigensolver callback (ARPACK's MV, called hundreds of times per step)

@@ -57,22 +57,23 @@ def test_xxz_idmrg_chi100_matches_oracle(ctx, precision):
     run.close()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bf16"])
 def test_coupled_ising_idmrg_matches_oracle(ctx, precision):
     """The north star's model as benchmarked: coupled transverse-field Ising
     chains, each vertex the periodic 12-site chain at g = 1.2 cut to its 64
     lowest states (Z2 parity), J_perp = 0.05 sum_i X_i X_i, MPO D = 26;
     iDMRG at chi = 32 for 5 steps against the oracle's rows (canonical-order
     block port; ``coupled_ising_12x64_chi32`` in oracle_configs.json).  The
-    device takes the canonical contraction order for this vertex.  Energies
+    device takes the canonical contraction order for this vertex: in FP32
+    under split TF32, on tcgen05 under split BF16.  Energies
     1e-9 relative, entropies 1e-8, kept bond dimension exact, truncation
     weights 1e-12 absolute or 1e-4 relative, fidelities 1e-7, kept singular
     values 1e-7."""
-    from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32
+    from chainamps_b200 import iDMRG, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_SPLIT_BF16
     from tests.helpers import ising_mpo
     ref = json.load(open(GOLD))["coupled_ising_12x64_chi32"]
     H = ising_mpo(12, 64)
-    prec = CMPS_FP64 if precision == "fp64" else CMPS_SPLIT_TF32
+    prec = {"fp64": CMPS_FP64, "mixed": CMPS_SPLIT_TF32, "mixed_bf16": CMPS_SPLIT_BF16}[precision]
     run = iDMRG(ctx, H.rules, to_tensor(H), precision=prec, tol=1e-12, krylov_dim=32)
     for step, e in enumerate(ref["rows"]):
         r = run.grow(ref["chi"], ref["trunc"])
