@@ -264,43 +264,19 @@ int build_canonical_tc(Heff& H) {
   }
   if (xb.size() > 65535) return fail(CMPS_ERR_ARG, "canonical tcgen05 form: too many theta blocks");
   T->n_xin = (int)xb.size();
-  // ---- B operand blocks: R^T (b2, t), W (bl, br, ci, co), L (b0, s) ----
-  std::map<std::array<int, 2>, int64_t> roff, loff;
-  std::map<Key4, int64_t> woff;
-  std::vector<SplitBlock> rsb, lsb, wsb;
-  std::vector<double> wre, wim;  // dense W blocks, contiguous [n_out][n_in]
-  for (const Key4& z : zset) {
-    const int b2 = z[0], t = csec[z[1]][z[3]];
-    if (roff.count({b2, t})) continue;
-    const int tp = H.R.partner[(size_t)b2 * ns2 + t];
-    roff[{b2, t}] = T->ops_len;
-    // stored [a2][a2'] (dim t x dim t'); wanted [a2'][a2], ld pad8(dim t)
-    rsb.push_back(SplitBlock{H.R.off[(size_t)b2 * ns2 + t], T->ops_len, (int32_t)A2.sdim[t], (int32_t)A2.sdim[tp],
-                             (int32_t)pad8(A2.sdim[t]), 1});
-    T->ops_len += align64(A2.sdim[tp] * pad8(A2.sdim[t]));
-  }
+  // ---- MPO class blocks on the host, dense [n_out][n_in], one after another ----
+  std::map<Key4, int64_t> wsrc;
+  std::vector<double> wre, wim;
   for (auto& wk : wblk) {
     const int ci = wk.first[2], co = wk.first[3];
-    woff[wk.first] = T->ops_len;
     const int64_t src = (int64_t)wre.size();
+    wsrc[wk.first] = src;
     wre.resize(src + ncl(co) * ncl(ci), 0.0);
     wim.resize(src + ncl(co) * ncl(ci), 0.0);
     for (auto& e : wk.second) {
       wre[(size_t)(src + e.first)] += e.second.first;
       wim[(size_t)(src + e.first)] += e.second.second;
     }
-    wsb.push_back(SplitBlock{src, T->ops_len, (int32_t)ncl(co), (int32_t)ncl(ci), (int32_t)pad8(ncl(ci)), 0});
-    T->ops_len += align64(ncl(co) * pad8(ncl(ci)));
-  }
-  for (auto& kv : v_alpha) {
-    const int b0 = kv.first.b0, s = kv.second;
-    if (loff.count({b0, s})) continue;
-    const int sp = H.L.partner[(size_t)b0 * ns0 + s];
-    loff[{b0, s}] = T->ops_len;
-    // stored [a0'][a0] (dim s' x dim s), kept as is with ld pad8(dim s)
-    lsb.push_back(SplitBlock{H.L.off[(size_t)b0 * ns0 + s], T->ops_len, (int32_t)A0.sdim[sp], (int32_t)A0.sdim[s],
-                             (int32_t)pad8(A0.sdim[s]), 0});
-    T->ops_len += align64(A0.sdim[sp] * pad8(A0.sdim[s]));
   }
   // ---- intermediates ----
   struct ZInfo {
@@ -370,6 +346,193 @@ int build_canonical_tc(Heff& H) {
   T->zv_len = std::max<int64_t>(64, std::max(z_len, v_len));
   T->y_len = std::max<int64_t>(64, y_len);
   T->xin_len = std::max<int64_t>(64, T->xin_len);
+
+  // ---- the stages as raw tasks: output run, A blocks, B source blocks ----
+  // A: (buffer 0 Theta_in / 1 Z,V / 2 Y, block offset, K, rows, ld), one map
+  // per A block and plan.  B: a block of the R environment (transposed), the
+  // L environment or the host-built MPO blocks.
+  enum { kSrcR = 0, kSrcL = 1, kSrcW = 2 };
+  struct BSrc {
+    int src;
+    int64_t off;
+    int32_t rows, cols, transpose;  // source block rows x cols, row-major
+    int32_t n() const { return transpose ? cols : rows; }  // B rows (the task's N)
+  };
+  struct RawTerm {
+    std::array<int64_t, 5> a;  // A block: buffer, offset, K, rows, ld
+    int32_t a_y0;
+    BSrc b;
+  };
+  struct RawTask {
+    int64_t out_off, col_stride, group;
+    int32_t m, n;
+    std::vector<RawTerm> terms;
+  };
+  std::vector<RawTask> rawR, rawW2, rawW1, rawL;
+  for (const Key4& z : zset) {
+    const int b2 = z[0], m = z[1], c1 = z[2], c2 = z[3];
+    const ZInfo& zi = zinfo.at(z);
+    const int t = csec[m][c2];
+    const int64_t d2 = A2.sdim[t];
+    RawTask rt{zi.off, zi.rows, (int64_t)(m * ncls + c1) * ncls + c2, (int32_t)zi.rows, zi.n, {}};
+    // R^{b2} stored [a2][a2'] (dim t x dim t'), used as [a2'][a2]
+    rt.terms.push_back(RawTerm{{0, xoff.at({m, c1, c2}), d2, zi.rows, pad8(d2)}, 0,
+                               BSrc{kSrcR, H.R.off[(size_t)b2 * ns2 + t], (int32_t)d2, zi.n, 1}});
+    rawR.push_back(std::move(rt));
+  }
+  for (auto& kv : yinfo) {
+    const Key4& yk = kv.first;
+    const YInfo& yi = kv.second;
+    RawTask rt{yi.off, yi.rows, (int64_t)yk[1] * ncls + yk[2], (int32_t)yi.rows, yi.n, {}};
+    for (auto& tm : yi.terms) {
+      const ZInfo& zi = zinfo.at(tm.first);
+      const int64_t n2 = ncl(tm.first[3]);
+      if (zi.rows / pad8(n2) * zi.n != yi.rows) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: W2 row mismatch");
+      rt.terms.push_back(RawTerm{{1, zi.off, n2, yi.rows, pad8(n2)}, 0,
+                                 BSrc{kSrcW, wsrc.at(tm.second), yi.n, (int32_t)n2, 0}});
+    }
+    rawW2.push_back(std::move(rt));
+  }
+  for (auto& kv : vinfo) {
+    const VKey& v = kv.first;
+    const VInfo& vi = kv.second;
+    RawTask rt{vi.off, vi.rows, (int64_t)v.mpp * ncls + v.c2p, (int32_t)vi.rows, vi.n, {}};
+    for (auto& tm : vi.terms) {
+      const YInfo& yi = yinfo.at(tm.first);
+      const int64_t n1 = ncl(tm.first[2]);
+      if (yi.rows / pad8(n1) * yi.n != vi.rows) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: W1 row mismatch");
+      rt.terms.push_back(RawTerm{{2, yi.off, n1, vi.rows, pad8(n1)}, 0,
+                                 BSrc{kSrcW, wsrc.at(tm.second), vi.n, (int32_t)n1, 0}});
+    }
+    rawW1.push_back(std::move(rt));
+  }
+  for (int mpp = 0; mpp < nm; ++mpp)
+    for (int c1p = 0; c1p < ncls; ++c1p) {
+      if (rcoff[mpp][c1p] < 0) continue;
+      const int64_t d0o = rcdim[mpp][c1p];  // a0' dim = N
+      for (int c2p = 0; c2p < ncls; ++c2p) {
+        if (ccoff[mpp][c2p] < 0) continue;
+        const int64_t run = ncl(c2p) * ccdim[mpp][c2p];  // (s2', a2') per s1' = M
+        for (int64_t pos = 0; pos < ncl(c1p); ++pos) {
+          RawTask rt{H.out_base[mpp] + (rcoff[mpp][c1p] + pos * d0o) * th.ncols[mpp] + ccoff[mpp][c2p],
+                     th.ncols[mpp], 0, (int32_t)run, (int32_t)d0o, {}};
+          for (int b0 = 0; b0 < H.D; ++b0) {
+            auto vit = vinfo.find(VKey{b0, mpp, c1p, c2p});
+            if (vit == vinfo.end()) continue;
+            const VInfo& vi = vit->second;
+            const int64_t d0 = A0.sdim[vi.alpha];
+            if (vi.rows != run * pad8(d0) || vi.n != ncl(c1p))
+              return fail(CMPS_ERR_STATE, "canonical tcgen05 form: L row mismatch");
+            // L^{b0} stored [a0'][a0] (dim a0' x dim a0), used as is
+            rt.terms.push_back(RawTerm{{1, vi.off, d0, vi.n * run, pad8(d0)}, (int32_t)(pos * run),
+                                       BSrc{kSrcL, H.L.off[(size_t)b0 * ns0 + vi.alpha], (int32_t)d0o, (int32_t)d0, 0}});
+          }
+          // a task without terms writes zeros; its run inside the output window
+          if (rt.out_off < 0 || rt.out_off + (rt.m - 1) + (int64_t)(rt.n - 1) * rt.col_stride >= H.out_len)
+            return fail(CMPS_ERR_STATE, "canonical tcgen05 form: output outside theta");
+          rawL.push_back(std::move(rt));
+        }
+      }
+    }
+
+  // ---- fusion: tasks with the same A blocks (the same rows, the same K
+  // list) become one task of up to four column segments and N <= 128, its
+  // B operand the members' B blocks stacked along N.  The MPO stages gain
+  // most: on a chain vertex every bond but one reads a single block. ----
+  struct FTerm {
+    std::array<int64_t, 5> a;
+    int32_t a_y0;
+    int64_t b_off;  // B block in ops, [N][pad8(K)]
+  };
+  struct FTask {
+    int64_t group, col_stride;
+    int32_t m, n, nseg;
+    int32_t seg_n0[4];
+    int64_t seg_off[4];
+    std::vector<FTerm> terms;
+  };
+  std::vector<SplitBlock> sb[3];
+  std::map<std::array<int64_t, 4>, int64_t> bdedup;  // (src, off, transpose, K) of a lone block -> ops offset
+  auto b_block = [&](const BSrc& b, int64_t dst, int64_t ld) {
+    sb[b.src].push_back(SplitBlock{b.off, dst, b.rows, b.cols, (int32_t)ld, b.transpose});
+  };
+  auto fuse = [&](std::vector<RawTask>& raw, bool allow, std::vector<FTask>& out) -> int {
+    std::map<std::vector<int64_t>, std::vector<size_t>> bysig;
+    std::vector<const std::vector<int64_t>*> order;
+    for (size_t i = 0; i < raw.size(); ++i) {
+      std::vector<int64_t> sig{raw[i].m, raw[i].group};
+      for (const RawTerm& t : raw[i].terms) {
+        sig.insert(sig.end(), t.a.begin(), t.a.end());
+        sig.push_back(t.a_y0);
+      }
+      if (!allow) sig.push_back((int64_t)i);
+      auto it = bysig.find(sig);
+      if (it == bysig.end()) {
+        it = bysig.emplace(sig, std::vector<size_t>()).first;
+        order.push_back(&it->first);
+      }
+      it->second.push_back(i);
+    }
+    for (const std::vector<int64_t>* sig : order) {
+      const std::vector<size_t>& mem = bysig.at(*sig);
+      size_t i = 0;
+      while (i < mem.size()) {
+        // members of this task: consecutive ones while N <= 128 and <= 4 segments
+        std::vector<size_t> part{mem[i++]};
+        int32_t ntot = raw[part[0]].n;
+        while (i < mem.size() && raw[part[0]].n <= 64 && raw[mem[i]].n <= 64 && part.size() < 4 &&
+               ntot + raw[mem[i]].n <= 128) {
+          ntot += raw[mem[i]].n;
+          part.push_back(mem[i++]);
+        }
+        const RawTask& r0 = raw[part[0]];
+        FTask f{r0.group, r0.col_stride, r0.m, ntot, (int32_t)part.size(), {}, {}, {}};
+        int32_t col = 0;
+        for (int q = 0; q < 4; ++q) {
+          f.seg_n0[q] = q < f.nseg ? col : 0x7fffffff;
+          f.seg_off[q] = q < f.nseg ? raw[part[q]].out_off : 0;
+          if (q < f.nseg) {
+            if (raw[part[q]].col_stride != f.col_stride) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: fusion");
+            col += raw[part[q]].n;
+          }
+        }
+        for (size_t q = 0; q < r0.terms.size(); ++q) {
+          const int64_t K = r0.terms[q].a[2], ld = pad8(K);
+          int64_t off;
+          if (part.size() == 1) {
+            const BSrc& b = r0.terms[q].b;
+            const std::array<int64_t, 4> key{b.src, b.off, b.transpose, K};
+            auto it = bdedup.find(key);
+            if (it != bdedup.end()) {
+              off = it->second;
+            } else {
+              off = T->ops_len;
+              b_block(b, off, ld);
+              T->ops_len += align64((int64_t)b.n() * ld);
+              bdedup[key] = off;
+            }
+          } else {
+            off = T->ops_len;
+            int64_t row = 0;
+            for (size_t s : part) {
+              const BSrc& b = raw[s].terms[q].b;
+              b_block(b, off + row * ld, ld);
+              row += b.n();
+            }
+            T->ops_len += align64(ntot * ld);
+          }
+          f.terms.push_back(FTerm{r0.terms[q].a, r0.terms[q].a_y0, off});
+        }
+        out.push_back(std::move(f));
+      }
+    }
+    return CMPS_OK;
+  };
+  std::vector<FTask> fR, fW2, fW1, fL;
+  CMPS_TRY(fuse(rawR, true, fR));
+  CMPS_TRY(fuse(rawW2, true, fW2));
+  CMPS_TRY(fuse(rawW1, true, fW1));
+  CMPS_TRY(fuse(rawL, false, fL));
   T->ops_len = std::max<int64_t>(64, T->ops_len);
 
   // ---- device buffers: the intermediates inside the FP64 canonical ones
@@ -408,9 +571,14 @@ int build_canonical_tc(Heff& H) {
       CMPS_TRY(copy_wait(wdev.im(), wim.data(), sizeof(double) * wim.size(), cudaMemcpyHostToDevice, st));
     }
     for (int pass = 0; pass < 3; ++pass) {
-      const std::vector<SplitBlock>& v = pass == 0 ? rsb : pass == 1 ? lsb : wsb;
-      const Planar& src = pass == 0 ? H.R.data : pass == 1 ? H.L.data : wdev;
+      const std::vector<SplitBlock>& v = sb[pass];
+      const Planar& src = pass == kSrcR ? H.R.data : pass == kSrcL ? H.L.data : wdev;
       if (v.empty()) continue;
+      for (const SplitBlock& b : v)
+        if (b.src_off < 0 || b.src_off + (int64_t)b.rows * b.cols > src.len || b.dst_off < 0 ||
+            b.dst_off + (int64_t)((b.transpose ? b.cols : b.rows) - 1) * b.ld_dst + (b.transpose ? b.rows : b.cols) >
+                T->ops_len)
+          return fail(CMPS_ERR_STATE, "canonical tcgen05 form: operand block outside its buffer");
       SplitBlock* d = nullptr;
       CMPS_CUDA(dmalloc(&d, sizeof(SplitBlock) * v.size()));
       int rc = copy_wait(d, v.data(), sizeof(SplitBlock) * v.size(), cudaMemcpyHostToDevice, st);
@@ -423,241 +591,94 @@ int build_canonical_tc(Heff& H) {
       if (rc != CMPS_OK) return rc;
     }
   }
-  // ---- plans ----
-  std::map<std::pair<int64_t, int>, int32_t> bmap_of;  // (ops offset, K) -> B map index, per plan
-  std::vector<int32_t> brows;
-  auto bmap = [&](tc::TcPlan& p, int64_t off, int64_t K, int64_t rows, int64_t ld, int32_t* out) -> int {
-    auto it = bmap_of.find({off, (int)K});
-    if (it != bmap_of.end()) {
-      *out = it->second;
-      return CMPS_OK;
-    }
-    CUtensorMap cm;
-    CMPS_TRY(tc::encode_map(true, T->ops + off, K, rows, ld, T->ops_len, T->ops_len - off,
-                            tc::b_box_rows((int32_t)rows), &cm));
-    *out = (int32_t)p.bmaps.size();
-    p.bmaps.push_back(cm);
-    brows.push_back((int32_t)rows);
-    bmap_of[{off, (int)K}] = *out;
-    return CMPS_OK;
-  };
-  auto amap = [&](tc::TcPlan& p, const uint16_t* buf, int64_t plane, int64_t off, int64_t K, int64_t rows, int64_t ld,
-                  int32_t* out) -> int {
-    CUtensorMap cm;
-    CMPS_TRY(tc::encode_map(true, buf + off, K, rows, ld, plane, plane - off, 128, &cm));
-    *out = (int32_t)p.amaps.size();
-    p.amaps.push_back(cm);
-    return CMPS_OK;
-  };
-  auto one_segment = [](tc::TcTask& t, int64_t off) {
-    t.out_off = off;
-    t.nseg = 1;
-    t.seg_n0[0] = 0;
-    t.seg_off[0] = off;
-    for (int q = 1; q < 4; ++q) {
-      t.seg_n0[q] = 0x7fffffff;
-      t.seg_off[q] = 0;
-    }
-  };
-  // Tiles of a group of tasks that read the same A rows: row tile by row
-  // tile across the group, so the tiles that run at the same time (dealt
-  // round-robin to the SMs) share their A tiles in L2.
-  auto group_tiles = [](tc::TcPlan& p, const std::vector<int32_t>& group) {
-    int32_t mmax = 0;
-    for (int32_t t : group) mmax = std::max(mmax, p.tasks[t].m);
-    for (int32_t m0 = 0; m0 < mmax; m0 += 128)
-      for (int32_t t : group) {
-        const tc::TcTask& k = p.tasks[t];
-        if (m0 >= k.m) continue;
-        for (int32_t n0 = 0; n0 < k.n; n0 += 128)
-          p.tiles.push_back(tc::TcTile{t, m0, n0, tc::b_box_rows(k.n), 0, ((std::min(128, k.n - n0)) + 15) & ~15});
-      }
-  };
-  auto term_flops = [](const tc::TcTask& t, int64_t k) { return 8.0 * t.m * (double)t.n * k; };
-
-  // stage R: Z^{b2}_{m,c1,c2}[a2'][rows] = Theta_in[rows][a2] . R^T[a2'][a2]
-  {
-    tc::TcPlan& p = T->pR;
-    bmap_of.clear();
-    brows.clear();
-    std::map<std::array<int, 3>, int32_t> xa;
-    std::map<std::array<int, 3>, std::vector<int32_t>> groups;
-    for (const Key4& z : zset) {
-      const int b2 = z[0], m = z[1], c1 = z[2], c2 = z[3];
-      const ZInfo& zi = zinfo.at(z);
-      const int t = csec[m][c2];
-      const int64_t d2 = A2.sdim[t];
-      auto it = xa.find({m, c1, c2});
-      int32_t a;
-      if (it == xa.end()) {
-        CMPS_TRY(amap(p, T->xin, T->xin_len, xoff.at({m, c1, c2}), d2, zi.rows, pad8(d2), &a));
-        xa[{m, c1, c2}] = a;
-      } else {
-        a = it->second;
-      }
-      int32_t b;
-      CMPS_TRY(bmap(p, roff.at({b2, t}), d2, zi.n, pad8(d2), &b));
+  // ---- plans: tensor maps, tasks, tiles ----
+  const uint16_t* abuf[3] = {T->xin, T->zv, T->y};
+  const int64_t alen[3] = {T->xin_len, T->zv_len, T->y_len};
+  auto build_plan = [&](tc::TcPlan& p, std::vector<FTask>& ft, bool grouped, const uint16_t* out,
+                        int64_t out_len) -> int {
+    std::map<std::array<int64_t, 5>, int32_t> amaps;
+    std::map<std::array<int64_t, 3>, int32_t> bmaps;  // (ops offset, K, rows)
+    std::vector<int32_t> brows;
+    std::map<int64_t, std::vector<int32_t>> groups;
+    for (const FTask& f : ft) {
       tc::TcTask task{};
-      one_segment(task, zi.off);
+      task.out_off = f.seg_off[0];
       task.row_stride = 1;
-      task.col_stride = zi.rows;
-      task.m = (int32_t)zi.rows;
-      task.n = zi.n;
+      task.col_stride = f.col_stride;
+      task.m = f.m;
+      task.n = f.n;
+      task.nseg = f.nseg;
+      for (int q = 0; q < 4; ++q) {
+        task.seg_n0[q] = f.seg_n0[q];
+        task.seg_off[q] = f.seg_off[q];
+      }
+      // every segment's run inside the output buffer
+      for (int q = 0; q < f.nseg; ++q) {
+        const int32_t nq = (q + 1 < f.nseg ? f.seg_n0[q + 1] : f.n) - f.seg_n0[q];
+        if (f.seg_off[q] < 0 || f.seg_off[q] + (f.m - 1) + (int64_t)(nq - 1) * f.col_stride >= out_len)
+          return fail(CMPS_ERR_STATE, "canonical tcgen05 form: output outside its buffer");
+      }
       task.t0 = (int32_t)p.terms.size();
-      p.terms.push_back(tc::TcTerm{a, b, 0, (int32_t)d2});
-      task.t1 = (int32_t)p.terms.size();
-      T->flops += term_flops(task, d2);
-      groups[{m, c1, c2}].push_back((int32_t)p.tasks.size());
-      p.tasks.push_back(task);
-    }
-    for (auto& g : groups) group_tiles(p, g.second);
-    CMPS_TRY(tc::finish_plan(p, true, true, brows, false));
-  }
-  // stage W2: Y^{b1}_{m,c1,c2'}[s2'][rows] = sum Z^{b2}_{m,c1,c2}[rows][s2] . W[s2'][s2]
-  {
-    tc::TcPlan& p = T->pW2;
-    bmap_of.clear();
-    brows.clear();
-    std::map<Key4, int32_t> za;
-    std::map<std::pair<int, int>, std::vector<int32_t>> groups;
-    for (auto& kv : yinfo) {
-      const Key4& yk = kv.first;
-      const YInfo& yi = kv.second;
-      tc::TcTask task{};
-      one_segment(task, yi.off);
-      task.row_stride = 1;
-      task.col_stride = yi.rows;
-      task.m = (int32_t)yi.rows;
-      task.n = yi.n;
-      task.t0 = (int32_t)p.terms.size();
-      for (auto& tm : yi.terms) {
-        const Key4& zk = tm.first;
-        const ZInfo& zi = zinfo.at(zk);
-        const int64_t n2 = ncl(zk[3]);
-        if (zi.rows / pad8(n2) * zi.n != yi.rows) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: W2 row mismatch");
-        int32_t a;
-        auto it = za.find(zk);
-        if (it == za.end()) {
-          CMPS_TRY(amap(p, T->zv, T->zv_len, zi.off, n2, yi.rows, pad8(n2), &a));
-          za[zk] = a;
+      for (const FTerm& t : f.terms) {
+        int32_t a, b;
+        auto ia = amaps.find(t.a);
+        if (ia != amaps.end()) {
+          a = ia->second;
         } else {
-          a = it->second;
+          const int buf = (int)t.a[0];
+          CUtensorMap cm;
+          CMPS_TRY(tc::encode_map(true, abuf[buf] + t.a[1], t.a[2], t.a[3], t.a[4], alen[buf], alen[buf] - t.a[1], 128,
+                                  &cm));
+          a = (int32_t)p.amaps.size();
+          p.amaps.push_back(cm);
+          amaps[t.a] = a;
         }
-        int32_t b;
-        CMPS_TRY(bmap(p, woff.at(tm.second), n2, yi.n, pad8(n2), &b));
-        p.terms.push_back(tc::TcTerm{a, b, 0, (int32_t)n2});
-        T->flops += term_flops(task, n2);
-      }
-      task.t1 = (int32_t)p.terms.size();
-      groups[{yk[1], yk[2]}].push_back((int32_t)p.tasks.size());
-      p.tasks.push_back(task);
-    }
-    for (auto& g : groups) group_tiles(p, g.second);
-    CMPS_TRY(tc::finish_plan(p, true, true, brows, false));
-  }
-  // stage W1: V^{b0}_{m'',c1',c2'}[s1'][rows] = sum Y^{b1}_{m,c1,c2'}[rows][s1] . W[s1'][s1]
-  {
-    tc::TcPlan& p = T->pW1;
-    bmap_of.clear();
-    brows.clear();
-    std::map<Key4, int32_t> ya;
-    std::map<std::pair<int, int>, std::vector<int32_t>> groups;
-    for (auto& kv : vinfo) {
-      const VKey& v = kv.first;
-      const VInfo& vi = kv.second;
-      tc::TcTask task{};
-      one_segment(task, vi.off);
-      task.row_stride = 1;
-      task.col_stride = vi.rows;
-      task.m = (int32_t)vi.rows;
-      task.n = vi.n;
-      task.t0 = (int32_t)p.terms.size();
-      for (auto& tm : vi.terms) {
-        const Key4& yk = tm.first;
-        const YInfo& yi = yinfo.at(yk);
-        const int64_t n1 = ncl(yk[2]);
-        if (yi.rows / pad8(n1) * yi.n != vi.rows) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: W1 row mismatch");
-        int32_t a;
-        auto it = ya.find(yk);
-        if (it == ya.end()) {
-          CMPS_TRY(amap(p, T->y, T->y_len, yi.off, n1, vi.rows, pad8(n1), &a));
-          ya[yk] = a;
+        const std::array<int64_t, 3> bk{t.b_off, t.a[2], f.n};
+        auto ib = bmaps.find(bk);
+        if (ib != bmaps.end()) {
+          b = ib->second;
         } else {
-          a = it->second;
+          CUtensorMap cm;
+          CMPS_TRY(tc::encode_map(true, T->ops + t.b_off, t.a[2], f.n, pad8(t.a[2]), T->ops_len, T->ops_len - t.b_off,
+                                  tc::b_box_rows(f.n), &cm));
+          b = (int32_t)p.bmaps.size();
+          p.bmaps.push_back(cm);
+          brows.push_back(f.n);
+          bmaps[bk] = b;
         }
-        int32_t b;
-        CMPS_TRY(bmap(p, woff.at(tm.second), n1, vi.n, pad8(n1), &b));
-        p.terms.push_back(tc::TcTerm{a, b, 0, (int32_t)n1});
-        T->flops += term_flops(task, n1);
+        tc::TcTerm tm{a, b, 0, (int32_t)t.a[2]};
+        tm.a_y0 = t.a_y0;
+        p.terms.push_back(tm);
+        T->flops += 8.0 * f.m * (double)f.n * t.a[2];
       }
       task.t1 = (int32_t)p.terms.size();
-      groups[{v.mpp, v.c2p}].push_back((int32_t)p.tasks.size());
+      if (grouped)
+        groups[f.group].push_back((int32_t)p.tasks.size());
+      else
+        tc::add_tiles(p, (int32_t)p.tasks.size(), task.m, task.n);
       p.tasks.push_back(task);
     }
-    for (auto& g : groups) group_tiles(p, g.second);
-    CMPS_TRY(tc::finish_plan(p, true, true, brows, false));
-  }
-  // stage L: Theta'_{m''}[(s1', a0')][(s2', a2')] = sum_b0 V^{b0}[s1'][(s2', a2')][a0] . L^{b0}[a0'][a0]
-  {
-    tc::TcPlan& p = T->pL;
-    bmap_of.clear();
-    brows.clear();
-    std::map<VKey, int32_t> va;
-    for (int mpp = 0; mpp < nm; ++mpp)
-      for (int c1p = 0; c1p < ncls; ++c1p) {
-        if (rcoff[mpp][c1p] < 0) continue;
-        const int64_t d0o = rcdim[mpp][c1p];  // a0' dim = N
-        for (int c2p = 0; c2p < ncls; ++c2p) {
-          if (ccoff[mpp][c2p] < 0) continue;
-          const int64_t run = ncl(c2p) * ccdim[mpp][c2p];  // (s2', a2') per s1' = M
-          for (int64_t pos = 0; pos < ncl(c1p); ++pos) {
-            tc::TcTask task{};
-            one_segment(task, H.out_base[mpp] + (rcoff[mpp][c1p] + pos * d0o) * th.ncols[mpp] + ccoff[mpp][c2p]);
-            task.row_stride = 1;
-            task.col_stride = th.ncols[mpp];
-            task.m = (int32_t)run;
-            task.n = (int32_t)d0o;
-            task.t0 = (int32_t)p.terms.size();
-            for (int b0 = 0; b0 < H.D; ++b0) {
-              const VKey vk{b0, mpp, c1p, c2p};
-              auto vit = vinfo.find(vk);
-              if (vit == vinfo.end()) continue;
-              const VInfo& vi = vit->second;
-              const int64_t d0 = A0.sdim[vi.alpha];
-              if (vi.rows != run * pad8(d0) || vi.n != ncl(c1p))
-                return fail(CMPS_ERR_STATE, "canonical tcgen05 form: L row mismatch");
-              int32_t a;
-              auto it = va.find(vk);
-              if (it == va.end()) {
-                CMPS_TRY(amap(p, T->zv, T->zv_len, vi.off, d0, vi.n * run, pad8(d0), &a));
-                va[vk] = a;
-              } else {
-                a = it->second;
-              }
-              int32_t b;
-              CMPS_TRY(bmap(p, loff.at({b0, vi.alpha}), d0, d0o, pad8(d0), &b));
-              tc::TcTerm tm{a, b, 0, (int32_t)d0};
-              tm.a_y0 = (int32_t)(pos * run);
-              p.terms.push_back(tm);
-              T->flops += term_flops(task, d0);
-            }
-            task.t1 = (int32_t)p.terms.size();  // a task without terms writes zeros
-            // the output run inside the output window
-            if (task.out_off < 0 || task.out_off + (task.m - 1) + (int64_t)(task.n - 1) * task.col_stride >= H.out_len)
-              return fail(CMPS_ERR_STATE, "canonical tcgen05 form: output outside theta");
-            tc::add_tiles(p, (int32_t)p.tasks.size(), task.m, task.n);
-            p.tasks.push_back(task);
-          }
+    // Tiles of a group of tasks that read the same A rows go row tile by row
+    // tile across the group, so the tiles that run at the same time (dealt
+    // round-robin to the SMs) share their A tiles in L2.
+    for (auto& g : groups) {
+      int32_t mmax = 0;
+      for (int32_t t : g.second) mmax = std::max(mmax, p.tasks[t].m);
+      for (int32_t m0 = 0; m0 < mmax; m0 += 128)
+        for (int32_t t : g.second) {
+          const tc::TcTask& k = p.tasks[t];
+          if (m0 >= k.m) continue;
+          for (int32_t n0 = 0; n0 < k.n; n0 += 128)
+            p.tiles.push_back(tc::TcTile{t, m0, n0, tc::b_box_rows(k.n), 0, ((std::min(128, k.n - n0)) + 15) & ~15});
         }
-      }
-    CMPS_TRY(tc::finish_plan(p, true, true, brows, true));
-  }
-  // every intermediate output range inside its buffer
-  for (const tc::TcPlan* p : {&T->pR, &T->pW2, &T->pW1}) {
-    const int64_t len = p == &T->pW2 ? T->y_len : T->zv_len;
-    for (const tc::TcTask& t : p->tasks)
-      if (t.out_off + (int64_t)t.m * t.n > len) return fail(CMPS_ERR_STATE, "canonical tcgen05 form: output outside buffer");
-  }
+    }
+    if (out) tc::mark_vector_stores(p, out, out_len);  // mode 3: BF16 output in 16-byte stores
+    return tc::finish_plan(p, true, true, brows, !grouped, true);
+  };
+  CMPS_TRY(build_plan(T->pR, fR, true, T->zv, T->zv_len));
+  CMPS_TRY(build_plan(T->pW2, fW2, true, T->y, T->y_len));
+  CMPS_TRY(build_plan(T->pW1, fW1, true, T->zv, T->zv_len));
+  CMPS_TRY(build_plan(T->pL, fL, false, nullptr, H.out_len));
   for (tc::TcPlan* p : {&T->pR, &T->pW2, &T->pW1, &T->pL}) CMPS_TRY(p->upload(st));
   CMPS_CUDA(cudaStreamSynchronize(st));
   return CMPS_OK;

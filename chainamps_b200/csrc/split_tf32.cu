@@ -171,7 +171,20 @@ void add_tiles(TcPlan& p, int32_t task, int32_t m, int32_t n) {
       p.tiles.push_back(TcTile{task, m0, n0, b_box_rows(n), 0, ((std::min(128, n - n0)) + 15) & ~15});
 }
 
-int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first) {
+void mark_vector_stores(TcPlan& p, const void* out, int64_t plane) {
+  for (TcTask& t : p.tasks) {
+    bool ok = ((uintptr_t)out & 15) == 0 && t.row_stride == 1 && t.m % 8 == 0 && t.col_stride % 8 == 0 &&
+              plane % 8 == 0 && t.nseg >= 1 && t.nseg <= 4;
+    for (int q = 0; q < t.nseg && ok; ++q) ok = t.seg_off[q] >= 0 && t.seg_off[q] % 8 == 0;
+    t.vstore = ok ? 1 : 0;
+  }
+}
+
+int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first,
+                bool wide_ok) {
+  for (const TcTask& t : p.tasks)
+    if (t.vstore && (t.row_stride != 1 || t.m % 8 || t.col_stride % 8))
+      return fail(CMPS_ERR_STATE, "tcgen05 plan: vector stores on an unsuitable output");
   // k-steps per tile (the MMA warp walks them without term lookups)
   const int32_t ks = kstep(bf16);
   for (TcTile& t : p.tiles) {
@@ -182,6 +195,7 @@ int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b
     for (int q = k.t0; q < k.t1; ++q) it += (p.terms[q].k + ks - 1) / ks;
     if (it > 0x7fffffff) return fail(CMPS_ERR_ARG, "tcgen05 plan: too many k-steps in one tile");
     t.kiters = (int32_t)it;
+    t.wide = wide_ok && bf16 && t.nmma <= 32 && t.b_rows == t.nmma ? 1 : 0;
   }
   // heaviest tiles first: the persistent kernel deals tiles round-robin to
   // the SMs, so this ordering balances the per-SM work
@@ -665,6 +679,7 @@ static int build_split(Heff& H, bool bf16) {
     tc::add_tiles(p2, (int32_t)p2.tasks.size(), task.m, task.n);
     p2.tasks.push_back(task);
   }
+  if (S->bf16) tc::mark_vector_stores(p1, S->at(S->ts_off), S->ts_len);
   CMPS_TRY(tc::finish_plan(p1, S->bf16, true, b1_rows, true));
   CMPS_TRY(tc::finish_plan(p2, S->bf16, S->bf16, b2_rows, true));
   if (!S->bf16)

@@ -76,12 +76,27 @@ template <int MODE>
 __host__ __device__ constexpr bool tma_a() {
   return MODE != 2;
 }
+// the four-plane MMA form of a narrow BF16 tile (TcTile::wide, set by the
+// host for N <= 32 with B planes of exactly N rows: 8N TMEM columns)
+template <int MODE>
+__device__ __forceinline__ bool wide_tile(const TcTile& t) {
+  return bf16_mode<MODE>() && t.wide && t.nmma <= 32 && t.b_rows == t.nmma;
+}
 constexpr int kStages = 3;
 constexpr int kBN = 128, kBK = 16;  // TF32 k-step; a BF16 k-step is 2 kBK wide
 constexpr int kPlaneTileBytes = 128 * kBK * 4;          // 8 KB: 128 rows x 64 B
 constexpr int kOperandBytes = 4 * kPlaneTileBytes;      // 32 KB: four planes
 constexpr int kStageBytes = 2 * kOperandBytes;          // A + B
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
+// Mode 3 stages its output through shared memory: per epilogue warp one
+// 32-row x 8-column x 4-plane BF16 box (rows innermost, 2 KB), after the
+// barriers.
+constexpr int kStoreBoxBytes = 32 * 8 * 4 * 2;
+template <int MODE>
+__host__ __device__ constexpr int smem_bytes_of() {
+  return kSmemBytes + (MODE == 3 ? epilogue_warps<3>() * kStoreBoxBytes : 0);
+}
+static_assert(smem_bytes_of<3>() <= 232448, "shared memory per CTA");
 constexpr uint32_t kTmemCols = 512;                      // two buffers of {Re at +0, Im at +128}
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 
@@ -135,6 +150,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
       ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
+}
+
+__device__ __forceinline__ void sts16(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.u16 [%0], %1;" ::"r"(addr), "h"((unsigned short)v) : "memory");
 }
 
 // UMMA shared-memory descriptor, K-major, SWIZZLE_64B: 64-byte rows, 8-row
@@ -272,41 +291,75 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
 
   if (warp == 0) {
     // ---------------- TMA producer: runs ahead across tile boundaries ----------------
-    if (lane == 0) {
-      int it = 0;  // global iteration counter of this CTA
-      bool ok = true;
-      for (int ti = blockIdx.x; ti < ntiles && ok; ti += gridDim.x) {
-        const TcTile tile = tiles[ti];
-        const TcTask task = tasks[tile.task];
-        for (int t = task.t0; t < task.t1 && ok; ++t) {
-          const TcTerm tm = terms[t];
-          if (tma_a<MODE>()) tensormap_acquire(amaps + tm.a_map);
-          tensormap_acquire(bmaps + tm.b_map);
-          constexpr int kStep = bf16_mode<MODE>() ? 2 * kBK : kBK;  // K columns per 64-byte row
-          for (int k0 = 0; k0 < tm.k; k0 += kStep, ++it) {
-            const int s = it % kStages;
-            const uint32_t ph = (uint32_t)((it / kStages) & 1);
-            if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
-              ok = false;
-              break;
+    // The records of this CTA's next 32 tiles (origin, B box rows, term
+    // range and first term) are loaded by the 32 lanes at once and handed to
+    // lane 0 by shuffles, so the dependent loads tile -> task -> term cost one
+    // round of latency per 32 tiles, not one per tile (a tile of one k-step
+    // would otherwise leave the ring empty while lane 0 waits on them).
+    // Lane 0 issues the copies and fetches each next term of a tile while
+    // the current one's copies go out.  `ok` is warp-uniform.
+    int it = 0;  // global iteration counter of this CTA (lane 0)
+    bool ok = true;
+    const int grid = (int)gridDim.x;
+    for (int base = blockIdx.x; base < ntiles && ok; base += 32 * grid) {
+      const int my = base + lane * grid;
+      int m0 = 0, n0 = 0, brows = 0, t0 = 0, t1 = 0;
+      TcTerm f{};
+      if (my < ntiles) {
+        const TcTile tl = tiles[my];
+        m0 = tl.m0;
+        n0 = tl.n0;
+        brows = tl.b_rows;
+        t0 = tasks[tl.task].t0;
+        t1 = tasks[tl.task].t1;
+        if (t1 > t0) f = terms[t0];
+      }
+      const int cnt = min(32, (ntiles - base + grid - 1) / grid);
+      for (int j = 0; j < cnt; ++j) {
+        const int jm0 = __shfl_sync(0xffffffffu, m0, j), jn0 = __shfl_sync(0xffffffffu, n0, j);
+        const int jb = __shfl_sync(0xffffffffu, brows, j);
+        const int jt0 = __shfl_sync(0xffffffffu, t0, j), jt1 = __shfl_sync(0xffffffffu, t1, j);
+        TcTerm tm;
+        tm.a_map = __shfl_sync(0xffffffffu, f.a_map, j);
+        tm.b_map = __shfl_sync(0xffffffffu, f.b_map, j);
+        tm.a_x0 = __shfl_sync(0xffffffffu, f.a_x0, j);
+        tm.k = __shfl_sync(0xffffffffu, f.k, j);
+        tm.a_y0 = __shfl_sync(0xffffffffu, f.a_y0, j);
+        if (lane == 0) {
+          for (int t = jt0; t < jt1 && ok; ++t) {
+            TcTerm nx{};
+            if (t + 1 < jt1) nx = terms[t + 1];  // in flight during this term's copies
+            if (tma_a<MODE>()) tensormap_acquire(amaps + tm.a_map);
+            tensormap_acquire(bmaps + tm.b_map);
+            constexpr int kStep = bf16_mode<MODE>() ? 2 * kBK : kBK;  // K columns per 64-byte row
+            for (int k0 = 0; k0 < tm.k; k0 += kStep, ++it) {
+              const int s = it % kStages;
+              const uint32_t ph = (uint32_t)((it / kStages) & 1);
+              if (!mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
+                ok = false;
+                break;
+              }
+              uint8_t* sa = smem + s * kStageBytes;
+              uint8_t* sb = sa + kOperandBytes;
+              // A: 128-row box (mode 1; written by the converter warps in mode 2);
+              // B: the task's b_rows-row box; both four planes
+              const uint32_t bbytes = 4u * 64u * (uint32_t)jb;
+              mbar_expect_tx(&full[s], (tma_a<MODE>() ? (uint32_t)kOperandBytes : 0u) + bbytes);
+              if (tma_a<MODE>()) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, jm0 + tm.a_y0, 0, &full[s]);
+              tma_load_3d(sb, bmaps + tm.b_map, k0, jn0, 0, &full[s]);
             }
-            uint8_t* sa = smem + s * kStageBytes;
-            uint8_t* sb = sa + kOperandBytes;
-            // A: 128-row box (mode 1; written by the converter warps in mode 2);
-            // B: the task's b_rows-row box; both four planes
-            const uint32_t bbytes = 4u * 64u * (uint32_t)tile.b_rows;
-            mbar_expect_tx(&full[s], (tma_a<MODE>() ? (uint32_t)kOperandBytes : 0u) + bbytes);
-            if (tma_a<MODE>()) tma_load_3d(sa, amaps + tm.a_map, tm.a_x0 + k0, tile.m0 + tm.a_y0, 0, &full[s]);
-            tma_load_3d(sb, bmaps + tm.b_map, k0, tile.n0, 0, &full[s]);
+            tm = nx;
           }
         }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) break;
       }
-      if (!ok) {
-        // let the copies already in flight land before the CTA exits
-        for (int j = max(0, it - kStages); j < it; ++j) {
-          const unsigned long long t0 = now_ns();
-          while (!mbar_try(&full[j % kStages], (uint32_t)((j / kStages) & 1)) && now_ns() - t0 < kWaitLimitNs) {
-          }
+    }
+    if (lane == 0 && !ok) {
+      // let the copies already in flight land before the CTA exits
+      for (int j = max(0, it - kStages); j < it; ++j) {
+        const unsigned long long t0w = now_ns();
+        while (!mbar_try(&full[j % kStages], (uint32_t)((j / kStages) & 1)) && now_ns() - t0w < kWaitLimitNs) {
         }
       }
     }
@@ -320,8 +373,16 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         const TcTile tile = nxt;
         if (ti + (int)gridDim.x < ntiles) nxt = tiles[ti + gridDim.x];  // in flight during this tile
         const int nmma = tile.nmma;  // multiple of 16 for M = 128
-        const uint32_t id_pos = bf16_mode<MODE>() ? idesc_bf16(nmma, false) : idesc_tf32(nmma, false);
-        const uint32_t id_neg = bf16_mode<MODE>() ? idesc_bf16(nmma, true) : idesc_tf32(nmma, true);
+        // A narrow BF16 tile (N <= 32) in a plan that opts in runs the
+        // four-plane form: the B planes re_hi, re_mid, im_hi, im_mid lie back
+        // to back in shared memory (b_rows = N rows each), so one MMA per A
+        // plane with N' = 4N forms every product of that plane; (A_hi +
+        // A_mid) . B_plane accumulates per plane block: 4 MMAs of 4N instead
+        // of 12 of N.
+        const bool wide = wide_tile<MODE>(tile);
+        const int nw = wide ? 4 * nmma : nmma;
+        const uint32_t id_pos = bf16_mode<MODE>() ? idesc_bf16(nw, false) : idesc_tf32(nw, false);
+        const uint32_t id_neg = bf16_mode<MODE>() ? idesc_bf16(nw, true) : idesc_tf32(nw, true);
         const int buf = tc & 1;
         const uint32_t use = (uint32_t)(tc >> 1);
         if (!mbar_wait(&tempty[buf], (use & 1u) ^ 1u, err, 4)) {
@@ -354,6 +415,14 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
               }
               const uint32_t acc = first ? 0u : 1u;
               first = false;
+              if (wide) {
+                // d_re = (A_re_hi + A_re_mid) . [B_re_hi | B_re_mid | B_im_hi | B_im_mid], d_im likewise
+                umma<MODE>(d_re, A[0], B[0], id_pos, acc);
+                umma<MODE>(d_re, A[1], B[0], id_pos, 1u);
+                umma<MODE>(d_im, A[2], B[0], id_pos, acc);
+                umma<MODE>(d_im, A[3], B[0], id_pos, 1u);
+                continue;
+              }
               // planes 1 and 3 are lo (TF32) or mid (BF16)
               umma<MODE>(d_re, A[0], B[0], id_pos, acc);
               umma<MODE>(d_re, A[0], B[1], id_pos, 1u);
@@ -494,6 +563,8 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
     const int quad = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = quad * 32 + lane;
     int tc = 0;
+    // mode 3, vector-store path: this warp's staging box
+    const uint32_t stg = smem_u32(smem + kStages * kStageBytes + 256) + (uint32_t)((warp - 2) * kStoreBoxBytes);
     // the next tile's records are loaded while this tile waits and drains
     TcTile nt = blockIdx.x < (unsigned)ntiles ? tiles[blockIdx.x] : TcTile{};
     TcTask nk = blockIdx.x < (unsigned)ntiles ? tasks[nt.task] : TcTask{};
@@ -527,13 +598,39 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
       // chunk c is stored (every lane issues and waits; tcgen05.ld is
       // warp-collective, so the row check comes after)
       uint32_t ra[16], ia[16];
-      if (have && c_first < nmma) {
+      const bool wide = wide_tile<MODE>(tile);
+      if (have && !wide && c_first < nmma) {
         tmem_ld16_issue(tbase + c_first, ra);
         tmem_ld16_issue(tbase + 128 + c_first, ia);
       }
       for (int c = c_first; c < nmma; c += c_step) {
         float vr[16], vi[16];
-        if (have) {
+        if (have && wide) {
+          // four-plane form: block q of d_re / d_im (columns q N ..) holds
+          // A_re . B_q / A_im . B_q for B planes re_hi, re_mid, im_hi, im_mid
+          //   re = d_re[0] + d_re[1] - d_im[2] - d_im[3]
+          //   im = d_re[2] + d_re[3] + d_im[0] + d_im[1]
+          tmem_ld16_issue(tbase + c, ra);
+          tmem_ld16_issue(tbase + nmma + c, ia);
+          tmem_wait(ra, ia);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) vr[i] = __uint_as_float(ra[i]) + __uint_as_float(ia[i]);
+          tmem_ld16_issue(tbase + 128 + 2 * nmma + c, ra);
+          tmem_ld16_issue(tbase + 128 + 3 * nmma + c, ia);
+          tmem_wait(ra, ia);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) vr[i] -= __uint_as_float(ra[i]) + __uint_as_float(ia[i]);
+          tmem_ld16_issue(tbase + 2 * nmma + c, ra);
+          tmem_ld16_issue(tbase + 3 * nmma + c, ia);
+          tmem_wait(ra, ia);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) vi[i] = __uint_as_float(ra[i]) + __uint_as_float(ia[i]);
+          tmem_ld16_issue(tbase + 128 + c, ra);
+          tmem_ld16_issue(tbase + 128 + nmma + c, ia);
+          tmem_wait(ra, ia);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) vi[i] += __uint_as_float(ra[i]) + __uint_as_float(ia[i]);
+        } else if (have) {
           tmem_wait(ra, ia);
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
@@ -547,6 +644,59 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
+        }
+        if (MODE == 3 && task.vstore) {
+          // Vector-store path, for a chunk inside one column segment: each
+          // 8-column half is split and written by every lane as its row of
+          // a [plane][column][row] box in shared memory, then read back as
+          // 16-byte runs of 8 rows and stored: lane l takes column l / 4,
+          // rows 8 (l % 4) .. +7, in the four planes.  Rows past the task
+          // (whole 8-row runs: its M is a multiple of 8) are not stored.
+          const int cnt = min(16, ntile - c);
+          const int colA = tile.n0 + c, colB = colA + cnt - 1;
+          const int qa = (colA >= task.seg_n0[1]) + (colA >= task.seg_n0[2]) + (colA >= task.seg_n0[3]);
+          const int qb = (colB >= task.seg_n0[1]) + (colB >= task.seg_n0[2]) + (colB >= task.seg_n0[3]);
+          const int row0 = tile.m0 + quad * 32;
+          if (cnt > 0 && qa == qb && row0 < task.m) {
+            const int n0 = qa == 0 ? 0 : qa == 1 ? task.seg_n0[1] : qa == 2 ? task.seg_n0[2] : task.seg_n0[3];
+            const int64_t so = qa == 0 ? task.seg_off[0] : qa == 1 ? task.seg_off[1] : qa == 2 ? task.seg_off[2]
+                                                                                            : task.seg_off[3];
+            const int lc = lane >> 2, lr = (lane & 3) * 8;
+            const bool rok8 = row0 + lr < task.m;
+            uint16_t* g = reinterpret_cast<uint16_t*>(out32) + so + row0 + lr +
+                          (int64_t)(colA - n0 + lc) * task.col_stride;
+            const uint32_t box = stg + (uint32_t)(lane * 2);
+            const uint32_t rd = stg + (uint32_t)(lc * 64 + lr * 2);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              if (h * 8 >= cnt) break;
+              __syncwarp();  // the previous half's reads are done
+#pragma unroll
+              for (int i = 0; i < 8; ++i) {
+                const float xr = vr[h * 8 + i], xi = vi[h * 8 + i];
+                const uint32_t h2 = bf16x2(xi, xr);
+                const float rh = __uint_as_float(h2 << 16), ih = __uint_as_float(h2 & 0xffff0000u);
+                const uint32_t m2 = bf16x2(xi - ih, xr - rh);
+                sts16(box + (uint32_t)((0 * 8 + i) * 64), h2);
+                sts16(box + (uint32_t)((1 * 8 + i) * 64), m2);
+                sts16(box + (uint32_t)((2 * 8 + i) * 64), h2 >> 16);
+                sts16(box + (uint32_t)((3 * 8 + i) * 64), m2 >> 16);
+              }
+              __syncwarp();
+              if (rok8 && h * 8 + lc < cnt) {
+                uint16_t* gh = g + (int64_t)(h * 8) * task.col_stride;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                  uint4 v;
+                  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                               : "r"(rd + (uint32_t)(j * 8 * 64)));
+                  *reinterpret_cast<uint4*>(gh + j * out32_plane) = v;
+                }
+              }
+            }
+            continue;
+          }
         }
         if (!row_ok) continue;
         if (MODE == 3) {
@@ -636,9 +786,10 @@ int launch(int mode, const TcPlan& p, float* out32, int64_t out32_plane, double*
   if (mode == 1 || mode == 3 || mode == 4) {
     if (!p.d_amaps) return fail(CMPS_ERR_STATE, "tcgen05: no A tensor maps");
     auto kern = mode == 1 ? tc_split_gemm<1> : mode == 3 ? tc_split_gemm<3> : tc_split_gemm<4>;
-    CMPS_TRY(ensure_smem_optin((const void*)kern, kSmemBytes));
+    const int smem = mode == 3 ? smem_bytes_of<3>() : kSmemBytes;
+    CMPS_TRY(ensure_smem_optin((const void*)kern, smem));
     const int threads = mode == 3 ? threads_of<3>() : threads_of<1>();
-    kern<<<grid, threads, kSmemBytes, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, nullptr,
+    kern<<<grid, threads, smem, st>>>(p.d_tiles, ntiles, p.d_tasks, p.d_terms, p.d_amaps, p.d_bmaps, nullptr,
                                             nullptr, 0, out32, out32_plane, out64, out64_plane, d_err);
   } else if (mode == 2) {
     if (!ain || !p.d_adescs) return fail(CMPS_ERR_STATE, "tcgen05 mode 2: no A operand");

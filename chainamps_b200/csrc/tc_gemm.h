@@ -17,6 +17,8 @@ namespace tc {
 // INT32_MAX), and element (i, j) of C lands at
 // seg_off[q] + i*row_stride + (j - seg_n0[q])*col_stride.  out_off repeats
 // seg_off[0].
+// vstore (mode 3): the output admits 16-byte stores of 8-row runs
+// (mark_vector_stores); else the epilogue stores element by element.
 struct TcTask {
   int64_t out_off;
   int64_t row_stride, col_stride;
@@ -25,6 +27,7 @@ struct TcTask {
   int32_t nseg;
   int32_t seg_n0[4];
   int64_t seg_off[4];
+  int32_t vstore;
 };
 // One K-concatenated term: A tile at (a_x0 + k, a_y0 + row) of map a_map, B
 // tile at (k, row) of b_map.  a_y0 (a row offset into the A map) applies to A
@@ -43,8 +46,12 @@ struct TcADesc {
 // 16, at most 128); the B tensor maps of that task are encoded with it.
 // kiters: k-steps (kstep() columns each) of the task's terms; nmma: the tile's N rounded up
 // to 16 (the MMA N) -- so the MMA warp needs no task or term lookups.
+// wide: the four-plane MMA form (BF16, N <= 32 with B planes of exactly N
+// rows): 4 MMAs of N' = 4N per k-step instead of 12 of N; it rounds
+// differently, so a plan opts in (finish_plan).
 struct TcTile {
   int32_t task, m0, n0, b_rows, kiters, nmma;
+  int32_t wide;
 };
 // B box rows for a task of N columns.
 inline int32_t b_box_rows(int32_t n) { return n >= 128 ? 128 : ((n + 15) & ~15); }
@@ -77,8 +84,15 @@ void add_tiles(TcPlan& p, int32_t task, int32_t m, int32_t n);
 // Completes a plan built term by term: k-steps per tile, optionally the
 // heaviest tiles first, and checks every term, task, segment list and tile.
 // by_tma: the A operands are tensor maps (else converter descriptors);
-// b_rows: the row count each B map was encoded with.
-int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first);
+// b_rows: the row count each B map was encoded with; wide_ok: narrow BF16
+// tiles take the four-plane MMA form.
+int finish_plan(TcPlan& p, bool bf16, bool by_tma, const std::vector<int32_t>& b_rows, bool heaviest_first,
+                bool wide_ok = false);
+// Mode 3: marks the tasks whose output takes 16-byte stores of 8-row runs
+// (rows contiguous, M a multiple of 8, segment starts and column / plane
+// strides multiples of 8 elements) for a BF16 output at `out` (16-byte
+// aligned) with plane stride `plane` elements.
+void mark_vector_stores(TcPlan& p, const void* out, int64_t plane);
 // K columns of one k-step: a 64-byte shared-memory row of 16 TF32 or 32 BF16
 inline int32_t kstep(bool bf16) { return bf16 ? 32 : 16; }
 // mode 1: A and B by TMA (four TF32 planes each); FP32 output in two planes
