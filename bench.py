@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--ising-chi", default="64,128", help="bond dimensions of the coupled-Ising steps")
     p.add_argument("--ising-folded-chi", type=int, default=64,
                    help="bond dimension at which the folded-order FP64 step is also timed (0: skip)")
+    p.add_argument("--ising-matvec-chi", default="128",
+                   help="bond dimensions of the coupled-Ising matvec timing per form ('': skip)")
     return p.parse_args()
 
 
@@ -482,6 +484,9 @@ def main():
             ising[f"chi_{chi}"] = idmrg_bench(ctx, iw, chi, a.ising_steps, dist, warm=2, forms=forms,
                                               unit_cell=False)
         line["idmrg_coupled_ising"] = ising
+    if a.ising_matvec_chi:
+        line["ising_matvec"] = ising_matvec_bench(
+            ctx, [int(c) for c in str(a.ising_matvec_chi).split(",") if c.strip()], dist, stream)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         t, setup, cores, _ = cpu_port(wl, 1)
         line["cpu_baseline"] = {"value": canonical / t / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
@@ -493,6 +498,45 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def ising_matvec_bench(ctx, chis, dist, stream, reps=5):
+    """The coupled-Ising H_eff matvec alone, on synthetic Z2 environments
+    (``models.ising_workload``, seed 20261203), in each form: FP64 (canonical
+    order), split TF32 (canonical order in FP32 FMA) and split BF16
+    (canonical order as four tcgen05 stages).  ms per matvec is the sum of
+    the library's stage events (gather, first half, second half, scatter;
+    mean of ``reps``), max over ranks; canonical TFLOP/s; and the largest
+    deviation from the FP64 matvec relative to its largest entry."""
+    import torch
+    from chainamps_b200 import models, TwoVertexComponents, CMPS_FP64, CMPS_SPLIT_TF32, CMPS_SPLIT_BF16
+    out = {}
+    for chi in chis:
+        wl = models.ising_workload(chi)
+        res, ref = {}, None
+        for name, prec in (("fp64", CMPS_FP64), ("split_tf32", CMPS_SPLIT_TF32), ("split_bf16", CMPS_SPLIT_BF16)):
+            h = TwoVertexComponents(ctx, wl["rules"], wl["L"], wl["Wt"], wl["R"], precision=prec)
+            x = torch.randn(h.n, dtype=torch.complex128, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+            y = torch.empty_like(x)
+            st = h.time_stages(x.data_ptr(), y.data_ptr(), stream.cuda_stream, reps=reps)
+            torch.cuda.synchronize()
+            h.status()
+            ms_t = torch.tensor([float(np.sum(st))], device="cuda", dtype=torch.float64)
+            if dist:
+                dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+            can, exe = h.flops()
+            r = {"ms_per_matvec": float(ms_t.item()), "canonical_tflops": can / (float(ms_t.item()) * 1e-3) / 1e12,
+                 "stage_ms": [float(v) for v in st], "split_form": h.split_form()}
+            if ref is None:
+                ref = y.clone()
+            else:
+                r["max_dev_vs_fp64"] = float((y - ref).abs().max() / ref.abs().max())
+            res[name] = r
+            del h
+        res["n_allowed"] = int(ref.numel())
+        res["speedup_bf16_vs_fp64"] = res["fp64"]["ms_per_matvec"] / res["split_bf16"]["ms_per_matvec"]
+        out[f"chi_{chi}"] = res
+    return out
 
 
 def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True, forms=None):

@@ -339,3 +339,21 @@ def ladder_workload(chi, seed=20261203, width=3.5, legs=4, j=1.0, j_perp=0.5):
     R = random_environment(rng, rules, bond, bq, used_r, right=True)
     Wt = mpo_tensor(ch, W, bq)
     return dict(rules=rules, ch=ch, W=W, bq=bq, bond=bond, L=L, R=R, Wt=Wt)
+
+
+def ising_workload(chi, seed=20261203, sites=12, g=1.2, keep=64, j_perp=0.05):
+    """The synthetic H_eff workload of the coupled-Ising chains: the
+    ``sites``-site chain vertex cut to ``keep`` states (Z2 parity), between
+    seeded random left and right environments on a Z2 bond of ``chi``
+    elements (two sectors of chi / 2), entries only on the MPO slots the MPO
+    uses.  Returns the model arrays and the three tensors (L, Wt, R)."""
+    rules, ch, W, bq = coupled_ising_model(sites, g, keep, j_perp)
+    used_l = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 2, 3)))[0]})
+    used_r = sorted({int(b) for b in np.nonzero(np.any(W != 0, axis=(0, 1, 2)))[0]})
+    bond = (np.arange(chi) % 2).reshape(-1, 1).astype(np.int64)
+    rng = np.random.default_rng(seed)
+    L = random_environment(rng, rules, bond, bq, used_l, right=False)
+    R = random_environment(rng, rules, bond, bq, used_r, right=True)
+    Wt = mpo_tensor(ch, W, bq)
+    return dict(rules=rules, ch=ch, W=W, bq=bq, bond=bond, L=L, R=R, Wt=Wt)
+
