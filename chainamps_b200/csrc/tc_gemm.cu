@@ -89,9 +89,9 @@ constexpr int kOperandBytes = 4 * kPlaneTileBytes;      // 32 KB: four planes
 constexpr int kStageBytes = 2 * kOperandBytes;          // A + B
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align*/ + 256 /*barriers*/;
 // Mode 3 stages its output through shared memory: per epilogue warp one
-// 32-row x 8-column x 4-plane BF16 box (rows innermost, 2 KB), after the
+// 32-row x 16-column x 4-plane BF16 box (rows innermost, 4 KB), after the
 // barriers.
-constexpr int kStoreBoxBytes = 32 * 8 * 4 * 2;
+constexpr int kStoreBoxBytes = 32 * 16 * 4 * 2;
 template <int MODE>
 __host__ __device__ constexpr int smem_bytes_of() {
   return kSmemBytes + (MODE == 3 ? epilogue_warps<3>() * kStoreBoxBytes : 0);
@@ -646,12 +646,13 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
           for (int i = 0; i < 16; ++i) vr[i] = vi[i] = 0.f;
         }
         if (MODE == 3 && task.vstore) {
-          // Vector-store path, for a chunk inside one column segment: each
-          // 8-column half is split and written by every lane as its row of
-          // a [plane][column][row] box in shared memory, then read back as
-          // 16-byte runs of 8 rows and stored: lane l takes column l / 4,
-          // rows 8 (l % 4) .. +7, in the four planes.  Rows past the task
-          // (whole 8-row runs: its M is a multiple of 8) are not stored.
+          // Vector-store path, for a chunk inside one column segment: the
+          // chunk is split and written by every lane as its row of a
+          // [plane][column][row] box in shared memory, then read back as
+          // 16-byte runs of 8 rows and stored: lane l takes columns l / 4
+          // and 8 + l / 4, rows 8 (l % 4) .. +7, in the four planes.  Rows
+          // past the task (whole 8-row runs: its M is a multiple of 8) are
+          // not stored.
           const int cnt = min(16, ntile - c);
           const int colA = tile.n0 + c, colB = colA + cnt - 1;
           const int qa = (colA >= task.seg_n0[1]) + (colA >= task.seg_n0[2]) + (colA >= task.seg_n0[3]);
@@ -667,33 +668,33 @@ tc_split_gemm(const TcTile* __restrict__ tiles, int ntiles, const TcTask* __rest
                           (int64_t)(colA - n0 + lc) * task.col_stride;
             const uint32_t box = stg + (uint32_t)(lane * 2);
             const uint32_t rd = stg + (uint32_t)(lc * 64 + lr * 2);
+            __syncwarp();  // the previous chunk's reads of the box are done
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const float xr = vr[i], xi = vi[i];
+              const uint32_t h2 = bf16x2(xi, xr);
+              const float rh = __uint_as_float(h2 << 16), ih = __uint_as_float(h2 & 0xffff0000u);
+              const uint32_t m2 = bf16x2(xi - ih, xr - rh);
+              sts16(box + (uint32_t)((0 * 16 + i) * 64), h2);
+              sts16(box + (uint32_t)((1 * 16 + i) * 64), m2);
+              sts16(box + (uint32_t)((2 * 16 + i) * 64), h2 >> 16);
+              sts16(box + (uint32_t)((3 * 16 + i) * 64), m2 >> 16);
+            }
+            __syncwarp();
+            uint4 v[2][4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+                asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                             : "=r"(v[h][j].x), "=r"(v[h][j].y), "=r"(v[h][j].z), "=r"(v[h][j].w)
+                             : "r"(rd + (uint32_t)((j * 16 + h * 8) * 64)));
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-              if (h * 8 >= cnt) break;
-              __syncwarp();  // the previous half's reads are done
+              if (!rok8 || h * 8 + lc >= cnt) continue;
+              uint16_t* gh = g + (int64_t)(h * 8) * task.col_stride;
 #pragma unroll
-              for (int i = 0; i < 8; ++i) {
-                const float xr = vr[h * 8 + i], xi = vi[h * 8 + i];
-                const uint32_t h2 = bf16x2(xi, xr);
-                const float rh = __uint_as_float(h2 << 16), ih = __uint_as_float(h2 & 0xffff0000u);
-                const uint32_t m2 = bf16x2(xi - ih, xr - rh);
-                sts16(box + (uint32_t)((0 * 8 + i) * 64), h2);
-                sts16(box + (uint32_t)((1 * 8 + i) * 64), m2);
-                sts16(box + (uint32_t)((2 * 8 + i) * 64), h2 >> 16);
-                sts16(box + (uint32_t)((3 * 8 + i) * 64), m2 >> 16);
-              }
-              __syncwarp();
-              if (rok8 && h * 8 + lc < cnt) {
-                uint16_t* gh = g + (int64_t)(h * 8) * task.col_stride;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                  uint4 v;
-                  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                               : "r"(rd + (uint32_t)(j * 8 * 64)));
-                  *reinterpret_cast<uint4*>(gh + j * out32_plane) = v;
-                }
-              }
+              for (int j = 0; j < 4; ++j) *reinterpret_cast<uint4*>(gh + j * out32_plane) = v[h][j];
             }
             continue;
           }
