@@ -621,56 +621,72 @@ int Heff::finish() {
   lp_off.clear();
   lp_blocks.clear();
   lp_terms.clear();
-  std::map<std::array<int, 4>, std::vector<AxpyTerm>> lpt;
+  // (block key, term) pairs sorted by key, terms of one key in W order: the
+  // blocks come out in key order with the terms as a per-key list would
+  // hold them, without a tree insert per term
+  struct KeyTerm {
+    std::array<int, 4> key;
+    AxpyTerm t;
+  };
+  auto by_key = [](const KeyTerm& a, const KeyTerm& b) { return a.key < b.key; };
+  std::vector<KeyTerm> lpt;
+  lpt.reserve(W.size() * (size_t)std::min(A0.nsec(), 8));
   for (const WEntry& w : W) {
     for (int s = 0; s < A0.nsec(); ++s) {
       int64_t lo = L.off[(size_t)w.bl * A0.nsec() + s];
       if (lo < 0) continue;
       QKey m = r.add(sigq[w.s], A0.sq[s]);
       if (th.find(m) < 0 || th.find(r.add(m, bq[w.br])) < 0) continue;
-      lpt[{w.br, w.sp, w.s, s}].push_back(AxpyTerm{lo, w.wr, w.wi});
+      lpt.push_back(KeyTerm{{w.br, w.sp, w.s, s}, AxpyTerm{lo, w.wr, w.wi}});
     }
   }
+  std::stable_sort(lpt.begin(), lpt.end(), by_key);
   int64_t lp_total = 0;
-  for (auto& kv2 : lpt) {
-    const auto& key = kv2.first;
+  for (size_t i = 0, j = 0; i < lpt.size(); i = j) {
+    const std::array<int, 4> key = lpt[i].key;
+    for (j = i; j < lpt.size() && lpt[j].key == key; ++j) {
+    }
     int s = key[3];
     // partner sector: q(s') = q(s) + q(b0) = q(s) + q(s1) + q(b1) - q(s1')
     QKey qsp = r.sub(r.add(r.add(A0.sq[s], sigq[key[2]]), bq[key[0]]), sigq[key[1]]);
     int sp = A0.find(qsp);
     if (sp < 0) continue;
     int64_t len = A0.sdim[sp] * A0.sdim[s];
-    lp_off[key] = lp_total;
-    lp_blocks.push_back(AxpyBlock{lp_total, len, (int32_t)lp_terms.size(), (int32_t)(lp_terms.size() + kv2.second.size())});
-    for (auto& t : kv2.second) lp_terms.push_back(t);
+    lp_off.emplace_hint(lp_off.end(), key, lp_total);
+    lp_blocks.push_back(AxpyBlock{lp_total, len, (int32_t)lp_terms.size(), (int32_t)(lp_terms.size() + (j - i))});
+    for (size_t q = i; q < j; ++q) lp_terms.push_back(lpt[q].t);
     lp_total += len;
   }
   // ---- RightPart blocks: key (b1, s2, s2', a2-sector t) ----
   rp_off.clear();
   rp_blocks.clear();
   rp_terms.clear();
-  std::map<std::array<int, 4>, std::vector<AxpyTerm>> rpt;
+  std::vector<KeyTerm> rpt;
+  rpt.reserve(W.size() * (size_t)std::min(A2.nsec(), 8));
   for (const WEntry& w : W) {
     for (int t = 0; t < A2.nsec(); ++t) {
       int64_t ro = R.off[(size_t)w.br * A2.nsec() + t];
       if (ro < 0) continue;
       QKey m = r.sub(A2.sq[t], sigq[w.s]);
       if (th.find(m) < 0 || th.find(r.add(m, bq[w.bl])) < 0) continue;
-      rpt[{w.bl, w.s, w.sp, t}].push_back(AxpyTerm{ro, w.wr, w.wi});
+      rpt.push_back(KeyTerm{{w.bl, w.s, w.sp, t}, AxpyTerm{ro, w.wr, w.wi}});
     }
   }
+  std::stable_sort(rpt.begin(), rpt.end(), by_key);
   int64_t rp_total = 0;
-  for (auto& kv2 : rpt) {
-    const auto& key = kv2.first;
+  for (size_t i = 0, j = 0; i < rpt.size(); i = j) {
+    const std::array<int, 4> key = rpt[i].key;
+    for (j = i; j < rpt.size() && rpt[j].key == key; ++j) {
+    }
     int t = key[3];
     // q(t') = q(t) + q(b2) = q(t) + q(s2') + q(b1) - q(s2)
     QKey qtp = r.sub(r.add(r.add(A2.sq[t], sigq[key[2]]), bq[key[0]]), sigq[key[1]]);
     int tp = A2.find(qtp);
     if (tp < 0) continue;
     int64_t len = A2.sdim[t] * A2.sdim[tp];
-    rp_off[key] = rp_total;
-    rp_blocks.push_back(AxpyBlock{rp_total, len, (int32_t)rp_terms.size(), (int32_t)(rp_terms.size() + kv2.second.size())});
-    for (auto& tt : kv2.second) rp_terms.push_back(tt);
+    rp_off.emplace_hint(rp_off.end(), key, rp_total);
+    rp_blocks.push_back(AxpyBlock{rp_total, len, (int32_t)rp_terms.size(), (int32_t)(rp_terms.size() + (j - i))});
+    for (size_t q = i; q < j; ++q) rp_terms.push_back(rpt[q].t);
     rp_total += len;
   }
   bt.mark("LP/RP block lists");
@@ -802,6 +818,32 @@ int Heff::build_plans() {
   T.release();
   if ((int)in_base.size() != nm || (int)out_base.size() != nm) return fail(CMPS_ERR_STATE, "window size");
   in_need.assign(nm, 0);
+  // Dense (b, sigma', sigma, sector) -> block offset tables of lp_off /
+  // rp_off for the plan loops below (several lookups per (b, m, sigma',
+  // sigma)), when they stay small; the maps otherwise.
+  const int64_t nlp = (int64_t)D * d * d * A0.nsec(), nrp = (int64_t)D * d * d * A2.nsec();
+  constexpr int64_t kDenseMax = int64_t(1) << 24;
+  std::vector<int64_t> lp_tab, rp_tab;
+  if (nlp <= kDenseMax) {
+    lp_tab.assign(nlp, -1);
+    for (auto& kv2 : lp_off)
+      lp_tab[(((int64_t)kv2.first[0] * d + kv2.first[1]) * d + kv2.first[2]) * A0.nsec() + kv2.first[3]] = kv2.second;
+  }
+  if (nrp <= kDenseMax) {
+    rp_tab.assign(nrp, -1);
+    for (auto& kv2 : rp_off)
+      rp_tab[(((int64_t)kv2.first[0] * d + kv2.first[1]) * d + kv2.first[2]) * A2.nsec() + kv2.first[3]] = kv2.second;
+  }
+  auto lp_at = [&](int b, int sp, int sg, int sec) -> int64_t {
+    if (!lp_tab.empty()) return lp_tab[(((int64_t)b * d + sp) * d + sg) * A0.nsec() + sec];
+    auto it = lp_off.find({b, sp, sg, sec});
+    return it == lp_off.end() ? -1 : it->second;
+  };
+  auto rp_at = [&](int b, int sg, int sp, int sec) -> int64_t {
+    if (!rp_tab.empty()) return rp_tab[(((int64_t)b * d + sg) * d + sp) * A2.nsec() + sec];
+    auto it = rp_off.find({b, sg, sp, sec});
+    return it == rp_off.end() ? -1 : it->second;
+  };
   // ---- stage 1: T^{b1}_m = LeftPart^{b1} . Theta_m ----
   std::set<int> b1s;
   for (auto& kv2 : lp_off) b1s.insert(kv2.first[0]);
@@ -832,10 +874,10 @@ int Heff::build_plans() {
         for (int s1 = 0; s1 < d; ++s1) {
           if (th.rowoff[m][s1] < 0) continue;
           int s = A0.find(r.sub(th.mq[m], sigq[s1]));
-          auto it = lp_off.find({b1, s1p, s1, s});
-          if (it == lp_off.end()) continue;
+          const int64_t lo = lp_at(b1, s1p, s1, s);
+          if (lo < 0) continue;
           GemmTerm tm{};
-          tm.a_off = it->second;
+          tm.a_off = lo;
           tm.lda = (int32_t)A0.sdim[s];
           tm.k = (int32_t)A0.sdim[s];
           if (in_base[m] < 0) return fail(CMPS_ERR_ARG, "input window lacks a sector the owned outputs read");
@@ -890,13 +932,13 @@ int Heff::build_plans() {
         for (int s2 = 0; s2 < d; ++s2) {
           if (th.coloff[m][s2] < 0) continue;
           int t = A2.find(r.add(th.mq[m], sigq[s2]));
-          auto it = rp_off.find({b1, s2, s2p, t});
-          if (it == rp_off.end()) continue;
+          const int64_t ro = rp_at(b1, s2, s2p, t);
+          if (ro < 0) continue;
           GemmTerm tm{};
           tm.a_off = tb + th.coloff[m][s2];
           tm.lda = (int32_t)th.ncols[m];
           tm.k = (int32_t)A2.sdim[t];
-          tm.b_off = it->second;
+          tm.b_off = ro;
           tm.ldb = (int32_t)A2.sdim[tp];
           stage2.terms.push_back(tm);
           flops_executed += 8.0 * task.m * (double)task.n * tm.k;
