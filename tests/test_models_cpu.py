@@ -133,3 +133,20 @@ def test_benchmark_workload_through_the_oracle_block_port():
     x = np.random.default_rng(2).standard_normal(bh.n) + 1j * np.random.default_rng(3).standard_normal(bh.n)
     a, b = bh.matvec(x), ref.matvec(x)
     assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
+
+
+def test_ising_workload_charge_rule():
+    """The synthetic coupled-Ising workload (the bench's ``ising_matvec``):
+    a Z2 bond of two equal sectors, and environment entries only where the
+    reference's charge rule allows them, on the MPO slots the MPO uses."""
+    wl = pm.ising_workload(12)
+    bond, bq = wl["bond"], wl["bq"]
+    assert bond.shape == (12, 1) and np.sum(bond == 0) == 6 and np.sum(bond == 1) == 6
+    assert wl["W"].shape == (64, 26, 64, 26)
+    D = bq.shape[0]
+    used_l = set(np.nonzero(np.any(wl["W"] != 0, axis=(0, 2, 3)))[0])
+    M = _dense(wl["L"])  # rows a', cols b + D a
+    r, c = np.nonzero(M)
+    b, a = c % D, c // D
+    assert r.size > 0 and set(np.unique(b)) <= used_l
+    assert np.all(q_eq(bond[r], q_add(bq[b], bond[a], wl["rules"])))
