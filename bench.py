@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--ising-chi", default="64,128", help="bond dimensions of the coupled-Ising steps")
     p.add_argument("--ising-folded-chi", type=int, default=64,
                    help="bond dimension at which the folded-order FP64 step is also timed (0: skip)")
+    p.add_argument("--ising-forms", default="fp64,mixed,mixed_bf16",
+                   help="forms of the coupled-Ising step: fp64, mixed (split TF32), mixed_bf16 (split BF16)")
     p.add_argument("--ising-matvec-chi", default="128",
                    help="bond dimensions of the coupled-Ising matvec timing per form ('': skip)")
     return p.parse_args()
@@ -477,8 +479,9 @@ def main():
                                          "stages for this vertex), FP64 Krylov, Rayleigh quotients and SVD",
                            "fp64_folded": "FP64 in the reference's folded order (LeftPart . V . RightPart)"}}
         for chi in [int(c) for c in str(a.ising_chi).split(",") if c.strip()]:
-            forms = [("fp64", CMPS_FP64, CMPS_ORDER_AUTO), ("mixed", CMPS_SPLIT_TF32, CMPS_ORDER_AUTO),
-                     ("mixed_bf16", CMPS_SPLIT_BF16, CMPS_ORDER_AUTO)]
+            allf = {"fp64": CMPS_FP64, "mixed": CMPS_SPLIT_TF32, "mixed_bf16": CMPS_SPLIT_BF16}
+            want = [f.strip() for f in str(a.ising_forms).split(",") if f.strip()]
+            forms = [(f, allf[f], CMPS_ORDER_AUTO) for f in want if f in allf]
             if chi == a.ising_folded_chi:
                 forms.append(("fp64_folded", CMPS_FP64, CMPS_ORDER_FOLDED))
             ising[f"chi_{chi}"] = idmrg_bench(ctx, iw, chi, a.ising_steps, dist, warm=2, forms=forms,
@@ -591,17 +594,20 @@ def idmrg_bench(ctx, wl, chi, steps, dist, warm=3, tol=1e-10, unit_cell=True, fo
                      "profile_median": {k: float(np.median([p[k] for p in prof])) for k in keys},
                      "profile_mean": {k: float(np.mean([p[k] for p in prof])) for k in keys}}
         energies[name] = np.array(e)
-    rel = np.abs(energies["mixed"] - energies["fp64"]) / np.abs(energies["fp64"])
-    out["max_rel_dE_mixed_vs_fp64"] = float(rel.max())
-    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
-    if "mixed_bf16" in out:
+    if "mixed" in out and "fp64" in out:
+        rel = np.abs(energies["mixed"] - energies["fp64"]) / np.abs(energies["fp64"])
+        out["max_rel_dE_mixed_vs_fp64"] = float(rel.max())
+        out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    if "mixed_bf16" in out and "fp64" in out:
         rel = np.abs(energies["mixed_bf16"] - energies["fp64"]) / np.abs(energies["fp64"])
         out["max_rel_dE_mixed_bf16_vs_fp64"] = float(rel.max())
         out["speedup_mixed_bf16_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed_bf16"]["ms_per_step"]
     if "fp64_folded" in out:
         rel = np.abs(energies["fp64_folded"] - energies["fp64"]) / np.abs(energies["fp64"])
         out["max_rel_dE_folded_vs_fp64"] = float(rel.max())
-        out["speedup_mixed_vs_fp64_folded"] = out["fp64_folded"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+        for f in ("mixed", "mixed_bf16"):
+            if f in out:
+                out[f"speedup_{f}_vs_fp64_folded"] = out["fp64_folded"]["ms_per_step"] / out[f]["ms_per_step"]
         out["speedup_fp64_vs_fp64_folded"] = out["fp64_folded"]["ms_per_step"] / out["fp64"]["ms_per_step"]
     return out
 
