@@ -540,17 +540,19 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
     };
     auto rand_lwork = [&](cusolverDnHandle_t sol, gesvdjInfo_t prm, int64_t ll, int64_t bb, int* lw) -> int {
       const int b32 = (int)bb, l32 = (int)ll;
-      int a = 0, q = 0, u = 0, g = 0, e = 0;
+      int a = 0, q = 0, u = 0, g = 0, e = 0, q2 = 0, u2 = 0;
       cuDoubleComplex* any = (cuDoubleComplex*)dA;
       if (cusolverDnZheevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, b32, any, b32, dS, &e) !=
               CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, b32, any, b32, &a) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZgeqrf_bufferSize(sol, l32, b32, any, l32, &q) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZungqr_bufferSize(sol, l32, b32, b32, any, l32, any, &u) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZgeqrf_bufferSize(sol, b32, b32, any, b32, &q2) != CUSOLVER_STATUS_SUCCESS ||
+          cusolverDnZungqr_bufferSize(sol, b32, b32, b32, any, b32, any, &u2) != CUSOLVER_STATUS_SUCCESS ||
           cusolverDnZgesvdj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, 1, b32, b32, any, b32, dS, any, b32, any, b32, &g,
                                        prm) != CUSOLVER_STATUS_SUCCESS)
         return fail(CMPS_ERR_SOLVER, "randomized SVD buffer query failed");
-      *lw = std::max(std::max(std::max(a, q), std::max(u, g)), std::max(e, 1));
+      *lw = std::max(std::max(std::max(a, q), std::max(u, g)), std::max(std::max(e, 1), std::max(q2, u2)));
       return CMPS_OK;
     };
     auto factor_rand = [&](int m, int64_t bb, FW& fw) -> int {
@@ -602,10 +604,20 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
       // Orthonormal basis of the columns of A_ (rows x bb, in place): shifted
       // Cholesky QR followed by two plain passes (shifted CholeskyQR3,
       // Fukaya, Kannan, Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci.
-      // Comput. 42 (2020) A477), stable up to a condition number ~1/eps; a
-      // factorisation that breaks down sets chol_bad and the sector goes to
-      // the Gram route.
+      // Comput. 42 (2020) A477), stable up to a condition number ~1/eps.  A
+      // Cholesky factorisation that breaks down (a sketch of a spectrum that
+      // decays below eps within the range) is redone by Householder QR
+      // (geqrf, ungqr) from a copy of A_ kept in Z2, which is free until B^H
+      // is formed; chol_bad stays set only if that fails too, and the sector
+      // then goes to the Gram route.
+      bool qr_unrecovered = false;  // a breakdown the Householder redo did not repair
       auto qr = [&](double2* A_, int64_t rows) {
+        if (rc != CMPS_OK) return;
+        if (cudaMemcpyAsync(Z2, A_, sizeof(double2) * rows * bb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaMemsetAsync(chol_bad, 0, sizeof(int), st) != cudaSuccess) {
+          rc = fail(CMPS_ERR_CUDA, "randomized SVD: QR copy failed");
+          return;
+        }
         for (int pass = 0; pass < 3 && rc == CMPS_OK; ++pass) {
           zg(CUBLAS_OP_C, CUBLAS_OP_N, bb, bb, rows, &one, A_, rows, A_, rows, &zero, Gb, bb);
           if (rc != CMPS_OK) return;
@@ -622,6 +634,30 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
               CUBLAS_STATUS_SUCCESS)
             rc = fail(CMPS_ERR_CUDA, "randomized SVD triangular solve failed");
         }
+        if (rc != CMPS_OK) return;
+        int broke = 0;
+        if (cudaMemcpyAsync(&broke, chol_bad, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+          rc = fail(CMPS_ERR_CUDA, "randomized SVD: QR check failed");
+          return;
+        }
+        if (!broke) return;
+        // Householder QR of the kept copy: A_ = Q R, Q (rows x bb) into A_
+        int hinfo = 0;
+        if (cudaMemcpyAsync(A_, Z2, sizeof(double2) * rows * bb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cusolverDnZgeqrf(sol, (int)rows, (int)bb, (cuDoubleComplex*)A_, (int)rows, (cuDoubleComplex*)tau, work,
+                             lwork, dinfo) != CUSOLVER_STATUS_SUCCESS ||
+            cusolverDnZungqr(sol, (int)rows, (int)bb, (int)bb, (cuDoubleComplex*)A_, (int)rows,
+                             (const cuDoubleComplex*)tau, work, lwork, dinfo) != CUSOLVER_STATUS_SUCCESS ||
+            cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+          rc = fail(CMPS_ERR_SOLVER, "randomized SVD: Householder QR failed");
+          return;
+        }
+        if (hinfo != 0)
+          qr_unrecovered = true;
+        else if (cudaMemsetAsync(chol_bad, 0, sizeof(int), st) != cudaSuccess)
+          rc = fail(CMPS_ERR_CUDA, "randomized SVD: QR flag reset failed");
       };
       if (rc == CMPS_OK) cudaMemsetAsync(chol_bad, 0, sizeof(int), st);
       if (rc == CMPS_OK) k_fill_random<<<grid_of(ll * bb), 256, 0, st>>>(Z, ll * bb, 0x5eed5eedull + (uint64_t)m);
@@ -633,6 +669,9 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
         zg(opM, CUBLAS_OP_N, pp, bb, ll, &one, dA, nr, Z, ll, &zero, Y, pp);   // Y = M Z
         qr(Y, pp);
       }
+      // every QR of the range finder resets the flag: an unrepaired breakdown sets it again
+      if (rc == CMPS_OK && qr_unrecovered && cudaMemsetAsync(chol_bad, 0x01, sizeof(int), st) != cudaSuccess)
+        rc = fail(CMPS_ERR_CUDA, "randomized SVD: QR flag failed");
       zg(opMH, CUBLAS_OP_N, ll, bb, pp, &one, dA, nr, Y, pp, &zero, Z, ll);    // Z = M^H Q = B^H
       if (rc == CMPS_OK && cudaMemcpyAsync(Z2, Z, sizeof(double2) * ll * bb, cudaMemcpyDeviceToDevice, st) !=
                                cudaSuccess)
