@@ -59,7 +59,7 @@ def test_xxz_idmrg_chi100_matches_oracle(ctx, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bf16"])
 def test_coupled_ising_idmrg_matches_oracle(ctx, precision):
-    """The north star's model as benchmarked: coupled transverse-field Ising
+    """The benchmarked coupled-chain model: coupled transverse-field Ising
     chains, each vertex the periodic 12-site chain at g = 1.2 cut to its 64
     lowest states (Z2 parity), J_perp = 0.05 sum_i X_i X_i, MPO D = 26;
     iDMRG at chi = 32 for 5 steps against the oracle's rows (canonical-order
