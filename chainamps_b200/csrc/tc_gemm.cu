@@ -23,17 +23,23 @@
 // product.  A 64-byte shared-memory row holds 32 BF16 K columns, so a stage
 // covers twice the K of the TF32 form for the same bytes, and each MMA runs
 // at twice the TF32 rate.  Stage 1 (mode 3) writes T split into four BF16
-// planes, so stage 2 (mode 4) reads it by TMA like any other operand.
+// planes, so stage 2 (mode 4) reads it by TMA like any other operand; the
+// canonical-order form (canonical_tc.cu) chains three mode-3 launches and a
+// mode-4 one the same way.  A plan may opt narrow tiles (N <= 32) into the
+// four-plane form: one MMA per A plane against all four B planes at once
+// (N' = 4N), 4 MMAs instead of 12, combined in the epilogue.
 //
 // Persistent: one CTA per SM walks a list of 128 x N (N <= 128) output tiles
-// (tile i of CTA b is tiles[b + i * gridDim]; the host orders tiles by
-// decreasing work), each the K-concatenation of its task's terms.  Warp 0
-// issues TMA loads into a 3-stage ring and runs ahead across tile boundaries,
-// warp 1 issues the MMAs into one of two TMEM accumulator buffers, warps 2-5
-// drain the other buffer and write the output, so the epilogue of a tile
-// overlaps the loads and MMAs of the next.  Every mbarrier wait is bounded:
-// on time-out the kernel raises an error word, skips the remaining work,
-// frees its TMEM and returns.
+// (tile i of CTA b is tiles[b + i * gridDim]; the host orders them by
+// decreasing work, or row tile by row tile within groups that share A),
+// each the K-concatenation of its task's terms.  Warp 0 issues TMA loads
+// into a 3-stage ring and runs ahead across tile boundaries (its lanes load
+// the next 32 tiles' records at once), warp 1 issues the MMAs into one of two
+// TMEM accumulator buffers, warps 2-5 (2-9 in mode 3) drain the other buffer
+// and write the output (mode 3 through a shared-memory box per warp, in
+// 16-byte runs), so the epilogue of a tile overlaps the loads and MMAs of the
+// next.  Every mbarrier wait is bounded: on time-out the kernel raises an
+// error word, skips the remaining work, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
