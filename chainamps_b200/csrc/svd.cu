@@ -1036,10 +1036,15 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
     // ---- global selection ----
     // Sectors of the randomized route contribute only their leading values.
     // Their result stands when it settles the truncation of the whole
-    // spectrum: (1) the bond-dimension cap, not the weight cut, decides the
-    // kept count (the weight from index cap - 1 on, computed values plus the
-    // sectors' tails, is at least max_trunc); (2) the degeneracy extension
-    // ends inside the computed values; (3) no value left out can rank above
+    // spectrum: (1) the kept count is decided inside the computed values,
+    // with a margin of 1 % on the trailing weight (computed values plus the
+    // sectors' tails): by the bond-dimension cap (the weight from index
+    // cap - 1 on is at least 1.01 max_trunc), or else by the weight cut (the
+    // rule's loop from the end, run over the computed values with the tails
+    // as the last weight, stops inside them, on a weight at least 1.01
+    // max_trunc whose predecessor is at most 0.99 max_trunc; a cut that close
+    // to the threshold goes to the Gram route at once); (2) the degeneracy
+    // extension ends inside the computed values; (3) no value left out can rank above
     // the first discarded one (each sector's tail, which bounds its largest
     // value left out, is below half of it); (4) every kept triplet has
     // converged: residual <= 1e-12 s_0 + 500 eps s_0^2 / s_j, the second term
@@ -1054,7 +1059,10 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
     int64_t length = 0;
     double tail_total = 0.0;
     bool settled = false;
-    for (int pass = 0; pass < 8 && status == CMPS_OK && !settled; ++pass) {
+    // Passes: at most one to make the values exact for a weight cut, one per
+    // doubling of a randomized range (six from 64 triplets in an 8192-wide
+    // sector), one to the Gram route, one to redo it exactly, one to settle.
+    for (int pass = 0; pass < 12 && status == CMPS_OK && !settled; ++pass) {
       all.clear();
       int64_t n_true = 0;
       bool any_rnd = false;
@@ -1075,15 +1083,58 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
       if (any_rnd) {
         const int64_t np = (int64_t)sv.size();
         const int64_t cap = (chi > 0 && chi < n_true) ? chi : n_true;
-        bool valid = cap < n_true && cap + 1 < np && sv[0] > 0.0;
-        int failed = valid ? 0 : 0x10;  // which check failed (CMPS_SVD_TRACE)
+        bool valid = sv[0] > 0.0;
+        // which check failed (CMPS_SVD_TRACE); 5: a weight cut within the margin, 6: a
+        // weight cut read from eigensolver values
+        int failed = valid ? 0 : 0x10;
+        int64_t len = cap;
         if (valid) {
           double beyond = tail_total;
-          for (int64_t i = cap - 1; i < np; ++i) beyond += sv[i] * sv[i];
-          valid = beyond >= 1.01 * max_trunc;                                   // (1)
-          if (!valid) failed = 1;
+          const bool cap_inside = cap < n_true && cap + 1 < np;
+          if (cap_inside)
+            for (int64_t i = cap - 1; i < np; ++i) beyond += sv[i] * sv[i];
+          bool exact_values = true;  // every value of the sectors involved has an absolute error ~eps s_0
+          for (int m = 0; m < nm; ++m)
+            if (!blk[m].rows.empty() && blk[m].eig && (blk[m].rnd ? !blk[m].red_exact : true)) exact_values = false;
+          if (!(cap_inside && beyond >= 1.01 * max_trunc)) {                   // (1), weight cut
+            if (!exact_values) {
+              // values of an eigensolver (the reduced one, or the Gram
+              // route's) carry ~eps s_0^2 on every s_j^2, which can exceed a
+              // small threshold by itself: first the same sectors exactly
+              valid = false;
+              failed = 6;
+            } else {
+              // truncation_length's loop, the tails standing for the values
+              // left out (all of them rank below the cut: check (3)).  The
+              // margin covers the error of the partial weights: ~2 eps s_0 s_j
+              // on each s_j^2, and the rounding of the tails.
+              double err = tail_total, before = tail_total, ssum = 0.0, entries = 0.0;
+              int64_t tl = np;
+              while (err < max_trunc && tl > 0) {
+                before = err;
+                err += sv[tl - 1] * sv[tl - 1];
+                ssum += sv[tl - 1];
+                --tl;
+              }
+              for (int m = 0; m < nm; ++m)
+                if (blk[m].rnd) entries += (double)blk[m].rows.size() * (double)blk[m].cols.size();
+              const double slack = std::max(0.01 * max_trunc, 64.0 * kEps * sv[0] * ssum +
+                                                                  64.0 * kEps * kEps * sv[0] * sv[0] * entries);
+              const bool clear = err < max_trunc ? err <= max_trunc - slack
+                                                 : err >= max_trunc + slack && before <= max_trunc - slack;
+              len = tl + 1;
+              if (len >= cap || len >= np) {
+                valid = false;
+                failed = 1;
+              } else if (!clear) {
+                valid = false;
+                failed = 5;
+              } else {
+                weight_decided = true;
+              }
+            }
+          }
         }
-        int64_t len = cap;
         if (valid) {
           while (len < n_true && len < np && (sv[len - 1] - sv[len]) / sv[len - 1] < 1.0e-3) ++len;
           valid = len < np;                                                     // (2)
@@ -1114,6 +1165,22 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
               std::fprintf(stderr, "  [m%d b=%lld tail=%.3g]", m, (long long)blk[m].bb, blk[m].tail);
           std::fprintf(stderr, "\n");
         }
+        if (!valid && failed == 6) {
+          // a weight cut read from eigensolver values: the randomized
+          // sectors again with the reduced SVD (same range), the Gram-route
+          // ones with the one-sided Jacobi SVD
+          for (int m = 0; m < nm && status == CMPS_OK; ++m) {
+            if (blk[m].rows.empty() || !blk[m].eig) continue;
+            if (blk[m].rnd) {
+              if (blk[m].red_exact) continue;
+              blk[m].red_exact = true;
+              status = factor(m, 3, main_fw);
+            } else {
+              status = factor(m, 2, main_fw);
+            }
+          }
+          continue;
+        }
         if (!valid && failed == 4) {
           // kept triplets of the reduced eigensolver not accurate enough:
           // those sectors again with the reduced SVD (QR + one-sided Jacobi),
@@ -1133,10 +1200,12 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
           // stays well under the sector's short side, else take the Gram
           // route.  Both cost far less than the one-sided Jacobi SVD that
           // the Gram route falls back to for kept values below 1e-5 s_0.
+          // A cut within 1 % of the threshold (check 5) depends on rounding
+          // the range cannot remove: the Gram route at once.
           for (int m = 0; m < nm && status == CMPS_OK; ++m) {
             if (!blk[m].rnd) continue;
             const int64_t mn = std::min(blk[m].rows.size(), blk[m].cols.size());
-            if (4 * (2 * blk[m].bb) <= 3 * mn) {
+            if (failed != 5 && 4 * (2 * blk[m].bb) <= 3 * mn) {
               blk[m].bb *= 2;
               status = factor(m, 3, main_fw);
             } else {

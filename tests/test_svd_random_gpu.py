@@ -8,9 +8,10 @@ Tolerances: kept counts per sector exact; values within
 1e-13 + 200 eps s_0^2 / s_j (the error class of a Gram-matrix eigenvalue,
 which the randomized route's last step shares with the Gram route); the
 truncated wavefunction within 1e-10 (max-norm); the discarded weight within
-1e-12.  Where the leading triplets do not settle the truncation (a flat
-spectrum, or a weight cut that decides the kept count), the route must step
-aside and the result must still match."""
+1e-12.  A weight cut below the cap is settled by the leading triplets and
+the weight outside the range.  Where they do not settle the truncation (a
+flat spectrum, or a weight cut within 1 % of a partial weight), the route
+must step aside and the result must still match."""
 import numpy as np
 import pytest
 
@@ -43,11 +44,16 @@ def case():
     ctx.close()
 
 
-def decaying(H, ref, flat, decay):
-    """The same singular vectors as `flat`, values exp(-k / decay) normalised."""
+def spectrum(H, ref, flat, decay):
+    """The prescribed values exp(-k / decay), normalised, one per value of `flat`."""
     d0 = od.block_svd(from_matrix(H.rules, ref.indices, 2, flat), 0, 0.0)
     s = np.exp(-np.arange(len(d0.values)) / decay)
-    s /= np.linalg.norm(s)
+    return d0, s / np.linalg.norm(s)
+
+
+def decaying(H, ref, flat, decay):
+    """The same singular vectors as `flat`, values exp(-k / decay) normalised."""
+    d0, s = spectrum(H, ref, flat, decay)
     return d0.U.matrix() @ np.diag(s) @ d0.Vd.matrix()
 
 
@@ -97,9 +103,22 @@ def test_randomized_route_steps_aside_for_a_flat_spectrum(case):
     assert routes["randomized"] == 0
 
 
-def test_randomized_route_steps_aside_when_the_weight_cut_decides(case):
-    """max_trunc = 1e-3 cuts below the cap: the count depends on the whole
-    tail, which the randomized route does not have."""
+def test_randomized_route_settles_a_weight_cut(case):
+    """max_trunc = 1e-3 cuts below the cap (35 values kept of at most 80):
+    the rule's loop over the computed values, with the weight outside the
+    range standing for the values left out, stops inside them, on partial
+    weights 1.11 and 0.91 times the threshold."""
     H, ref, gpu, flat = case
     routes = check(H, ref, gpu, decaying(H, ref, flat, 10.0), 80, 1e-3)
+    assert routes["randomized"] == 1
+
+
+def test_randomized_route_steps_aside_near_the_weight_threshold(case):
+    """A threshold 0.5 % below the partial weight of the last kept value:
+    the cut is not left to the randomized route's rounding."""
+    H, ref, gpu, flat = case
+    _, s = spectrum(H, ref, flat, 10.0)
+    tail = np.cumsum((s * s)[::-1])[::-1]  # tail[i] = sum_{j >= i} s_j^2
+    assert tail[34] >= 1e-3 > tail[35]      # the previous test's cut: 35 kept
+    routes = check(H, ref, gpu, decaying(H, ref, flat, 10.0), 80, tail[34] / 1.005)
     assert routes["randomized"] == 0
