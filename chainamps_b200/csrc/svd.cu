@@ -1097,7 +1097,13 @@ int theta_svd(Heff& H, int64_t chi, double max_trunc, SvdResult& out, const std:
           for (int m = 0; m < nm; ++m)
             if (!blk[m].rows.empty() && blk[m].eig && (blk[m].rnd ? !blk[m].red_exact : true)) exact_values = false;
           if (!(cap_inside && beyond >= 1.01 * max_trunc)) {                   // (1), weight cut
-            if (!exact_values) {
+            if (!(tail_total < max_trunc)) {
+              // the weight left out reaches the threshold by itself: the cut
+              // lies beyond the computed values, and only a wider range can
+              // settle it
+              valid = false;
+              failed = 1;
+            } else if (!exact_values) {
               // values of an eigensolver (the reduced one, or the Gram
               // route's) carry ~eps s_0^2 on every s_j^2, which can exceed a
               // small threshold by itself: first the same sectors exactly
